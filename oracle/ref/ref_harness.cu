@@ -1,0 +1,110 @@
+// ref_harness.cu - C entry points over the reference cudaCompress library,
+// compiled from the reference's own sources by oracle/ref/Makefile into
+// oracle/_ref/libref_gpu.so.  TEST INFRASTRUCTURE ONLY: it lets the tests pin
+// the CPU oracle against the reference's table design (CPU-only entry points)
+// and, on a GPU, produce reference bitstreams and DWT outputs.
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <queue>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+// HuffmanEncodeTable::build and the decode table internals are private in the
+// reference; expose them to this harness only.
+#define private public
+#include <cudaCompress/Instance.h>
+#include <cudaCompress/InstanceImpl.h>
+#include <cudaCompress/HuffmanTable.h>
+#include <cudaCompress/Encode.h>
+#include <cudaCompress/util/DWT.h>
+#include <cudaCompress/util/Quantize.h>
+#undef private
+
+using namespace cudaCompress;
+
+extern "C" {
+
+// Reference table build + serialization (HuffmanTable.cu:470-596) on the CPU.
+int ref_huffman_build(const uint32_t* hist, uint32_t bins, uint32_t symbolMax, uint32_t log2Max,
+                      uint32_t* codewords, uint32_t* lengths, uint32_t* tableWords, uint32_t cap,
+                      uint32_t* tableBits) {
+    Instance inst;
+    inst.m_log2HuffmanDistinctSymbolCountMax = log2Max;
+    int maxLen;
+    {
+        HuffmanEncodeTable t(&inst);
+        t.build(hist, bins);
+        t.m_symbolMax = symbolMax;
+        for (uint32_t i = 0; i < t.m_codewordTableSize; ++i) {
+            codewords[i] = t.m_pCodewords[i];
+            lengths[i] = t.m_pCodewordLengths[i];
+        }
+        std::vector<uint> v;
+        BitStream bs(&v);
+        t.writeToBitStream(&inst, bs);
+        *tableBits = bs.getBitSize();
+        if (v.size() > cap) return -2;
+        std::memcpy(tableWords, v.data(), v.size() * 4);
+        maxLen = int(t.m_codewordCountPerLength.size());
+    }
+    return maxLen;
+}
+
+void* ref_create(int dev, uint32_t streamCountMax, uint32_t elemMax, uint32_t cb, uint32_t log2Max) {
+    return createInstance(dev, streamCountMax, elemMax, cb, log2Max);
+}
+void ref_destroy(void* p) { destroyInstance(static_cast<Instance*>(p)); }
+
+// kind 0 = encodeRLHuff, 1 = encodeHuff; streams contiguous on the device.
+int ref_encode(void* p, int kind, int symBytes, void* dSymbols, uint32_t S, uint32_t n,
+               uint32_t* words, uint32_t cap, uint32_t* bitSize, uint32_t* bitPos) {
+    Instance* inst = static_cast<Instance*>(p);
+    std::vector<uint> v(words, words + (*bitSize + 31) / 32);
+    BitStream bs(&v);
+    bs.setBitSize(*bitSize);
+    bs.setBitPosition(*bitPos);
+    bool ok;
+    if (symBytes == 2) {
+        std::vector<Symbol16*> s(S);
+        for (uint32_t i = 0; i < S; ++i) s[i] = static_cast<Symbol16*>(dSymbols) + size_t(i) * n;
+        ok = kind == 0 ? encodeRLHuff(inst, bs, s.data(), S, n) : encodeHuff(inst, bs, s.data(), S, n);
+    } else {
+        std::vector<Symbol32*> s(S);
+        for (uint32_t i = 0; i < S; ++i) s[i] = static_cast<Symbol32*>(dSymbols) + size_t(i) * n;
+        ok = kind == 0 ? encodeRLHuff(inst, bs, s.data(), S, n) : encodeHuff(inst, bs, s.data(), S, n);
+    }
+    cudaDeviceSynchronize();
+    if (!ok) return -1;
+    if (v.size() > cap) return -2;
+    std::memcpy(words, v.data(), v.size() * 4);
+    *bitSize = bs.getBitSize();
+    *bitPos = bs.getBitPosition();
+    return 0;
+}
+
+void ref_dwt_float3d_fwd(float* dst, float* buf2, float* buf1, const float* src, int nx, int ny, int nz) {
+    util::dwtFloat3DForward(dst, buf2, buf1, src, nx, ny, nz);
+    cudaDeviceSynchronize();
+}
+void ref_dwt_float3d_inv(float* dst, float* buf2, float* buf1, const float* src, int nx, int ny, int nz) {
+    util::dwtFloat3DInverse(dst, buf2, buf1, src, nx, ny, nz);
+    cudaDeviceSynchronize();
+}
+void ref_dwt_int_fwd(short* dst, short* buf, const short* src, int nx, int ny, int nz) {
+    util::dwtIntForward(dst, buf, src, nx, ny, nz);
+    cudaDeviceSynchronize();
+}
+void ref_dwt_int_inv(short* dst, short* buf, const short* src, int nx, int ny, int nz) {
+    util::dwtIntInverse(dst, buf, src, nx, ny, nz);
+    cudaDeviceSynchronize();
+}
+void ref_quantize_to_symbols(uint16_t* out, const float* src, uint32_t nx, uint32_t ny, uint32_t nz, float step,
+                             uint32_t rowPitch, uint32_t slicePitch) {
+    util::quantizeToSymbols(out, src, nx, ny, nz, step, rowPitch, slicePitch);
+    cudaDeviceSynchronize();
+}
+
+}
