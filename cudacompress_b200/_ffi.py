@@ -1,0 +1,95 @@
+"""ctypes bindings of the C ABI (include/cudacompress_b200.h).
+
+Loading fails loudly when the CUDA library is missing: there is no CPU
+fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcudacompress_b200.so")
+
+c_u32 = ctypes.c_uint32
+c_u64 = ctypes.c_uint64
+c_int = ctypes.c_int
+c_float = ctypes.c_float
+c_vp = ctypes.c_void_p
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_vpp = ctypes.POINTER(ctypes.c_void_p)
+
+_SIGS = {
+    "cc_last_error": (ctypes.c_char_p, []),
+    "cc_version": (ctypes.c_char_p, []),
+    "cc_create_instance": (c_int, [ctypes.POINTER(c_vp), c_int, c_u32, c_u32, c_u32, c_u32]),
+    "cc_destroy_instance": (None, [c_vp]),
+    "cc_get_instance_cuda_device": (c_int, [c_vp]),
+    "cc_get_instance_stream_count_max": (c_u32, [c_vp]),
+    "cc_get_instance_elem_count_per_stream_max": (c_u32, [c_vp]),
+    "cc_get_instance_coding_block_size": (c_u32, [c_vp]),
+    "cc_get_instance_log2_huffman_distinct_symbol_count_max": (c_u32, [c_vp]),
+    "cc_get_instance_use_long_symbols": (c_int, [c_vp]),
+    "cc_set_instance_stream": (None, [c_vp, c_vp]),
+    "cc_get_instance_stream": (c_vp, [c_vp]),
+    "cc_encode_get_required_memory": (ctypes.c_size_t, [c_vp]),
+    "cc_encode": (c_int, [c_vp, c_int, c_int, c_vpp, c_u32, c_u32, c_u32p]),
+    "cc_encoded_segment": (c_int, [c_vp, c_u32, ctypes.POINTER(c_u32p), c_u32p, c_u32p, c_u32p]),
+    "cc_encode_to_buffer": (c_int, [c_vp, c_int, c_int, c_vpp, c_u32, c_u32, c_u32p, c_u32, c_u32p, c_u32p]),
+    "cc_decode": (c_int, [c_vp, c_int, c_int, ctypes.POINTER(c_u32p), c_u32p, c_u32p, c_u32, c_u32p, c_vpp, c_u32, c_u32]),
+    "cc_decode_status": (c_int, [c_vp]),
+    "cc_dwt_float_forward": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_dwt_float_inverse": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_dwt_float_inverse_from_symbols": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_float, c_int, c_int, c_int,
+                                                  c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_dwt_int_forward": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_dwt_int_inverse": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_quantize_to_symbols": (c_int, [c_vp, c_int, c_vp, c_u32, c_u32, c_u32, c_float, c_u32, c_u32, c_int, c_vp]),
+    "cc_quantize_to_symbols_roundtrip": (c_int, [c_vp, c_int, c_vp, c_u32, c_u32, c_u32, c_float, c_u32, c_u32, c_int, c_vp]),
+    "cc_unquantize_from_symbols": (c_int, [c_vp, c_vp, c_int, c_u32, c_u32, c_u32, c_float, c_u32, c_u32, c_int, c_vp]),
+    "cc_symbolize": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32, c_vp]),
+    "cc_unsymbolize": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32, c_vp]),
+    "cc_quantize_to_short": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_float, c_u32, c_u32, c_int, c_vp]),
+    "cc_unquantize_from_short": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_float, c_u32, c_u32, c_int, c_vp]),
+    "cc_get_max_abs": (c_int, [c_vp, c_vp, c_u32, c_vp]),
+    "cc_compress_volume_float": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_vp, c_u64, c_u32p]),
+    "cc_decompress_volume_float": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_vp, c_u32]),
+    "cc_compress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u64, c_u32p]),
+    "cc_decompress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u32]),
+}
+
+_lib = None
+
+
+def exported_names():
+    """Every entry point this module binds (the C header's declarations)."""
+    return sorted(_SIGS)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"cudacompress_b200 CUDA library not found at {LIB_PATH}; build it with "
+                "`python -m cudacompress_b200.build` (there is no CPU fallback)")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+class CudaCompressError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        msg = lib().cc_last_error().decode(errors="replace")
+        super().__init__(f"{what}: status {status}: {msg}")
+        self.status = status
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise CudaCompressError(status, what)

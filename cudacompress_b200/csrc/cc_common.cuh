@@ -1,0 +1,94 @@
+// cc_common.cuh - shared types, error plumbing and warp/block primitives for
+// the cudacompress_b200 library (sm_100a).
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "../../include/cudacompress_b200.h"
+
+#define CC_HD __host__ __device__ __forceinline__
+
+namespace ccb {
+
+typedef uint8_t u8;
+typedef uint16_t u16;
+typedef uint32_t u32;
+typedef uint64_t u64;
+typedef int16_t i16;
+typedef int32_t i32;
+
+// Device-side error flags (bit set, OR-ed by kernels, read back by the host).
+enum DeviceError : u32 {
+    DEV_ERR_SYMBOL_RANGE = 1u,
+    DEV_ERR_CODEWORD_TOO_LONG = 2u,
+    DEV_ERR_CORRUPT = 4u,
+    DEV_ERR_TIMEOUT = 8u,
+    DEV_ERR_TABLE_CAPACITY = 16u,
+};
+
+constexpr u32 kMaxCodewordBits = 32;      // EncodeCommon.h:24-25
+constexpr u32 kZeroCountMax = 255;        // EncodeCommon.h:31
+constexpr u32 kWarp = 32;
+
+CC_HD u32 requiredBits(u32 v) { return v ? 32u - u32(__builtin_clz(v)) : 0u; }
+
+CC_HD u64 ceilDiv(u64 a, u64 b) { return (a + b - 1) / b; }
+CC_HD u64 alignUp(u64 a, u64 b) { return (a + b - 1) / b * b; }
+
+#ifdef __CUDACC__
+// Inclusive warp scan (sum).
+__device__ __forceinline__ u32 warpInclusiveSum(u32 v) {
+    const u32 lane = threadIdx.x & 31u;
+#pragma unroll
+    for (u32 o = 1; o < 32; o <<= 1) {
+        u32 t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+__device__ __forceinline__ u32 warpSum(u32 v) {
+#pragma unroll
+    for (u32 o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ u32 warpMax(u32 v) {
+#pragma unroll
+    for (u32 o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide exclusive scan of one u32 per thread; returns the exclusive
+// prefix and writes the block total to *total.  `scratch` holds >= 33 u32.
+template <int kThreads>
+__device__ __forceinline__ u32 blockExclusiveSum(u32 v, u32* scratch, u32* total) {
+    static_assert(kThreads % 32 == 0 && kThreads <= 1024, "block size");
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    u32 inc = warpInclusiveSum(v);
+    if (lane == 31) scratch[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        u32 w = lane < kThreads / 32 ? scratch[lane] : 0u;
+        u32 wi = warpInclusiveSum(w);
+        scratch[lane] = wi - w;
+        if (lane == 31) scratch[32] = wi;
+    }
+    __syncthreads();
+    u32 r = scratch[warp] + inc - v;
+    if (total) *total = scratch[32];
+    __syncthreads();
+    return r;
+}
+
+// Warp-aggregated increment of `bins[key]`: lanes with equal keys are merged
+// with match_any so each distinct key issues one shared/global atomic.
+__device__ __forceinline__ void aggregatedIncrement(u32* bins, u32 key, bool active) {
+    const u32 mask = __ballot_sync(0xffffffffu, active);
+    if (!active) return;
+    const u32 peers = __match_any_sync(mask, key);
+    if ((threadIdx.x & 31u) == u32(__ffs(peers) - 1)) atomicAdd(bins + key, u32(__popc(peers)));
+}
+#endif
+
+}  // namespace ccb

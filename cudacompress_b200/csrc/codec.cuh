@@ -1,0 +1,188 @@
+// codec.cuh - device data structures of the entropy coder (run-length +
+// Huffman) and the instance that owns their memory.
+//
+// Byte format (written by encode, read by decode) follows the reference
+// exactly (Encode.cpp:400-463 for encodeRLHuff, :751-782 for encodeHuff):
+//   RLHuff stream: u32 compactCount | table(sym) | u32 bits | codewords | u16 offsets
+//                  | table(zero counts) | u32 bits | codewords | u16 offsets
+//   Huff stream:   table | u32 bits | codewords | u16 offsets
+// where every "u32"/codeword/offset block is word aligned before and after,
+// tables are bit packed (HuffmanTable.cu:470-485) and offsets are the 16-bit
+// increments of the coding-block bit offsets (PackInc.cu:210-219).
+#pragma once
+
+#include <cstddef>
+#include <vector>
+
+#include "cc_common.cuh"
+
+namespace ccb {
+
+enum CodecKind : int { KIND_RLHUFF = 0, KIND_HUFF = 1 };
+
+// Tile of the run-length passes: 256 threads x 8 symbols.
+constexpr u32 kRleThreads = 256;
+constexpr u32 kRlePerThread = 8;
+constexpr u32 kRleTile = kRleThreads * kRlePerThread;
+
+// Per-stream input of one encode call.
+struct EncStream {
+    const void* in;      // device symbols (u16 or u32)
+    u32 n;               // symbol count
+    u32 startBit;        // bit offset (0..31) of the segment start in its first word
+    u32 groupFirst;      // first stream of the reference call this stream belongs to
+    u32 groupSize;       // streams in that call
+};
+
+// Summary of a run of symbols for the zero-run RLE scan.  Positions are
+// stored +1 so that the virtual "nonzero before the stream" sits at 0.
+struct RunSum {
+    u32 cnt;       // nonzero symbols
+    u32 ext;       // extra (0, 255) entries for the gaps between them
+    u32 firstP1;   // position+1 of the first nonzero (valid if cnt)
+    u32 lastP1;    // position+1 of the last nonzero (valid if cnt)
+};
+
+CC_HD RunSum runCombine(const RunSum& a, const RunSum& b) {
+    if (a.cnt == 0) return b;
+    if (b.cnt == 0) return a;
+    RunSum r;
+    r.cnt = a.cnt + b.cnt;
+    r.ext = a.ext + b.ext + (b.firstP1 - a.lastP1 - 1u) / 256u;
+    r.firstP1 = a.firstP1;
+    r.lastP1 = b.lastP1;
+    return r;
+}
+
+// Per-tile result of the scan: where its output starts and the position+1
+// of the last nonzero before the tile (0 = none).
+struct TileStart {
+    u32 out;
+    u32 prevP1;
+};
+
+// One Huffman table of an encode call (a stream's symbols or zero counts).
+struct TableMeta {
+    u32 count;        // symbols coded with this table
+    u32 symbolMax;    // largest symbol (0 for an empty stream)
+    u32 leaves;       // distinct symbols
+    u32 maxLen;       // longest codeword
+    u32 headerBits;   // serialized table size
+    u32 codeBits;     // total codeword bits
+    u32 blocks;       // coding blocks
+    u32 pad;
+};
+
+// Where the pieces of one stream's segment go in the device output buffer.
+struct SegmentLayout {
+    u64 startWord;        // first word of the segment
+    u32 words;            // segment size in words
+    u32 startBit;         // bit offset of the first written bit inside word 0
+    u32 bitLength;        // bits from word 0 bit 0 to the end of the segment
+    u32 hdrWord[2];       // relative word of each table header
+    u32 cwWord[2];        // relative word of each codeword block
+    u32 offWord[2];       // relative word of each offset block
+    u32 countWord;        // relative word of compactCount (RLHuff)
+};
+
+// Decode-side table descriptor (filled by the host walk of the bit stream).
+struct DecTableDesc {
+    u64 hdrBit;       // absolute bit of the table header in the staged words
+    u64 cwWord;       // first codeword word
+    u32 cwBits;       // codeword bits
+    u32 count;        // symbols to decode
+    u64 offWord;      // first word of the u16 offset increments
+    u32 symbolBits;   // bits per symbol in the header
+    u32 nLen;         // number of codeword lengths
+    u32 nSym;         // symbols in the table
+    u32 pad;
+};
+
+struct DecStreamDesc {
+    void* out;        // device output symbols
+    u32 n;            // output symbol count
+    u32 m;            // compact count (RLHuff) / n (Huff)
+};
+
+// Decode tables in device memory: canonical description + fast lookup.
+constexpr u32 kLutBits = 10;
+struct DecTable {
+    int firstIndex[32];
+    int minCode[32];
+    int maxCode[32];
+    u32 nSym;
+    u32 single;       // symbol when nSym <= 1
+    u32 pad[2];
+};
+
+}  // namespace ccb
+
+// The instance: limits, stream, device arena and host staging.
+struct cc_instance {
+    int device = -1;
+    unsigned streamCountMax = 0;
+    unsigned elemCountPerStreamMax = 0;
+    unsigned codingBlockSize = 0;
+    unsigned log2Max = 0;
+    cudaStream_t stream = nullptr;
+
+    // derived sizes
+    ccb::u32 bins = 0;          // 1 << log2Max
+    ccb::u32 symBytes = 0;      // 2, or 4 when log2Max > 16
+    ccb::u32 tilesMax = 0;      // run-length tiles per stream
+    ccb::u32 blocksMax = 0;     // coding blocks per stream
+    ccb::u32 hdrWordsMax = 0;   // serialized table words
+    ccb::u32 leavesMax = 0;     // distinct symbols per table
+    ccb::u64 outWordsMax = 0;   // device output words
+
+    // device memory (one allocation)
+    char* arena = nullptr;
+    size_t arenaBytes = 0;
+    void* compact = nullptr;    // [S][n] symbols (encode: compact symbols; decode: decoded zero counts)
+    void* zc = nullptr;         // [S][n] zero counts
+    ccb::RunSum* tiles = nullptr;
+    ccb::TileStart* tileStart = nullptr;
+    ccb::u32* hist = nullptr;          // [2S][bins]
+    uint2* enc = nullptr;              // [2S][bins] (code, len)
+    ccb::TableMeta* meta = nullptr;    // [2S]
+    ccb::u32* headers = nullptr;       // [2S][hdrWordsMax]
+    ccb::u32* blockBits = nullptr;     // [2S][blocksMax]
+    ccb::u32* blockOff = nullptr;      // [2S][blocksMax]
+    ccb::SegmentLayout* layout = nullptr;  // [S]
+    ccb::u32* out = nullptr;           // [outWordsMax]
+    ccb::u32* counts = nullptr;        // [S]
+    ccb::u32* errors = nullptr;        // [4]
+    ccb::u64* totals = nullptr;        // [4]
+    ccb::EncStream* dStreams = nullptr;
+    ccb::u64* leafWork = nullptr;      // [2S][leavesMax] heap keys
+    ccb::u32* parentWork = nullptr;    // [2S][2*leavesMax]
+    ccb::u32* orderWork = nullptr;     // [2S][leavesMax]
+    ccb::u32* leafSymWork = nullptr;   // [2S][leavesMax]
+    // decode
+    ccb::DecTableDesc* dDecTables = nullptr;  // [2S]
+    ccb::DecStreamDesc* dDecStreams = nullptr; // [S]
+    ccb::DecTable* decTables = nullptr;       // [2S]
+    ccb::u32* decSyms = nullptr;              // [2S][leavesMax]
+    ccb::u32* decLut = nullptr;               // [2S][1 << kLutBits]
+    ccb::u32* stagedWords = nullptr;          // decode input words
+    ccb::u64 stagedWordsMax = 0;
+    ccb::u32* blockSum = nullptr;             // [S][blocksMax]
+
+    // host staging: ring of slots for uploads, one buffer for downloads
+    static constexpr int kRing = 8;
+    char* hostRing[kRing] = {};
+    size_t hostRingBytes = 0;
+    cudaEvent_t ringEvent[kRing] = {};
+    int ringNext = 0;
+    char* hostDown = nullptr;
+    size_t hostDownBytes = 0;
+    ccb::u32* hostWords = nullptr;   // encoded words (host)
+    ccb::u64 hostWordsMax = 0;
+    std::vector<ccb::SegmentLayout> lastLayout;
+
+    // whole-pipeline workspace (volume / heightfield codecs), grown on demand
+    char* pipeWork = nullptr;
+    size_t pipeWorkBytes = 0;
+
+    char* takeRingSlot();
+};

@@ -1,0 +1,397 @@
+// dwt.cu - separable one-level wavelet transforms (util::dwt*, DWT.h:21-157).
+//
+// Float: CDF 9/7 as a 9-tap FIR per axis (DWTFloatKernels.cui:13-875, taps
+// DWTFloatFilters.cuh:42-49) with whole-sample symmetric extension
+// (DWTCommon.cuh:54-55); the taps of an output are chosen by the parity of its
+// position and accumulated as fma(c[i], v[i], sum), i = 0..8, from 0.0f, so
+// results are bit-identical to the reference kernels.  Forward writes even
+// positions to the low half and odd ones to the high half of each axis; the
+// inverse reads the halves as one interleaved signal.  Axis order: X, Y, Z
+// forward; Z, Y, X inverse; intermediates are float32 in the caller's buffers
+// with the reference's pitches (DWTFloat.cu:84-463).
+//
+// Int: CDF 5/3 lifting on shorts (DWTIntKernels.cui:14-1188) with the
+// reference's rounding (DWTCommon.cuh:133-142), including the narrowing of
+// every intermediate to 16 bits.
+#include "capi_internal.cuh"
+
+namespace ccb {
+
+__constant__ float c_fwd[2][9] = {
+    {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+    {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+__constant__ float c_inv[2][9] = {
+    {0.0f, 0.0337282f, -0.0575435f, -0.5337281f, 1.1150871f, -0.5337281f, -0.0575435f, 0.0337282f, 0.0f},
+    {0.0534975f, -0.0912718f, -0.1564465f, 0.5912718f, 1.2058980f, 0.5912718f, -0.1564465f, -0.0912718f, 0.0534975f}};
+
+// whole-sample symmetric extension (valid for n >= 5 and |overhang| < n)
+__device__ __forceinline__ int mirrorIdx(int i, int n) {
+    i = i < 0 ? -i : i;
+    return i > n - 1 ? 2 * (n - 1) - i : i;
+}
+// position of interleaved index j (inverse domain) in the [L|H] layout
+__device__ __forceinline__ int splitPos(int j, int n) { return (j & 1) ? (n >> 1) + (j >> 1) : (j >> 1); }
+
+template <bool kInverse>
+__device__ __forceinline__ float fir9(const float* v, int parity) {
+    const float* c = kInverse ? c_inv[parity] : c_fwd[parity];
+    float sum = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) sum = __fmaf_rn(c[i], v[i], sum);
+    return sum;
+}
+
+// ---- element conversions (DWTCommon.cuh:14-50) ----
+template <class T> __device__ __forceinline__ float toF(T v);
+template <> __device__ __forceinline__ float toF<float>(float v) { return v; }
+template <> __device__ __forceinline__ float toF<u8>(u8 v) { return float(v) - 128.0f; }
+template <class T> __device__ __forceinline__ T fromF(float v);
+template <> __device__ __forceinline__ float fromF<float>(float v) { return v; }
+template <> __device__ __forceinline__ u8 fromF<u8>(float v) { return u8(fminf(fmaxf(v + 128.5f, 0.0f), 255.0f)); }
+
+// ---------------------------------------------------------------------------
+// Row pass (axis X).  Block: 256 threads, 512 outputs of one row.
+// ---------------------------------------------------------------------------
+constexpr int kRowTile = 512;
+
+template <class TIn, class TOut, bool kInverse>
+__global__ void __launch_bounds__(256) k_firRows(TOut* __restrict__ dst, const TIn* __restrict__ src, int nx,
+                                                 int srcElem, int srcRow, int srcSlice, int dstElem, int dstRow,
+                                                 int dstSlice) {
+    __shared__ float s[kRowTile + 8];
+    const int y = blockIdx.y, z = blockIdx.z;
+    const int x0 = blockIdx.x * kRowTile;
+    const TIn* in = src + size_t(z) * srcSlice + size_t(y) * srcRow;
+    TOut* out = dst + size_t(z) * dstSlice + size_t(y) * dstRow;
+    for (int k = threadIdx.x; k < kRowTile + 8; k += 256) {
+        int j = x0 - 4 + k;
+        if (j < nx + 4) {
+            int m = mirrorIdx(j, nx);
+            s[k] = toF<TIn>(in[size_t(kInverse ? splitPos(m, nx) : m) * srcElem]);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kRowTile; k += 256) {
+        int x = x0 + k;
+        if (x >= nx) break;
+        float r = fir9<kInverse>(s + k, x & 1);
+        int o = kInverse ? x : splitPos(x, nx);
+        out[size_t(o) * dstElem] = fromF<TOut>(r);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass (axis Y or Z).  Block 32 x 8 threads: 32 adjacent columns, 64
+// outputs along the axis.  The loader maps (x, a, c) -> value, a = axis
+// position (in the [L|H] layout for the inverse), c = the remaining coordinate.
+// ---------------------------------------------------------------------------
+constexpr int kColTile = 64;
+
+struct PitchLoad {
+    const float* p;
+    int sx, sa, sc;   // strides for x, axis, other
+    __device__ __forceinline__ float operator()(int x, int a, int c) const {
+        return p[size_t(x) * sx + size_t(a) * sa + size_t(c) * sc];
+    }
+};
+
+// Dequantizing loader of the first inverse pass of dwtFloat*InverseFromSymbols
+// (DWTFloatFromSymbolsKernels.cui:18-464): the lowpass block comes from a
+// float array with pitches, every other block from a symbol band (band index
+// x+2y+4z-1, dense), dequantized as Quantize.cuh:104-110.
+template <class Sym>
+struct SymbolLoad {
+    const float* lp;
+    int lpRow, lpSlice;
+    const Sym* const* bands;
+    float step;
+    int hx, hy, hz;     // half sizes
+    bool axisIsZ;       // axis Z (3D) or Y (2D)
+    __device__ __forceinline__ float operator()(int x, int a, int c) const {
+        int y = axisIsZ ? c : a;
+        int z = axisIsZ ? a : 0;
+        int bx = x >= hx, by = y >= hy, bz = axisIsZ && z >= hz;
+        int lx = x - bx * hx, ly = y - by * hy, lz = z - bz * hz;
+        int b = bx + 2 * by + 4 * bz;
+        if (b == 0) return lp[size_t(lz) * lpSlice + size_t(ly) * lpRow + lx];
+        u32 sym = u32(bands[b - 1][(size_t(lz) * hy + ly) * hx + lx]);
+        int neg = int(sym & 1u);
+        int q = (1 - 2 * neg) * int((sym + u32(neg)) >> 1);
+        float sg = q > 0 ? 1.0f : (q < 0 ? -1.0f : 0.0f);
+        return (float(q) + sg * 0.5f) * step;
+    }
+};
+
+template <class Load, bool kInverse>
+__global__ void __launch_bounds__(256) k_firCols(float* __restrict__ dst, Load load, int nx, int na, int dx, int da,
+                                                 int dc) {
+    __shared__ float s[kColTile + 8][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = blockIdx.x * 32 + tx;
+    const int a0 = blockIdx.y * kColTile;
+    const int c = blockIdx.z;
+    if (x < nx) {
+        for (int k = ty; k < kColTile + 8; k += 8) {
+            int j = a0 - 4 + k;
+            if (j < na + 4) {
+                int m = mirrorIdx(j, na);
+                s[k][tx] = load(x, kInverse ? splitPos(m, na) : m, c);
+            }
+        }
+    }
+    __syncthreads();
+    if (x >= nx) return;
+    for (int k = ty; k < kColTile; k += 8) {
+        int a = a0 + k;
+        if (a >= na) break;
+        float v[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) v[i] = s[k + i][tx];
+        float r = fir9<kInverse>(v, a & 1);
+        int o = kInverse ? a : splitPos(a, na);
+        dst[size_t(x) * dx + size_t(o) * da + size_t(c) * dc] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Integer 5/3 lifting: same tiling; the tile keeps two extra samples each side.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ i16 div2(i16 v) { v = i16(v + ((v >= 0) ? 1 : -1)); return i16(v / 2); }
+__device__ __forceinline__ i16 div4(i16 v) { v = i16(v + ((v >= 0) ? 2 : -2)); return i16(v / 4); }
+
+// Lifts the samples in s[0 .. len) (s[k] <-> position base + k); forward: s
+// holds natural samples; inverse: s holds the interleaved L/H signal.
+// Positions whose neighbours are outside s are not valid afterwards.
+template <bool kInverse>
+__device__ __forceinline__ void liftLine(i16* s, int len, int base) {
+    if (!kInverse) {
+        for (int k = 1; k + 1 < len; ++k)
+            if (((base + k) & 1) == 1) s[k] = i16(s[k] - div2(i16(s[k - 1] + s[k + 1])));
+        for (int k = 2; k + 2 < len; ++k)
+            if (((base + k) & 1) == 0) s[k] = i16(s[k] + div4(i16(s[k - 1] + s[k + 1])));
+    } else {
+        for (int k = 1; k + 1 < len; ++k)
+            if (((base + k) & 1) == 0) s[k] = i16(s[k] - div4(i16(s[k - 1] + s[k + 1])));
+        for (int k = 2; k + 2 < len; ++k)
+            if (((base + k) & 1) == 1) s[k] = i16(s[k] + div2(i16(s[k - 1] + s[k + 1])));
+    }
+}
+
+// Generic int lifting pass along one axis: block (32, 8): 32 adjacent lines of
+// the fastest non-axis coordinate (x for Y/Z passes; for the X pass the lines
+// are rows and the block covers 32 rows), kColTile outputs per line.
+template <bool kInverse>
+__global__ void __launch_bounds__(256) k_liftAxis(i16* __restrict__ dst, const i16* __restrict__ src, int nLines,
+                                                  int na, int sLine, int sAxis, int sOther, int dLine, int dAxis,
+                                                  int dOther) {
+    __shared__ i16 s[32][kColTile + 8];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int line = blockIdx.x * 32 + tx;
+    const int a0 = blockIdx.y * kColTile;
+    const int c = blockIdx.z;
+    // stage positions a0-4 .. a0+kColTile+3
+    if (line < nLines) {
+        for (int k = ty; k < kColTile + 8; k += 8) {
+            int j = a0 - 4 + k;
+            if (j < na + 4) {
+                int m = mirrorIdx(j, na);
+                int ap = kInverse ? splitPos(m, na) : m;
+                s[tx][k] = src[size_t(line) * sLine + size_t(ap) * sAxis + size_t(c) * sOther];
+            }
+        }
+    }
+    __syncthreads();
+    if (line >= nLines) return;
+    if (ty == 0) {
+        int len = min(kColTile + 8, na + 4 - (a0 - 4));
+        liftLine<kInverse>(s[tx], len, a0 - 4);
+    }
+    __syncthreads();
+    for (int k = ty; k < kColTile; k += 8) {
+        int a = a0 + k;
+        if (a >= na) break;
+        int o = kInverse ? a : splitPos(a, na);
+        dst[size_t(line) * dLine + size_t(o) * dAxis + size_t(c) * dOther] = s[tx][k + 4];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side pass launchers.
+// ---------------------------------------------------------------------------
+template <class TIn, class TOut, bool kInverse>
+static void rowPass(TOut* dst, const TIn* src, int nx, int ny, int nz, int srcElem, int srcRow, int srcSlice,
+                    int dstElem, int dstRow, int dstSlice, cudaStream_t st) {
+    dim3 g(unsigned(ceilDiv(nx, kRowTile)), ny, nz);
+    k_firRows<TIn, TOut, kInverse><<<g, 256, 0, st>>>(dst, src, nx, srcElem, srcRow, srcSlice, dstElem, dstRow, dstSlice);
+}
+
+// axis 1 (Y, other = Z) or 2 (Z, other = Y)
+template <bool kInverse, class Load>
+static void colPass(float* dst, Load load, int nx, int ny, int nz, int axis, int dstRow, int dstSlice, cudaStream_t st) {
+    int na = axis == 1 ? ny : nz;
+    int nc = axis == 1 ? nz : ny;
+    dim3 g(unsigned(ceilDiv(nx, 32)), unsigned(ceilDiv(na, kColTile)), nc);
+    int da = axis == 1 ? dstRow : dstSlice;
+    int dc = axis == 1 ? dstSlice : dstRow;
+    k_firCols<Load, kInverse><<<g, dim3(32, 8), 0, st>>>(dst, load, nx, na, 1, da, dc);
+}
+
+static PitchLoad pitchLoad(const float* p, int axis, int row, int slice) {
+    PitchLoad l;
+    l.p = p;
+    l.sx = 1;
+    l.sa = axis == 1 ? row : slice;
+    l.sc = axis == 1 ? slice : row;
+    return l;
+}
+
+template <bool kInverse>
+static void liftPass(i16* dst, const i16* src, int nx, int ny, int nz, int axis, int srcRow, int srcSlice, int dstRow,
+                     int dstSlice, cudaStream_t st) {
+    // lines: X pass -> rows indexed by y (other = z); Y pass -> x (other = z); Z pass -> x (other = y)
+    int nLines, na, nc, sLine, sAxis, sOther, dLine, dAxis, dOther;
+    if (axis == 0) {
+        nLines = ny; na = nx; nc = nz;
+        sLine = srcRow; sAxis = 1; sOther = srcSlice;
+        dLine = dstRow; dAxis = 1; dOther = dstSlice;
+    } else if (axis == 1) {
+        nLines = nx; na = ny; nc = nz;
+        sLine = 1; sAxis = srcRow; sOther = srcSlice;
+        dLine = 1; dAxis = dstRow; dOther = dstSlice;
+    } else {
+        nLines = nx; na = nz; nc = ny;
+        sLine = 1; sAxis = srcSlice; sOther = srcRow;
+        dLine = 1; dAxis = dstSlice; dOther = dstRow;
+    }
+    dim3 g(unsigned(ceilDiv(nLines, 32)), unsigned(ceilDiv(na, kColTile)), nc);
+    k_liftAxis<kInverse><<<g, dim3(32, 8), 0, st>>>(dst, src, nLines, na, sLine, sAxis, sOther, dLine, dAxis, dOther);
+}
+
+static bool checkSizes(int sx, int sy, int sz, const char* what) {
+    bool ok = sx >= 8 && sy >= 8 && sz >= 1 && (sx % 2 == 0) && (sy % 2 == 0) && (sz == 1 || (sz >= 8 && sz % 2 == 0));
+    if (!ok) setError("%s: sizes must be even and >= 8 (got %d x %d x %d)", what, sx, sy, sz);
+    return ok;
+}
+
+}  // namespace ccb
+
+using namespace ccb;
+
+extern "C" {
+
+int cc_dwt_float_forward(float* dst, float* buf2, float* buf1, const float* src, int sx, int sy, int sz, int ch,
+                         int dstRow, int dstSlice, int srcRow, int srcSlice, void* stream) {
+    if (!checkSizes(sx, sy, sz, "dwtFloatForward")) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx * ch;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool do3D = sz > 1;
+    rowPass<float, float, false>(buf1, src, sx, sy, sz, ch, srcRow, srcSlice, 1, dstRow, dstSlice, st);
+    float* yDst = do3D ? buf2 : dst;
+    colPass<false>(yDst, pitchLoad(buf1, 1, dstRow, dstSlice), sx, sy, sz, 1, dstRow, dstSlice, st);
+    if (do3D) colPass<false>(dst, pitchLoad(buf2, 2, dstRow, dstSlice), sx, sy, sz, 2, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatForward");
+    return CC_OK;
+}
+
+int cc_dwt_float_inverse(float* dst, float* buf2, float* buf1, const float* src, int sx, int sy, int sz, int ch,
+                         int dstRow, int dstSlice, int srcRow, int srcSlice, void* stream) {
+    if (!checkSizes(sx, sy, sz, "dwtFloatInverse")) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx * ch;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool do3D = sz > 1;
+    const float* ySrc = src;
+    if (do3D) {
+        colPass<true>(buf2, pitchLoad(src, 2, srcRow, srcSlice), sx, sy, sz, 2, srcRow, srcSlice, st);
+        ySrc = buf2;
+    }
+    colPass<true>(buf1, pitchLoad(ySrc, 1, srcRow, srcSlice), sx, sy, sz, 1, srcRow, srcSlice, st);
+    rowPass<float, float, true>(dst, buf1, sx, sy, sz, 1, srcRow, srcSlice, ch, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatInverse");
+    return CC_OK;
+}
+
+int cc_dwt_float_inverse_from_symbols(float* dst, float* buf2, float* buf1, const float* lowpass,
+                                      const void* const* highpass, int symBytes, float step, int sx, int sy, int sz,
+                                      int ch, int dstRow, int dstSlice, int lpRow, int lpSlice, void* stream) {
+    if (!checkSizes(sx, sy, sz, "dwtFloatInverseFromSymbols")) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (symBytes != 2 && symBytes != 4) { setError("symbol size must be 2 or 4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx * ch;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (lpRow <= 0) lpRow = sx;
+    if (lpSlice <= 0) lpSlice = sy * lpRow;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool do3D = sz > 1;
+    const int bRow = sx, bSlice = sx * sy;   // DWTFloat.cu:354-355: tight intermediates
+    auto first = [&](auto tag, float* out, int axis) {
+        using Sym = decltype(tag);
+        SymbolLoad<Sym> l;
+        l.lp = lowpass;
+        l.lpRow = lpRow;
+        l.lpSlice = lpSlice;
+        l.bands = reinterpret_cast<const Sym* const*>(highpass);
+        l.step = step;
+        l.hx = sx / 2;
+        l.hy = sy / 2;
+        l.hz = do3D ? sz / 2 : 1;
+        l.axisIsZ = axis == 2;
+        colPass<true>(out, l, sx, sy, sz, axis, bRow, bSlice, st);
+    };
+    if (do3D) {
+        if (symBytes == 2) first(u16(), buf2, 2); else first(u32(), buf2, 2);
+        colPass<true>(buf1, pitchLoad(buf2, 1, bRow, bSlice), sx, sy, sz, 1, bRow, bSlice, st);
+    } else {
+        if (symBytes == 2) first(u16(), buf1, 1); else first(u32(), buf1, 1);
+    }
+    rowPass<float, float, true>(dst, buf1, sx, sy, sz, 1, bRow, bSlice, ch, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatInverseFromSymbols");
+    return CC_OK;
+}
+
+int cc_dwt_int_forward(int16_t* dst, int16_t* buf, const int16_t* src, int sx, int sy, int sz, int dstRow,
+                       int dstSlice, int srcRow, int srcSlice, void* stream) {
+    if (!checkSizes(sx, sy, sz, "dwtIntForward")) return CC_ERR_INVALID_ARGUMENT;
+    if (dstRow <= 0) dstRow = sx;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool do3D = sz > 1;
+    i16* xDst = do3D ? dst : buf;                       // DWTInt.cu:111
+    liftPass<false>(xDst, src, sx, sy, sz, 0, srcRow, srcSlice, dstRow, dstSlice, st);
+    i16* yDst = do3D ? buf : dst;                       // DWTInt.cu:138
+    liftPass<false>(yDst, xDst, sx, sy, sz, 1, dstRow, dstSlice, dstRow, dstSlice, st);
+    if (do3D) liftPass<false>(dst, buf, sx, sy, sz, 2, dstRow, dstSlice, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), "dwtIntForward");
+    return CC_OK;
+}
+
+int cc_dwt_int_inverse(int16_t* dst, int16_t* buf, const int16_t* src, int sx, int sy, int sz, int dstRow,
+                       int dstSlice, int srcRow, int srcSlice, void* stream) {
+    if (!checkSizes(sx, sy, sz, "dwtIntInverse")) return CC_ERR_INVALID_ARGUMENT;
+    if (dstRow <= 0) dstRow = sx;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool do3D = sz > 1;
+    const i16* ySrc = src;
+    if (do3D) {
+        liftPass<true>(dst, src, sx, sy, sz, 2, srcRow, srcSlice, srcRow, srcSlice, st);
+        ySrc = dst;
+    }
+    liftPass<true>(buf, ySrc, sx, sy, sz, 1, srcRow, srcSlice, srcRow, srcSlice, st);
+    liftPass<true>(dst, buf, sx, sy, sz, 0, srcRow, srcSlice, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), "dwtIntInverse");
+    return CC_OK;
+}
+
+}  // extern "C"

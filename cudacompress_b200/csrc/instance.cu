@@ -1,0 +1,219 @@
+// instance.cu - cc_instance lifetime, device arena and host staging
+// (replaces Instance.cpp:8-67 and InstanceImpl.cpp:46-279 of the reference).
+//
+// All device memory an instance needs is allocated once at creation, sized
+// from (streamCountMax, elemCountPerStreamMax, codingBlockSize,
+// log2HuffmanDistinctSymbolCountMax); calls never allocate.
+#include <cstring>
+#include <string>
+
+#include "capi_internal.cuh"
+
+using namespace ccb;
+
+namespace ccb {
+
+static thread_local std::string g_lastError;
+
+void setError(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+}
+
+int cudaFail(cudaError_t e, const char* what) {
+    setError("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CC_ERR_OUT_OF_MEMORY : CC_ERR_CUDA;
+}
+
+u32 headerWordsFor(u32 leaves, u32 log2Max) {
+    u64 symBits = log2Max > 16 ? 24 : 16;
+    u64 bits = 5 + 31ull * log2Max + log2Max + 5 + u64(leaves) * symBits;
+    return u32(ceilDiv(bits, 32) + 2);
+}
+
+// Worst-case words of one stream's segment: Huffman output never exceeds a
+// fixed-length code of ceil(log2(distinct)) bits per symbol (Huffman codes are
+// optimal among prefix codes), i.e. log2Max bits for symbols and 8 bits for
+// zero counts (at most 256 distinct values).
+u64 segmentWordsMax(u32 n, u32 cb, u32 log2Max, u32 hdrWords) {
+    u64 offs = ceilDiv(ceilDiv(n, cb), 2);
+    u64 sym = ceilDiv(u64(n) * log2Max, 32) + 1;
+    u64 zc = ceilDiv(u64(n) * 8, 32) + 1;
+    return 1 + 2ull * hdrWords + 2 + sym + zc + 2 * offs + 4;
+}
+
+int ensurePipelineWork(cc_instance* I, size_t bytes) {
+    if (I->pipeWorkBytes >= bytes) return CC_OK;
+    cudaStreamSynchronize(I->stream);
+    if (I->pipeWork) cudaFree(I->pipeWork);
+    I->pipeWork = nullptr;
+    I->pipeWorkBytes = 0;
+    cudaError_t e = cudaMalloc(&I->pipeWork, bytes);
+    if (e != cudaSuccess) return cudaFail(e, "cudaMalloc(pipeline workspace)");
+    I->pipeWorkBytes = bytes;
+    return CC_OK;
+}
+
+}  // namespace ccb
+
+char* cc_instance::takeRingSlot() {
+    int i = ringNext;
+    ringNext = (ringNext + 1) % kRing;
+    cudaEventSynchronize(ringEvent[i]);
+    return hostRing[i];
+}
+
+namespace {
+
+struct Carver {
+    char* base;
+    size_t off = 0;
+    template <class T>
+    T* take(u64 count) {
+        off = alignUp(off, 256);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+void layoutArena(cc_instance* I, char* base, size_t* total) {
+    Carver c{base};
+    u32 S = I->streamCountMax, N = I->elemCountPerStreamMax;
+    u32 T = 2 * S;
+    I->compact = c.take<char>(u64(S) * N * I->symBytes + 64);
+    I->zc = c.take<char>(u64(S) * N * I->symBytes + 64);
+    I->tiles = c.take<RunSum>(u64(S) * I->tilesMax);
+    I->tileStart = c.take<TileStart>(u64(S) * I->tilesMax);
+    I->hist = c.take<u32>(u64(T) * I->bins);
+    I->enc = c.take<uint2>(u64(T) * I->bins);
+    I->meta = c.take<TableMeta>(T);
+    I->headers = c.take<u32>(u64(T) * I->hdrWordsMax);
+    I->blockBits = c.take<u32>(u64(T) * I->blocksMax + 1);
+    I->blockOff = c.take<u32>(u64(T) * I->blocksMax + 1);
+    I->layout = c.take<SegmentLayout>(S);
+    I->out = c.take<u32>(I->outWordsMax);
+    I->counts = c.take<u32>(S);
+    I->errors = c.take<u32>(8);
+    I->totals = c.take<u64>(8);
+    I->dStreams = c.take<EncStream>(S);
+    I->leafWork = c.take<u64>(u64(T) * I->leavesMax);
+    I->parentWork = c.take<u32>(u64(T) * 2 * I->leavesMax);
+    I->orderWork = c.take<u32>(u64(T) * I->leavesMax);
+    I->leafSymWork = c.take<u32>(u64(T) * I->leavesMax);
+    I->dDecTables = c.take<DecTableDesc>(T);
+    I->dDecStreams = c.take<DecStreamDesc>(S);
+    I->decTables = c.take<DecTable>(T);
+    I->decSyms = c.take<u32>(u64(T) * I->leavesMax);
+    I->decLut = c.take<u32>(u64(T) << kLutBits);
+    I->stagedWordsMax = I->outWordsMax + 64;
+    I->stagedWords = c.take<u32>(I->stagedWordsMax);
+    I->blockSum = c.take<u32>(u64(S) * I->blocksMax + 1);
+    *total = alignUp(c.off, 256);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cc_last_error(void) { return g_lastError.c_str(); }
+const char* cc_version(void) { return "cudacompress_b200 0.1 (sm_100a)"; }
+
+int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMax, uint32_t elemCountPerStreamMax,
+                       uint32_t codingBlockSize, uint32_t log2Max) {
+    if (!out) { setError("cc_create_instance: out is NULL"); return CC_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    if (codingBlockSize == 0) codingBlockSize = 128;          // InstanceImpl.cpp:65-69
+    if (log2Max == 0) log2Max = 14;                           // InstanceImpl.cpp:71-75
+    if (log2Max > 24) { setError("log2HuffmanDistinctSymbolCountMax must be <= 24 (got %u)", log2Max); return CC_ERR_INVALID_ARGUMENT; }
+    if (codingBlockSize != 32 && codingBlockSize != 64 && codingBlockSize != 128 && codingBlockSize != 256) {
+        setError("codingBlockSize must be 32, 64, 128 or 256 (got %u)", codingBlockSize);  // Huffman.h:42
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    if (streamCountMax == 0 || elemCountPerStreamMax == 0) { setError("stream/elem count max must be > 0"); return CC_ERR_INVALID_ARGUMENT; }
+    cudaError_t e;
+    if (cudaDevice >= 0) {
+        if ((e = cudaSetDevice(cudaDevice)) != cudaSuccess) return cudaFail(e, "cudaSetDevice");
+    } else {
+        if ((e = cudaGetDevice(&cudaDevice)) != cudaSuccess) return cudaFail(e, "cudaGetDevice");
+    }
+    cc_instance* I = new cc_instance();
+    I->device = cudaDevice;
+    I->streamCountMax = streamCountMax;
+    I->elemCountPerStreamMax = elemCountPerStreamMax;
+    I->codingBlockSize = codingBlockSize;
+    I->log2Max = log2Max;
+    I->bins = 1u << log2Max;
+    I->symBytes = log2Max > 16 ? 4 : 2;
+    I->tilesMax = u32(ceilDiv(elemCountPerStreamMax, kRleTile));
+    I->blocksMax = u32(ceilDiv(elemCountPerStreamMax, codingBlockSize));
+    I->leavesMax = std::max<u32>(1u, std::min<u32>(I->bins, elemCountPerStreamMax));
+    I->hdrWordsMax = headerWordsFor(I->leavesMax, log2Max);
+    I->outWordsMax = u64(streamCountMax) * segmentWordsMax(elemCountPerStreamMax, codingBlockSize, log2Max, I->hdrWordsMax);
+
+    size_t bytes = 0;
+    layoutArena(I, nullptr, &bytes);
+    if ((e = cudaMalloc(&I->arena, bytes)) != cudaSuccess) { delete I; return cudaFail(e, "cudaMalloc(instance arena)"); }
+    I->arenaBytes = bytes;
+    layoutArena(I, I->arena, &bytes);
+    cudaMemset(I->arena, 0, bytes);
+
+    u32 T = 2 * streamCountMax;
+    I->hostRingBytes = alignUp(u64(T) * sizeof(DecTableDesc) + u64(streamCountMax) * sizeof(DecStreamDesc) +
+                               u64(streamCountMax) * sizeof(EncStream) + 4096, 4096);
+    for (int i = 0; i < cc_instance::kRing; ++i) {
+        if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostRing[i]), I->hostRingBytes, cudaHostAllocDefault)) != cudaSuccess) {
+            cc_destroy_instance(I);
+            return cudaFail(e, "cudaHostAlloc(ring)");
+        }
+        cudaEventCreateWithFlags(&I->ringEvent[i], cudaEventDisableTiming);
+        cudaEventRecord(I->ringEvent[i], 0);
+    }
+    I->hostDownBytes = alignUp(u64(streamCountMax) * sizeof(SegmentLayout) + 256, 4096);
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostDown), I->hostDownBytes, cudaHostAllocDefault)) != cudaSuccess) {
+        cc_destroy_instance(I);
+        return cudaFail(e, "cudaHostAlloc(down)");
+    }
+    I->hostWordsMax = I->outWordsMax;
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostWords), I->hostWordsMax * 4, cudaHostAllocDefault)) != cudaSuccess) {
+        cc_destroy_instance(I);
+        return cudaFail(e, "cudaHostAlloc(words)");
+    }
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) { cc_destroy_instance(I); return cudaFail(e, "instance init"); }
+    *out = I;
+    return CC_OK;
+}
+
+void cc_destroy_instance(cc_instance* I) {
+    if (!I) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (I->device >= 0) cudaSetDevice(I->device);
+    cudaDeviceSynchronize();
+    for (int i = 0; i < cc_instance::kRing; ++i) {
+        if (I->ringEvent[i]) cudaEventDestroy(I->ringEvent[i]);
+        if (I->hostRing[i]) cudaFreeHost(I->hostRing[i]);
+    }
+    if (I->hostDown) cudaFreeHost(I->hostDown);
+    if (I->hostWords) cudaFreeHost(I->hostWords);
+    if (I->arena) cudaFree(I->arena);
+    if (I->pipeWork) cudaFree(I->pipeWork);
+    if (prev >= 0) cudaSetDevice(prev);
+    delete I;
+}
+
+int cc_get_instance_cuda_device(const cc_instance* I) { return I ? I->device : -1; }
+uint32_t cc_get_instance_stream_count_max(const cc_instance* I) { return I ? I->streamCountMax : 0; }
+uint32_t cc_get_instance_elem_count_per_stream_max(const cc_instance* I) { return I ? I->elemCountPerStreamMax : 0; }
+uint32_t cc_get_instance_coding_block_size(const cc_instance* I) { return I ? I->codingBlockSize : 0; }
+uint32_t cc_get_instance_log2_huffman_distinct_symbol_count_max(const cc_instance* I) { return I ? I->log2Max : 0; }
+int cc_get_instance_use_long_symbols(const cc_instance* I) { return I && I->log2Max > 16 ? 1 : 0; }
+void cc_set_instance_stream(cc_instance* I, void* s) { if (I) I->stream = static_cast<cudaStream_t>(s); }
+void* cc_get_instance_stream(const cc_instance* I) { return I ? static_cast<void*>(I->stream) : nullptr; }
+size_t cc_encode_get_required_memory(const cc_instance* I) { return I ? I->arenaBytes : 0; }
+
+}  // extern "C"

@@ -1,0 +1,178 @@
+/*
+ * cudacompress_b200.h - C ABI of the B200-native cudaCompress hot path.
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA device addresses
+ * (e.g. from cudaMalloc or a framework allocator); streams are cudaStream_t
+ * passed as void*.  Every function returning int returns CC_OK (0) or a
+ * negative status; cc_last_error() describes the last failure on the calling
+ * thread.  The C++ drop-in layer (include/cudaCompress/*.h, namespace
+ * cudaCompress) is built on these entry points.
+ *
+ * Each declaration cites the reference interface it replaces (paths relative
+ * to the cudaCompress project root).
+ */
+#ifndef CUDACOMPRESS_B200_H
+#define CUDACOMPRESS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CC_OK 0
+#define CC_ERR_INVALID_ARGUMENT (-1)
+#define CC_ERR_CUDA (-2)
+#define CC_ERR_OUT_OF_MEMORY (-3)
+#define CC_ERR_SYMBOL_RANGE (-4)
+#define CC_ERR_CODEWORD_TOO_LONG (-5)
+#define CC_ERR_CORRUPT_STREAM (-6)
+#define CC_ERR_CAPACITY (-7)
+#define CC_ERR_DEVICE_TIMEOUT (-8)
+
+#define CC_KIND_RLHUFF 0
+#define CC_KIND_HUFF 1
+
+typedef struct cc_instance cc_instance;
+
+/* Last error message of the calling thread ("" if none). */
+const char* cc_last_error(void);
+/* Library version string. */
+const char* cc_version(void);
+
+/* ---- Instance (include/cudaCompress/Instance.h:26-45, src/cudaCompress/Instance.cpp:8-67) ---- */
+
+/* createInstance(cudaDevice, streamCountMax, elemCountPerStreamMax,
+ * codingBlockSize = 0 -> 128, log2HuffmanDistinctSymbolCountMax = 0 -> 14).
+ * Instance.h:26-31.  *out is NULL on failure. */
+int cc_create_instance(cc_instance** out, int cuda_device, uint32_t stream_count_max,
+                       uint32_t elem_count_per_stream_max, uint32_t coding_block_size,
+                       uint32_t log2_huffman_distinct_symbol_count_max);
+/* destroyInstance, Instance.h:33. */
+void cc_destroy_instance(cc_instance* inst);
+/* getInstance* queries, Instance.h:36-41. */
+int cc_get_instance_cuda_device(const cc_instance* inst);
+uint32_t cc_get_instance_stream_count_max(const cc_instance* inst);
+uint32_t cc_get_instance_elem_count_per_stream_max(const cc_instance* inst);
+uint32_t cc_get_instance_coding_block_size(const cc_instance* inst);
+uint32_t cc_get_instance_log2_huffman_distinct_symbol_count_max(const cc_instance* inst);
+int cc_get_instance_use_long_symbols(const cc_instance* inst);
+/* setInstanceCudaStream / getInstanceCudaStream, Instance.h:44-45
+ * (defined as setInstanceStream / getInstanceStream in Instance.cpp:59-67). */
+void cc_set_instance_stream(cc_instance* inst, void* cuda_stream);
+void* cc_get_instance_stream(const cc_instance* inst);
+/* encodeGetRequiredMemory, Encode.h:17: device bytes the instance holds. */
+size_t cc_encode_get_required_memory(const cc_instance* inst);
+
+/* ---- Entropy coding (include/cudaCompress/Encode.h:28-52, src/cudaCompress/Encode.cpp:207-1042) ----
+ *
+ * Encode: `kind` CC_KIND_RLHUFF (encodeRLHuff) or CC_KIND_HUFF (encodeHuff);
+ * `symbol_bytes` 2 (Symbol16) or 4 (Symbol32, instances with log2Max > 16).
+ * d_streams[i] holds symbol_count_per_stream symbols.  Input buffers are not
+ * modified (the reference pads encodeHuff inputs; this library needs no
+ * padding).  The result is one segment per stream, each a run of 32-bit
+ * words; start_bits[i] (0..31, NULL = all 0) is the bit offset, inside its
+ * first word, at which stream i's segment starts - only meaningful for
+ * encodeHuff streams that start a bit stream at an unaligned position.
+ * Segments stay in the instance's host staging until the next call.
+ * Synchronous, like the reference (Encode.cpp:394,744). */
+int cc_encode(cc_instance* inst, int kind, int symbol_bytes, const void* const* d_streams,
+              uint32_t stream_count, uint32_t symbol_count_per_stream, const uint32_t* start_bits);
+/* Segment i of the last cc_encode: host words, word count, bit offset of its
+ * first bit in word 0, and bit length measured from word 0 bit 0. */
+int cc_encoded_segment(const cc_instance* inst, uint32_t i, const uint32_t** words, uint32_t* word_count,
+                       uint32_t* start_bit, uint32_t* bit_length);
+
+/* Convenience form of the single-bit-stream overloads (Encode.h:28-38): the
+ * bit stream is a caller-owned word buffer with its bit size and write
+ * position (in/out), appended to exactly as BitStream::write* would.
+ * CC_ERR_CAPACITY (with *bit_size = required bits) if it does not fit. */
+int cc_encode_to_buffer(cc_instance* inst, int kind, int symbol_bytes, const void* const* d_streams,
+                        uint32_t stream_count, uint32_t symbol_count_per_stream, uint32_t* words,
+                        uint32_t capacity_words, uint32_t* bit_size, uint32_t* bit_pos);
+
+/* Decode (decodeRLHuff / decodeHuff, Encode.h:29-52).  Stream i is read from
+ * bit stream bs_index[i] (NULL = all from bit stream 0) of `bitstream_count`
+ * host word buffers; positions advance in stream order.  Outputs of
+ * decodeRLHuff must be zeroed by the caller (Encode.h:22); no output padding
+ * is required.  Asynchronous on the instance stream: returns once the work is
+ * queued; host memory may be reused on return. */
+int cc_decode(cc_instance* inst, int kind, int symbol_bytes, const uint32_t* const* words,
+              const uint32_t* bit_sizes, uint32_t* bit_positions, uint32_t bitstream_count,
+              const uint32_t* bs_index, void* const* d_out_streams, uint32_t stream_count,
+              uint32_t symbol_count_per_stream);
+
+/* Synchronizes the instance stream and reports whether the last decode found
+ * the bit stream corrupt (CC_ERR_CORRUPT_STREAM) - the device-side checks of
+ * an asynchronous decode surface here. */
+int cc_decode_status(cc_instance* inst);
+
+/* ---- util::DWT (include/cudaCompress/util/DWT.h:21-157, src/cudaCompress/util/DWTFloat.cu, DWTInt.cu) ----
+ * Same argument meaning as the reference; pitches in elements, 0 = tight;
+ * channel counts 1..4; all sizes even.  stream: cudaStream_t as void*. */
+int cc_dwt_float_forward(float* d_dst, float* d_buf2, float* d_buf1, const float* d_src, int size_x, int size_y,
+                         int size_z, int src_channel_count, int dst_row_pitch, int dst_slice_pitch,
+                         int src_row_pitch, int src_slice_pitch, void* stream);
+int cc_dwt_float_inverse(float* d_dst, float* d_buf2, float* d_buf1, const float* d_src, int size_x, int size_y,
+                         int size_z, int dst_channel_count, int dst_row_pitch, int dst_slice_pitch,
+                         int src_row_pitch, int src_slice_pitch, void* stream);
+/* dwtFloat{2D,3D}InverseFromSymbols: d_highpass is a device array of 3 (2D) or
+ * 7 (3D) device pointers to the quantized highpass bands (band index
+ * x+2y+4z-1); symbol_bytes 2 or 4. */
+int cc_dwt_float_inverse_from_symbols(float* d_dst, float* d_buf2, float* d_buf1, const float* d_lowpass,
+                                      const void* const* d_highpass, int symbol_bytes, float quant_step,
+                                      int size_x, int size_y, int size_z, int dst_channel_count,
+                                      int dst_row_pitch, int dst_slice_pitch, int lowpass_row_pitch,
+                                      int lowpass_slice_pitch, void* stream);
+int cc_dwt_int_forward(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int size_x, int size_y, int size_z,
+                       int dst_row_pitch, int dst_slice_pitch, int src_row_pitch, int src_slice_pitch, void* stream);
+int cc_dwt_int_inverse(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int size_x, int size_y, int size_z,
+                       int dst_row_pitch, int dst_slice_pitch, int src_row_pitch, int src_slice_pitch, void* stream);
+
+/* ---- util::Quantize (include/cudaCompress/util/Quantize.h:25-65, src/cudaCompress/util/Quantize.cu) ----
+ * quant_type 0 = QUANTIZE_DEADZONE, 1 = QUANTIZE_UNIFORM.  The reference
+ * launches these on the default stream; `stream` NULL does the same. */
+int cc_quantize_to_symbols(void* d_symbols, int symbol_bytes, const float* d_data, uint32_t size_x,
+                           uint32_t size_y, uint32_t size_z, float quant_step, uint32_t row_pitch_src,
+                           uint32_t slice_pitch_src, int quant_type, void* stream);
+int cc_quantize_to_symbols_roundtrip(void* d_symbols, int symbol_bytes, float* d_data, uint32_t size_x,
+                                     uint32_t size_y, uint32_t size_z, float quant_step, uint32_t row_pitch_src,
+                                     uint32_t slice_pitch_src, int quant_type, void* stream);
+int cc_unquantize_from_symbols(float* d_data, const void* d_symbols, int symbol_bytes, uint32_t size_x,
+                               uint32_t size_y, uint32_t size_z, float quant_step, uint32_t row_pitch_dst,
+                               uint32_t slice_pitch_dst, int quant_type, void* stream);
+int cc_symbolize(uint16_t* d_symbols, const int16_t* d_data, uint32_t size_x, uint32_t size_y, uint32_t size_z,
+                 uint32_t row_pitch_src, uint32_t slice_pitch_src, void* stream);
+int cc_unsymbolize(int16_t* d_data, const uint16_t* d_symbols, uint32_t size_x, uint32_t size_y, uint32_t size_z,
+                   uint32_t row_pitch_dst, uint32_t slice_pitch_dst, void* stream);
+int cc_quantize_to_short(int16_t* d_quant, const float* d_data, uint32_t size_x, uint32_t size_y, uint32_t size_z,
+                         float quant_step, uint32_t row_pitch_src, uint32_t slice_pitch_src, int quant_type,
+                         void* stream);
+int cc_unquantize_from_short(float* d_data, const int16_t* d_quant, uint32_t size_x, uint32_t size_y,
+                             uint32_t size_z, float quant_step, uint32_t row_pitch_dst, uint32_t slice_pitch_dst,
+                             int quant_type, void* stream);
+/* getMaxAbs(pInstance, dpImage, elemCount, dpValMax): max |x| into d_max. */
+int cc_get_max_abs(cc_instance* inst, const float* d_data, uint32_t elem_count, float* d_max);
+
+/* ---- Volume / heightfield codecs (examples CompressVolume.cpp:312-516, CompressHeightfield.cpp:82-216) ----
+ * Whole-pipeline entry points: device-resident input, device-resident bit
+ * stream (32-bit words).  The byte stream equals the reference pipeline's
+ * (LP encodeHuff, then per level coarse->fine the HP bands encodeRLHuff).
+ * *bit_size receives the stream length; capacity in words. */
+int cc_compress_volume_float(cc_instance* inst, const float* d_volume, uint32_t size_x, uint32_t size_y,
+                             uint32_t size_z, uint32_t levels, float quant_step_level0, uint32_t* d_words,
+                             uint64_t capacity_words, uint32_t* bit_size);
+int cc_decompress_volume_float(cc_instance* inst, float* d_volume, uint32_t size_x, uint32_t size_y,
+                               uint32_t size_z, uint32_t levels, float quant_step_level0, const uint32_t* d_words,
+                               uint32_t bit_size);
+int cc_compress_heightfield(cc_instance* inst, const int16_t* d_image, uint32_t size_x, uint32_t size_y,
+                            uint32_t levels, uint32_t* d_words, uint64_t capacity_words, uint32_t* bit_size);
+int cc_decompress_heightfield(cc_instance* inst, int16_t* d_image, uint32_t size_x, uint32_t size_y,
+                              uint32_t levels, const uint32_t* d_words, uint32_t bit_size);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDACOMPRESS_B200_H */

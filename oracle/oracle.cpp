@@ -653,7 +653,9 @@ static void dwtInt(const i16* src, i16* dst, long nx, long ny, long nz, bool inv
 // ---------------------------------------------------------------------------
 // Quantization (util/Quantize.cuh:55-147, util/Quantize.cu:78-100).
 // ---------------------------------------------------------------------------
-static inline u32 symbolize(int v) { return 2u * u32(std::abs(v)) + (v < 0 ? 1u : 0u); }   // Quantize.cuh:55-59
+// Quantize.cuh:26-35,55-59: 2|v| + getNegativeSign(v), where getNegativeSign is
+// -1 for negative values: v >= 0 -> 2v (even), v < 0 -> 2|v|-1 (odd).
+static inline u32 symbolize(int v) { return 2u * u32(std::abs(v)) - (v < 0 ? 1u : 0u); }
 static inline int unsymbolize(u32 s) { int neg = int(s % 2); return (1 - 2 * neg) * int((s + u32(neg)) / 2); }
 static inline int quantDeadzone(float v, float inv) { return int(v * inv); }                  // Quantize.cuh:75-82
 static inline float unquantDeadzone(int q, float step) {                                     // Quantize.cuh:104-110
