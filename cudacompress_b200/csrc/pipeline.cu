@@ -187,7 +187,7 @@ int cc_decompress_volume_float(cc_instance* I, float* out, uint32_t nx, uint32_t
     for (int l = int(L) - 1; l >= 0; --l) {
         const int sx = int(nx >> l), sy = int(ny >> l), sz = int(nz >> l);
         rc = cc_dwt_float_inverse_from_symbols(l == 0 ? out : cur, t2, t1, cur, dPtrs + l * 8, 2, q0 / float(1u << l),
-                                               sx, sy, sz, 1, 0, 0, 0, 0, st);
+                                               sx, sy, sz, 1, 0, 0, sx / 2, (sx / 2) * (sy / 2), st);
         if (rc) return rc;
     }
     CC_TRY_CUDA(cudaStreamSynchronize(st), "decompressVolumeFloat");
