@@ -1,0 +1,419 @@
+#!/usr/bin/env python3
+"""Benchmark of the cudaCompress hot path on B200.
+
+Workload (default): the 3-component 256^3 float32 vector field - each
+component a seeded k^(-5/3) random-phase field (1024 modes, |k| <= 64, unit
+std) - compressed with the lossy volume codec (3-level CDF 9/7 DWT, deadzone
+quantization with step 0.01*std, zero-run RLE + Huffman, coding block 128)
+and decompressed again.  One step = encode + decode of all 3 components.
+
+  value   raw field bytes / step time, inputs and outputs resident in HBM
+          (GB/s raw, encode+decode); encode_gbs / decode_gbs split it
+  e2e     the same through the public API with host buffers: H2D of the field,
+          D2H of the stream, H2D of the stream, D2H of the reconstruction
+          inside the timed region
+  roofline  the dominant kernel section (CUDA-event timed inside the library)
+          against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own CPU coder (src/CPU RunLengthCPU /
+          HuffmanTableCPU / HuffmanCPU, built from the reference sources into
+          oracle/_ref) plus the oracle's CPU DWT/quantize port (the reference
+          has no CPU DWT), on one component, all host threads
+
+`--impl reference` times that CPU path as the reference arm.  Multi-GPU runs
+(torchrun) are weak-scaling replicas: every rank codes its own field, no
+collective on the data path; the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "vector-field-256": dict(n=256, comps=3, levels=3, q0=0.01, seeds=(1002, 1003, 1004), modes=1024, kmax=64,
+                             desc="3 x 256^3 float32 k^-5/3 velocity, 3-level CDF 9/7, q0=0.01*std, RLE+Huffman cb=128"),
+    "volume-128": dict(n=128, comps=1, levels=3, q0=0.01, seeds=(1000,), modes=512, kmax=32,
+                       desc="128^3 float32 k^-5/3 field, 3-level CDF 9/7, q0=0.01*std, RLE+Huffman cb=128"),
+}
+FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 1024 * 1024
+
+
+def load_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.lines = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(gpu_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ fields
+def make_fields(wl, rank=0):
+    from cudacompress_b200 import fields
+    return [fields.turbulence_field(wl["n"], wl["modes"], wl["kmax"], s + 100 * rank) for s in wl["seeds"]]
+
+
+# -------------------------------------------------------------- CPU paths
+def cpu_reference_step(vol, wl, threads):
+    """Reference CPU coder on one component: oracle DWT + quantize (the
+    reference has no CPU DWT), the reference's own src/CPU RLE+Huffman for
+    every band stream, then the inverse.  Returns (encode_s, decode_s, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import Oracle
+    orc = Oracle()
+    n, L, q0 = wl["n"], wl["levels"], wl["q0"]
+    total = n ** 3
+    refcpu_path = os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")
+    t0 = time.perf_counter()
+    syms = np.zeros(total, np.uint16)
+    orc.lib.orc_volume_symbols(vol, n, n, n, L, q0, syms)
+    if os.path.exists(refcpu_path):
+        kind = "reference"
+        ref = ctypes.CDLL(refcpu_path)
+        vp = ctypes.c_void_p
+        ref.refcpu_encode_rlhuff.restype = ctypes.c_long
+        ref.refcpu_encode_rlhuff.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp,
+                                             ctypes.c_long, vp]
+        ref.refcpu_decode_rlhuff.restype = ctypes.c_int
+        ref.refcpu_decode_rlhuff.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
+        # stream groups as the codec calls them: LP (1 stream), then per level
+        # coarse->fine the 7 bands (equal sizes, contiguous)
+        groups = [(0, 1, (n >> L) ** 3)]
+        off = (n >> L) ** 3
+        for l in range(L - 1, -1, -1):
+            bn = (n >> (l + 1)) ** 3
+            groups.append((off, 7, bn))
+            off += 7 * bn
+        outs = []
+        for (o, S, cnt) in groups:
+            cap = S * cnt * 2 + 4096 * S
+            words = np.zeros(cap, np.uint32)
+            sw = np.zeros(S, np.uint32)
+            r = ref.refcpu_encode_rlhuff(syms[o:].ctypes.data, S, cnt, 128, threads, words.ctypes.data,
+                                         ctypes.c_long(cap), sw.ctypes.data)
+            assert r >= 0
+            outs.append((words, sw, o, S, cnt))
+        t1 = time.perf_counter()
+        dec = np.zeros(total, np.uint16)
+        for (words, sw, o, S, cnt) in outs:
+            ref.refcpu_decode_rlhuff(words.ctypes.data, sw.ctypes.data, S, cnt, 128, threads, dec[o:].ctypes.data)
+        rec = np.zeros(vol.shape, np.float32)
+        orc.lib.orc_volume_from_symbols(dec, rec, n, n, n, L, q0)
+        t2 = time.perf_counter()
+        assert np.array_equal(dec, syms), "reference CPU coder round trip mismatch"
+        return t1 - t0, t2 - t1, kind
+    kind = "port"
+    words, bits = orc.compress_volume(vol, L, q0)
+    t1 = time.perf_counter()
+    orc.decompress_volume(words, bits, vol.shape, L, q0)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1, kind
+
+
+def run_reference(args, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    vol = make_fields(wl)[0]
+    for _ in range(args.warmup):
+        cpu_reference_step(vol, wl, threads)
+    times = []
+    kind = "port"
+    for _ in range(args.steps):
+        e, d, kind = cpu_reference_step(vol, wl, threads)
+        times.append(e + d)
+    raw = wl["n"] ** 3 * 4
+    step = sum(times) / len(times)
+    value = raw / step / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": wl["desc"], "sample": "one component per step"},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
+                         "sample": f"1 of {wl['comps']} components ({wl['n']}^3 f32) encode+decode per step"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "enc/dec GB/s raw (%HBM peak); batched vs per-brick GB/s at fixed PSNR; p99"
+
+
+# ---------------------------------------------------------- section bytes
+def section_bytes(name, wl, coded_bytes, counts):
+    """Compulsory HBM bytes of one timed section over one step (algorithmic:
+    each input read once, each output written once)."""
+    n, L, C = wl["n"], wl["levels"], wl["comps"]
+    vols = [(n >> l) ** 3 for l in range(L)]
+    hp = sum(7 * v // 8 for v in vols)
+    lp = vols[-1] // 8
+    m = {
+        "pipe.dwt_forward": sum(8 * v for v in vols) * C,
+        "pipe.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
+        "pipe.quantize": (hp + lp) * 6 * C,
+        "enc.rle_summary": hp * 2 * C,
+        "enc.rle_write_hist": hp * 2 * C + counts.get("compact", 0) * 4,
+        "enc.histogram": lp * 2 * C,
+        "enc.block_bits": (lp * C + 2 * counts.get("compact", 0)) * 2,
+        "enc.pack": (lp * C + 2 * counts.get("compact", 0)) * 2 + coded_bytes,
+        "dec.huffman": lp * 2 * C,
+        "dec.zero_counts": counts.get("compact", 0) * 2,
+        "dec.symbols_scatter": counts.get("compact", 0) * 4 + hp * 2 * C,
+    }
+    return m.get(name)
+
+
+# ---------------------------------------------------------------- ours
+def run_ours(args, wl):
+    import torch
+    import cudacompress_b200 as cc
+    from cudacompress_b200 import fields
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    n, L, q0, C = wl["n"], wl["levels"], wl["q0"], wl["comps"]
+    vols_h = make_fields(wl, rank)
+    vols = [torch.from_numpy(v).to(dev) for v in vols_h]
+    inst = cc.Instance(local, 7, (n // 2) ** 3, 128, 14)
+    cap = cc.volume_stream_capacity_words(n, n, n)
+    words = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(C)]
+    recon = [torch.empty_like(v) for v in vols]
+    bits = [0] * C
+
+    def step(ev=None):
+        for c in range(C):
+            if ev is not None:
+                ev[c][0].record()
+            _, bits[c] = cc.compress_volume_float(inst, vols[c], L, q0, words[c])
+            if ev is not None:
+                ev[c][1].record()
+            cc.decompress_volume_float(inst, recon[c], L, q0, words[c], bits[c])
+            if ev is not None:
+                ev[c][2].record()
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    # quality (not timed)
+    psnr = [fields.psnr(vols_h[c], recon[c].cpu().numpy()) for c in range(C)]
+    coded_bytes = sum(b // 8 for b in bits)
+    # timed device-resident region
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(C)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = cc.lib().cc_kernel_launches()
+    sampler = ClockSampler(local)
+    start.record()
+    for k in range(args.steps):
+        step(evs[k])
+    end.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = cc.lib().cc_kernel_launches() - launches0
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end) / args.steps
+    enc_ms = sum(evs[k][c][0].elapsed_time(evs[k][c][1]) for k in range(args.steps) for c in range(C)) / args.steps
+    dec_ms = sum(evs[k][c][1].elapsed_time(evs[k][c][2]) for k in range(args.steps) for c in range(C)) / args.steps
+    if dist:
+        t = torch.tensor([ms, enc_ms, dec_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, enc_ms, dec_ms = t.tolist()
+    raw_step = C * n ** 3 * 4
+    value = world * raw_step / (ms / 1e3) / 1e9
+
+    # end to end through the public API with host buffers
+    pinned_in = [torch.from_numpy(v).pin_memory() for v in vols_h]
+    pinned_words = [torch.empty(cap, dtype=torch.int32).pin_memory() for _ in range(C)]
+    pinned_out = [torch.empty(v.shape, dtype=torch.float32).pin_memory() for v in vols_h]
+    dev_in = [torch.empty_like(v) for v in vols]
+    h2d = d2h = 0
+
+    def e2e_step():
+        nonlocal h2d, d2h
+        h2d = d2h = 0
+        for c in range(C):
+            dev_in[c].copy_(pinned_in[c], non_blocking=True)
+            _, b = cc.compress_volume_float(inst, dev_in[c], L, q0, words[c])
+            nw = (b + 31) // 32
+            pinned_words[c][:nw].copy_(words[c][:nw], non_blocking=True)
+            words[c][:nw].copy_(pinned_words[c][:nw], non_blocking=True)
+            cc.decompress_volume_float(inst, recon[c], L, q0, words[c], b)
+            pinned_out[c].copy_(recon[c], non_blocking=True)
+            h2d += n ** 3 * 4 + nw * 4
+            d2h += n ** 3 * 4 + nw * 4
+        torch.cuda.synchronize()
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e2.record()
+    torch.cuda.synchronize()
+    e2e_ms = s2.elapsed_time(e2) / args.steps
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = t.item()
+    e2e_value = world * raw_step / (e2e_ms / 1e3) / 1e9
+
+    # per-kernel sections (one extra step with event timing on)
+    lib = cc.lib()
+    lib.cc_reset_timings(inst.handle)
+    lib.cc_set_timing(inst.handle, 1)
+    step()
+    torch.cuda.synchronize()
+    nsec = lib.cc_timing_count(inst.handle)
+    sections = {}
+    for i in range(nsec):
+        name = ctypes.c_char_p()
+        t_ms = ctypes.c_double()
+        cnt = ctypes.c_uint32()
+        lib.cc_timing_entry(inst.handle, i, ctypes.byref(name), ctypes.byref(t_ms), ctypes.byref(cnt))
+        sections[name.value.decode()] = (t_ms.value, cnt.value)
+    lib.cc_set_timing(inst.handle, 0)
+    peak, peak_kind = load_peak()
+    total_sec = sum(v[0] for v in sections.values()) or 1.0
+    dom = max(sections.items(), key=lambda kv: kv[1][0]) if sections else ("none", (0.0, 0))
+    counts = {"compact": 0}
+    dom_bytes = section_bytes(dom[0], wl, coded_bytes, counts)
+    achieved = (dom_bytes / (dom[1][0] / 1e3) / 1e9) if dom_bytes and dom[1][0] > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(dom[0])
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": traffic, "launches": dom[1][1], "share": dom[1][0] / total_sec,
+                "algorithmic_bytes_per_step": dom_bytes}
+    step_alg = 2 * (raw_step + coded_bytes)
+    pipeline = {"achieved": step_alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": step_alg / (ms / 1e3) / 1e9 / peak,
+                "algorithmic_bytes_per_step": step_alg}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        e, d, kind = cpu_reference_step(vols_h[0], wl, threads)
+        cpu = {"value": n ** 3 * 4 / (e + d) / 1e9, "unit": "GB/s", "cores": threads, "kind": kind,
+               "sample": f"1 of {C} components ({n}^3 f32) encode+decode; DWT/quantize stages are the oracle port"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded k^-5/3 random-phase fields)",
+            "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": f"replicas{world}",
+                       "l2": f"inputs {C * n ** 3 * 4 >> 20} MiB per step > L2 126 MiB"},
+            "encode_gbs": world * raw_step / (enc_ms / 1e3) / 1e9,
+            "decode_gbs": world * raw_step / (dec_ms / 1e3) / 1e9,
+            "compression_ratio": raw_step / max(coded_bytes, 1), "psnr_db": psnr,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": roofline, "pipeline_roofline": pipeline,
+            "sections_ms": {k: round(v[0], 4) for k, v in sorted(sections.items(), key=lambda kv: -kv[1][0])},
+            "clocks": clocks, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    inst.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="vector-field-256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, wl)
+    else:
+        run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

@@ -22,6 +22,7 @@ c_vpp = ctypes.POINTER(ctypes.c_void_p)
 _SIGS = {
     "cc_last_error": (ctypes.c_char_p, []),
     "cc_version": (ctypes.c_char_p, []),
+    "cc_kernel_launches": (c_u64, []),
     "cc_create_instance": (c_int, [ctypes.POINTER(c_vp), c_int, c_u32, c_u32, c_u32, c_u32]),
     "cc_destroy_instance": (None, [c_vp]),
     "cc_get_instance_cuda_device": (c_int, [c_vp]),
@@ -33,6 +34,10 @@ _SIGS = {
     "cc_set_instance_stream": (None, [c_vp, c_vp]),
     "cc_get_instance_stream": (c_vp, [c_vp]),
     "cc_encode_get_required_memory": (ctypes.c_size_t, [c_vp]),
+    "cc_set_timing": (None, [c_vp, c_int]),
+    "cc_timing_count": (c_int, [c_vp]),
+    "cc_timing_entry": (c_int, [c_vp, c_u32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double), c_u32p]),
+    "cc_reset_timings": (None, [c_vp]),
     "cc_encode": (c_int, [c_vp, c_int, c_int, c_vpp, c_u32, c_u32, c_u32p]),
     "cc_encoded_segment": (c_int, [c_vp, c_u32, ctypes.POINTER(c_u32p), c_u32p, c_u32p, c_u32p]),
     "cc_encode_to_buffer": (c_int, [c_vp, c_int, c_int, c_vpp, c_u32, c_u32, c_u32p, c_u32, c_u32p, c_u32p]),

@@ -10,6 +10,9 @@
 
 namespace ccb {
 
+// Counts kernel launches issued by this library (cc_kernel_launches).
+void countLaunch(unsigned n = 1);
+
 void setError(const char* fmt, ...);
 int cudaFail(cudaError_t e, const char* what);
 u32 headerWordsFor(u32 leaves, u32 log2Max);
@@ -39,5 +42,27 @@ int encodeDevice(cc_instance* I, int kind, const EncStream* streams, u32 S, bool
 int ensurePipelineWork(cc_instance* I, size_t bytes);
 int decodeDevice(cc_instance* I, int kind, const u32* const* words, const u32* bitSizes, u32* bitPos, u32 bsCount,
                  const u32* bsIndex, void* const* outs, u32 S, u32 n);
+
+// Records a named, event-timed section on the instance stream when the
+// instance has timing enabled (setTimingDetail / cc_set_timing).
+struct SectionTimer {
+    cc_instance* I;
+    const char* name;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    SectionTimer(cc_instance* inst, const char* n, cudaStream_t s) : I(inst), name(n), st(s) {
+        if (I && I->timing) {
+            a = I->takeEvent();
+            cudaEventRecord(a, st);
+        }
+    }
+    ~SectionTimer() {
+        if (a) {
+            cudaEvent_t b = I->takeEvent();
+            cudaEventRecord(b, st);
+            I->pendingSections.push_back({name, a, b});
+        }
+    }
+};
 
 }  // namespace ccb

@@ -12,6 +12,8 @@
 #pragma once
 
 #include <cstddef>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "cc_common.cuh"
@@ -179,6 +181,15 @@ struct cc_instance {
     ccb::u32* hostWords = nullptr;   // encoded words (host)
     ccb::u64 hostWordsMax = 0;
     std::vector<ccb::SegmentLayout> lastLayout;
+
+    // kernel timing (cudaEvent pairs on the instance stream, resolved lazily)
+    bool timing = false;
+    struct Section { const char* name; cudaEvent_t a, b; };
+    std::vector<Section> pendingSections;
+    std::vector<cudaEvent_t> freeEvents;
+    std::map<std::string, std::pair<double, unsigned>> timings;
+    cudaEvent_t takeEvent();
+    void resolveTimings();
 
     // whole-pipeline workspace (volume / heightfield codecs), grown on demand
     char* pipeWork = nullptr;

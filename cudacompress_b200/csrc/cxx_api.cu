@@ -174,14 +174,28 @@ CC_DEFINE_CODEC(Symbol16)
 CC_DEFINE_CODEC(Symbol32)
 #undef CC_DEFINE_CODEC
 
-// ---- timing (no sections are recorded) ----
-void setTimingDetail(Instance*, ETimingDetail) {}
-void getTimings(Instance*, std::vector<std::string>& names, std::vector<float>& times) {
+// ---- timing: CUDA-event sections per kernel, accumulated by name ----
+void setTimingDetail(Instance* p, ETimingDetail detail) { cc_set_timing(p->h, detail != TIMING_DETAIL_NONE); }
+void getTimings(Instance* p, std::vector<std::string>& names, std::vector<float>& times) {
     names.clear();
     times.clear();
+    const int n = cc_timing_count(p->h);
+    for (int i = 0; i < n; ++i) {
+        const char* name;
+        double ms;
+        uint32_t count;
+        cc_timing_entry(p->h, uint32_t(i), &name, &ms, &count);
+        names.push_back(name);
+        times.push_back(float(ms));
+    }
 }
-void printTimings(Instance*) {}
-void resetTimings(Instance*) {}
+void printTimings(Instance* p) {
+    std::vector<std::string> names;
+    std::vector<float> times;
+    getTimings(p, names, times);
+    for (size_t i = 0; i < names.size(); ++i) std::printf("%-32s %10.3f ms\n", names[i].c_str(), times[i]);
+}
+void resetTimings(Instance* p) { cc_reset_timings(p->h); }
 
 namespace util {
 

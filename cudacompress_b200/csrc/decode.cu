@@ -353,18 +353,18 @@ template <class Sym>
 static int launchDecode(cc_instance* I, const DecParams& p, u32 nMax, u32 mMax) {
     cudaStream_t st = I->stream;
     const u32 T = p.kind == KIND_RLHUFF ? 2 * p.S : p.S;
-    k_decTables<<<T, kDecThreads, 0, st>>>(p);
+    { SectionTimer t(I, "dec.tables", st); k_decTables<<<T, kDecThreads, 0, st>>>(p); countLaunch(); }
     if (p.kind == KIND_HUFF) {
         const u32 blocks = std::max<u32>(1u, u32(ceilDiv(nMax, p.cb)));
         const size_t smem = size_t(32) * (p.cb + 2) * sizeof(Sym);
         CC_TRY_CUDA(cudaFuncSetAttribute(k_decHuff<Sym>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "decHuff smem");
-        k_decHuff<Sym><<<dim3(u32(ceilDiv(blocks, 32)), p.S), 32, smem, st>>>(p);
+        { SectionTimer t(I, "dec.huffman", st); k_decHuff<Sym><<<dim3(u32(ceilDiv(blocks, 32)), p.S), 32, smem, st>>>(p); countLaunch(); }
     } else {
         const u32 blocks = std::max<u32>(1u, u32(ceilDiv(mMax, p.cb)));
         dim3 g(u32(ceilDiv(blocks, 128)), p.S);
-        k_decZc<Sym><<<g, 128, 0, st>>>(p);
-        k_decScan<<<p.S, 1024, 0, st>>>(p);
-        k_decSymScatter<Sym><<<g, 128, 0, st>>>(p);
+        { SectionTimer t(I, "dec.zero_counts", st); k_decZc<Sym><<<g, 128, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.symbols_scatter", st); k_decSymScatter<Sym><<<g, 128, 0, st>>>(p); countLaunch(); }
     }
     CC_TRY_CUDA(cudaGetLastError(), "decode launch");
     return CC_OK;

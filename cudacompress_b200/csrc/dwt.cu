@@ -222,7 +222,7 @@ template <class TIn, class TOut, bool kInverse>
 static void rowPass(TOut* dst, const TIn* src, int nx, int ny, int nz, int srcElem, int srcRow, int srcSlice,
                     int dstElem, int dstRow, int dstSlice, cudaStream_t st) {
     dim3 g(unsigned(ceilDiv(nx, kRowTile)), ny, nz);
-    k_firRows<TIn, TOut, kInverse><<<g, 256, 0, st>>>(dst, src, nx, srcElem, srcRow, srcSlice, dstElem, dstRow, dstSlice);
+    k_firRows<TIn, TOut, kInverse><<<g, 256, 0, st>>>(dst, src, nx, srcElem, srcRow, srcSlice, dstElem, dstRow, dstSlice); countLaunch();
 }
 
 // axis 1 (Y, other = Z) or 2 (Z, other = Y)
@@ -233,7 +233,7 @@ static void colPass(float* dst, Load load, int nx, int ny, int nz, int axis, int
     dim3 g(unsigned(ceilDiv(nx, 32)), unsigned(ceilDiv(na, kColTile)), nc);
     int da = axis == 1 ? dstRow : dstSlice;
     int dc = axis == 1 ? dstSlice : dstRow;
-    k_firCols<Load, kInverse><<<g, dim3(32, 8), 0, st>>>(dst, load, nx, na, 1, da, dc);
+    k_firCols<Load, kInverse><<<g, dim3(32, 8), 0, st>>>(dst, load, nx, na, 1, da, dc); countLaunch();
 }
 
 static PitchLoad pitchLoad(const float* p, int axis, int row, int slice) {
@@ -264,7 +264,7 @@ static void liftPass(i16* dst, const i16* src, int nx, int ny, int nz, int axis,
         dLine = 1; dAxis = dstSlice; dOther = dstRow;
     }
     dim3 g(unsigned(ceilDiv(nLines, 32)), unsigned(ceilDiv(na, kColTile)), nc);
-    k_liftAxis<kInverse><<<g, dim3(32, 8), 0, st>>>(dst, src, nLines, na, sLine, sAxis, sOther, dLine, dAxis, dOther);
+    k_liftAxis<kInverse><<<g, dim3(32, 8), 0, st>>>(dst, src, nLines, na, sLine, sAxis, sOther, dLine, dAxis, dOther); countLaunch();
 }
 
 static bool checkSizes(int sx, int sy, int sz, const char* what) {

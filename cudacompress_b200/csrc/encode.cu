@@ -773,23 +773,23 @@ static int launchEncode(cc_instance* I, const EncParams& p, u32 nMax) {
     CC_TRY_CUDA(cudaMemsetAsync(I->hist, 0, u64(T) * I->bins * sizeof(u32), st), "memset histograms");
     dim3 gTiles(tiles, p.S);
     if (p.kind == KIND_RLHUFF) {
-        k_rleSummary<Sym><<<gTiles, kRleThreads, 0, st>>>(p);
-        k_rleScan<<<p.S, 1024, 0, st>>>(p);
-        k_rleWrite<Sym><<<gTiles, kRleThreads, 0, st>>>(p);
+        { SectionTimer t(I, "enc.rle_summary", st); k_rleSummary<Sym><<<gTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "enc.rle_scan", st); k_rleScan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "enc.rle_write_hist", st); k_rleWrite<Sym><<<gTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
     } else {
-        k_histPlain<Sym><<<gTiles, kRleThreads, 0, st>>>(p);
+        { SectionTimer t(I, "enc.histogram", st); k_histPlain<Sym><<<gTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
     }
     const size_t buildSmem = size_t(p.heapCap) * (sizeof(u64) + sizeof(u32));
     CC_TRY_CUDA(cudaFuncSetAttribute(k_tableBuild, cudaFuncAttributeMaxDynamicSharedMemorySize, int(buildSmem) > 0 ? int(buildSmem) : 1), "tableBuild smem");
-    k_tableBuild<<<T, kBuildThreads, buildSmem, st>>>(p);
+    { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
     const u32 blocks = std::max<u32>(1u, u32(ceilDiv(nMax, p.cb)));
     dim3 gBlocks(u32(ceilDiv(blocks, kPackWarps)), T);
-    k_blockBits<Sym><<<gBlocks, kPackWarps * 32, 0, st>>>(p);
-    k_blockScan<<<T, 1024, 0, st>>>(p);
-    k_layout<<<1, 1024, 0, st>>>(p);
+    { SectionTimer t(I, "enc.block_bits", st); k_blockBits<Sym><<<gBlocks, kPackWarps * 32, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.block_scan", st); k_blockScan<<<T, 1024, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
     const size_t packSmem = size_t(kPackWarps) * (p.cb + 2) * sizeof(u32);
-    k_pack<Sym><<<gBlocks, kPackWarps * 32, packSmem, st>>>(p);
-    k_headers<<<p.S, 128, 0, st>>>(p);
+    { SectionTimer t(I, "enc.pack", st); k_pack<Sym><<<gBlocks, kPackWarps * 32, packSmem, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 128, 0, st>>>(p); countLaunch(); }
     CC_TRY_CUDA(cudaGetLastError(), "encode launch");
     return CC_OK;
 }

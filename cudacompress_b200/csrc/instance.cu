@@ -4,7 +4,9 @@
 // All device memory an instance needs is allocated once at creation, sized
 // from (streamCountMax, elemCountPerStreamMax, codingBlockSize,
 // log2HuffmanDistinctSymbolCountMax); calls never allocate.
+#include <atomic>
 #include <cstring>
+#include <iterator>
 #include <string>
 
 #include "capi_internal.cuh"
@@ -14,6 +16,9 @@ using namespace ccb;
 namespace ccb {
 
 static thread_local std::string g_lastError;
+static std::atomic<unsigned long long> g_launches{0};
+
+void countLaunch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void setError(const char* fmt, ...) {
     char buf[512];
@@ -59,6 +64,31 @@ int ensurePipelineWork(cc_instance* I, size_t bytes) {
 }
 
 }  // namespace ccb
+
+cudaEvent_t cc_instance::takeEvent() {
+    if (!freeEvents.empty()) {
+        cudaEvent_t e = freeEvents.back();
+        freeEvents.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void cc_instance::resolveTimings() {
+    for (const Section& s : pendingSections) {
+        cudaEventSynchronize(s.b);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s.a, s.b);
+        auto& acc = timings[s.name];
+        acc.first += ms;
+        acc.second += 1;
+        freeEvents.push_back(s.a);
+        freeEvents.push_back(s.b);
+    }
+    pendingSections.clear();
+}
 
 char* cc_instance::takeRingSlot() {
     int i = ringNext;
@@ -121,6 +151,7 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
 extern "C" {
 
 const char* cc_last_error(void) { return g_lastError.c_str(); }
+uint64_t cc_kernel_launches(void) { return g_launches.load(); }
 const char* cc_version(void) { return "cudacompress_b200 0.1 (sm_100a)"; }
 
 int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMax, uint32_t elemCountPerStreamMax,
@@ -200,6 +231,8 @@ void cc_destroy_instance(cc_instance* I) {
     }
     if (I->hostDown) cudaFreeHost(I->hostDown);
     if (I->hostWords) cudaFreeHost(I->hostWords);
+    I->resolveTimings();
+    for (cudaEvent_t e : I->freeEvents) cudaEventDestroy(e);
     if (I->arena) cudaFree(I->arena);
     if (I->pipeWork) cudaFree(I->pipeWork);
     if (prev >= 0) cudaSetDevice(prev);
@@ -215,5 +248,31 @@ int cc_get_instance_use_long_symbols(const cc_instance* I) { return I && I->log2
 void cc_set_instance_stream(cc_instance* I, void* s) { if (I) I->stream = static_cast<cudaStream_t>(s); }
 void* cc_get_instance_stream(const cc_instance* I) { return I ? static_cast<void*>(I->stream) : nullptr; }
 size_t cc_encode_get_required_memory(const cc_instance* I) { return I ? I->arenaBytes : 0; }
+
+void cc_set_timing(cc_instance* I, int enable) {
+    if (I) I->timing = enable != 0;
+}
+
+int cc_timing_count(cc_instance* I) {
+    if (!I) return 0;
+    I->resolveTimings();
+    return int(I->timings.size());
+}
+
+int cc_timing_entry(cc_instance* I, uint32_t i, const char** name, double* ms, uint32_t* count) {
+    if (!I || i >= I->timings.size()) { setError("cc_timing_entry: index out of range"); return CC_ERR_INVALID_ARGUMENT; }
+    auto it = I->timings.begin();
+    std::advance(it, i);
+    if (name) *name = it->first.c_str();
+    if (ms) *ms = it->second.first;
+    if (count) *count = it->second.second;
+    return CC_OK;
+}
+
+void cc_reset_timings(cc_instance* I) {
+    if (!I) return;
+    I->resolveTimings();
+    I->timings.clear();
+}
 
 }  // extern "C"

@@ -81,7 +81,7 @@ int cc_compress_volume_float(cc_instance* I, const float* vol, uint32_t nx, uint
         const float* src = l == 0 ? vol : coef[l - 1];
         const int sr = l == 0 ? 0 : int(nx >> (l - 1));
         const int ss = l == 0 ? 0 : int((nx >> (l - 1)) * (ny >> (l - 1)));
-        rc = cc_dwt_float_forward(coef[l], t2, t1, src, sx, sy, sz, 1, 0, 0, sr, ss, st);
+        { SectionTimer t(I, "pipe.dwt_forward", st); rc = cc_dwt_float_forward(coef[l], t2, t1, src, sx, sy, sz, 1, 0, 0, sr, ss, st); }
         if (rc) return rc;
     }
     // quantize: LP then levels coarse -> fine, bands 1..7
@@ -100,7 +100,7 @@ int cc_compress_volume_float(cc_instance* I, const float* vol, uint32_t nx, uint
         for (u32 bi = 1; bi < 8; ++bi) {
             const u32 x = bi % 2, y = (bi / 2) % 2, z = bi / 4;
             const float* src = coef[l] + u64(z) * hz * sx * sy + u64(y) * hy * sx + u64(x) * hx;
-            rc = cc_quantize_to_symbols(next, 2, src, hx, hy, hz, step, sx, sx * sy, 0, st);
+            { SectionTimer t(I, "pipe.quantize", st); rc = cc_quantize_to_symbols(next, 2, src, hx, hy, hz, step, sx, sx * sy, 0, st); }
             if (rc) return rc;
             bands[l][bi - 1] = next;
             next += cube(hx, hy, hz);
@@ -186,6 +186,7 @@ int cc_decompress_volume_float(cc_instance* I, float* out, uint32_t nx, uint32_t
     // back over `cur` (the first pass has consumed it by then) or into `out`
     for (int l = int(L) - 1; l >= 0; --l) {
         const int sx = int(nx >> l), sy = int(ny >> l), sz = int(nz >> l);
+        SectionTimer tInv(I, "pipe.dwt_inverse", st);
         rc = cc_dwt_float_inverse_from_symbols(l == 0 ? out : cur, t2, t1, cur, dPtrs + l * 8, 2, q0 / float(1u << l),
                                                sx, sy, sz, 1, 0, 0, sx / 2, (sx / 2) * (sy / 2), st);
         if (rc) return rc;

@@ -127,6 +127,7 @@ int cc_quantize_to_symbols(void* out, int symBytes, const float* in, uint32_t nx
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (symBytes == 2) k_quantize<u16><<<gridFor(b), 256, 0, st>>>(static_cast<u16*>(out), in, b, inv, type);
     else k_quantize<u32><<<gridFor(b), 256, 0, st>>>(static_cast<u32*>(out), in, b, inv, type);
+    countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "quantizeToSymbols");
     return CC_OK;
 }
@@ -140,6 +141,7 @@ int cc_quantize_to_symbols_roundtrip(void* out, int symBytes, float* data, uint3
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (symBytes == 2) k_quantizeRoundtrip<u16><<<gridFor(b), 256, 0, st>>>(static_cast<u16*>(out), data, b, step, inv, type);
     else k_quantizeRoundtrip<u32><<<gridFor(b), 256, 0, st>>>(static_cast<u32*>(out), data, b, step, inv, type);
+    countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "quantizeToSymbolsRoundtrip");
     return CC_OK;
 }
@@ -152,6 +154,7 @@ int cc_unquantize_from_symbols(float* data, const void* in, int symBytes, uint32
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (symBytes == 2) k_unquantize<u16><<<gridFor(b), 256, 0, st>>>(data, static_cast<const u16*>(in), b, step, type);
     else k_unquantize<u32><<<gridFor(b), 256, 0, st>>>(data, static_cast<const u32*>(in), b, step, type);
+    countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "unquantizeFromSymbols");
     return CC_OK;
 }
@@ -160,7 +163,7 @@ int cc_symbolize(uint16_t* out, const int16_t* in, uint32_t nx, uint32_t ny, uin
                  void* stream) {
     Box b = makeBox(nx, ny, nz, row, slice);
     if (!u64(nx) * ny * nz) return CC_OK;
-    k_symbolize<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b);
+    k_symbolize<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b); countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "symbolize");
     return CC_OK;
 }
@@ -169,7 +172,7 @@ int cc_unsymbolize(int16_t* out, const uint16_t* in, uint32_t nx, uint32_t ny, u
                    uint32_t slice, void* stream) {
     Box b = makeBox(nx, ny, nz, row, slice);
     if (!u64(nx) * ny * nz) return CC_OK;
-    k_unsymbolize<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b);
+    k_unsymbolize<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b); countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "unsymbolize");
     return CC_OK;
 }
@@ -178,7 +181,7 @@ int cc_quantize_to_short(int16_t* out, const float* in, uint32_t nx, uint32_t ny
                          uint32_t row, uint32_t slice, int type, void* stream) {
     Box b = makeBox(nx, ny, nz, row, slice);
     if (!u64(nx) * ny * nz) return CC_OK;
-    k_quantizeShort<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b, 1.0f / step, type);
+    k_quantizeShort<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b, 1.0f / step, type); countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "quantizeToShort");
     return CC_OK;
 }
@@ -187,7 +190,7 @@ int cc_unquantize_from_short(float* out, const int16_t* in, uint32_t nx, uint32_
                              uint32_t row, uint32_t slice, int type, void* stream) {
     Box b = makeBox(nx, ny, nz, row, slice);
     if (!u64(nx) * ny * nz) return CC_OK;
-    k_unquantizeShort<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b, step, type);
+    k_unquantizeShort<<<gridFor(b), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, in, b, step, type); countLaunch();
     CC_TRY_CUDA(cudaGetLastError(), "unquantizeFromShort");
     return CC_OK;
 }
@@ -196,7 +199,10 @@ int cc_get_max_abs(cc_instance* I, const float* in, uint32_t n, float* dMax) {
     if (!I) { setError("getMaxAbs: null instance"); return CC_ERR_INVALID_ARGUMENT; }
     cudaStream_t st = I->stream;
     CC_TRY_CUDA(cudaMemsetAsync(dMax, 0, sizeof(float), st), "getMaxAbs");
-    if (n) k_maxAbs<<<std::min<u32>(1184u, u32(ceilDiv(n, 256))), 256, 0, st>>>(in, n, dMax);
+    if (n) {
+        k_maxAbs<<<std::min<u32>(1184u, u32(ceilDiv(n, 256))), 256, 0, st>>>(in, n, dMax);
+        countLaunch();
+    }
     CC_TRY_CUDA(cudaGetLastError(), "getMaxAbs");
     return CC_OK;
 }

@@ -38,6 +38,8 @@ typedef struct cc_instance cc_instance;
 
 /* Last error message of the calling thread ("" if none). */
 const char* cc_last_error(void);
+/* Kernel launches issued by the library in this process so far. */
+uint64_t cc_kernel_launches(void);
 /* Library version string. */
 const char* cc_version(void);
 
@@ -64,6 +66,16 @@ void cc_set_instance_stream(cc_instance* inst, void* cuda_stream);
 void* cc_get_instance_stream(const cc_instance* inst);
 /* encodeGetRequiredMemory, Encode.h:17: device bytes the instance holds. */
 size_t cc_encode_get_required_memory(const cc_instance* inst);
+
+/* Kernel timing (Timing.h:15-27 / util::CudaTimer): when enabled, named
+ * sections are timed with CUDA events on the instance stream and accumulated
+ * per name.  cc_timing_count resolves pending sections (synchronizing) and
+ * returns the number of names; cc_timing_entry reads one (name, total
+ * milliseconds, section count). */
+void cc_set_timing(cc_instance* inst, int enable);
+int cc_timing_count(cc_instance* inst);
+int cc_timing_entry(cc_instance* inst, uint32_t i, const char** name, double* ms, uint32_t* count);
+void cc_reset_timings(cc_instance* inst);
 
 /* ---- Entropy coding (include/cudaCompress/Encode.h:28-52, src/cudaCompress/Encode.cpp:207-1042) ----
  *

@@ -549,8 +549,11 @@ static void firAxis(const T* src, T* dst, long nx, long ny, long nz, int axis, b
     long n = axis == 0 ? nx : axis == 1 ? ny : nz;
     long stride = axis == 0 ? 1 : axis == 1 ? nx : nx * ny;
     long h = n / 2;
-    std::vector<T> line(n), outl(n);
     long lines = nx * ny * nz / n;
+#pragma omp parallel
+    {
+    std::vector<T> line(n), outl(n);
+#pragma omp for schedule(static)
     for (long li = 0; li < lines; ++li) {
         long base;
         if (axis == 0) base = li * nx;
@@ -575,6 +578,7 @@ static void firAxis(const T* src, T* dst, long nx, long ny, long nz, int axis, b
             long o = inverse ? x : ((x & 1) ? (h + x / 2) : (x / 2));
             dst[base + o * stride] = outl[x];
         }
+    }
     }
 }
 
@@ -605,7 +609,10 @@ static void liftAxis(const i16* src, i16* dst, long nx, long ny, long nz, int ax
     long stride = axis == 0 ? 1 : axis == 1 ? nx : nx * ny;
     long h = n / 2;
     long lines = nx * ny * nz / n;
+#pragma omp parallel
+    {
     std::vector<i16> s(n + 2);
+#pragma omp for schedule(static)
     for (long li = 0; li < lines; ++li) {
         long base;
         if (axis == 0) base = li * nx;
@@ -634,6 +641,7 @@ static void liftAxis(const i16* src, i16* dst, long nx, long ny, long nz, int ax
             }
             for (long k = 0; k < n; ++k) dst[base + k * stride] = s[k];
         }
+    }
     }
 }
 
@@ -705,6 +713,7 @@ void orc_dwt_int_inv(const i16* src, i16* dst, long nx, long ny, long nz) { dwtI
 // Quantize.cu:78-100 on a dense (nx,ny,nz) block with the reference's pitches.
 void orc_quantize_to_symbols16(u16* out, const float* src, long nx, long ny, long nz, float step, long rowPitch, long slicePitch) {
     float inv = 1.0f / step;
+#pragma omp parallel for schedule(static)
     for (long z = 0; z < nz; ++z)
         for (long y = 0; y < ny; ++y)
             for (long x = 0; x < nx; ++x)
@@ -894,6 +903,31 @@ void orc_volume_symbols(const float* vol, long nx, long ny, long nz, int levels,
             out += bandN;
         }
     }
+}
+
+// Inverse of orc_volume_symbols: dequantize LP + bands, inverse DWT per level.
+void orc_volume_from_symbols(const u16* syms, float* out, long nx, long ny, long nz, int levels, float q0) {
+    long sx = nx >> levels, sy = ny >> levels, sz = nz >> levels;
+    std::vector<float> cur(sx * sy * sz);
+    orc_unquantize_from_symbols16(cur.data(), syms, sx, sy, sz, q0 / float(1 << (levels - 1)), sx, sx * sy);
+    syms += sx * sy * sz;
+    for (int l = levels - 1; l >= 0; --l) {
+        long n0 = nx >> l, n1 = ny >> l, n2 = nz >> l;
+        long bandN = (n0 / 2) * (n1 / 2) * (n2 / 2);
+        float step = q0 / float(1 << l);
+        std::vector<float> coef(n0 * n1 * n2);
+        for (long z = 0; z < n2 / 2; ++z)
+            for (long y = 0; y < n1 / 2; ++y)
+                for (long x = 0; x < n0 / 2; ++x)
+                    coef[(z * n1 + y) * n0 + x] = cur[(z * (n1 / 2) + y) * (n0 / 2) + x];
+        for (int b = 1; b < 8; ++b) {
+            unquantizeBand(coef.data(), n0, n1, n2, b % 2, (b / 2) % 2, b / 4, step, syms);
+            syms += bandN;
+        }
+        cur.resize(coef.size());
+        dwtFloat(coef.data(), cur.data(), n0, n1, n2, true);
+    }
+    std::copy(cur.begin(), cur.end(), out);
 }
 
 // ---------------------------------------------------------------------------

@@ -116,6 +116,7 @@ class Oracle:
         L.orc_decompress_volume_float.argtypes = [U32P, c.c_uint32, F32P, c.c_long, c.c_long, c.c_long, c.c_int,
                                                   c.c_float, c.c_uint32, c.c_uint32]
         L.orc_volume_symbols.argtypes = [F32P, c.c_long, c.c_long, c.c_long, c.c_int, c.c_float, U16P]
+        L.orc_volume_from_symbols.argtypes = [U16P, F32P, c.c_long, c.c_long, c.c_long, c.c_int, c.c_float]
         L.orc_compress_heightfield.argtypes = [I16P, c.c_long, c.c_long, c.c_int, c.c_uint32, c.c_uint32, U32P,
                                                c.c_uint32, c.POINTER(c.c_uint32)]
         L.orc_decompress_heightfield.argtypes = [U32P, c.c_uint32, I16P, c.c_long, c.c_long, c.c_int, c.c_uint32,
