@@ -15,8 +15,6 @@ void countLaunch(unsigned n = 1);
 
 void setError(const char* fmt, ...);
 int cudaFail(cudaError_t e, const char* what);
-u32 headerWordsFor(u32 leaves, u32 log2Max);
-u64 segmentWordsMax(u32 n, u32 cb, u32 log2Max, u32 hdrWords);
 
 // Maps the device error flags of a call to a status (and message).
 inline int deviceErrorStatus(u32 flags, const char* what) {
@@ -24,7 +22,8 @@ inline int deviceErrorStatus(u32 flags, const char* what) {
     if (flags & DEV_ERR_SYMBOL_RANGE) { setError("%s: symbol out of range for log2HuffmanDistinctSymbolCountMax", what); return CC_ERR_SYMBOL_RANGE; }
     if (flags & DEV_ERR_CODEWORD_TOO_LONG) { setError("%s: Huffman codeword longer than 31 bits", what); return CC_ERR_CODEWORD_TOO_LONG; }
     if (flags & DEV_ERR_TIMEOUT) { setError("%s: device wait timed out", what); return CC_ERR_DEVICE_TIMEOUT; }
-    if (flags & DEV_ERR_TABLE_CAPACITY) { setError("%s: table exceeds instance capacity", what); return CC_ERR_CAPACITY; }
+    if (flags & DEV_ERR_TABLE_CAPACITY) { setError("%s: tables exceed the instance capacity", what); return CC_ERR_CAPACITY; }
+    if (flags & DEV_ERR_OUTPUT_CAPACITY) { setError("%s: output buffer too small", what); return CC_ERR_CAPACITY; }
     setError("%s: corrupt or truncated bit stream", what);
     return CC_ERR_CORRUPT_STREAM;
 }
@@ -36,8 +35,16 @@ inline int deviceErrorStatus(u32 flags, const char* what) {
     } while (0)
 
 // Encode / decode entry points used by the C ABI and the fused pipelines.
-// `streams` are host descriptors; results land in the instance buffers.
-int encodeDevice(cc_instance* I, int kind, const EncStream* streams, u32 S, bool download, u64* totalWords = nullptr);
+// `streams` are host descriptors of any sizes and kinds; the segments are
+// written back to back (each word aligned) into `out.words` (device, at most
+// `out.capacity` words) or, when that is null, the instance output buffer.
+// The call waits for the device; the layout is kept in I->lastLayout.
+struct EncOutput {
+    u32* words = nullptr;
+    u64 capacity = 0;
+};
+int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutput& out, bool download,
+                 u64* totalWords = nullptr);
 // Grows the instance's pipeline workspace to at least `bytes` (allocates only when it must grow).
 int ensurePipelineWork(cc_instance* I, size_t bytes);
 int decodeDevice(cc_instance* I, int kind, const u32* const* words, const u32* bitSizes, u32* bitPos, u32 bsCount,

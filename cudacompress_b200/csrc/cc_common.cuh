@@ -26,6 +26,7 @@ enum DeviceError : u32 {
     DEV_ERR_CORRUPT = 4u,
     DEV_ERR_TIMEOUT = 8u,
     DEV_ERR_TABLE_CAPACITY = 16u,
+    DEV_ERR_OUTPUT_CAPACITY = 32u,
 };
 
 constexpr u32 kMaxCodewordBits = 32;      // EncodeCommon.h:24-25

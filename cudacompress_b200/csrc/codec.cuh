@@ -27,13 +27,45 @@ constexpr u32 kRleThreads = 256;
 constexpr u32 kRlePerThread = 8;
 constexpr u32 kRleTile = kRleThreads * kRlePerThread;
 
-// Per-stream input of one encode call.
+// Leaves of a table whose Huffman build runs in shared memory (20 bytes per
+// leaf: heap key, sort key, two parent links); larger tables use global memory.
+constexpr u32 kBuildSmemLeaves = 8192;
+
+// Words of a serialized table with `leaves` symbols (HuffmanTable.cu:470-485
+// field sizes at their maxima: 31 codeword lengths, 24-bit symbols) plus two
+// words of slack.
+CC_HD u32 headerWordsFor(u32 leaves, u32 log2Max) {
+    const u64 symBits = log2Max > 16 ? 24 : 16;
+    const u64 bits = 5 + 31ull * log2Max + log2Max + 5 + u64(leaves) * symBits;
+    return u32(ceilDiv(bits, 32) + 2);
+}
+
+// Per-stream input of one encode call (host side).
 struct EncStream {
     const void* in;      // device symbols (u16 or u32)
     u32 n;               // symbol count
     u32 startBit;        // bit offset (0..31) of the segment start in its first word
     u32 groupFirst;      // first stream of the reference call this stream belongs to
     u32 groupSize;       // streams in that call
+    u32 kind;            // KIND_RLHUFF or KIND_HUFF
+};
+
+// Device copy of a stream with its offsets into the call's work arrays.
+struct EncStreamDev {
+    const void* in;
+    u32 n, kind, startBit, groupFirst, groupSize;
+    u32 tileOff;         // first run-length tile of the stream
+    u32 tableFirst;      // first Huffman table of the stream
+    u32 pad;
+    u64 compactOff;      // element offset of its compact symbols / zero counts
+};
+
+// One Huffman table of a call: the symbols of a Huff stream, or the compact
+// symbols (which 0) / zero counts (which 1) of an RLHuff stream.
+struct EncTableDev {
+    u32 stream, which;
+    u32 blockOff;        // first coding block in the call's block arrays
+    u32 blocksMax;       // coding blocks if every symbol is coded (ceil(n / cb))
 };
 
 // Summary of a run of symbols for the zero-run RLE scan.  Positions are
@@ -63,7 +95,7 @@ struct TileStart {
     u32 prevP1;
 };
 
-// One Huffman table of an encode call (a stream's symbols or zero counts).
+// Per-table results of an encode call (device).
 struct TableMeta {
     u32 count;        // symbols coded with this table
     u32 symbolMax;    // largest symbol (0 for an empty stream)
@@ -72,7 +104,10 @@ struct TableMeta {
     u32 headerBits;   // serialized table size
     u32 codeBits;     // total codeword bits
     u32 blocks;       // coding blocks
-    u32 pad;
+    u32 histSize;     // histogram bins of this table
+    u64 histOff;      // offset of its histogram and code table
+    u64 leafOff;      // offset of its table-builder arrays (by leaf)
+    u64 hdrOff;       // offset of its serialized header (words)
 };
 
 // Where the pieces of one stream's segment go in the device output buffer.
@@ -137,29 +172,40 @@ struct cc_instance {
     ccb::u32 leavesMax = 0;     // distinct symbols per table
     ccb::u64 outWordsMax = 0;   // device output words
 
+    // capacities of one encode call (totals over its streams / tables)
+    ccb::u32 capStreams = 0;    // streams (>= streamCountMax; batched pipelines use more)
+    ccb::u64 capCompact = 0;    // run-length output symbols
+    ccb::u32 capTiles = 0;      // run-length tiles
+    ccb::u32 capTables = 0;     // Huffman tables
+    ccb::u32 capBlocks = 0;     // coding blocks
+    ccb::u64 capHist = 0;       // histogram bins
+    ccb::u64 capLeaves = 0;     // table-builder leaves
+    ccb::u64 capHdr = 0;        // serialized header words
+
     // device memory (one allocation)
     char* arena = nullptr;
     size_t arenaBytes = 0;
-    void* compact = nullptr;    // [S][n] symbols (encode: compact symbols; decode: decoded zero counts)
-    void* zc = nullptr;         // [S][n] zero counts
+    void* compact = nullptr;    // encode: compact symbols; decode: staging of decoded zero counts
+    void* zc = nullptr;         // zero counts
     ccb::RunSum* tiles = nullptr;
     ccb::TileStart* tileStart = nullptr;
-    ccb::u32* hist = nullptr;          // [2S][bins]
-    uint2* enc = nullptr;              // [2S][bins] (code, len)
-    ccb::TableMeta* meta = nullptr;    // [2S]
-    ccb::u32* headers = nullptr;       // [2S][hdrWordsMax]
-    ccb::u32* blockBits = nullptr;     // [2S][blocksMax]
-    ccb::u32* blockOff = nullptr;      // [2S][blocksMax]
-    ccb::SegmentLayout* layout = nullptr;  // [S]
+    ccb::u32* streamMax = nullptr;     // [capStreams] largest symbol
+    ccb::u32* hist = nullptr;          // [capHist]
+    uint2* enc = nullptr;              // [capHist] (code, len) by symbol
+    ccb::TableMeta* meta = nullptr;    // [capTables]
+    ccb::u32* headers = nullptr;       // [capHdr]
+    ccb::u32* blockBits = nullptr;     // [capBlocks]
+    ccb::u32* blockOff = nullptr;      // [capBlocks]
+    ccb::SegmentLayout* layout = nullptr;  // [capStreams]
     ccb::u32* out = nullptr;           // [outWordsMax]
-    ccb::u32* counts = nullptr;        // [S]
-    ccb::u32* errors = nullptr;        // [4]
-    ccb::u64* totals = nullptr;        // [4]
-    ccb::EncStream* dStreams = nullptr;
-    ccb::u64* leafWork = nullptr;      // [2S][leavesMax] heap keys
-    ccb::u32* parentWork = nullptr;    // [2S][2*leavesMax]
-    ccb::u32* orderWork = nullptr;     // [2S][leavesMax]
-    ccb::u32* leafSymWork = nullptr;   // [2S][leavesMax]
+    ccb::u32* counts = nullptr;        // [capStreams]
+    ccb::u32* errors = nullptr;        // [8]
+    ccb::u64* totals = nullptr;        // [8]
+    void* dPlan = nullptr;             // stream + table descriptors of the current call
+    ccb::u64* leafWork = nullptr;      // [capLeaves] heap keys (tables too large for shared memory)
+    ccb::u32* parentWork = nullptr;    // [2 capLeaves]
+    ccb::u32* orderWork = nullptr;     // [capLeaves]
+    ccb::u32* leafSymWork = nullptr;   // [capLeaves]
     // decode
     ccb::DecTableDesc* dDecTables = nullptr;  // [2S]
     ccb::DecStreamDesc* dDecStreams = nullptr; // [S]

@@ -4,10 +4,15 @@
 // Tier-0 pieces they call (RunLength.cu:82-188, Histogram.cu:109-289,
 // HuffmanTable.cu:385-596, Huffman.cu:73-187, PackInc.cu:210-219).
 //
-// Launch sequence of one call (no host round trip until the result is read):
-//   RLHuff: rleSummary -> rleScan -> rleWrite(+histograms) ->
-//   Huff:   histPlain ->
-//   both:   tableBuild -> blockBits -> blockScan -> layout -> pack -> headers
+// One call codes a batch of streams of any sizes and of both kinds (a whole
+// volume: the lowpass band with encodeHuff and every level's bands with
+// encodeRLHuff, or many bricks).  Work is flattened: run-length tiles and
+// coding blocks are numbered across all streams and found back by binary
+// search over the per-stream / per-table offsets, so one launch of each
+// kernel covers the batch and all Huffman tables are built concurrently.
+// Launch sequence (no host round trip until the result is read):
+//   summary -> scan -> histPlan -> zeroHist -> write(+histograms)
+//   -> tableBuild -> blockBits -> blockScan -> layout -> pack -> headers
 #include <cstring>
 
 #include "capi_internal.cuh"
@@ -16,54 +21,79 @@
 namespace ccb {
 
 struct EncParams {
-    int kind;
-    u32 S;
-    u32 cb;
-    u32 log2Max;
-    u32 bins;
-    u32 symBytes;
-    const EncStream* streams;
+    u32 S, T;
+    u32 totalTiles, totalBlocks;
+    u32 cb, log2Max, bins, symBytes;
+    const EncStreamDev* streams;
+    const EncTableDev* tables;
     char* compact;
     char* zc;
-    u64 nStride;
     RunSum* tiles;
     TileStart* tileStart;
-    u32 tilesMax;
+    u32* streamMax;
+    u32* counts;
     u32* hist;
     uint2* enc;
     TableMeta* meta;
     u32* headers;
-    u32 hdrWordsMax;
     u32* blockBits;
     u32* blockOff;
-    u32 blocksMax;
     SegmentLayout* layout;
     u32* out;
     u64 outWordsMax;
-    u32* counts;
+    u64 capHist, capLeaves, capHdr;
     u32* errors;
     u64* totals;
     u64* leafWork;
     u32* parentWork;
     u32* orderWork;
     u32* leafSymWork;
-    u32 leavesMax;
-    u32 heapCap;      // leaves that fit the shared-memory heap of tableBuild
+    u32 heapCap;      // leaves that fit the shared-memory builder of tableBuild
 };
 
 constexpr u32 kSmemSymBins = 4096;
 
-__device__ __forceinline__ u32 numTables(const EncParams& p) { return p.kind == KIND_RLHUFF ? 2 * p.S : p.S; }
+// Error flag of the call, read once per block and shared so that every
+// thread of the block takes the same branch.
+__device__ __forceinline__ bool blockFailed(const EncParams& p) {
+    __shared__ u32 sFailed;
+    if (threadIdx.x == 0) sFailed = *reinterpret_cast<volatile const u32*>(p.errors);
+    __syncthreads();
+    return sFailed != 0;
+}
+__device__ __forceinline__ bool warpFailed(const EncParams& p) {
+    return __any_sync(0xffffffffu, *reinterpret_cast<volatile const u32*>(p.errors) != 0);
+}
 
-template <class Sym>
-__device__ __forceinline__ const Sym* tableInput(const EncParams& p, u32 t, u32& count) {
-    if (p.kind == KIND_RLHUFF) {
-        u32 s = t < p.S ? t : t - p.S;
-        count = p.counts[s];
-        return reinterpret_cast<const Sym*>(t < p.S ? p.compact : p.zc) + u64(s) * p.nStride;
+// Stream owning flattened tile `tile` (largest s with tileOff <= tile).
+__device__ __forceinline__ u32 streamOfTile(const EncParams& p, u32 tile) {
+    u32 lo = 0, hi = p.S;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (p.streams[mid].tileOff <= tile) lo = mid; else hi = mid;
     }
-    count = p.streams[t].n;
-    return reinterpret_cast<const Sym*>(p.streams[t].in);
+    return lo;
+}
+// Table owning flattened coding block `gb`.
+__device__ __forceinline__ u32 tableOfBlock(const EncParams& p, u32 gb) {
+    u32 lo = 0, hi = p.T;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (p.tables[mid].blockOff <= gb) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Input symbols of table t and their count.
+template <class Sym>
+__device__ __forceinline__ const Sym* tableInput(const EncParams& p, const EncTableDev& td, u32& count) {
+    const EncStreamDev& sd = p.streams[td.stream];
+    if (sd.kind == KIND_RLHUFF) {
+        count = p.counts[td.stream];
+        return reinterpret_cast<const Sym*>(td.which ? p.zc : p.compact) + sd.compactOff;
+    }
+    count = sd.n;
+    return reinterpret_cast<const Sym*>(sd.in);
 }
 
 // Loads kRlePerThread symbols starting at `base` (zero beyond n).
@@ -87,32 +117,30 @@ __device__ __forceinline__ void loadSyms(const Sym* in, u32 base, u32 n, u32 (&v
     }
 }
 
-__device__ __forceinline__ RunSum shflRun(RunSum r, int delta, bool up) {
+__device__ __forceinline__ RunSum shflUpRun(RunSum r, int delta) {
     RunSum t;
-    if (up) {
-        t.cnt = __shfl_up_sync(0xffffffffu, r.cnt, delta);
-        t.ext = __shfl_up_sync(0xffffffffu, r.ext, delta);
-        t.firstP1 = __shfl_up_sync(0xffffffffu, r.firstP1, delta);
-        t.lastP1 = __shfl_up_sync(0xffffffffu, r.lastP1, delta);
-    } else {
-        t.cnt = __shfl_down_sync(0xffffffffu, r.cnt, delta);
-        t.ext = __shfl_down_sync(0xffffffffu, r.ext, delta);
-        t.firstP1 = __shfl_down_sync(0xffffffffu, r.firstP1, delta);
-        t.lastP1 = __shfl_down_sync(0xffffffffu, r.lastP1, delta);
-    }
+    t.cnt = __shfl_up_sync(0xffffffffu, r.cnt, delta);
+    t.ext = __shfl_up_sync(0xffffffffu, r.ext, delta);
+    t.firstP1 = __shfl_up_sync(0xffffffffu, r.firstP1, delta);
+    t.lastP1 = __shfl_up_sync(0xffffffffu, r.lastP1, delta);
     return t;
 }
 
-// Order-preserving block scan of RunSum (256 threads); returns the exclusive
+__device__ __forceinline__ RunSum warpInclusiveRun(RunSum r) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        RunSum t = shflUpRun(r, o);
+        if (lane >= o) r = runCombine(t, r);
+    }
+    return r;
+}
+
+// Order-preserving block scan of RunSum (kRleThreads threads): exclusive
 // prefix of the calling thread; *total receives the block aggregate.
 __device__ RunSum blockScanRun(RunSum r, RunSum* smem /*[9]*/, RunSum* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    RunSum inc = r;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        RunSum t = shflRun(inc, o, true);
-        if (lane >= o) inc = runCombine(t, inc);
-    }
+    RunSum inc = warpInclusiveRun(r);
     if (lane == 31) smem[warp] = inc;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -125,7 +153,7 @@ __device__ RunSum blockScanRun(RunSum r, RunSum* smem /*[9]*/, RunSum* total) {
         smem[8] = acc;
     }
     __syncthreads();
-    RunSum exclLane = shflRun(inc, 1, true);
+    RunSum exclLane = shflUpRun(inc, 1);
     if (lane == 0) exclLane = RunSum{0, 0, 0, 0};
     RunSum res = runCombine(smem[warp], exclLane);
     if (total) *total = smem[8];
@@ -152,42 +180,56 @@ __device__ __forceinline__ RunSum threadRun(const u32 (&v)[kRlePerThread], u32 b
 // Run-length encode (RunLength.cu:82-188 semantics: each nonzero symbol with
 // the count of zeros before it; runs of 256+ zeros emit (0, 255) entries;
 // trailing zeros dropped).
+// Pass 1: per tile, the run summary (RLHuff) and the largest symbol.
 // ---------------------------------------------------------------------------
 template <class Sym>
-__global__ void __launch_bounds__(kRleThreads) k_rleSummary(EncParams p) {
+__global__ void __launch_bounds__(kRleThreads) k_summary(EncParams p) {
     __shared__ RunSum smem[9];
-    const u32 s = blockIdx.y, tile = blockIdx.x;
-    const u32 n = p.streams[s].n;
-    if (tile * kRleTile >= n) return;
-    const Sym* in = reinterpret_cast<const Sym*>(p.streams[s].in);
-    const u32 base = tile * kRleTile + threadIdx.x * kRlePerThread;
+    __shared__ u32 sStream, sMaxSym;
+    const u32 tile = blockIdx.x;
+    if (threadIdx.x == 0) { sStream = streamOfTile(p, tile); sMaxSym = 0; }
+    __syncthreads();
+    const u32 s = sStream;
+    const EncStreamDev sd = p.streams[s];
+    const u32 n = sd.n;
+    const Sym* in = reinterpret_cast<const Sym*>(sd.in);
+    const u32 base = (tile - sd.tileOff) * kRleTile + threadIdx.x * kRlePerThread;
     u32 v[kRlePerThread];
     loadSyms(in, base, n, v);
-    RunSum r = threadRun(v, base, n), total;
-    blockScanRun(r, smem, &total);
-    if (threadIdx.x == 0) p.tiles[u64(s) * p.tilesMax + tile] = total;
+    u32 m = 0;
+#pragma unroll
+    for (u32 i = 0; i < kRlePerThread; ++i) m = max(m, v[i]);
+    m = warpMax(m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(&sMaxSym, m);
+    if (sd.kind == KIND_RLHUFF) {
+        RunSum total;
+        blockScanRun(threadRun(v, base, n), smem, &total);   // synchronizes the block
+        if (threadIdx.x == 0) p.tiles[tile] = total;
+    } else {
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && sMaxSym) atomicMax(p.streamMax + s, sMaxSym);
 }
 
-// One block per stream: scans the tile summaries.
-__global__ void __launch_bounds__(1024) k_rleScan(EncParams p) {
+// Pass 2: one block per stream scans its tile summaries.
+__global__ void __launch_bounds__(1024) k_scan(EncParams p) {
     __shared__ RunSum warpTot[32];
     __shared__ RunSum carry;
     const u32 s = blockIdx.x;
-    const u32 n = p.streams[s].n;
-    const u32 tiles = u32(ceilDiv(n, kRleTile));
-    RunSum* T = p.tiles + u64(s) * p.tilesMax;
-    TileStart* TS = p.tileStart + u64(s) * p.tilesMax;
+    const EncStreamDev sd = p.streams[s];
+    if (sd.kind != KIND_RLHUFF) {
+        if (threadIdx.x == 0) p.counts[s] = sd.n;
+        return;
+    }
+    const u32 tiles = u32(ceilDiv(sd.n, kRleTile));
+    const RunSum* T = p.tiles + sd.tileOff;
+    TileStart* TS = p.tileStart + sd.tileOff;
     if (threadIdx.x == 0) carry = RunSum{0, 0, 0, 0};
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (u32 base = 0; base < tiles; base += 1024) {
-        u32 i = base + threadIdx.x;
-        RunSum r = i < tiles ? T[i] : RunSum{0, 0, 0, 0};
-        RunSum inc = r;
-        for (int o = 1; o < 32; o <<= 1) {
-            RunSum t = shflRun(inc, o, true);
-            if (lane >= o) inc = runCombine(t, inc);
-        }
+        const u32 i = base + threadIdx.x;
+        RunSum inc = warpInclusiveRun(i < tiles ? T[i] : RunSum{0, 0, 0, 0});
         if (lane == 31) warpTot[warp] = inc;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -200,7 +242,7 @@ __global__ void __launch_bounds__(1024) k_rleScan(EncParams p) {
             carry = acc;
         }
         __syncthreads();
-        RunSum ex = shflRun(inc, 1, true);
+        RunSum ex = shflUpRun(inc, 1);
         if (lane == 0) ex = RunSum{0, 0, 0, 0};
         RunSum E = runCombine(warpTot[warp], ex);
         if (i < tiles) {
@@ -212,38 +254,108 @@ __global__ void __launch_bounds__(1024) k_rleScan(EncParams p) {
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        RunSum E = carry;
+        const RunSum E = carry;
         p.counts[s] = E.cnt ? E.cnt + E.ext + (E.firstP1 - 1u) / 256u : 0u;
     }
 }
 
-// Writes the compact symbols and zero counts and accumulates both histograms.
+// Pass 3 (one block): histogram / builder / header offsets of every table,
+// sized from the largest symbol of its stream.  A symbol outside the
+// instance's 2^log2Max range fails the call (HuffmanTable.cu:411-419).
+__global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
+    __shared__ u32 scratch[40];
+    __shared__ unsigned long long cH, cL, cW;
+    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; }
+    __syncthreads();
+    for (u32 base = 0; base < p.T; base += 1024) {
+        const u32 t = base + threadIdx.x;
+        u32 hs = 0, ls = 0, ws = 0;
+        TableMeta m{};
+        if (t < p.T) {
+            const EncTableDev td = p.tables[t];
+            const u32 smax = p.streamMax[td.stream];
+            const u32 count = p.counts[td.stream];
+            if (td.which == 0 && smax >= p.bins) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
+            hs = td.which ? min(256u, p.bins) : min(smax, p.bins - 1u) + 1u;
+            ls = min(hs, count + 1u);
+            ws = headerWordsFor(ls, p.log2Max);
+            m.count = count;
+            m.histSize = hs;
+            m.blocks = u32(ceilDiv(count, p.cb));
+        }
+        u32 tH, tL, tW;
+        const u32 eH = blockExclusiveSum<1024>(hs, scratch, &tH);
+        const u32 eL = blockExclusiveSum<1024>(ls, scratch, &tL);
+        const u32 eW = blockExclusiveSum<1024>(ws, scratch, &tW);
+        if (t < p.T) {
+            m.histOff = cH + eH;
+            m.leafOff = cL + eL;
+            m.hdrOff = cW + eW;
+            p.meta[t] = m;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        p.totals[1] = cH;
+        if (cH > p.capHist || cL > p.capLeaves || cW > p.capHdr) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_zeroHist(EncParams p) {
+    if (*reinterpret_cast<volatile const u32*>(p.errors)) return;   // no barriers in this kernel
+    const u64 total = p.totals[1];
+    for (u64 i = u64(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += u64(gridDim.x) * blockDim.x) p.hist[i] = 0;
+}
+
+// Pass 4: compact symbols + zero counts (RLHuff) and both histograms, or the
+// plain histogram of a Huff stream.  Bins below kSmemSymBins are counted in
+// shared memory with warp-aggregated increments.
 template <class Sym>
-__global__ void __launch_bounds__(kRleThreads) k_rleWrite(EncParams p) {
+__global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
     __shared__ RunSum smem[9];
     __shared__ u32 hSym[kSmemSymBins];
     __shared__ u32 hZc[256];
-    __shared__ u32 extraTotal;
-    const u32 s = blockIdx.y, tile = blockIdx.x;
-    const u32 n = p.streams[s].n;
-    if (tile * kRleTile >= n) return;
-    const u32 smemBins = min(p.bins, kSmemSymBins);
+    __shared__ u32 extraTotal, sStream;
+    if (threadIdx.x == 0) sStream = streamOfTile(p, blockIdx.x);
+    if (blockFailed(p)) return;   // synchronizes (sStream visible)
+    const u32 tile = blockIdx.x;
+    const u32 s = sStream;
+    const EncStreamDev sd = p.streams[s];
+    const u32 n = sd.n;
+    const TableMeta mS = p.meta[sd.tableFirst];
+    const u32 smemBins = min(mS.histSize, kSmemSymBins);
     for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads) hSym[i] = 0;
     hZc[threadIdx.x] = 0;
     if (threadIdx.x == 0) extraTotal = 0;
-    const Sym* in = reinterpret_cast<const Sym*>(p.streams[s].in);
-    const u32 base = tile * kRleTile + threadIdx.x * kRlePerThread;
+    const Sym* in = reinterpret_cast<const Sym*>(sd.in);
+    const u32 base = (tile - sd.tileOff) * kRleTile + threadIdx.x * kRlePerThread;
     u32 v[kRlePerThread];
     loadSyms(in, base, n, v);
-    RunSum r = threadRun(v, base, n);
-    RunSum E = blockScanRun(r, smem, nullptr);   // includes __syncthreads (smem hist zeroed)
-    const TileStart ts = p.tileStart[u64(s) * p.tilesMax + tile];
+    u32* gSym = p.hist + mS.histOff;
+    if (sd.kind != KIND_RLHUFF) {
+        __syncthreads();
+#pragma unroll
+        for (u32 i = 0; i < kRlePerThread; ++i) {
+            const bool valid = base + i < n;
+            const bool toSmem = valid && v[i] < smemBins;
+            aggregatedIncrement(hSym, toSmem ? v[i] : 0u, toSmem);
+            if (valid && !toSmem && v[i] < mS.histSize) atomicAdd(gSym + v[i], 1u);
+        }
+        __syncthreads();
+        for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads)
+            if (hSym[i]) atomicAdd(gSym + i, hSym[i]);
+        return;
+    }
+    const TableMeta mZ = p.meta[sd.tableFirst + 1];
+    u32* gZc = p.hist + mZ.histOff;
+    const RunSum E = blockScanRun(threadRun(v, base, n), smem, nullptr);   // synchronizes (histograms zeroed)
+    const TileStart ts = p.tileStart[tile];
     u32 prevP1 = E.cnt ? E.lastP1 : ts.prevP1;
     u32 outPos = ts.out + (E.cnt ? E.cnt + E.ext + (E.firstP1 - ts.prevP1 - 1u) / 256u : 0u);
-    Sym* comp = reinterpret_cast<Sym*>(p.compact) + u64(s) * p.nStride;
-    Sym* zcs = reinterpret_cast<Sym*>(p.zc) + u64(s) * p.nStride;
-    u32* gSym = p.hist + u64(s) * p.bins;
-    u32* gZc = p.hist + u64(p.S + s) * p.bins;
+    Sym* comp = reinterpret_cast<Sym*>(p.compact) + sd.compactOff;
+    Sym* zcs = reinterpret_cast<Sym*>(p.zc) + sd.compactOff;
     u32 extras = 0;
     bool rangeErr = false;
 #pragma unroll
@@ -266,65 +378,33 @@ __global__ void __launch_bounds__(kRleThreads) k_rleWrite(EncParams p) {
             prevP1 = q;
         }
         const u32 sym = v[i];
-        const bool inRange = sym < p.bins;
-        rangeErr |= nz && !inRange;
-        const bool toSmem = nz && inRange && sym < smemBins;
+        const bool toSmem = nz && sym < smemBins;
         aggregatedIncrement(hSym, toSmem ? sym : 0u, toSmem);
-        if (nz && inRange && !toSmem) atomicAdd(gSym + sym, 1u);
-        const bool zcOk = (z & 255u) < p.bins;
+        if (nz && !toSmem && sym < mS.histSize) atomicAdd(gSym + sym, 1u);
+        const bool zcOk = (z & 255u) < mZ.histSize;
         rangeErr |= nz && !zcOk;
         aggregatedIncrement(hZc, z & 255u, nz && zcOk);
     }
     if (rangeErr) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
-    u32 e = warpSum(extras);
+    const u32 e = warpSum(extras);
     if ((threadIdx.x & 31) == 0 && e) atomicAdd(&extraTotal, e);
     __syncthreads();
     if (threadIdx.x == 0 && extraTotal) {
         hSym[0] += extraTotal;
-        if (p.bins > 255u) hZc[255] += extraTotal;
+        if (mZ.histSize > 255u) hZc[255] += extraTotal;
         else atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
     }
     __syncthreads();
     for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads)
         if (hSym[i]) atomicAdd(gSym + i, hSym[i]);
-    if (threadIdx.x < p.bins && hZc[threadIdx.x]) atomicAdd(gZc + threadIdx.x, hZc[threadIdx.x]);
-}
-
-// encodeHuff histogram (no run-length stage).
-template <class Sym>
-__global__ void __launch_bounds__(kRleThreads) k_histPlain(EncParams p) {
-    __shared__ u32 hSym[kSmemSymBins];
-    const u32 s = blockIdx.y, tile = blockIdx.x;
-    const u32 n = p.streams[s].n;
-    if (tile * kRleTile >= n) return;
-    const u32 smemBins = min(p.bins, kSmemSymBins);
-    for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads) hSym[i] = 0;
-    __syncthreads();
-    const Sym* in = reinterpret_cast<const Sym*>(p.streams[s].in);
-    const u32 base = tile * kRleTile + threadIdx.x * kRlePerThread;
-    u32 v[kRlePerThread];
-    loadSyms(in, base, n, v);
-    u32* gSym = p.hist + u64(s) * p.bins;
-    bool rangeErr = false;
-#pragma unroll
-    for (u32 i = 0; i < kRlePerThread; ++i) {
-        const bool valid = base + i < n;
-        const bool inRange = v[i] < p.bins;
-        rangeErr |= valid && !inRange;
-        const bool toSmem = valid && inRange && v[i] < smemBins;
-        aggregatedIncrement(hSym, toSmem ? v[i] : 0u, toSmem);
-        if (valid && inRange && !toSmem) atomicAdd(gSym + v[i], 1u);
-    }
-    if (rangeErr) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
-    __syncthreads();
-    for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads)
-        if (hSym[i]) atomicAdd(gSym + i, hSym[i]);
+    if (threadIdx.x < mZ.histSize && hZc[threadIdx.x]) atomicAdd(gZc + threadIdx.x, hZc[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------------------
-// Table construction: one block per table.  Leaf gathering, depths, canonical
-// codes and serialization are block parallel; the heap merge and the sort
-// run in thread 0 with the tie-breaking of huffman_build.cuh.
+// Table construction: one block per table, all tables of the call at once.
+// Leaf gathering, canonical codes and serialization are block parallel; the
+// heap merge, depths and the sort run in thread 0 with the tie-breaking of
+// huffman_build.cuh, on shared memory when the table fits.
 // ---------------------------------------------------------------------------
 constexpr u32 kBuildThreads = 256;
 
@@ -345,50 +425,41 @@ __device__ __forceinline__ void putBits(u32* words, u32 pos, u32 value, u32 coun
 
 __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     extern __shared__ __align__(16) unsigned char dyn[];
-    if (*(volatile u32*)p.errors) return;
     __shared__ u32 sScan[40];
-    __shared__ u32 sMax, sL, sMaxLen, sAllEmpty;
+    __shared__ u32 sMax, sMaxLen, sAllEmpty;
     __shared__ u32 lenCount[32], firstIndex[33], firstCode[33];
+    if (threadIdx.x == 0) { sMax = 0; sAllEmpty = 1; }
+    if (blockFailed(p)) return;
     const u32 t = blockIdx.x;
-    const u32 S = p.S;
-    u32 count;
-    // every table's input is u16 or u32; only the count is needed here
-    if (p.kind == KIND_RLHUFF) count = p.counts[t < S ? t : t - S];
-    else count = p.streams[t].n;
-    u32* hist = p.hist + u64(t) * p.bins;
-    const bool isZc = p.kind == KIND_RLHUFF && t >= S;
+    const EncTableDev td = p.tables[t];
+    const EncStreamDev es = p.streams[td.stream];
+    TableMeta meta = p.meta[t];
+    const u32 count = meta.count;
+    const u32* hist = p.hist + meta.histOff;
+    const bool isZc = es.kind == KIND_RLHUFF && td.which == 1;
 
     // 1. largest present symbol
-    const u32 sIdx = t < S ? t : t - S;
-    const EncStream es = p.streams[sIdx];
-    if (threadIdx.x == 0) { sMax = 0; sAllEmpty = 1; }
-    __syncthreads();
-    if (p.kind == KIND_RLHUFF)
+    if (es.kind == KIND_RLHUFF)
         for (u32 s = es.groupFirst + threadIdx.x; s < es.groupFirst + es.groupSize; s += kBuildThreads)
             if (p.counts[s]) atomicAnd(&sAllEmpty, 0u);
     u32 localMax = 0;
     bool any = false;
-    const u32 scanBins = isZc ? min(256u, p.bins) : p.bins;
-    for (u32 b = threadIdx.x; b < scanBins; b += kBuildThreads)
+    for (u32 b = threadIdx.x; b < meta.histSize; b += kBuildThreads)
         if (hist[b]) { localMax = b; any = true; }
     if (any) atomicMax(&sMax, localMax);
     __syncthreads();
-    u32 symbolMax = count ? sMax : 0u;
-    // Histogram.cu:117-121: with every stream of the call empty the reference
-    // builds its tables from stale arena words; for zero-count table i that
-    // word is the low half of a device pointer when 2+2i < S (nonzero), else
-    // the all-zero run-length scan output.
-    const bool quirkLeaf = isZc && sAllEmpty && (2u + 2u * (sIdx - es.groupFirst) < es.groupSize);
+    const u32 symbolMax = count ? sMax : 0u;
+    // Histogram.cu:117-121: with every stream of the reference call empty the
+    // reference builds its tables from stale arena words; for zero-count table
+    // i that word is the low half of a device pointer when 2+2i < S (nonzero),
+    // else the all-zero run-length scan output.
+    const bool quirkLeaf = isZc && sAllEmpty && (2u + 2u * (td.stream - es.groupFirst) < es.groupSize);
     // 2. leaves in symbol order
-    const bool smemHeap = true;
+    u32* leafSym = p.leafSymWork + meta.leafOff;
+    u64* heapG = p.leafWork + meta.leafOff;
     u32 L;
-    u32* leafSym = p.leafSymWork + u64(t) * p.leavesMax;
-    u64* heapG = p.leafWork + u64(t) * p.leavesMax;
-    u32* parent = p.parentWork + u64(t) * 2 * p.leavesMax;
-    u32* orderG = p.orderWork + u64(t) * p.leavesMax;
     if (quirkLeaf) {
-        if (threadIdx.x == 0) { leafSym[0] = 0; heapG[0] = (u64(1) << 32) | 0u; sL = 1; }
-        __syncthreads();
+        if (threadIdx.x == 0) { leafSym[0] = 0; heapG[0] = (u64(1) << 32) | 0u; }
         L = 1;
     } else if (count == 0) {
         L = 0;
@@ -401,10 +472,6 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         u32 tot;
         u32 off = blockExclusiveSum<kBuildThreads>(c, sScan, &tot);
         L = tot;
-        if (L > p.leavesMax) {
-            if (threadIdx.x == 0) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
-            return;
-        }
         const bool quirk65535 = p.symBytes == 2 && p.bins == 65536u && symbolMax == 65535u;
         for (u32 b = b0; b < b1; ++b) {
             u32 h = hist[b];
@@ -415,11 +482,13 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
                 ++off;
             }
         }
-        __syncthreads();
     }
-    const bool inSmem = smemHeap && L <= p.heapCap;
+    __syncthreads();
+    const bool inSmem = L <= p.heapCap;
     u64* heap = inSmem ? reinterpret_cast<u64*>(dyn) : heapG;
-    u32* order = inSmem ? reinterpret_cast<u32*>(dyn + sizeof(u64) * p.heapCap) : orderG;
+    u32* order = inSmem ? reinterpret_cast<u32*>(dyn + sizeof(u64) * p.heapCap) : p.orderWork + meta.leafOff;
+    u32* parent = inSmem ? reinterpret_cast<u32*>(dyn + (sizeof(u64) + sizeof(u32)) * p.heapCap)
+                         : p.parentWork + 2 * meta.leafOff;
     if (inSmem)
         for (u32 i = threadIdx.x; i < L; i += kBuildThreads) heap[i] = heapG[i];
     __syncthreads();
@@ -428,7 +497,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         u32 maxLen = 0;
         if (L >= 1) {
             hb::buildTree(heap, parent, int(L));
-            // depths in place over the parent links
+            // depths in place over the parent links (parents have larger ids)
             const int nodes = int(2 * L - 1);
             parent[nodes - 1] = 0;
             for (int id = nodes - 2; id >= 0; --id) {
@@ -468,7 +537,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         }
     }
     __syncthreads();
-    uint2* enc = p.enc + u64(t) * p.bins;
+    uint2* enc = p.enc + meta.histOff;
     for (u32 k = threadIdx.x; k < L; k += kBuildThreads) {
         u32 len = order[k] >> 27;
         u32 sym = leafSym[order[k] & hb::kLeafMask];
@@ -480,12 +549,8 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     const u32 symbolBits = requiredBits(symbolMax);
     const u32 fixedBits = 5 + maxLen * p.log2Max + p.log2Max + (longSym ? 5u : 4u);
     const u32 headerBits = fixedBits + L * symbolBits;
-    u32* hdr = p.headers + u64(t) * p.hdrWordsMax;
+    u32* hdr = p.headers + meta.hdrOff;
     const u32 hdrWords = u32(ceilDiv(headerBits, 32));
-    if (hdrWords > p.hdrWordsMax) {
-        if (threadIdx.x == 0) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
-        return;
-    }
     for (u32 w = threadIdx.x; w < hdrWords; w += kBuildThreads) hdr[w] = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -498,59 +563,57 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     for (u32 k = threadIdx.x; k < L; k += kBuildThreads)
         putBits(hdr, fixedBits + k * symbolBits, leafSym[order[k] & hb::kLeafMask], symbolBits);
     if (threadIdx.x == 0) {
-        TableMeta m;
-        m.count = count;
-        m.symbolMax = symbolMax;
-        m.leaves = L;
-        m.maxLen = maxLen;
-        m.headerBits = headerBits;
-        m.codeBits = 0;
-        m.blocks = u32(ceilDiv(count, p.cb));
-        m.pad = 0;
-        p.meta[t] = m;
+        meta.symbolMax = symbolMax;
+        meta.leaves = L;
+        meta.maxLen = maxLen;
+        meta.headerBits = headerBits;
+        meta.codeBits = 0;
+        p.meta[t] = meta;
     }
 }
 
 // ---------------------------------------------------------------------------
 // Huffman encode (Huffman.cu:73-187): per coding block bit totals, per table
-// scan to block offsets, then packing.
+// scan to block offsets, then packing.  One warp per coding block.
 // ---------------------------------------------------------------------------
 constexpr u32 kPackWarps = 8;
 
 template <class Sym>
 __global__ void __launch_bounds__(kPackWarps * 32) k_blockBits(EncParams p) {
-    if (*(volatile u32*)p.errors) return;
-    const u32 t = blockIdx.y;
-    const u32 b = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
+    const u32 gb = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
     const u32 lane = threadIdx.x & 31;
+    if (gb >= p.totalBlocks || warpFailed(p)) return;
+    const u32 t = tableOfBlock(p, gb);
+    const EncTableDev td = p.tables[t];
+    const u32 b = gb - td.blockOff;
     u32 count;
-    const Sym* in = tableInput<Sym>(p, t, count);
-    const u32 blocks = u32(ceilDiv(count, p.cb));
-    if (b >= blocks) return;
-    const uint2* enc = p.enc + u64(t) * p.bins;
+    const Sym* in = tableInput<Sym>(p, td, count);
+    const TableMeta& m = p.meta[t];
+    if (b >= m.blocks) return;
+    const uint2* enc = p.enc + m.histOff;
+    const u32 hs = m.histSize;
     const u32 i0 = b * p.cb, i1 = min(count, i0 + p.cb);
     u32 bits = 0;
-    for (u32 i = i0 + lane; i < i1; i += 32) bits += enc[min(u32(in[i]), p.bins - 1u)].y;
+    for (u32 i = i0 + lane; i < i1; i += 32) bits += enc[min(u32(in[i]), hs - 1u)].y;
     bits = warpSum(bits);
-    if (lane == 0) p.blockBits[u64(t) * p.blocksMax + b] = bits;
+    if (lane == 0) p.blockBits[gb] = bits;
 }
 
+// Exclusive scan of one table's block bits (one block per table).
 __global__ void __launch_bounds__(1024) k_blockScan(EncParams p) {
-    if (*(volatile u32*)p.errors) return;
     __shared__ u32 scratch[40];
     __shared__ u32 carry;
-    const u32 t = blockIdx.x;
-    const TableMeta m = p.meta[t];
-    const u32 blocks = m.blocks;
-    const u32* bb = p.blockBits + u64(t) * p.blocksMax;
-    u32* bo = p.blockOff + u64(t) * p.blocksMax;
     if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
+    if (blockFailed(p)) return;
+    const u32 t = blockIdx.x;
+    const u32 blocks = p.meta[t].blocks;
+    const u32* bb = p.blockBits + p.tables[t].blockOff;
+    u32* bo = p.blockOff + p.tables[t].blockOff;
     for (u32 base = 0; base < blocks; base += 1024) {
-        u32 i = base + threadIdx.x;
-        u32 v = i < blocks ? bb[i] : 0u;
+        const u32 i = base + threadIdx.x;
+        const u32 v = i < blocks ? bb[i] : 0u;
         u32 tot;
-        u32 ex = blockExclusiveSum<1024>(v, scratch, &tot);
+        const u32 ex = blockExclusiveSum<1024>(v, scratch, &tot);
         if (i < blocks) bo[i] = carry + ex;
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
@@ -561,19 +624,20 @@ __global__ void __launch_bounds__(1024) k_blockScan(EncParams p) {
 
 // Segment layout per stream and exclusive scan over streams (one block).
 __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
-    if (*(volatile u32*)p.errors) return;
     __shared__ u32 scratch[40];
     __shared__ unsigned long long carry;
     if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
+    if (blockFailed(p)) return;
     for (u32 base = 0; base < p.S; base += 1024) {
         const u32 s = base + threadIdx.x;
         SegmentLayout L{};
         u32 words = 0;
         if (s < p.S) {
-            if (p.kind == KIND_RLHUFF) {
-                const TableMeta ms = p.meta[s], mz = p.meta[p.S + s];
-                const u32 offW = u32(ceilDiv(ceilDiv(p.counts[s], p.cb), 2));
+            const EncStreamDev sd = p.streams[s];
+            const u32 offW = u32(ceilDiv(ceilDiv(p.counts[s], p.cb), 2));
+            const TableMeta ms = p.meta[sd.tableFirst];
+            if (sd.kind == KIND_RLHUFF) {
+                const TableMeta mz = p.meta[sd.tableFirst + 1];
                 L.countWord = 0;
                 L.hdrWord[0] = 1;
                 L.cwWord[0] = L.hdrWord[0] + u32(ceilDiv(ms.headerBits, 32)) + 1;
@@ -584,9 +648,7 @@ __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
                 words = L.offWord[1] + offW;
                 L.startBit = 0;
             } else {
-                const TableMeta ms = p.meta[s];
-                const u32 r = p.streams[s].startBit;
-                const u32 offW = u32(ceilDiv(ceilDiv(p.streams[s].n, p.cb), 2));
+                const u32 r = sd.startBit;
                 L.hdrWord[0] = 0;
                 L.cwWord[0] = u32(ceilDiv(r + ms.headerBits, 32)) + 1;
                 L.offWord[0] = L.cwWord[0] + u32(ceilDiv(ms.codeBits, 32));
@@ -598,7 +660,7 @@ __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
         }
         // 64-bit carry across chunks; within a chunk a 32-bit scan suffices
         u32 tot;
-        u32 ex = blockExclusiveSum<1024>(words, scratch, &tot);
+        const u32 ex = blockExclusiveSum<1024>(words, scratch, &tot);
         if (s < p.S) {
             L.startWord = carry + ex;
             p.layout[s] = L;
@@ -609,7 +671,7 @@ __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
     }
     if (threadIdx.x == 0) {
         p.totals[0] = carry;
-        if (carry > p.outWordsMax) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+        if (carry > p.outWordsMax) atomicOr(p.errors, DEV_ERR_OUTPUT_CAPACITY);
     }
 }
 
@@ -634,24 +696,26 @@ __device__ __forceinline__ void orCodeword(u32* win, u32 wLo, u32 wHi, u32 pos, 
 template <class Sym>
 __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
     extern __shared__ u32 winAll[];
-    if (*(volatile u32*)p.errors) return;
-    const u32 t = blockIdx.y;
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const u32 b = blockIdx.x * kPackWarps + warp;
-    const u32 winWords = p.cb + 2;
-    u32* win = winAll + warp * winWords;
+    const u32 gb = blockIdx.x * kPackWarps + warp;
+    if (gb >= p.totalBlocks || warpFailed(p)) return;
+    const u32 t = tableOfBlock(p, gb);
+    const EncTableDev td = p.tables[t];
+    const u32 b = gb - td.blockOff;
+    u32* win = winAll + warp * (p.cb + 2);
     u32 count;
-    const Sym* in = tableInput<Sym>(p, t, count);
+    const Sym* in = tableInput<Sym>(p, td, count);
     const TableMeta m = p.meta[t];
     if (b >= m.blocks) return;
-    const u32* bo = p.blockOff + u64(t) * p.blocksMax;
+    const u32* bo = p.blockOff + td.blockOff;
     const u32 off0 = bo[b];
     const u32 off1 = (b + 1 < m.blocks) ? bo[b + 1] : m.codeBits;
     const u32 wLo = (off0 + 31) >> 5, wHi = (off1 + 31) >> 5;
     if (wLo >= wHi) return;
     for (u32 w = lane; w < wHi - wLo; w += 32) win[w] = 0;
     __syncwarp();
-    const uint2* enc = p.enc + u64(t) * p.bins;
+    const uint2* enc = p.enc + m.histOff;
+    const u32 hs = m.histSize;
     const u32 i0 = b * p.cb;
     const u32 per = p.cb / 32;
     const u32 j0 = i0 + lane * per;
@@ -659,7 +723,7 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
     u32 lsum = 0;
     for (u32 k = 0; k < per; ++k) {
         const u32 j = j0 + k;
-        cw[k] = j < count ? enc[min(u32(in[j]), p.bins - 1u)] : make_uint2(0, 0);
+        cw[k] = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
         lsum += cw[k].y;
     }
     u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
@@ -670,30 +734,31 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
     // bits of the next block inside the last owned word
     if (b + 1 < m.blocks && (wHi << 5) > off1) {
         const u32 j = (b + 1) * p.cb + lane;
-        uint2 c = j < count ? enc[min(u32(in[j]), p.bins - 1u)] : make_uint2(0, 0);
+        uint2 c = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
         u32 q = off1 + warpInclusiveSum(c.y) - c.y;
         if (q < (wHi << 5)) orCodeword(win, wLo, wHi, q, c.x, c.y);
     }
     __syncwarp();
-    const u32 s = p.kind == KIND_RLHUFF ? (t < p.S ? t : t - p.S) : t;
-    const u32 which = (p.kind == KIND_RLHUFF && t >= p.S) ? 1u : 0u;
-    const SegmentLayout L = p.layout[s];
+    const u32 which = (p.streams[td.stream].kind == KIND_RLHUFF && td.which) ? 1u : 0u;
+    const SegmentLayout& L = p.layout[td.stream];
     u32* dst = p.out + L.startWord + L.cwWord[which];
     for (u32 w = lane; w < wHi - wLo; w += 32) dst[wLo + w] = win[w];
 }
 
 // Count words, table headers, codeword bit counts and offset increments.
 __global__ void __launch_bounds__(128) k_headers(EncParams p) {
-    if (*(volatile u32*)p.errors) return;
+    if (blockFailed(p)) return;
     const u32 s = blockIdx.x;
+    const EncStreamDev sd = p.streams[s];
     const SegmentLayout L = p.layout[s];
     u32* seg = p.out + L.startWord;
-    const u32 parts = p.kind == KIND_RLHUFF ? 2u : 1u;
-    if (p.kind == KIND_RLHUFF && threadIdx.x == 0) seg[L.countWord] = p.counts[s];
+    const bool rl = sd.kind == KIND_RLHUFF;
+    const u32 parts = rl ? 2u : 1u;
+    if (rl && threadIdx.x == 0) seg[L.countWord] = p.counts[s];
     for (u32 part = 0; part < parts; ++part) {
-        const u32 t = part == 0 ? s : p.S + s;
+        const u32 t = sd.tableFirst + part;
         const TableMeta m = p.meta[t];
-        const u32* hdr = p.headers + u64(t) * p.hdrWordsMax;
+        const u32* hdr = p.headers + m.hdrOff;
         const u32 r = part == 0 ? L.startBit : 0u;
         const u32 hw = u32(ceilDiv(r + m.headerBits, 32));
         u32* dst = seg + L.hdrWord[part];
@@ -712,7 +777,7 @@ __global__ void __launch_bounds__(128) k_headers(EncParams p) {
         if (threadIdx.x == 0) seg[L.cwWord[part] - 1] = m.codeBits;
         // offsets: u16 increments, two per word, first in the low half (LE memcpy)
         const u32 nOff = m.blocks;
-        const u32* bo = p.blockOff + u64(t) * p.blocksMax;
+        const u32* bo = p.blockOff + p.tables[t].blockOff;
         u32* od = seg + L.offWord[part];
         for (u32 w = threadIdx.x; w < (nOff + 1) / 2; w += blockDim.x) {
             const u32 k0 = 2 * w, k1 = 2 * w + 1;
@@ -726,93 +791,141 @@ __global__ void __launch_bounds__(128) k_headers(EncParams p) {
 // ---------------------------------------------------------------------------
 // Host orchestration.
 // ---------------------------------------------------------------------------
-static EncParams makeParams(cc_instance* I, int kind, u32 S) {
+struct HostPlan {
+    u32 T = 0, tiles = 0, blocks = 0, maxCount = 0;
+    u64 compact = 0;
+    size_t offTables = 0, bytes = 0;
+};
+
+// Writes the stream and table descriptors of a call into `slot` (pinned).
+static int buildPlan(cc_instance* I, const EncStream* streams, u32 S, char* slot, HostPlan& hp) {
+    for (u32 s = 0; s < S; ++s) {
+        const EncStream& e = streams[s];
+        const u64 nb = ceilDiv(e.n, I->codingBlockSize);
+        hp.T += e.kind == KIND_RLHUFF ? 2u : 1u;
+        hp.tiles += u32(ceilDiv(e.n, kRleTile));
+        hp.blocks += u32(e.kind == KIND_RLHUFF ? 2 * nb : nb);
+        hp.maxCount = std::max(hp.maxCount, e.n);
+        if (e.kind == KIND_RLHUFF) hp.compact += e.n;
+    }
+    if (S > I->capStreams || hp.T > I->capTables || hp.tiles > I->capTiles || hp.blocks > I->capBlocks ||
+        hp.compact > I->capCompact) {
+        setError("encode: call exceeds the instance capacity (%u streams, %llu run-length symbols)", S,
+                 (unsigned long long)hp.compact);
+        return CC_ERR_CAPACITY;
+    }
+    hp.offTables = alignUp(sizeof(EncStreamDev) * S, 64);
+    hp.bytes = hp.offTables + sizeof(EncTableDev) * hp.T;
+    if (hp.bytes > I->hostRingBytes) { setError("encode: descriptors exceed the staging slot"); return CC_ERR_CAPACITY; }
+    EncStreamDev* sd = reinterpret_cast<EncStreamDev*>(slot);
+    EncTableDev* td = reinterpret_cast<EncTableDev*>(slot + hp.offTables);
+    u32 tile = 0, table = 0, block = 0;
+    u64 compact = 0;
+    for (u32 s = 0; s < S; ++s) {
+        const EncStream& e = streams[s];
+        EncStreamDev d{};
+        d.in = e.in;
+        d.n = e.n;
+        d.kind = e.kind;
+        d.startBit = e.kind == KIND_HUFF ? (e.startBit & 31u) : 0u;
+        d.groupFirst = e.groupFirst;
+        d.groupSize = e.groupSize;
+        d.tileOff = tile;
+        d.tableFirst = table;
+        d.compactOff = compact;
+        sd[s] = d;
+        tile += u32(ceilDiv(e.n, kRleTile));
+        if (e.kind == KIND_RLHUFF) compact += e.n;
+        const u32 parts = e.kind == KIND_RLHUFF ? 2u : 1u;
+        const u32 nb = u32(ceilDiv(e.n, I->codingBlockSize));
+        for (u32 w = 0; w < parts; ++w) {
+            td[table++] = EncTableDev{s, w, block, nb};
+            block += nb;
+        }
+    }
+    return CC_OK;
+}
+
+template <class Sym>
+static int launchEncode(cc_instance* I, const EncParams& p) {
+    cudaStream_t st = I->stream;
+    CC_TRY_CUDA(cudaMemsetAsync(I->errors, 0, 4 * sizeof(u32), st), "memset errors");
+    CC_TRY_CUDA(cudaMemsetAsync(I->streamMax, 0, sizeof(u32) * p.S, st), "memset stream max");
+    if (p.totalTiles) { SectionTimer t(I, "enc.summary", st); k_summary<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.rle_scan", st); k_scan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
+    if (p.totalTiles) { SectionTimer t(I, "enc.rle_write_hist", st); k_write<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
+    const size_t buildSmem = std::max<size_t>(16, size_t(p.heapCap) * (sizeof(u64) + 3 * sizeof(u32)));
+    CC_TRY_CUDA(cudaFuncSetAttribute(k_tableBuild, cudaFuncAttributeMaxDynamicSharedMemorySize, int(buildSmem)), "tableBuild smem");
+    { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
+    if (p.totalBlocks) {
+        const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
+        { SectionTimer t(I, "enc.block_bits", st); k_blockBits<Sym><<<g, kPackWarps * 32, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "enc.block_scan", st); k_blockScan<<<p.T, 1024, 0, st>>>(p); countLaunch(); }
+    }
+    { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
+    if (p.totalBlocks) {
+        const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
+        const size_t packSmem = size_t(kPackWarps) * (p.cb + 2) * sizeof(u32);
+        SectionTimer t(I, "enc.pack", st);
+        k_pack<Sym><<<g, kPackWarps * 32, packSmem, st>>>(p);
+        countLaunch();
+    }
+    { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 128, 0, st>>>(p); countLaunch(); }
+    CC_TRY_CUDA(cudaGetLastError(), "encode launch");
+    return CC_OK;
+}
+
+int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutput& outSpec, bool download,
+                 u64* totalWords) {
+    if (totalWords) *totalWords = 0;
+    if (S == 0) { I->lastLayout.clear(); return CC_OK; }
+    cudaStream_t st = I->stream;
+    char* slot = I->takeRingSlot();
+    HostPlan hp;
+    int rc = buildPlan(I, streams, S, slot, hp);
+    if (rc) return rc;
+    char* dPlan = reinterpret_cast<char*>(I->dPlan);
+    CC_TRY_CUDA(cudaMemcpyAsync(dPlan, slot, hp.bytes, cudaMemcpyHostToDevice, st), "upload plan");
+    cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
     EncParams p{};
-    p.kind = kind;
     p.S = S;
+    p.T = hp.T;
+    p.totalTiles = hp.tiles;
+    p.totalBlocks = hp.blocks;
     p.cb = I->codingBlockSize;
     p.log2Max = I->log2Max;
     p.bins = I->bins;
     p.symBytes = I->symBytes;
-    p.streams = I->dStreams;
+    p.streams = reinterpret_cast<const EncStreamDev*>(dPlan);
+    p.tables = reinterpret_cast<const EncTableDev*>(dPlan + hp.offTables);
     p.compact = static_cast<char*>(I->compact);
     p.zc = static_cast<char*>(I->zc);
-    p.nStride = I->elemCountPerStreamMax;
     p.tiles = I->tiles;
     p.tileStart = I->tileStart;
-    p.tilesMax = I->tilesMax;
+    p.streamMax = I->streamMax;
+    p.counts = I->counts;
     p.hist = I->hist;
     p.enc = I->enc;
     p.meta = I->meta;
     p.headers = I->headers;
-    p.hdrWordsMax = I->hdrWordsMax;
     p.blockBits = I->blockBits;
     p.blockOff = I->blockOff;
-    p.blocksMax = I->blocksMax;
     p.layout = I->layout;
-    p.out = I->out;
-    p.outWordsMax = I->outWordsMax;
-    p.counts = I->counts;
+    p.out = outSpec.words ? outSpec.words : I->out;
+    p.outWordsMax = outSpec.words ? outSpec.capacity : I->outWordsMax;
+    p.capHist = I->capHist;
+    p.capLeaves = I->capLeaves;
+    p.capHdr = I->capHdr;
     p.errors = I->errors;
     p.totals = I->totals;
     p.leafWork = I->leafWork;
     p.parentWork = I->parentWork;
     p.orderWork = I->orderWork;
     p.leafSymWork = I->leafSymWork;
-    p.leavesMax = I->leavesMax;
-    p.heapCap = std::min<u32>(I->leavesMax, 12288u);
-    return p;
-}
-
-template <class Sym>
-static int launchEncode(cc_instance* I, const EncParams& p, u32 nMax) {
-    cudaStream_t st = I->stream;
-    const u32 T = p.kind == KIND_RLHUFF ? 2 * p.S : p.S;
-    const u32 tiles = std::max<u32>(1u, u32(ceilDiv(nMax, kRleTile)));
-    CC_TRY_CUDA(cudaMemsetAsync(I->errors, 0, 8 * sizeof(u32), st), "memset errors");
-    CC_TRY_CUDA(cudaMemsetAsync(I->hist, 0, u64(T) * I->bins * sizeof(u32), st), "memset histograms");
-    dim3 gTiles(tiles, p.S);
-    if (p.kind == KIND_RLHUFF) {
-        { SectionTimer t(I, "enc.rle_summary", st); k_rleSummary<Sym><<<gTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "enc.rle_scan", st); k_rleScan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "enc.rle_write_hist", st); k_rleWrite<Sym><<<gTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
-    } else {
-        { SectionTimer t(I, "enc.histogram", st); k_histPlain<Sym><<<gTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
-    }
-    const size_t buildSmem = size_t(p.heapCap) * (sizeof(u64) + sizeof(u32));
-    CC_TRY_CUDA(cudaFuncSetAttribute(k_tableBuild, cudaFuncAttributeMaxDynamicSharedMemorySize, int(buildSmem) > 0 ? int(buildSmem) : 1), "tableBuild smem");
-    { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
-    const u32 blocks = std::max<u32>(1u, u32(ceilDiv(nMax, p.cb)));
-    dim3 gBlocks(u32(ceilDiv(blocks, kPackWarps)), T);
-    { SectionTimer t(I, "enc.block_bits", st); k_blockBits<Sym><<<gBlocks, kPackWarps * 32, 0, st>>>(p); countLaunch(); }
-    { SectionTimer t(I, "enc.block_scan", st); k_blockScan<<<T, 1024, 0, st>>>(p); countLaunch(); }
-    { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
-    const size_t packSmem = size_t(kPackWarps) * (p.cb + 2) * sizeof(u32);
-    { SectionTimer t(I, "enc.pack", st); k_pack<Sym><<<gBlocks, kPackWarps * 32, packSmem, st>>>(p); countLaunch(); }
-    { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 128, 0, st>>>(p); countLaunch(); }
-    CC_TRY_CUDA(cudaGetLastError(), "encode launch");
-    return CC_OK;
-}
-
-int encodeDevice(cc_instance* I, int kind, const EncStream* streams, u32 S, bool download, u64* totalWords) {
-    if (totalWords) *totalWords = 0;
-    if (S == 0) { I->lastLayout.clear(); return CC_OK; }
-    if (S > I->streamCountMax) { setError("stream count %u exceeds instance limit %u", S, I->streamCountMax); return CC_ERR_CAPACITY; }
-    u32 nMax = 0;
-    for (u32 i = 0; i < S; ++i) {
-        if (streams[i].n > I->elemCountPerStreamMax) {
-            setError("symbol count %u exceeds instance limit %u", streams[i].n, I->elemCountPerStreamMax);
-            return CC_ERR_CAPACITY;
-        }
-        nMax = std::max(nMax, streams[i].n);
-    }
-    cudaStream_t st = I->stream;
-    char* slot = I->takeRingSlot();
-    std::memcpy(slot, streams, sizeof(EncStream) * S);
-    CC_TRY_CUDA(cudaMemcpyAsync(I->dStreams, slot, sizeof(EncStream) * S, cudaMemcpyHostToDevice, st), "upload streams");
-    cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
-    EncParams p = makeParams(I, kind, S);
-    int rc = I->symBytes == 2 ? launchEncode<u16>(I, p, nMax) : launchEncode<u32>(I, p, nMax);
+    p.heapCap = std::min<u32>(std::min<u32>(I->leavesMax, kBuildSmemLeaves), hp.maxCount + 1u);
+    rc = I->symBytes == 2 ? launchEncode<u16>(I, p) : launchEncode<u32>(I, p);
     if (rc) return rc;
     // results: layout, total words, error flags
     char* down = I->hostDown;
@@ -821,13 +934,14 @@ int encodeDevice(cc_instance* I, int kind, const EncStream* streams, u32 S, bool
     CC_TRY_CUDA(cudaMemcpyAsync(tail, I->totals, sizeof(u64), cudaMemcpyDeviceToHost, st), "download totals");
     CC_TRY_CUDA(cudaMemcpyAsync(tail + 64, I->errors, sizeof(u32), cudaMemcpyDeviceToHost, st), "download errors");
     CC_TRY_CUDA(cudaStreamSynchronize(st), "encode");
-    u32 flags = *reinterpret_cast<u32*>(tail + 64);
+    const u32 flags = *reinterpret_cast<u32*>(tail + 64);
     if (flags) return deviceErrorStatus(flags, "encode");
-    u64 total = *reinterpret_cast<u64*>(tail);
+    const u64 total = *reinterpret_cast<u64*>(tail);
     I->lastLayout.assign(reinterpret_cast<SegmentLayout*>(down), reinterpret_cast<SegmentLayout*>(down) + S);
     if (totalWords) *totalWords = total;
     if (download && total) {
-        CC_TRY_CUDA(cudaMemcpyAsync(I->hostWords, I->out, total * 4, cudaMemcpyDeviceToHost, st), "download words");
+        if (total > I->hostWordsMax) { setError("encode: result larger than the host staging"); return CC_ERR_CAPACITY; }
+        CC_TRY_CUDA(cudaMemcpyAsync(I->hostWords, p.out, total * 4, cudaMemcpyDeviceToHost, st), "download words");
         CC_TRY_CUDA(cudaStreamSynchronize(st), "download words");
     }
     return CC_OK;
@@ -848,6 +962,8 @@ int cc_encode(cc_instance* I, int kind, int symbolBytes, const void* const* dStr
                  symbolBytes, symbolBytes == 2 ? "<=" : ">");
         return CC_ERR_INVALID_ARGUMENT;
     }
+    if (S > I->streamCountMax) { setError("stream count %u exceeds instance limit %u", S, I->streamCountMax); return CC_ERR_CAPACITY; }
+    if (n > I->elemCountPerStreamMax) { setError("symbol count %u exceeds instance limit %u", n, I->elemCountPerStreamMax); return CC_ERR_CAPACITY; }
     cudaSetDevice(I->device);
     std::vector<EncStream> st(S);
     for (u32 i = 0; i < S; ++i) {
@@ -856,8 +972,9 @@ int cc_encode(cc_instance* I, int kind, int symbolBytes, const void* const* dStr
         st[i].startBit = (kind == KIND_HUFF && startBits) ? (startBits[i] & 31u) : 0u;
         st[i].groupFirst = 0;
         st[i].groupSize = S;
+        st[i].kind = u32(kind);
     }
-    return encodeDevice(I, kind, st.data(), S, true);
+    return encodeDevice(I, st.data(), S, EncOutput{}, true);
 }
 
 int cc_encoded_segment(const cc_instance* I, uint32_t i, const uint32_t** words, uint32_t* wordCount,

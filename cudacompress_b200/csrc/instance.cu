@@ -34,23 +34,6 @@ int cudaFail(cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? CC_ERR_OUT_OF_MEMORY : CC_ERR_CUDA;
 }
 
-u32 headerWordsFor(u32 leaves, u32 log2Max) {
-    u64 symBits = log2Max > 16 ? 24 : 16;
-    u64 bits = 5 + 31ull * log2Max + log2Max + 5 + u64(leaves) * symBits;
-    return u32(ceilDiv(bits, 32) + 2);
-}
-
-// Worst-case words of one stream's segment: Huffman output never exceeds a
-// fixed-length code of ceil(log2(distinct)) bits per symbol (Huffman codes are
-// optimal among prefix codes), i.e. log2Max bits for symbols and 8 bits for
-// zero counts (at most 256 distinct values).
-u64 segmentWordsMax(u32 n, u32 cb, u32 log2Max, u32 hdrWords) {
-    u64 offs = ceilDiv(ceilDiv(n, cb), 2);
-    u64 sym = ceilDiv(u64(n) * log2Max, 32) + 1;
-    u64 zc = ceilDiv(u64(n) * 8, 32) + 1;
-    return 1 + 2ull * hdrWords + 2 + sym + zc + 2 * offs + 4;
-}
-
 int ensurePipelineWork(cc_instance* I, size_t bytes) {
     if (I->pipeWorkBytes >= bytes) return CC_OK;
     cudaStreamSynchronize(I->stream);
@@ -113,28 +96,30 @@ struct Carver {
 
 void layoutArena(cc_instance* I, char* base, size_t* total) {
     Carver c{base};
-    u32 S = I->streamCountMax, N = I->elemCountPerStreamMax;
-    u32 T = 2 * S;
-    I->compact = c.take<char>(u64(S) * N * I->symBytes + 64);
-    I->zc = c.take<char>(u64(S) * N * I->symBytes + 64);
-    I->tiles = c.take<RunSum>(u64(S) * I->tilesMax);
-    I->tileStart = c.take<TileStart>(u64(S) * I->tilesMax);
-    I->hist = c.take<u32>(u64(T) * I->bins);
-    I->enc = c.take<uint2>(u64(T) * I->bins);
-    I->meta = c.take<TableMeta>(T);
-    I->headers = c.take<u32>(u64(T) * I->hdrWordsMax);
-    I->blockBits = c.take<u32>(u64(T) * I->blocksMax + 1);
-    I->blockOff = c.take<u32>(u64(T) * I->blocksMax + 1);
-    I->layout = c.take<SegmentLayout>(S);
+    const u32 S = I->streamCountMax, T = 2 * S;
+    const u64 SN = u64(S) * I->elemCountPerStreamMax;
+    I->compact = c.take<char>(I->capCompact * I->symBytes + 64);
+    I->zc = c.take<char>(I->capCompact * I->symBytes + 64);
+    I->tiles = c.take<RunSum>(I->capTiles);
+    I->tileStart = c.take<TileStart>(I->capTiles);
+    I->streamMax = c.take<u32>(I->capStreams);
+    I->hist = c.take<u32>(I->capHist);
+    I->enc = c.take<uint2>(I->capHist);
+    I->meta = c.take<TableMeta>(I->capTables);
+    I->headers = c.take<u32>(I->capHdr);
+    I->blockBits = c.take<u32>(I->capBlocks + 1);
+    I->blockOff = c.take<u32>(I->capBlocks + 1);
+    I->layout = c.take<SegmentLayout>(I->capStreams);
     I->out = c.take<u32>(I->outWordsMax);
-    I->counts = c.take<u32>(S);
+    I->counts = c.take<u32>(I->capStreams);
     I->errors = c.take<u32>(8);
     I->totals = c.take<u64>(8);
-    I->dStreams = c.take<EncStream>(S);
-    I->leafWork = c.take<u64>(u64(T) * I->leavesMax);
-    I->parentWork = c.take<u32>(u64(T) * 2 * I->leavesMax);
-    I->orderWork = c.take<u32>(u64(T) * I->leavesMax);
-    I->leafSymWork = c.take<u32>(u64(T) * I->leavesMax);
+    I->dPlan = c.take<char>(I->hostRingBytes);
+    I->leafWork = c.take<u64>(I->capLeaves);
+    I->parentWork = c.take<u32>(2 * I->capLeaves);
+    I->orderWork = c.take<u32>(I->capLeaves);
+    I->leafSymWork = c.take<u32>(I->capLeaves);
+    // decode (one call of at most streamCountMax streams)
     I->dDecTables = c.take<DecTableDesc>(T);
     I->dDecStreams = c.take<DecStreamDesc>(S);
     I->decTables = c.take<DecTable>(T);
@@ -142,8 +127,37 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->decLut = c.take<u32>(u64(T) << kLutBits);
     I->stagedWordsMax = I->outWordsMax + 64;
     I->stagedWords = c.take<u32>(I->stagedWordsMax);
-    I->blockSum = c.take<u32>(u64(S) * I->blocksMax + 1);
+    I->blockSum = c.take<u32>(SN / I->codingBlockSize + S + 1);
     *total = alignUp(c.off, 256);
+}
+
+// Capacities of one encode call.  The instance promises streamCountMax
+// streams of elemCountPerStreamMax symbols; internally a call may split the
+// same symbol budget over up to capStreams streams of any sizes.
+void sizeCapacities(cc_instance* I) {
+    const u32 S = I->streamCountMax;
+    const u64 SN = u64(S) * I->elemCountPerStreamMax;
+    I->capStreams = std::max<u32>(S, 1024u);
+    I->capTables = 2 * I->capStreams;
+    I->capCompact = SN;
+    I->capTiles = u32(ceilDiv(SN, kRleTile) + I->capStreams);
+    I->capBlocks = u32(2 * (ceilDiv(SN, I->codingBlockSize) + I->capStreams));
+    // histograms: at most 2^log2Max bins for symbols and 256 for zero counts
+    // per stream of a full call
+    I->capHist = u64(S) * I->bins + u64(S) * std::min<u32>(256u, I->bins);
+    I->capLeaves = std::min<u64>(I->capHist, 2 * SN + I->capTables);
+    const u64 symBits = I->log2Max > 16 ? 24 : 16;
+    I->capHdr = u64(I->capTables) * (headerWordsFor(0, I->log2Max) + 1) + ceilDiv(I->capLeaves * symBits, 32);
+    // output: headers + per-segment words + codewords (a Huffman code is never
+    // longer than a fixed-length one: log2Max bits per symbol, 8 per zero
+    // count) + 16-bit offsets
+    I->outWordsMax = I->capHdr + 16ull * I->capStreams + ceilDiv(SN * (I->log2Max + 8), 32) +
+                     ceilDiv(SN, I->codingBlockSize) + 64;
+    I->hostRingBytes = alignUp(std::max<u64>(u64(I->capStreams) * sizeof(EncStreamDev) + 64 +
+                                                 u64(I->capTables) * sizeof(EncTableDev),
+                                             2ull * S * sizeof(DecTableDesc) + u64(S) * sizeof(DecStreamDesc) + 64) +
+                                   4096,
+                               4096);
 }
 
 }  // namespace
@@ -184,7 +198,12 @@ int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMa
     I->blocksMax = u32(ceilDiv(elemCountPerStreamMax, codingBlockSize));
     I->leavesMax = std::max<u32>(1u, std::min<u32>(I->bins, elemCountPerStreamMax));
     I->hdrWordsMax = headerWordsFor(I->leavesMax, log2Max);
-    I->outWordsMax = u64(streamCountMax) * segmentWordsMax(elemCountPerStreamMax, codingBlockSize, log2Max, I->hdrWordsMax);
+    if (u64(streamCountMax) * elemCountPerStreamMax > (1ull << 36)) {
+        delete I;
+        setError("streamCountMax * elemCountPerStreamMax must be <= 2^36");
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    sizeCapacities(I);
 
     size_t bytes = 0;
     layoutArena(I, nullptr, &bytes);
@@ -193,9 +212,6 @@ int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMa
     layoutArena(I, I->arena, &bytes);
     cudaMemset(I->arena, 0, bytes);
 
-    u32 T = 2 * streamCountMax;
-    I->hostRingBytes = alignUp(u64(T) * sizeof(DecTableDesc) + u64(streamCountMax) * sizeof(DecStreamDesc) +
-                               u64(streamCountMax) * sizeof(EncStream) + 4096, 4096);
     for (int i = 0; i < cc_instance::kRing; ++i) {
         if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostRing[i]), I->hostRingBytes, cudaHostAllocDefault)) != cudaSuccess) {
             cc_destroy_instance(I);
@@ -204,7 +220,7 @@ int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMa
         cudaEventCreateWithFlags(&I->ringEvent[i], cudaEventDisableTiming);
         cudaEventRecord(I->ringEvent[i], 0);
     }
-    I->hostDownBytes = alignUp(u64(streamCountMax) * sizeof(SegmentLayout) + 256, 4096);
+    I->hostDownBytes = alignUp(u64(I->capStreams) * sizeof(SegmentLayout) + 256, 4096);
     if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostDown), I->hostDownBytes, cudaHostAllocDefault)) != cudaSuccess) {
         cc_destroy_instance(I);
         return cudaFail(e, "cudaHostAlloc(down)");

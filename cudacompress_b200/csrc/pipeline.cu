@@ -32,9 +32,63 @@ u64 cube(u64 a, u64 b, u64 c) { return a * b * c; }
 
 }  // namespace
 
-static int copyWords(cc_instance* I, u32* dst, u64 cap, u64 at, u64 words) {
-    if (at + words > cap) { setError("output capacity %llu words too small", (unsigned long long)cap); return CC_ERR_CAPACITY; }
-    if (words) CC_TRY_CUDA(cudaMemcpyAsync(dst + at, I->out, words * 4, cudaMemcpyDeviceToDevice, I->stream), "copy stream");
+// One reference encode call of a pipeline: `count` streams from `first`.
+struct EncGroup {
+    u32 first, count;
+};
+
+// Encodes the groups back to back into dWords (word aligned segments; the
+// reference's BitStream is word aligned at every group start here), batching
+// as many groups per device call as the instance's symbol and stream budget
+// allows.  A batch whose histograms exceed the instance's table capacity is
+// redone one group per call (the capacity every instance guarantees).
+static int encodeGroups(cc_instance* I, const std::vector<EncStream>& streams, const std::vector<EncGroup>& groups,
+                        u32* dWords, u64 cap, u64* wordsOut) {
+    u64 at = 0;
+    size_t g = 0;
+    while (g < groups.size()) {
+        // greedy batch [g, h)
+        size_t h = g;
+        u64 compact = 0, tiles = 0, blocks = 0, nStreams = 0;
+        while (h < groups.size()) {
+            u64 c2 = compact, t2 = tiles, b2 = blocks;
+            for (u32 i = 0; i < groups[h].count; ++i) {
+                const EncStream& e = streams[groups[h].first + i];
+                const u64 nb = ceilDiv(e.n, I->codingBlockSize);
+                if (e.kind == KIND_RLHUFF) c2 += e.n;
+                t2 += ceilDiv(e.n, kRleTile);
+                b2 += e.kind == KIND_RLHUFF ? 2 * nb : nb;
+            }
+            const u64 s2 = nStreams + groups[h].count;
+            const bool fits = s2 <= I->capStreams && c2 <= I->capCompact && t2 <= I->capTiles && b2 <= I->capBlocks;
+            if (!fits && h > g) break;
+            compact = c2; tiles = t2; blocks = b2; nStreams = s2;
+            ++h;
+            if (!fits) break;   // a single group that does not fit reports the error below
+        }
+        const u32 first = groups[g].first;
+        const u32 count = groups[h - 1].first + groups[h - 1].count - first;
+        std::vector<EncStream> batch(streams.begin() + first, streams.begin() + first + count);
+        for (EncStream& e : batch) e.groupFirst -= first;
+        u64 words = 0;
+        int rc = encodeDevice(I, batch.data(), count, EncOutput{dWords + at, cap - at}, false, &words);
+        if (rc == CC_ERR_CAPACITY && h - g > 1) {
+            for (size_t k = g; k < h; ++k) {
+                std::vector<EncStream> one(streams.begin() + groups[k].first,
+                                           streams.begin() + groups[k].first + groups[k].count);
+                for (EncStream& e : one) e.groupFirst -= groups[k].first;
+                if ((rc = encodeDevice(I, one.data(), groups[k].count, EncOutput{dWords + at, cap - at}, false, &words)))
+                    return rc;
+                at += words;
+            }
+        } else if (rc) {
+            return rc;
+        } else {
+            at += words;
+        }
+        g = h;
+    }
+    *wordsOut = at;
     return CC_OK;
 }
 
@@ -106,25 +160,19 @@ int cc_compress_volume_float(cc_instance* I, const float* vol, uint32_t nx, uint
             next += cube(hx, hy, hz);
         }
     }
-    // entropy coding in stream order
-    u64 at = 0, words = 0;
-    EncStream es{};
-    es.in = lp;
-    es.n = u32(cube(lx, ly, lz));
-    es.groupFirst = 0;
-    es.groupSize = 1;
-    if ((rc = encodeDevice(I, KIND_HUFF, &es, 1, false, &words))) return rc;
-    if ((rc = copyWords(I, dWords, cap, at, words))) return rc;
-    at += words;
+    // entropy coding in stream order: LP (encodeHuff), then levels coarse -> fine (encodeRLHuff of 7 bands)
+    std::vector<EncStream> es;
+    std::vector<EncGroup> groups;
+    es.push_back(EncStream{lp, u32(cube(lx, ly, lz)), 0, 0, 1, KIND_HUFF});
+    groups.push_back(EncGroup{0, 1});
     for (int l = int(L) - 1; l >= 0; --l) {
-        EncStream s7[7];
-        for (u32 i = 0; i < 7; ++i) {
-            s7[i] = EncStream{bands[l][i], u32(cube(nx >> (l + 1), ny >> (l + 1), nz >> (l + 1))), 0, 0, 7};
-        }
-        if ((rc = encodeDevice(I, KIND_RLHUFF, s7, 7, false, &words))) return rc;
-        if ((rc = copyWords(I, dWords, cap, at, words))) return rc;
-        at += words;
+        const u32 first = u32(es.size());
+        for (u32 i = 0; i < 7; ++i)
+            es.push_back(EncStream{bands[l][i], u32(cube(nx >> (l + 1), ny >> (l + 1), nz >> (l + 1))), 0, first, 7, KIND_RLHUFF});
+        groups.push_back(EncGroup{first, 7});
     }
+    u64 at = 0;
+    if ((rc = encodeGroups(I, es, groups, dWords, cap, &at))) return rc;
     CC_TRY_CUDA(cudaStreamSynchronize(st), "compressVolumeFloat");
     if (at * 32 > 0xffffffffull) { setError("compressVolumeFloat: stream exceeds 2^32 bits"); return CC_ERR_CAPACITY; }
     *bitSize = u32(at * 32);
@@ -250,20 +298,20 @@ int cc_compress_heightfield(cc_instance* I, const int16_t* img, uint32_t nx, uin
     u16* lp = next;
     rc = cc_symbolize(lp, coef[L - 1], lx, ly, 1, nx >> (L - 1), 0, st);
     if (rc) return rc;
-    u64 at = 0, words = 0;
-    EncStream es{lp, lx * ly, 0, 0, 1};
-    if ((rc = encodeDevice(I, KIND_HUFF, &es, 1, false, &words))) return rc;
-    if ((rc = copyWords(I, dWords, cap, at, words))) return rc;
-    at += words;
+    std::vector<EncStream> es;
+    std::vector<EncGroup> groups;
+    es.push_back(EncStream{lp, lx * ly, 0, 0, 1, KIND_HUFF});
+    groups.push_back(EncGroup{0, 1});
     for (int l = int(L) - 1; l >= 0; --l) {
         const u32 n = (nx >> (l + 1)) * (ny >> (l + 1));
-        EncStream s3[3];
-        for (u32 i = 0; i < 3; ++i) s3[i] = EncStream{bands[l][i], n, 0, 0, 3};
-        if ((rc = encodeDevice(I, KIND_RLHUFF, s3, 3, false, &words))) return rc;
-        if ((rc = copyWords(I, dWords, cap, at, words))) return rc;
-        at += words;
+        const u32 first = u32(es.size());
+        for (u32 i = 0; i < 3; ++i) es.push_back(EncStream{bands[l][i], n, 0, first, 3, KIND_RLHUFF});
+        groups.push_back(EncGroup{first, 3});
     }
+    u64 at = 0;
+    if ((rc = encodeGroups(I, es, groups, dWords, cap, &at))) return rc;
     CC_TRY_CUDA(cudaStreamSynchronize(st), "compressHeightfield");
+    if (at * 32 > 0xffffffffull) { setError("compressHeightfield: stream exceeds 2^32 bits"); return CC_ERR_CAPACITY; }
     *bitSize = u32(at * 32);
     return CC_OK;
 }
