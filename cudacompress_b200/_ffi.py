@@ -47,6 +47,7 @@ _SIGS = {
     "cc_dwt_float_inverse": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
     "cc_dwt_float_inverse_from_symbols": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_float, c_int, c_int, c_int,
                                                   c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_dwt_float_forward_static": (c_int, [c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
     "cc_dwt_int_forward": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
     "cc_dwt_int_inverse": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
     "cc_quantize_to_symbols": (c_int, [c_vp, c_int, c_vp, c_u32, c_u32, c_u32, c_float, c_u32, c_u32, c_int, c_vp]),

@@ -273,6 +273,37 @@ static bool checkSizes(int sx, int sy, int sz, const char* what) {
     return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Fixed scratch of cc_dwt_float_forward_static: the two intermediate volumes
+// of the forward transform live in this file-scope device array instead of
+// caller buffers, for callers that cannot allocate device memory (code that
+// runs while a host allocator lock is held, inside a stream capture, or under
+// a host application that owns the device's memory pool).  Every GPU that
+// loads the library holds these 8 MiB until the process exits.
+// ---------------------------------------------------------------------------
+constexpr u64 kStaticScratchFloats = u64(1) << 20;   // per intermediate volume (4 MiB)
+static __device__ __align__(256) float g_dwtScratch[2 * kStaticScratchFloats];
+
+// Device address of g_dwtScratch per device, resolved once with that device
+// current (a host reference to g_dwtScratch is a host-side stand-in, not a
+// device address).
+constexpr int kMaxDevices = 64;
+static float* g_dwtScratchDev[kMaxDevices] = {};
+
+static int dwtScratchFor(int device, float** out) {
+    if (device < 0 || device >= kMaxDevices) { setError("dwtFloatForwardStatic: device %d out of range", device); return CC_ERR_INVALID_ARGUMENT; }
+    float* p = __atomic_load_n(&g_dwtScratchDev[device], __ATOMIC_ACQUIRE);
+    if (!p) {
+        void* addr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&addr, g_dwtScratch);
+        if (e != cudaSuccess) return cudaFail(e, "dwtFloatForwardStatic: cudaGetSymbolAddress");
+        p = static_cast<float*>(addr);
+        __atomic_store_n(&g_dwtScratchDev[device], p, __ATOMIC_RELEASE);
+    }
+    *out = p;
+    return CC_OK;
+}
+
 }  // namespace ccb
 
 using namespace ccb;
@@ -391,6 +422,51 @@ int cc_dwt_int_inverse(int16_t* dst, int16_t* buf, const int16_t* src, int sx, i
     liftPass<true>(buf, ySrc, sx, sy, sz, 1, srcRow, srcSlice, srcRow, srcSlice, st);
     liftPass<true>(dst, buf, sx, sy, sz, 0, srcRow, srcSlice, dstRow, dstSlice, st);
     CC_TRY_CUDA(cudaGetLastError(), "dwtIntInverse");
+    return CC_OK;
+}
+
+
+// Forward float DWT with its intermediates in the library's fixed device
+// scratch (no counterpart in the reference).  Same arguments and results as
+// cc_dwt_float_forward without the two buffers; runs on the current device.
+// The first call on a device resolves the scratch address there (set-up);
+// make that first call before any stream capture.  All calls share one
+// scratch per device and it keeps the last call's contents: calls that
+// overlap on the GPU (other streams, other threads) race.  Nothing in it has
+// to start at zero: each pass writes every element the next pass reads.
+int cc_dwt_float_forward_static(float* dst, const float* src, int sx, int sy, int sz, int ch, int dstRow,
+                                int dstSlice, int srcRow, int srcSlice, void* stream) {
+    if (!checkSizes(sx, sy, sz, "dwtFloatForwardStatic")) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx * ch;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    if (dstRow < sx || (sz > 1 && dstSlice < sy * dstRow)) {
+        setError("dwtFloatForwardStatic: destination pitches smaller than the volume");
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    // extent of one intermediate volume (it uses the destination's pitches)
+    const u64 extent = u64(sz - 1) * u64(dstSlice) + u64(sy - 1) * u64(dstRow) + u64(sx);
+    if (extent > kStaticScratchFloats) {
+        setError("dwtFloatForwardStatic: volume needs %llu scratch floats, the fixed scratch holds %llu",
+                 (unsigned long long)extent, (unsigned long long)kStaticScratchFloats);
+        return CC_ERR_CAPACITY;
+    }
+    int device = -1;
+    CC_TRY_CUDA(cudaGetDevice(&device), "dwtFloatForwardStatic: cudaGetDevice");
+    float* scratch = nullptr;
+    const int rc = dwtScratchFor(device, &scratch);
+    if (rc) return rc;
+    float* buf1 = scratch;
+    float* buf2 = scratch + kStaticScratchFloats;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool do3D = sz > 1;
+    rowPass<float, float, false>(buf1, src, sx, sy, sz, ch, srcRow, srcSlice, 1, dstRow, dstSlice, st);
+    float* yDst = do3D ? buf2 : dst;
+    colPass<false>(yDst, pitchLoad(buf1, 1, dstRow, dstSlice), sx, sy, sz, 1, dstRow, dstSlice, st);
+    if (do3D) colPass<false>(dst, pitchLoad(buf2, 2, dstRow, dstSlice), sx, sy, sz, 2, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatForwardStatic");
     return CC_OK;
 }
 

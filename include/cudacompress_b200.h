@@ -137,6 +137,19 @@ int cc_dwt_float_inverse_from_symbols(float* d_dst, float* d_buf2, float* d_buf1
                                       int size_x, int size_y, int size_z, int dst_channel_count,
                                       int dst_row_pitch, int dst_slice_pitch, int lowpass_row_pitch,
                                       int lowpass_slice_pitch, void* stream);
+/* No counterpart in the reference (whose dwtFloat{2D,3D}Forward take two
+ * caller-allocated buffers): cc_dwt_float_forward with both intermediates in
+ * a fixed 8 MiB device array inside this library, for callers that cannot
+ * allocate device memory (under a host allocator lock, inside a stream
+ * capture, or in a host application that owns the device memory pool).
+ * Limit: (size_z-1)*dst_slice_pitch + (size_y-1)*dst_row_pitch + size_x
+ * <= 2^20 floats (e.g. 128 x 128 x 64, or 1024 x 1024 in 2D); larger volumes
+ * are rejected with CC_ERR_CAPACITY.  Runs on the current device; its first
+ * call there resolves the array's device address (make it before any stream
+ * capture).  Calls share the array: calls that overlap on the GPU race. */
+int cc_dwt_float_forward_static(float* d_dst, const float* d_src, int size_x, int size_y, int size_z,
+                                int src_channel_count, int dst_row_pitch, int dst_slice_pitch, int src_row_pitch,
+                                int src_slice_pitch, void* stream);
 int cc_dwt_int_forward(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int size_x, int size_y, int size_z,
                        int dst_row_pitch, int dst_slice_pitch, int src_row_pitch, int src_slice_pitch, void* stream);
 int cc_dwt_int_inverse(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int size_x, int size_y, int size_z,
