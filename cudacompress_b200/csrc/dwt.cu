@@ -159,22 +159,39 @@ __global__ void __launch_bounds__(256) k_firCols(float* __restrict__ dst, Load l
 __device__ __forceinline__ i16 div2(i16 v) { v = i16(v + ((v >= 0) ? 1 : -1)); return i16(v / 2); }
 __device__ __forceinline__ i16 div4(i16 v) { v = i16(v + ((v >= 0) ? 2 : -2)); return i16(v / 4); }
 
-// Lifts the samples in s[0 .. len) (s[k] <-> position base + k); forward: s
-// holds natural samples; inverse: s holds the interleaved L/H signal.
-// Positions whose neighbours are outside s are not valid afterwards.
+// Lifts the samples in s[0 .. len) (s[k] <-> position base + k, positions
+// outside [0, na) hold mirrored samples); forward: s holds natural samples;
+// inverse: s holds the interleaved L/H signal.  A position is lifted when the
+// sample it mirrors lies below liftEnd.  Positions whose neighbours are
+// outside s are not valid afterwards.
 template <bool kInverse>
-__device__ __forceinline__ void liftLine(i16* s, int len, int base) {
+__device__ __forceinline__ void liftLine(i16* s, int len, int base, int na, int liftEnd) {
     if (!kInverse) {
         for (int k = 1; k + 1 < len; ++k)
-            if (((base + k) & 1) == 1) s[k] = i16(s[k] - div2(i16(s[k - 1] + s[k + 1])));
+            if (((base + k) & 1) == 1 && mirrorIdx(base + k, na) < liftEnd)
+                s[k] = i16(s[k] - div2(i16(s[k - 1] + s[k + 1])));
         for (int k = 2; k + 2 < len; ++k)
-            if (((base + k) & 1) == 0) s[k] = i16(s[k] + div4(i16(s[k - 1] + s[k + 1])));
+            if (((base + k) & 1) == 0 && mirrorIdx(base + k, na) < liftEnd)
+                s[k] = i16(s[k] + div4(i16(s[k - 1] + s[k + 1])));
     } else {
         for (int k = 1; k + 1 < len; ++k)
-            if (((base + k) & 1) == 0) s[k] = i16(s[k] - div4(i16(s[k - 1] + s[k + 1])));
+            if (((base + k) & 1) == 0 && mirrorIdx(base + k, na) < liftEnd)
+                s[k] = i16(s[k] - div4(i16(s[k - 1] + s[k + 1])));
         for (int k = 2; k + 2 < len; ++k)
-            if (((base + k) & 1) == 1) s[k] = i16(s[k] + div2(i16(s[k - 1] + s[k + 1])));
+            if (((base + k) & 1) == 1 && mirrorIdx(base + k, na) < liftEnd)
+                s[k] = i16(s[k] + div2(i16(s[k - 1] + s[k + 1])));
     }
+}
+
+// DWTInt.cu:111-135 with DWTIntKernels.cui:104-200 (inverse DWTInt.cu:271-310,
+// DWTIntKernels.cui:596-780): the reference's X pass lifts whole 256-sample
+// blocks, then the remainder in 32-sample blocks of which its predict/update
+// loops cover only whole pairs.  With an odd count of remainder blocks the
+// last one is not lifted (its samples are only split into L and H); results
+// stay identical to the reference by lifting only below this position.
+static int intDwtXLiftEnd(int n) {
+    const int done = n / 256 * 256, rest = n - done, blocks = (rest + 31) / 32;
+    return std::min(n, done + 64 * (blocks / 2));
 }
 
 // Generic int lifting pass along one axis: block (32, 8): 32 adjacent lines of
@@ -182,8 +199,8 @@ __device__ __forceinline__ void liftLine(i16* s, int len, int base) {
 // are rows and the block covers 32 rows), kColTile outputs per line.
 template <bool kInverse>
 __global__ void __launch_bounds__(256) k_liftAxis(i16* __restrict__ dst, const i16* __restrict__ src, int nLines,
-                                                  int na, int sLine, int sAxis, int sOther, int dLine, int dAxis,
-                                                  int dOther) {
+                                                  int na, int liftEnd, int sLine, int sAxis, int sOther, int dLine,
+                                                  int dAxis, int dOther) {
     __shared__ i16 s[32][kColTile + 8];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int line = blockIdx.x * 32 + tx;
@@ -204,7 +221,7 @@ __global__ void __launch_bounds__(256) k_liftAxis(i16* __restrict__ dst, const i
     if (line >= nLines) return;
     if (ty == 0) {
         int len = min(kColTile + 8, na + 4 - (a0 - 4));
-        liftLine<kInverse>(s[tx], len, a0 - 4);
+        liftLine<kInverse>(s[tx], len, a0 - 4, na, liftEnd);
     }
     __syncthreads();
     for (int k = ty; k < kColTile; k += 8) {
@@ -264,7 +281,10 @@ static void liftPass(i16* dst, const i16* src, int nx, int ny, int nz, int axis,
         dLine = 1; dAxis = dstSlice; dOther = dstRow;
     }
     dim3 g(unsigned(ceilDiv(nLines, 32)), unsigned(ceilDiv(na, kColTile)), nc);
-    k_liftAxis<kInverse><<<g, dim3(32, 8), 0, st>>>(dst, src, nLines, na, sLine, sAxis, sOther, dLine, dAxis, dOther); countLaunch();
+    const int liftEnd = axis == 0 ? intDwtXLiftEnd(na) : na;
+    k_liftAxis<kInverse><<<g, dim3(32, 8), 0, st>>>(dst, src, nLines, na, liftEnd, sLine, sAxis, sOther, dLine, dAxis,
+                                                    dOther);
+    countLaunch();
 }
 
 static bool checkSizes(int sx, int sy, int sz, const char* what) {

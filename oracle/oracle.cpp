@@ -604,8 +604,20 @@ static void dwtFloat(const T* src, T* dst, long nx, long ny, long nz, bool inver
 static inline i16 div2(i16 v) { v = i16(v + ((v >= 0) ? 1 : -1)); return i16(v / 2); }
 static inline i16 div4(i16 v) { v = i16(v + ((v >= 0) ? 2 : -2)); return i16(v / 4); }
 
+// DWTInt.cu:111-135 with DWTIntKernels.cui:104-200 (and the inverse,
+// DWTInt.cu:271-310, DWTIntKernels.cui:596-780): the X pass lifts whole
+// 256-sample blocks, then the remainder in 32-sample blocks of which the
+// kernel's predict/update loops cover only whole pairs (blockCount/2).  With
+// an odd count of remainder blocks the last one is not lifted: its samples
+// are only split into the L and H halves.  Y and Z passes lift every sample.
+static long xLiftEnd(long n) {
+    long done = n / 256 * 256, rest = n - done, blocks = (rest + 31) / 32;
+    return std::min(n, done + 64 * (blocks / 2));
+}
+
 static void liftAxis(const i16* src, i16* dst, long nx, long ny, long nz, int axis, bool inverse) {
     long n = axis == 0 ? nx : axis == 1 ? ny : nz;
+    const long end = axis == 0 ? xLiftEnd(n) : n;   // samples at or beyond `end` stay unlifted
     long stride = axis == 0 ? 1 : axis == 1 ? nx : nx * ny;
     long h = n / 2;
     long lines = nx * ny * nz / n;
@@ -620,22 +632,22 @@ static void liftAxis(const i16* src, i16* dst, long nx, long ny, long nz, int ax
         else base = li;
         if (!inverse) {
             for (long k = 0; k < n; ++k) s[k] = src[base + k * stride];
-            for (long k = 1; k < n; k += 2) {
+            for (long k = 1; k < end; k += 2) {
                 i16 r = (k + 1 < n) ? s[k + 1] : s[n - 2];
                 s[k] = i16(s[k] - div2(i16(s[k - 1] + r)));
             }
-            for (long k = 0; k < n; k += 2) {
+            for (long k = 0; k < end; k += 2) {
                 i16 l = (k > 0) ? s[k - 1] : s[1];
                 s[k] = i16(s[k] + div4(i16(l + s[k + 1])));
             }
             for (long k = 0; k < n; ++k) dst[base + ((k & 1) ? (h + k / 2) : (k / 2)) * stride] = s[k];
         } else {
             for (long k = 0; k < n; ++k) s[k] = src[base + ((k & 1) ? (h + k / 2) : (k / 2)) * stride];
-            for (long k = 0; k < n; k += 2) {
+            for (long k = 0; k < end; k += 2) {
                 i16 l = (k > 0) ? s[k - 1] : s[1];
                 s[k] = i16(s[k] - div4(i16(l + s[k + 1])));
             }
-            for (long k = 1; k < n; k += 2) {
+            for (long k = 1; k < end; k += 2) {
                 i16 r = (k + 1 < n) ? s[k + 1] : s[n - 2];
                 s[k] = i16(s[k] + div2(i16(s[k - 1] + r)));
             }

@@ -85,6 +85,35 @@ int ref_encode(void* p, int kind, int symBytes, void* dSymbols, uint32_t S, uint
     return 0;
 }
 
+// As ref_encode with stream i at dSymbols + i * stride elements: encodeHuff
+// pads each input stream with 0xFFFF up to a multiple of 8 symbols
+// (Histogram.cu:90-106), so the generator leaves that slack between streams.
+int ref_encode_strided(void* p, int kind, int symBytes, void* dSymbols, uint32_t S, uint32_t n, uint32_t stride,
+                       uint32_t* words, uint32_t cap, uint32_t* bitSize, uint32_t* bitPos) {
+    Instance* inst = static_cast<Instance*>(p);
+    std::vector<uint> v(words, words + (*bitSize + 31) / 32);
+    BitStream bs(&v);
+    bs.setBitSize(*bitSize);
+    bs.setBitPosition(*bitPos);
+    bool ok;
+    if (symBytes == 2) {
+        std::vector<Symbol16*> s(S);
+        for (uint32_t i = 0; i < S; ++i) s[i] = static_cast<Symbol16*>(dSymbols) + size_t(i) * stride;
+        ok = kind == 0 ? encodeRLHuff(inst, bs, s.data(), S, n) : encodeHuff(inst, bs, s.data(), S, n);
+    } else {
+        std::vector<Symbol32*> s(S);
+        for (uint32_t i = 0; i < S; ++i) s[i] = static_cast<Symbol32*>(dSymbols) + size_t(i) * stride;
+        ok = kind == 0 ? encodeRLHuff(inst, bs, s.data(), S, n) : encodeHuff(inst, bs, s.data(), S, n);
+    }
+    cudaDeviceSynchronize();
+    if (!ok) return -1;
+    if (v.size() > cap) return -2;
+    std::memcpy(words, v.data(), v.size() * 4);
+    *bitSize = bs.getBitSize();
+    *bitPos = bs.getBitPosition();
+    return 0;
+}
+
 void ref_dwt_float3d_fwd(float* dst, float* buf2, float* buf1, const float* src, int nx, int ny, int nz) {
     util::dwtFloat3DForward(dst, buf2, buf1, src, nx, ny, nz);
     cudaDeviceSynchronize();
