@@ -16,7 +16,7 @@
 #include <cstring>
 
 #include "capi_internal.cuh"
-#include "huffman_build.cuh"
+#include "table_build.cuh"
 
 namespace ccb {
 
@@ -402,9 +402,11 @@ __global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
 
 // ---------------------------------------------------------------------------
 // Table construction: one block per table, all tables of the call at once.
-// Leaf gathering, canonical codes and serialization are block parallel; the
-// heap merge, depths and the sort run in thread 0 with the tie-breaking of
-// huffman_build.cuh, on shared memory when the table fits.
+// Leaf gathering, depths, the sort (an exact warp-parallel replay of
+// std::sort), canonical codes and serialization are block parallel; the heap
+// merge runs in one thread on shared memory (table_build.cuh).  Tables with
+// more leaves than the shared-memory builder holds run sequentially on
+// global memory (huffman_build.cuh).
 // ---------------------------------------------------------------------------
 constexpr u32 kBuildThreads = 256;
 
@@ -428,6 +430,8 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     __shared__ u32 sScan[40];
     __shared__ u32 sMax, sMaxLen, sAllEmpty;
     __shared__ u32 lenCount[32], firstIndex[33], firstCode[33];
+    __shared__ tb::Seg sSegA[tb::kMaxSegs], sSegB[tb::kMaxSegs];
+    __shared__ int sSegCount[4];
     if (threadIdx.x == 0) { sMax = 0; sAllEmpty = 1; }
     if (blockFailed(p)) return;
     const u32 t = blockIdx.x;
@@ -454,13 +458,21 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     // i that word is the low half of a device pointer when 2+2i < S (nonzero),
     // else the all-zero run-length scan output.
     const bool quirkLeaf = isZc && sAllEmpty && (2u + 2u * (td.stream - es.groupFirst) < es.groupSize);
-    // 2. leaves in symbol order
+    // 2. leaves in symbol order: heap keys go straight to the shared-memory
+    //    heap (1-based, see table_build.cuh) when the table fits
     u32* leafSym = p.leafSymWork + meta.leafOff;
     u64* heapG = p.leafWork + meta.leafOff;
+    u64* H = reinterpret_cast<u64*>(dyn);                                        // [heapCap + 2]
+    u32* parentS = reinterpret_cast<u32*>(dyn + sizeof(u64) * (p.heapCap + 2));  // [2 heapCap]
+    u32* orderS = parentS + 2 * p.heapCap;                                       // [heapCap]
     u32 L;
     if (quirkLeaf) {
-        if (threadIdx.x == 0) { leafSym[0] = 0; heapG[0] = (u64(1) << 32) | 0u; }
         L = 1;
+        if (threadIdx.x == 0) {
+            leafSym[0] = 0;
+            const u64 key = (u64(1) << 32) | 0u;
+            if (L <= p.heapCap) H[1] = key; else heapG[0] = key;
+        }
     } else if (count == 0) {
         L = 0;
     } else {
@@ -472,48 +484,64 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         u32 tot;
         u32 off = blockExclusiveSum<kBuildThreads>(c, sScan, &tot);
         L = tot;
+        const bool toSmem = L <= p.heapCap;
         const bool quirk65535 = p.symBytes == 2 && p.bins == 65536u && symbolMax == 65535u;
         for (u32 b = b0; b < b1; ++b) {
             u32 h = hist[b];
             if (h) {
                 if (quirk65535 && b == 65535u) h += count & 1u;   // HistogramKernels.cui:165,200 padding word
                 leafSym[off] = b;
-                heapG[off] = (u64(h) << 32) | off;
+                const u64 key = (u64(h) << 32) | off;
+                if (toSmem) H[off + 1] = key; else heapG[off] = key;
                 ++off;
             }
         }
     }
-    __syncthreads();
     const bool inSmem = L <= p.heapCap;
-    u64* heap = inSmem ? reinterpret_cast<u64*>(dyn) : heapG;
-    u32* order = inSmem ? reinterpret_cast<u32*>(dyn + sizeof(u64) * p.heapCap) : p.orderWork + meta.leafOff;
-    u32* parent = inSmem ? reinterpret_cast<u32*>(dyn + (sizeof(u64) + sizeof(u32)) * p.heapCap)
-                         : p.parentWork + 2 * meta.leafOff;
-    if (inSmem)
-        for (u32 i = threadIdx.x; i < L; i += kBuildThreads) heap[i] = heapG[i];
+    u32* order = inSmem ? orderS : p.orderWork + meta.leafOff;
+    if (threadIdx.x == 0) sMaxLen = 0;
     __syncthreads();
-    // 3. tree, depths and sort (thread 0)
-    if (threadIdx.x == 0) {
-        u32 maxLen = 0;
-        if (L >= 1) {
-            hb::buildTree(heap, parent, int(L));
-            // depths in place over the parent links (parents have larger ids)
-            const int nodes = int(2 * L - 1);
-            parent[nodes - 1] = 0;
-            for (int id = nodes - 2; id >= 0; --id) {
-                u32 d = parent[parent[id]] + 1u;
-                parent[id] = d > 255u ? 255u : d;
-            }
-            for (u32 i = 0; i < L; ++i) {
-                u32 d = parent[i];
-                maxLen = max(maxLen, d);
-                order[i] = (min(d, 31u) << 27) | i;
-            }
-            if (maxLen <= 31) hb::introsort(order, int(L), hb::LenLess());
+    // 3. tree, depths and sort
+    if (inSmem) {
+        if (threadIdx.x == 0 && L >= 2) tb::buildTree(H, parentS, int(L));
+        __syncthreads();
+        const u32 root = L >= 2 ? 2 * L - 2 : 0;
+        u32 localMax = 0;
+        for (u32 i = threadIdx.x; i < L; i += kBuildThreads) {
+            u32 d = 0, node = i;
+            while (node != root && d < 32) { node = parentS[node]; ++d; }
+            order[i] = (min(d, 31u) << 27) | i;
+            localMax = max(localMax, d);
         }
+        if (localMax) atomicMax(&sMaxLen, localMax);
+        __syncthreads();
+        if (sMaxLen <= 31) {
+            u16* lList = reinterpret_cast<u16*>(dyn);            // reuses the heap area (5 bytes per key)
+            u16* rList = lList + p.heapCap;
+            u8* mark = reinterpret_cast<u8*>(rList + p.heapCap);
+            tb::blockIntrosort<kBuildThreads>(order, int(L), lList, rList, mark, sSegA, sSegB, sSegCount);
+        }
+    } else if (threadIdx.x == 0) {
+        // tables larger than the shared-memory builder: sequential, global memory
+        u32* parent = p.parentWork + 2 * meta.leafOff;
+        u32 maxLen = 0;
+        hb::buildTree(heapG, parent, int(L));
+        const int nodes = int(2 * L - 1);
+        parent[nodes - 1] = 0;
+        for (int id = nodes - 2; id >= 0; --id) {
+            u32 d = parent[parent[id]] + 1u;
+            parent[id] = d > 255u ? 255u : d;
+        }
+        for (u32 i = 0; i < L; ++i) {
+            u32 d = parent[i];
+            maxLen = max(maxLen, d);
+            order[i] = (min(d, 31u) << 27) | i;
+        }
+        if (maxLen <= 31) hb::introsort(order, int(L), hb::LenLess());
         sMaxLen = maxLen;
-        for (int l = 0; l < 32; ++l) lenCount[l] = 0;
     }
+    if (threadIdx.x == 0)
+        for (int l = 0; l < 32; ++l) lenCount[l] = 0;
     __syncthreads();
     const u32 maxLen = sMaxLen;
     if (maxLen > 31) {
@@ -856,7 +884,7 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) { SectionTimer t(I, "enc.rle_write_hist", st); k_write<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
-    const size_t buildSmem = std::max<size_t>(16, size_t(p.heapCap) * (sizeof(u64) + 3 * sizeof(u32)));
+    const size_t buildSmem = sizeof(u64) * (p.heapCap + 2) + 3 * sizeof(u32) * size_t(p.heapCap);
     CC_TRY_CUDA(cudaFuncSetAttribute(k_tableBuild, cudaFuncAttributeMaxDynamicSharedMemorySize, int(buildSmem)), "tableBuild smem");
     { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
     if (p.totalBlocks) {
