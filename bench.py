@@ -46,6 +46,9 @@ WORKLOADS = {
     "volume-128": dict(n=128, comps=1, levels=3, q0=0.01, seeds=(1000,), modes=512, kmax=32,
                        desc="128^3 float32 k^-5/3 field, 3-level CDF 9/7, q0=0.01*std, RLE+Huffman cb=128"),
 }
+WORKLOADS["bricks-4096"] = dict(count=4096, levels=2, seed=1005, plain_sample=256,
+                                desc="4096 float32 bricks, edges {16,24,32,48,64} per axis, q0 log-uniform "
+                                     "[0.002,0.05]*std, 2-level CDF 9/7, RLE+Huffman cb=128, per-brick tables")
 FALLBACK_HBM_GBS = 6650.0
 L2_BYTES = 126 * 1024 * 1024
 
@@ -213,9 +216,13 @@ def section_bytes(name, wl, coded_bytes, counts):
     lp = vols[-1] // 8
     m = {
         "pipe.dwt_forward": sum(8 * v for v in vols) * C,
+        "batch.dwt_forward": sum(8 * v for v in vols) * C,
+        "batch.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
+        "batch.quantize": (hp + lp) * 6 * C,
         "pipe.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
         "pipe.quantize": (hp + lp) * 6 * C,
         "enc.rle_summary": hp * 2 * C,
+        "enc.summary": (hp + lp) * 2 * C,
         "enc.rle_write_hist": hp * 2 * C + counts.get("compact", 0) * 4,
         "enc.histogram": lp * 2 * C,
         "enc.block_bits": (lp * C + 2 * counts.get("compact", 0)) * 2,
@@ -225,6 +232,93 @@ def section_bytes(name, wl, coded_bytes, counts):
         "dec.symbols_scatter": counts.get("compact", 0) * 4 + hp * 2 * C,
     }
     return m.get(name)
+
+
+# ---------------------------------------------------------------- bricks
+def measure_bricks(count, levels, seed, steps, warmup, plain_sample, local):
+    """Batched uneven bricks (one batch, CUDA graphs) against per-brick calls
+    of the plain codec (cc_compress_volume_float / cc_decompress_volume_float
+    one brick at a time) on the same bricks; both give the same streams and
+    reconstructions, hence the same PSNR (checked on the sampled bricks)."""
+    import torch
+    import cudacompress_b200 as cc
+    from cudacompress_b200 import fields
+    dev = torch.device("cuda", local)
+    bricks, q = fields.brick_set(count, seed)
+    vols = [torch.from_numpy(b).to(dev) for b in bricks]
+    raw = sum(b.size for b in bricks) * 4
+    inst = cc.Instance(local, 7, 32 ** 3, 128, 14)
+    batch = cc.VolumeBatch(inst, [b.shape for b in bricks], levels, [float(v) for v in q], graph=True)
+    outs = [torch.empty_like(v) for v in vols]
+    for _ in range(max(warmup, 1)):
+        batch.compress(vols)
+        batch.decompress(outs)
+    batch.status()
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0.record()
+    for _ in range(steps):
+        batch.compress(vols)
+        batch.decompress(outs)
+    e0.record()
+    torch.cuda.synchronize()
+    batch.status()
+    batch_ms = s0.elapsed_time(e0) / steps
+    # per-brick plain path on a sample (every brick a call of its own)
+    P = min(plain_sample, count)
+    cap = cc.volume_stream_capacity_words(64, 64, 64)
+    words = torch.empty(cap, dtype=torch.int32, device=dev)
+    pout = [torch.empty_like(vols[i]) for i in range(P)]
+
+    def plain(i):
+        _, b = cc.compress_volume_float(inst, vols[i], levels, float(q[i]), words)
+        cc.decompress_volume_float(inst, pout[i], levels, float(q[i]), words, b)
+
+    for i in range(min(P, 8)):
+        plain(i)
+    torch.cuda.synchronize()
+    s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s1.record()
+    for i in range(P):
+        plain(i)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms_per_brick = s1.elapsed_time(e1) / P
+    same = all(torch.equal(pout[i].view(torch.int32), outs[i].view(torch.int32)) for i in range(P))
+    ps = [fields.psnr(bricks[i], outs[i].cpu().numpy()) for i in range(P)]
+    bits = sum(batch.read_stream(i)[1] for i in range(min(count, 64)))
+    batch.close()
+    inst.close()
+    batched_bps = count / (batch_ms / 1e3)
+    plain_bps = 1e3 / plain_ms_per_brick
+    return {
+        "bricks": count, "levels": levels, "raw_bytes": raw,
+        "batched_ms_per_pass": batch_ms, "batched_bricks_per_s": batched_bps,
+        "batched_gbs_raw": raw / (batch_ms / 1e3) / 1e9,
+        "per_brick_ms": plain_ms_per_brick, "per_brick_bricks_per_s": plain_bps,
+        "per_brick_sample": P, "speedup": batched_bps / plain_bps,
+        "same_reconstruction_on_sample": bool(same), "psnr_db_mean_sample": float(np.mean(ps)),
+        "sample_bits_per_voxel": bits / sum(bricks[i].size for i in range(min(count, 64))),
+    }
+
+
+def run_bricks(args, wl):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    sampler = ClockSampler(local)
+    r = measure_bricks(wl["count"], wl["levels"], wl["seed"], args.steps, args.warmup, wl["plain_sample"], local)
+    clocks = sampler.stop()
+    ms = r["batched_ms_per_pass"]
+    line = {
+        "metric": METRIC, "value": r["batched_gbs_raw"], "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded k^-5/3 random-phase fields)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": "replicas1",
+                   "l2": f"inputs {r['raw_bytes'] >> 20} MiB per pass"},
+        "batched_vs_per_brick": r, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------- ours
@@ -247,30 +341,35 @@ def run_ours(args, wl):
     vols_h = make_fields(wl, rank)
     vols = [torch.from_numpy(v).to(dev) for v in vols_h]
     inst = cc.Instance(local, 7, (n // 2) ** 3, 128, 14)
-    cap = cc.volume_stream_capacity_words(n, n, n)
-    words = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(C)]
+    # the batched codec: all components in one batch, the whole step replayed as CUDA graphs
+    batch = cc.VolumeBatch(inst, [v.shape for v in vols], L, [q0] * C, graph=True)
     recon = [torch.empty_like(v) for v in vols]
-    bits = [0] * C
 
     def step(ev=None):
-        for c in range(C):
-            if ev is not None:
-                ev[c][0].record()
-            _, bits[c] = cc.compress_volume_float(inst, vols[c], L, q0, words[c])
-            if ev is not None:
-                ev[c][1].record()
-            cc.decompress_volume_float(inst, recon[c], L, q0, words[c], bits[c])
-            if ev is not None:
-                ev[c][2].record()
+        if ev is not None:
+            ev[0].record()
+        batch.compress(vols)
+        if ev is not None:
+            ev[1].record()
+        batch.decompress(recon)
+        if ev is not None:
+            ev[2].record()
 
     for _ in range(max(args.warmup, 1)):
         step()
-    torch.cuda.synchronize()
-    # quality (not timed)
+    batch.status()
+    # quality and parity (not timed): each batch stream equals the plain codec's
     psnr = [fields.psnr(vols_h[c], recon[c].cpu().numpy()) for c in range(C)]
-    coded_bytes = sum(b // 8 for b in bits)
+    streams = [batch.read_stream(c) for c in range(C)]
+    coded_bytes = sum(b // 8 for _, b in streams)
+    cap = cc.volume_stream_capacity_words(n, n, n)
+    plain_words = torch.empty(cap, dtype=torch.int32, device=dev)
+    _, pbits = cc.compress_volume_float(inst, vols[0], L, q0, plain_words)
+    torch.cuda.synchronize()
+    same_as_plain = pbits == streams[0][1] and np.array_equal(
+        plain_words[: (pbits + 31) // 32].cpu().numpy().view(np.uint32), streams[0][0])
     # timed device-resident region
-    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(C)] for _ in range(args.steps)]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
         dist.barrier()
@@ -284,11 +383,12 @@ def run_ours(args, wl):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = cc.lib().cc_kernel_launches() - launches0
+    batch.status()
     if dist:
         dist.barrier()
     ms = start.elapsed_time(end) / args.steps
-    enc_ms = sum(evs[k][c][0].elapsed_time(evs[k][c][1]) for k in range(args.steps) for c in range(C)) / args.steps
-    dec_ms = sum(evs[k][c][1].elapsed_time(evs[k][c][2]) for k in range(args.steps) for c in range(C)) / args.steps
+    enc_ms = sum(evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)) / args.steps
+    dec_ms = sum(evs[k][1].elapsed_time(evs[k][2]) for k in range(args.steps)) / args.steps
     if dist:
         t = torch.tensor([ms, enc_ms, dec_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -296,27 +396,44 @@ def run_ours(args, wl):
     raw_step = C * n ** 3 * 4
     value = world * raw_step / (ms / 1e3) / 1e9
 
+    # the plain per-component path (cc_compress_volume_float / decompress), for comparison
+    plain_out = torch.empty_like(vols[0])
+
+    def plain_step():
+        for c in range(C):
+            _, b = cc.compress_volume_float(inst, vols[c], L, q0, plain_words)
+            cc.decompress_volume_float(inst, plain_out, L, q0, plain_words, b)
+
+    plain_step()
+    torch.cuda.synchronize()
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(max(1, args.steps // 2)):
+        plain_step()
+    e0.record()
+    torch.cuda.synchronize()
+    plain_ms = s0.elapsed_time(e0) / max(1, args.steps // 2)
+
     # end to end through the public API with host buffers
     pinned_in = [torch.from_numpy(v).pin_memory() for v in vols_h]
-    pinned_words = [torch.empty(cap, dtype=torch.int32).pin_memory() for _ in range(C)]
     pinned_out = [torch.empty(v.shape, dtype=torch.float32).pin_memory() for v in vols_h]
     dev_in = [torch.empty_like(v) for v in vols]
     h2d = d2h = 0
 
     def e2e_step():
         nonlocal h2d, d2h
-        h2d = d2h = 0
         for c in range(C):
             dev_in[c].copy_(pinned_in[c], non_blocking=True)
-            _, b = cc.compress_volume_float(inst, dev_in[c], L, q0, words[c])
-            nw = (b + 31) // 32
-            pinned_words[c][:nw].copy_(words[c][:nw], non_blocking=True)
-            words[c][:nw].copy_(pinned_words[c][:nw], non_blocking=True)
-            cc.decompress_volume_float(inst, recon[c], L, q0, words[c], b)
+        batch.compress(dev_in)
+        host_streams = [batch.read_stream(c) for c in range(C)]          # D2H of the streams
+        batch.load_streams([w for w, _ in host_streams], [b for _, b in host_streams])   # H2D
+        batch.decompress(recon)
+        for c in range(C):
             pinned_out[c].copy_(recon[c], non_blocking=True)
-            h2d += n ** 3 * 4 + nw * 4
-            d2h += n ** 3 * 4 + nw * 4
         torch.cuda.synchronize()
+        nw = sum(len(w) for w, _ in host_streams) * 4
+        h2d = raw_step + nw
+        d2h = raw_step + nw
 
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
@@ -340,8 +457,11 @@ def run_ours(args, wl):
     lib = cc.lib()
     lib.cc_reset_timings(inst.handle)
     lib.cc_set_timing(inst.handle, 1)
+    lib.cc_volume_batch_use_graph(batch.handle, 0)
     step()
     torch.cuda.synchronize()
+    batch.collect_timings()
+    lib.cc_volume_batch_use_graph(batch.handle, 1)
     nsec = lib.cc_timing_count(inst.handle)
     sections = {}
     for i in range(nsec):
@@ -371,6 +491,10 @@ def run_ours(args, wl):
                 "frac": step_alg / (ms / 1e3) / 1e9 / peak,
                 "algorithmic_bytes_per_step": step_alg}
 
+    bricks = None
+    if rank == 0 and world == 1 and not args.no_bricks:
+        bricks = measure_bricks(1024, 2, 1005, max(2, args.steps // 2), 2, 128, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -387,6 +511,8 @@ def run_ours(args, wl):
             "encode_gbs": world * raw_step / (enc_ms / 1e3) / 1e9,
             "decode_gbs": world * raw_step / (dec_ms / 1e3) / 1e9,
             "compression_ratio": raw_step / max(coded_bytes, 1), "psnr_db": psnr,
+            "plain_path_ms_per_step": plain_ms, "streams_identical_to_plain_codec": bool(same_as_plain),
+            "batched_vs_per_brick": bricks,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roofline, "pipeline_roofline": pipeline,
@@ -394,6 +520,7 @@ def run_ours(args, wl):
             "clocks": clocks, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
+    batch.close()
     inst.close()
     if dist:
         dist.destroy_process_group()
@@ -407,10 +534,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="vector-field-256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-bricks", action="store_true", help="skip the batched-vs-per-brick measurement")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)
+    elif args.workload.startswith("bricks"):
+        run_bricks(args, wl)
     else:
         run_ours(args, wl)
 

@@ -10,6 +10,6 @@ from .codec import (  # noqa: F401
     decompress_volume_float, dwt_float_forward, dwt_float_inverse, dwt_float_inverse_from_symbols, dwt_int_forward,
     dwt_int_inverse, encode_huff, encode_rlhuff, get_max_abs, last_error, quantize_to_short, quantize_to_symbols,
     quantize_to_symbols_roundtrip, symbolize, unquantize_from_short, unquantize_from_symbols, unsymbolize,
-    volume_stream_capacity_words)
+    volume_stream_capacity_words, VolumeBatch)
 
 __version__ = "0.1.0"

@@ -62,6 +62,17 @@ _SIGS = {
     "cc_decompress_volume_float": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_vp, c_u32]),
     "cc_compress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u64, c_u32p]),
     "cc_decompress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u32]),
+    "cc_volume_batch_create": (c_int, [c_vp, c_u32, c_u32p, c_u32, ctypes.POINTER(c_float), ctypes.POINTER(c_vp)]),
+    "cc_volume_batch_destroy": (None, [c_vp]),
+    "cc_volume_batch_use_graph": (c_int, [c_vp, c_int]),
+    "cc_volume_batch_compress": (c_int, [c_vp, c_vpp]),
+    "cc_volume_batch_decompress": (c_int, [c_vp, c_vpp]),
+    "cc_volume_batch_stream": (c_int, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), ctypes.POINTER(c_vp),
+                                       ctypes.POINTER(c_u64)]),
+    "cc_volume_batch_read_stream": (c_int, [c_vp, c_u32, c_vp, c_u64, ctypes.POINTER(c_u64)]),
+    "cc_volume_batch_load_streams": (c_int, [c_vp, c_vpp, ctypes.POINTER(c_u64)]),
+    "cc_volume_batch_status": (c_int, [c_vp]),
+    "cc_volume_batch_collect_timings": (None, [c_vp]),
 }
 
 _lib = None

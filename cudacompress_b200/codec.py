@@ -324,3 +324,77 @@ def decompress_heightfield(inst: Instance, out: torch.Tensor, levels: int, words
     ny, nx = out.shape
     check(lib().cc_decompress_heightfield(inst.handle, out.data_ptr(), nx, ny, levels, words.data_ptr(), bit_size),
           "decompressHeightfield")
+
+
+# ------------------------------------------------------ batched volume codec
+class VolumeBatch:
+    """Batched lossy volume codec (cc_volume_batch_*): `sizes` is a list of
+    (z, y, x) shapes, `quant_steps` one step per volume.  Each volume's
+    stream equals compress_volume_float's."""
+
+    def __init__(self, inst: Instance, sizes, levels: int, quant_steps, graph: bool = False):
+        self.inst = inst
+        self.count = len(sizes)
+        self.shapes = [tuple(int(v) for v in s) for s in sizes]
+        flat = []
+        for (nz, ny, nx) in self.shapes:
+            flat += [nx, ny, nz]
+        arr = (ctypes.c_uint32 * len(flat))(*flat)
+        steps = (ctypes.c_float * self.count)(*[float(q) for q in quant_steps])
+        h = ctypes.c_void_p()
+        check(lib().cc_volume_batch_create(inst.handle, self.count, arr, levels, steps, ctypes.byref(h)),
+              "cc_volume_batch_create")
+        self.handle = h
+        self.levels = levels
+        if graph:
+            check(lib().cc_volume_batch_use_graph(self.handle, 1), "cc_volume_batch_use_graph")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cc_volume_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def compress(self, volumes) -> None:
+        arr = (ctypes.c_void_p * self.count)(*[v.data_ptr() for v in volumes])
+        check(lib().cc_volume_batch_compress(self.handle, arr), "cc_volume_batch_compress")
+
+    def decompress(self, outs) -> None:
+        arr = (ctypes.c_void_p * self.count)(*[o.data_ptr() for o in outs])
+        check(lib().cc_volume_batch_decompress(self.handle, arr), "cc_volume_batch_decompress")
+
+    def status(self) -> None:
+        check(lib().cc_volume_batch_status(self.handle), "cc_volume_batch_status")
+
+    def read_stream(self, v: int):
+        """(host words, bit size) of volume v's stream (synchronizes)."""
+        bits = ctypes.c_uint64()
+        check(lib().cc_volume_batch_read_stream(self.handle, v, None, 0, ctypes.byref(bits)), "read_stream")
+        words = np.zeros((bits.value + 31) // 32, np.uint32)
+        check(lib().cc_volume_batch_read_stream(self.handle, v, words.ctypes.data, len(words), ctypes.byref(bits)),
+              "read_stream")
+        return words, int(bits.value)
+
+    def load_streams(self, words, bit_sizes) -> None:
+        """Loads one stream per volume (host numpy uint32 arrays, or CUDA
+        int32 tensors) for decompress()."""
+        ptrs = []
+        for w in words:
+            ptrs.append(w.data_ptr() if isinstance(w, torch.Tensor) else np.ascontiguousarray(w, np.uint32).ctypes.data)
+        arr = (ctypes.c_void_p * self.count)(*ptrs)
+        bits = (ctypes.c_uint64 * self.count)(*[int(b) for b in bit_sizes])
+        check(lib().cc_volume_batch_load_streams(self.handle, arr, bits), "cc_volume_batch_load_streams")
+
+    def collect_timings(self) -> None:
+        lib().cc_volume_batch_collect_timings(self.handle)

@@ -1,0 +1,608 @@
+// batch.cu - batched lossy volume codec: any number of float32 volumes
+// ("bricks") of any sizes, each with its own quantization step, compressed
+// and decompressed with one launch per stage for the whole batch.
+//
+// Each volume's bit stream is exactly cc_compress_volume_float's (the
+// reference's compressVolumeFloat layout, CompressVolume.cpp:312-409: the
+// lowpass band with encodeHuff, then per level coarse -> fine the 7 highpass
+// bands with encodeRLHuff), so the batch is a drop-in for N calls of the
+// plain codec.  Everything a call needs is planned once at creation and kept
+// on the device: DWT / quantizer descriptors, the encoder's stream and table
+// descriptors, the decoder's descriptors (its header walk runs on the
+// device).  A compress or decompress call therefore enqueues only kernels,
+// device memsets and one small upload of the volume pointer table, on the
+// instance stream, with no host synchronization - and can run as a CUDA
+// graph that replays the whole sequence in one launch.
+//
+// Work areas (one allocation): per level l a dense level-l volume for every
+// brick (forward coefficients, and the reconstructions on the way back),
+// two transform temporaries, the symbols (per brick: lowpass, then the 7
+// bands of each level coarse -> fine, every band 16-byte aligned), the
+// descriptors, and per brick the word offset and bit size of its stream in
+// the batch's output words.
+#include <cstring>
+
+#include "batch.cuh"
+
+struct cc_volume_batch {
+    cc_instance* I = nullptr;          // own instance, sized for the batch
+    cc_instance* user = nullptr;
+    ccb::u32 count = 0, levels = 0;
+    std::vector<ccb::u32> nx, ny, nz;
+    std::vector<float> q0;
+    char* mem = nullptr;               // device
+    size_t memBytes = 0;
+    char* hostPlan = nullptr;          // pinned: pointer tables
+    ccb::u64* hostExt = nullptr;       // pinned: loaded streams' offsets and sizes
+    cudaEvent_t extEvent = nullptr;
+    cudaEvent_t tabEvent = nullptr;
+    // device pieces
+    ccb::u16* syms = nullptr;
+    size_t symBytes = 0;
+    const float** inTab = nullptr;
+    float** outTab = nullptr;
+    ccb::u64* wordOff = nullptr;
+    ccb::u64* bitSize = nullptr;
+    ccb::u32* volFirstStream = nullptr;   // [count + 1]
+    // launch lists
+    struct Rows { const ccb::BRowDesc* d; ccb::u32 n, ctas; };
+    struct Cols { const ccb::BColDesc* d; ccb::u32 n, ctas; };
+    struct Quant { const ccb::BQuantDesc* d; ccb::u32 n, ctas; };
+    std::vector<Rows> fwdRows, invRows;        // per level
+    std::vector<Cols> fwdY, fwdZ, invZ, invY;  // per level
+    Quant quant{}, dequantLP{};
+    ccb::EncPlan enc;
+    ccb::DecPlan dec;
+    // graphs
+    bool useGraph = false;
+    cudaGraphExec_t gCompress = nullptr, gDecompress = nullptr;
+    cudaStream_t captureStream = nullptr;
+    unsigned launchesCompress = 0, launchesDecompress = 0;
+};
+
+namespace ccb {
+
+namespace {
+
+struct Arena {
+    size_t off = 0;
+    size_t take(size_t bytes, size_t align = 256) {
+        off = alignUp(off, align);
+        const size_t at = off;
+        off += bytes;
+        return at;
+    }
+};
+
+u64 vol3(u32 x, u32 y, u32 z) { return u64(x) * y * z; }
+
+void addRows(std::vector<BRowDesc>& v, u32& ctas, BRowDesc d) {
+    batchRowTiling(d.nx, d.W, d.R);
+    d.tilesX = int(ceilDiv(d.nx, d.W));
+    d.ctaOff = ctas;
+    ctas += u32(d.tilesX) * u32(ceilDiv(u64(d.ny) * d.nz, d.R));
+    v.push_back(d);
+}
+
+void addCols(std::vector<BColDesc>& v, u32& ctas, BColDesc d) {
+    d.tilesX = u32(ceilDiv(d.nx, 32));
+    d.tilesA = u32(ceilDiv(d.na, 64));
+    d.ctaOff = ctas;
+    ctas += d.tilesX * d.tilesA * u32(d.nc);
+    v.push_back(d);
+}
+
+void addQuant(std::vector<BQuantDesc>& v, u32& ctas, BQuantDesc d) {
+    d.ctaOff = ctas;
+    ctas += u32(ceilDiv(vol3(d.nx, d.ny, d.nz), kBQuantPerCta));
+    v.push_back(d);
+}
+
+// Symbol layout of one volume: lowpass, then levels L-1 .. 0, 7 bands each.
+struct SymLayout {
+    u64 lp = 0;                 // offset of the lowpass (symbols)
+    std::vector<u64> level;     // offset of the first band of level l
+    std::vector<u64> bandStride;
+    u64 total = 0;
+};
+
+SymLayout symLayout(u32 nx, u32 ny, u32 nz, u32 L) {
+    SymLayout s;
+    s.level.assign(L, 0);
+    s.bandStride.assign(L, 0);
+    u64 at = 0;
+    s.lp = at;
+    at = alignUp(at + vol3(nx >> L, ny >> L, nz >> L), 8);
+    for (int l = int(L) - 1; l >= 0; --l) {
+        const u64 band = alignUp(vol3(nx >> (l + 1), ny >> (l + 1), nz >> (l + 1)), 8);
+        s.level[l] = at;
+        s.bandStride[l] = band;
+        at += 7 * band;
+    }
+    s.total = at;
+    return s;
+}
+
+}  // namespace
+
+static int batchEnqueueCompress(cc_volume_batch* b) {
+    cc_instance* I = b->I;
+    cudaStream_t st = I->stream;
+    for (u32 l = 0; l < b->levels; ++l) {
+        SectionTimer t(I, "batch.dwt_forward", st);
+        launchBatchRows(b->fwdRows[l].d, b->fwdRows[l].n, b->fwdRows[l].ctas, false, b->inTab, b->outTab, st);
+        launchBatchCols(b->fwdY[l].d, b->fwdY[l].n, b->fwdY[l].ctas, false, false, st);
+        launchBatchCols(b->fwdZ[l].d, b->fwdZ[l].n, b->fwdZ[l].ctas, false, false, st);
+    }
+    { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, b->quant.n, b->quant.ctas, false, st); }
+    int rc = encodeLaunch(I, b->enc, I->out, I->outWordsMax);
+    if (rc) return rc;
+    volumeExtents(I, b->volFirstStream, b->count, b->wordOff, b->bitSize, st);
+    CC_TRY_CUDA(cudaGetLastError(), "batch compress");
+    return CC_OK;
+}
+
+static int batchEnqueueDecompress(cc_volume_batch* b) {
+    cc_instance* I = b->I;
+    cudaStream_t st = I->stream;
+    CC_TRY_CUDA(cudaMemsetAsync(b->syms, 0, b->symBytes, st), "zero symbols");
+    int rc = decodeLaunch(I, b->dec);
+    if (rc) return rc;
+    { SectionTimer t(I, "batch.dequantize", st); launchBatchQuant(b->dequantLP.d, b->dequantLP.n, b->dequantLP.ctas, true, st); }
+    for (int l = int(b->levels) - 1; l >= 0; --l) {
+        SectionTimer t(I, "batch.dwt_inverse", st);
+        launchBatchCols(b->invZ[l].d, b->invZ[l].n, b->invZ[l].ctas, true, true, st);
+        launchBatchCols(b->invY[l].d, b->invY[l].n, b->invY[l].ctas, true, false, st);
+        launchBatchRows(b->invRows[l].d, b->invRows[l].n, b->invRows[l].ctas, true, b->inTab, b->outTab, st);
+    }
+    CC_TRY_CUDA(cudaGetLastError(), "batch decompress");
+    return CC_OK;
+}
+
+// Copies a volume pointer table to the device (outside any captured graph).
+static int uploadTable(cc_volume_batch* b, const void* const* ptrs, void* dTable) {
+    cudaEventSynchronize(b->tabEvent);   // the previous upload has read the pinned buffer
+    std::memcpy(b->hostPlan, ptrs, sizeof(void*) * b->count);
+    CC_TRY_CUDA(cudaMemcpyAsync(dTable, b->hostPlan, sizeof(void*) * b->count, cudaMemcpyHostToDevice, b->I->stream),
+                "upload volume pointers");
+    cudaEventRecord(b->tabEvent, b->I->stream);
+    return CC_OK;
+}
+
+using Enqueue = int (*)(cc_volume_batch*);
+
+// Runs an enqueue function directly, or through its CUDA graph (captured on
+// the first use; later calls replay it).
+static int runMaybeGraph(cc_volume_batch* b, Enqueue fn, cudaGraphExec_t& exec, unsigned& launches) {
+    cc_instance* I = b->I;
+    if (!b->useGraph) return fn(b);
+    if (!exec) {
+        // Capture on the batch's own stream (the instance stream may be the
+        // legacy default stream, which cannot be captured); the graph is then
+        // launched on the instance stream.
+        if (!b->captureStream)
+            CC_TRY_CUDA(cudaStreamCreateWithFlags(&b->captureStream, cudaStreamNonBlocking), "capture stream");
+        const bool timing = I->timing;
+        cudaStream_t userStream = I->stream;
+        I->timing = false;   // no event records inside the graph
+        I->stream = b->captureStream;
+        cudaError_t e = cudaStreamBeginCapture(I->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { I->stream = userStream; I->timing = timing; return cudaFail(e, "begin capture"); }
+        const unsigned long long c0 = cc_kernel_launches();
+        int rc = fn(b);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(I->stream, &g);
+        I->stream = userStream;
+        I->timing = timing;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cudaFail(e, "end capture");
+        launches = unsigned(cc_kernel_launches() - c0);
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { exec = nullptr; return cudaFail(e, "graph instantiate"); }
+    }
+    CC_TRY_CUDA(cudaGraphLaunch(exec, I->stream), "graph launch");
+    countLaunch(launches);
+    return CC_OK;
+}
+
+}  // namespace ccb
+
+using namespace ccb;
+
+extern "C" {
+
+int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* sizes, uint32_t levels,
+                           const float* quantSteps, cc_volume_batch** out) {
+    if (!out) { setError("cc_volume_batch_create: out is NULL"); return CC_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    if (!user || !sizes || !quantSteps || count == 0 || levels == 0 || levels > 8) {
+        setError("cc_volume_batch_create: bad argument");
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    if (user->symBytes != 2) { setError("cc_volume_batch_create: needs a 16-bit-symbol instance (log2 symbol count <= 16)"); return CC_ERR_INVALID_ARGUMENT; }
+    const u32 L = levels, f = 1u << L;
+    u64 N0sum = 0, histBins = 0;
+    u32 maxStream = 1;
+    for (u32 v = 0; v < count; ++v) {
+        const u32 x = sizes[3 * v], y = sizes[3 * v + 1], z = sizes[3 * v + 2];
+        if (x % f || y % f || z % f || (x >> (L - 1)) < 8 || (y >> (L - 1)) < 8 || (z >> (L - 1)) < 8) {
+            setError("cc_volume_batch_create: volume %u (%u x %u x %u): sizes must be divisible by 2^levels with the coarsest level >= 8",
+                     v, x, y, z);
+            return CC_ERR_INVALID_ARGUMENT;
+        }
+        if (!(quantSteps[v] > 0.0f)) { setError("cc_volume_batch_create: volume %u: quantization step must be > 0", v); return CC_ERR_INVALID_ARGUMENT; }
+        N0sum += vol3(x, y, z);
+        maxStream = std::max<u32>(maxStream, u32(vol3(x >> 1, y >> 1, z >> 1)));
+    }
+    const u32 S = count * (1 + 7 * L);
+    // histogram bins: every table at most 2^log2Max; budget 2^26 bins (the
+    // device plan fails a call that needs more)
+    histBins = std::min<u64>(u64(2 * S) * user->bins, u64(1) << 26);
+    cudaSetDevice(user->device);
+    cc_volume_batch* b = new cc_volume_batch();
+    b->user = user;
+    b->count = count;
+    b->levels = L;
+    for (u32 v = 0; v < count; ++v) {
+        b->nx.push_back(sizes[3 * v]);
+        b->ny.push_back(sizes[3 * v + 1]);
+        b->nz.push_back(sizes[3 * v + 2]);
+        b->q0.push_back(quantSteps[v]);
+    }
+    // symbols: every stream's (the lowpass streams' coding blocks count too)
+    InstanceCaps caps{S, std::max<u64>(N0sum, 1), histBins};
+    int rc = createInstance(&b->I, user->device, S, maxStream, user->codingBlockSize, user->log2Max, &caps);
+    if (rc) { delete b; return rc; }
+    cc_instance* I = b->I;
+    I->stream = user->stream;
+    I->timing = user->timing;
+    // kernel attributes set once here, so that captured launches do not set them
+    rc = prepareKernelAttributes(I);
+    if (rc) { cc_destroy_instance(I); delete b; return rc; }
+
+    // ---- layout of the work areas ----
+    // Descriptors hold offsets until the allocation exists, and a null
+    // pointer means "the volume pointer table": no piece may start at 0.
+    Arena A;
+    A.take(256);
+    std::vector<std::vector<u64>> levOff(L + 1, std::vector<u64>(count));
+    std::vector<size_t> levAt(L + 1);
+    for (u32 l = 0; l <= L; ++l) {
+        u64 tot = 0;
+        for (u32 v = 0; v < count; ++v) {
+            levOff[l][v] = tot;
+            tot += alignUp(vol3(b->nx[v] >> l, b->ny[v] >> l, b->nz[v] >> l), 64);
+        }
+        levAt[l] = A.take(tot * sizeof(float));
+    }
+    std::vector<u64> tOff(count);
+    u64 tTot = 0;
+    for (u32 v = 0; v < count; ++v) { tOff[v] = tTot; tTot += alignUp(vol3(b->nx[v], b->ny[v], b->nz[v]), 64); }
+    const size_t t1At = A.take(tTot * sizeof(float)), t2At = A.take(tTot * sizeof(float));
+    std::vector<SymLayout> sl(count);
+    std::vector<u64> symOff(count);
+    u64 symTot = 0;
+    for (u32 v = 0; v < count; ++v) {
+        sl[v] = symLayout(b->nx[v], b->ny[v], b->nz[v], L);
+        symOff[v] = symTot;
+        symTot += sl[v].total;
+    }
+    const size_t symAt = A.take((symTot + 64) * sizeof(u16));
+    const size_t inTabAt = A.take(sizeof(void*) * count), outTabAt = A.take(sizeof(void*) * count);
+    const size_t wordOffAt = A.take(sizeof(u64) * count), bitSizeAt = A.take(sizeof(u64) * count);
+    const size_t firstAt = A.take(sizeof(u32) * (count + 1));
+
+    // ---- descriptors (host) ----
+    auto lev = [&](u32 l, u32 v) { return reinterpret_cast<float*>(levAt[l]) + levOff[l][v]; };   // offsets, rebased below
+    auto t1 = [&](u32 v) { return reinterpret_cast<float*>(t1At) + tOff[v]; };
+    auto t2 = [&](u32 v) { return reinterpret_cast<float*>(t2At) + tOff[v]; };
+    auto sy = [&](u32 v) { return reinterpret_cast<u16*>(symAt) + symOff[v]; };
+    std::vector<std::vector<BRowDesc>> fr(L), ir(L);
+    std::vector<std::vector<BColDesc>> fy(L), fz(L), iz(L), iy(L);
+    std::vector<u32> frC(L, 0), irC(L, 0), fyC(L, 0), fzC(L, 0), izC(L, 0), iyC(L, 0);
+    std::vector<BQuantDesc> qd, dq;
+    u32 qC = 0, dqC = 0;
+    std::vector<EncStream> es;
+    std::vector<DecStreamSpec> ds;
+    std::vector<DecSourceSpec> dsrc(count);
+    std::vector<u32> firstStream(count + 1);
+    for (u32 v = 0; v < count; ++v) {
+        const u32 X = b->nx[v], Y = b->ny[v], Z = b->nz[v];
+        for (u32 l = 0; l < L; ++l) {
+            const int sx = int(X >> l), syz = int(Y >> l), sz = int(Z >> l);
+            // X: input (level 0: the caller's volume, tight; else the LLL octant of level l-1) -> t1
+            BRowDesc r{};
+            r.vol = int(v);
+            r.src = l == 0 ? nullptr : lev(l - 1, v);
+            r.dst = t1(v);
+            r.nx = sx; r.ny = syz; r.nz = sz;
+            r.srcRow = l == 0 ? int(X) : int(X >> (l - 1));
+            r.srcSlice = l == 0 ? int(X * Y) : int((X >> (l - 1)) * (Y >> (l - 1)));
+            r.dstRow = sx; r.dstSlice = sx * syz;
+            addRows(fr[l], frC[l], r);
+            // Y: t1 -> t2 (dense level l)
+            BColDesc c{};
+            c.src = t1(v); c.dst = t2(v);
+            c.nx = sx; c.na = syz; c.nc = sz;
+            c.sx = 1; c.sa = sx; c.sc = sx * syz;
+            c.dx = 1; c.da = sx; c.dc = sx * syz;
+            addCols(fy[l], fyC[l], c);
+            // Z: t2 -> level l coefficients
+            BColDesc cz = c;
+            cz.src = t2(v); cz.dst = lev(l, v);
+            cz.na = sz; cz.nc = syz;
+            cz.sa = sx * syz; cz.sc = sx;
+            cz.da = sx * syz; cz.dc = sx;
+            addCols(fz[l], fzC[l], cz);
+            // inverse of level l: Z from symbols (lowpass = level l+1 reconstruction) -> t2, Y -> t1, X -> level l
+            BColDesc ic{};
+            ic.src = lev(l + 1, v);
+            ic.dst = t2(v);
+            ic.nx = sx; ic.na = sz; ic.nc = syz;
+            ic.dx = 1; ic.da = sx * syz; ic.dc = sx;
+            ic.bands = sy(v) + sl[v].level[l];
+            ic.bandStride = sl[v].bandStride[l];
+            ic.step = b->q0[v] / float(1u << l);
+            ic.hx = sx / 2; ic.hy = syz / 2; ic.hz = sz / 2;
+            ic.lpRow = sx / 2; ic.lpSlice = (sx / 2) * (syz / 2);
+            addCols(iz[l], izC[l], ic);
+            BColDesc iyd{};
+            iyd.src = t2(v); iyd.dst = t1(v);
+            iyd.nx = sx; iyd.na = syz; iyd.nc = sz;
+            iyd.sx = 1; iyd.sa = sx; iyd.sc = sx * syz;
+            iyd.dx = 1; iyd.da = sx; iyd.dc = sx * syz;
+            addCols(iy[l], iyC[l], iyd);
+            BRowDesc irw{};
+            irw.vol = int(v);
+            irw.src = t1(v);
+            irw.dst = l == 0 ? nullptr : lev(l, v);
+            irw.nx = sx; irw.ny = syz; irw.nz = sz;
+            irw.srcRow = sx; irw.srcSlice = sx * syz;
+            irw.dstRow = sx; irw.dstSlice = sx * syz;
+            addRows(ir[l], irC[l], irw);
+        }
+        // quantization: lowpass (step q0 / 2^(L-1)), then levels coarse -> fine (step q0 / 2^l)
+        const u32 Lx = X >> (L - 1), Ly = Y >> (L - 1);
+        BQuantDesc q{};
+        q.src = lev(L - 1, v);
+        q.sym = sy(v) + sl[v].lp;
+        q.nx = int(X >> L); q.ny = int(Y >> L); q.nz = int(Z >> L);
+        q.row = int(Lx); q.slice = int(Lx * Ly);
+        q.step = b->q0[v] / float(1u << (L - 1));
+        q.inv = 1.0f / q.step;   // Quantize.cu:90: reciprocal computed on the host
+        addQuant(qd, qC, q);
+        BQuantDesc d = q;
+        d.src = nullptr;
+        d.dstF = lev(L, v);
+        addQuant(dq, dqC, d);
+        firstStream[v] = u32(es.size());
+        es.push_back(EncStream{reinterpret_cast<void*>(q.sym), u32(vol3(X >> L, Y >> L, Z >> L)), 0, 0, 1, KIND_HUFF});
+        ds.push_back(DecStreamSpec{KIND_HUFF, u32(vol3(X >> L, Y >> L, Z >> L)), q.sym, v});
+        for (int l = int(L) - 1; l >= 0; --l) {
+            const u32 sx = X >> l, syv = Y >> l, sz = Z >> l;
+            const u32 hx = sx / 2, hy = syv / 2, hz = sz / 2;
+            const u32 first = u32(es.size());
+            for (u32 bi = 1; bi < 8; ++bi) {
+                const u32 x = bi % 2, y = (bi / 2) % 2, z = bi / 4;
+                BQuantDesc qb{};
+                qb.src = lev(u32(l), v) + u64(z) * hz * sx * syv + u64(y) * hy * sx + u64(x) * hx;
+                qb.sym = sy(v) + sl[v].level[l] + (bi - 1) * sl[v].bandStride[l];
+                qb.nx = int(hx); qb.ny = int(hy); qb.nz = int(hz);
+                qb.row = int(sx); qb.slice = int(sx * syv);
+                qb.step = b->q0[v] / float(1u << l);
+                qb.inv = 1.0f / qb.step;
+                addQuant(qd, qC, qb);
+                es.push_back(EncStream{reinterpret_cast<void*>(qb.sym), hx * hy * hz, 0, first, 7, KIND_RLHUFF});
+                ds.push_back(DecStreamSpec{KIND_RLHUFF, hx * hy * hz, qb.sym, v});
+            }
+        }
+        dsrc[v] = DecSourceSpec{nullptr, 0, 0};
+    }
+    firstStream[count] = u32(es.size());
+
+    // ---- device plan ----
+    auto bytesOf = [](size_t n, size_t e) { return n * e; };
+    std::vector<size_t> frAt(L), irAt(L), fyAt(L), fzAt(L), izAt(L), iyAt(L);
+    A.off = alignUp(A.off, 256);
+    for (u32 l = 0; l < L; ++l) {
+        frAt[l] = A.take(bytesOf(fr[l].size(), sizeof(BRowDesc)), 64);
+        irAt[l] = A.take(bytesOf(ir[l].size(), sizeof(BRowDesc)), 64);
+        fyAt[l] = A.take(bytesOf(fy[l].size(), sizeof(BColDesc)), 64);
+        fzAt[l] = A.take(bytesOf(fz[l].size(), sizeof(BColDesc)), 64);
+        izAt[l] = A.take(bytesOf(iz[l].size(), sizeof(BColDesc)), 64);
+        iyAt[l] = A.take(bytesOf(iy[l].size(), sizeof(BColDesc)), 64);
+    }
+    const size_t qAt = A.take(bytesOf(qd.size(), sizeof(BQuantDesc)), 64);
+    const size_t dqAt = A.take(bytesOf(dq.size(), sizeof(BQuantDesc)), 64);
+    // encoder / decoder descriptors: sized by preparing into a host buffer
+    const size_t planMax = size_t(I->hostRingBytes);
+    std::vector<char> encHost(planMax), decHost(planMax);
+    rc = encodePrepare(I, es.data(), u32(es.size()), encHost.data(), planMax, b->enc);
+    if (!rc) rc = decodePrepare(I, ds.data(), u32(ds.size()), dsrc.data(), count, decHost.data(), planMax, b->dec);
+    if (rc) { cc_destroy_instance(I); delete b; return rc; }
+    const size_t encAt = A.take(b->enc.bytes, 256), decAt = A.take(b->dec.bytes, 256);
+    b->memBytes = alignUp(A.off, 256);
+    cudaError_t e = cudaMalloc(&b->mem, b->memBytes);
+    if (e != cudaSuccess) { cc_destroy_instance(I); delete b; return cudaFail(e, "cudaMalloc(volume batch)"); }
+    char* base = b->mem;
+    // rebase the device pointers written as offsets
+    auto rebaseF = [&](const float* p) -> float* { return p ? reinterpret_cast<float*>(base + reinterpret_cast<uintptr_t>(p)) : nullptr; };
+    auto rebaseS = [&](const u16* p) -> u16* { return p ? reinterpret_cast<u16*>(base + reinterpret_cast<uintptr_t>(p)) : nullptr; };
+    for (u32 l = 0; l < L; ++l) {
+        for (auto& d : fr[l]) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); }
+        for (auto& d : ir[l]) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); }
+        for (auto* vv : {&fy[l], &fz[l], &iz[l], &iy[l]})
+            for (auto& d : *vv) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); d.bands = rebaseS(d.bands); }
+    }
+    for (auto& d : qd) { d.src = rebaseF(d.src); d.sym = rebaseS(d.sym); }
+    for (auto& d : dq) { d.sym = rebaseS(d.sym); d.dstF = rebaseF(d.dstF); }
+    // encoder inputs and decoder outputs are symbol pointers: rebase inside the prepared descriptors
+    {
+        EncStreamDev* sdv = reinterpret_cast<EncStreamDev*>(encHost.data());
+        for (u32 s = 0; s < b->enc.S; ++s) sdv[s].in = base + reinterpret_cast<uintptr_t>(sdv[s].in);
+        DecStreamDesc* ddv = reinterpret_cast<DecStreamDesc*>(decHost.data());
+        for (u32 s = 0; s < b->dec.S; ++s) ddv[s].out = base + reinterpret_cast<uintptr_t>(ddv[s].out);
+    }
+    b->syms = reinterpret_cast<u16*>(base + symAt);
+    b->symBytes = size_t(symTot) * sizeof(u16);
+    b->inTab = reinterpret_cast<const float**>(base + inTabAt);
+    b->outTab = reinterpret_cast<float**>(base + outTabAt);
+    b->wordOff = reinterpret_cast<u64*>(base + wordOffAt);
+    b->bitSize = reinterpret_cast<u64*>(base + bitSizeAt);
+    b->volFirstStream = reinterpret_cast<u32*>(base + firstAt);
+    b->enc.dev = base + encAt;
+    b->dec.dev = base + decAt;
+    b->dec.wordsBase = I->out;
+    b->dec.wordOff = b->wordOff;
+    b->dec.bitSize = b->bitSize;
+    // upload everything once
+    auto up = [&](size_t at, const void* src, size_t bytes) -> cudaError_t {
+        return bytes ? cudaMemcpy(base + at, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    e = cudaMemset(b->mem, 0, b->memBytes);
+    for (u32 l = 0; l < L && e == cudaSuccess; ++l) {
+        e = up(frAt[l], fr[l].data(), fr[l].size() * sizeof(BRowDesc));
+        if (e == cudaSuccess) e = up(irAt[l], ir[l].data(), ir[l].size() * sizeof(BRowDesc));
+        if (e == cudaSuccess) e = up(fyAt[l], fy[l].data(), fy[l].size() * sizeof(BColDesc));
+        if (e == cudaSuccess) e = up(fzAt[l], fz[l].data(), fz[l].size() * sizeof(BColDesc));
+        if (e == cudaSuccess) e = up(izAt[l], iz[l].data(), iz[l].size() * sizeof(BColDesc));
+        if (e == cudaSuccess) e = up(iyAt[l], iy[l].data(), iy[l].size() * sizeof(BColDesc));
+    }
+    if (e == cudaSuccess) e = up(qAt, qd.data(), qd.size() * sizeof(BQuantDesc));
+    if (e == cudaSuccess) e = up(dqAt, dq.data(), dq.size() * sizeof(BQuantDesc));
+    if (e == cudaSuccess) e = up(encAt, encHost.data(), b->enc.bytes);
+    if (e == cudaSuccess) e = up(decAt, decHost.data(), b->dec.bytes);
+    if (e == cudaSuccess) e = up(firstAt, firstStream.data(), sizeof(u32) * (count + 1));
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&b->hostPlan), sizeof(void*) * count, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->tabEvent, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&b->hostExt), 2 * sizeof(u64) * count, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->extEvent, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { cc_volume_batch_destroy(b); return cudaFail(e, "volume batch set-up"); }
+    b->fwdRows.resize(L); b->invRows.resize(L); b->fwdY.resize(L); b->fwdZ.resize(L); b->invZ.resize(L); b->invY.resize(L);
+    for (u32 l = 0; l < L; ++l) {
+        b->fwdRows[l] = {reinterpret_cast<const BRowDesc*>(base + frAt[l]), u32(fr[l].size()), frC[l]};
+        b->invRows[l] = {reinterpret_cast<const BRowDesc*>(base + irAt[l]), u32(ir[l].size()), irC[l]};
+        b->fwdY[l] = {reinterpret_cast<const BColDesc*>(base + fyAt[l]), u32(fy[l].size()), fyC[l]};
+        b->fwdZ[l] = {reinterpret_cast<const BColDesc*>(base + fzAt[l]), u32(fz[l].size()), fzC[l]};
+        b->invZ[l] = {reinterpret_cast<const BColDesc*>(base + izAt[l]), u32(iz[l].size()), izC[l]};
+        b->invY[l] = {reinterpret_cast<const BColDesc*>(base + iyAt[l]), u32(iy[l].size()), iyC[l]};
+    }
+    b->quant = {reinterpret_cast<const BQuantDesc*>(base + qAt), u32(qd.size()), qC};
+    b->dequantLP = {reinterpret_cast<const BQuantDesc*>(base + dqAt), u32(dq.size()), dqC};
+    *out = b;
+    return CC_OK;
+}
+
+void cc_volume_batch_destroy(cc_volume_batch* b) {
+    if (!b) return;
+    if (b->I) cudaSetDevice(b->I->device);
+    cudaDeviceSynchronize();
+    if (b->gCompress) cudaGraphExecDestroy(b->gCompress);
+    if (b->gDecompress) cudaGraphExecDestroy(b->gDecompress);
+    if (b->captureStream) cudaStreamDestroy(b->captureStream);
+    if (b->tabEvent) cudaEventDestroy(b->tabEvent);
+    if (b->hostPlan) cudaFreeHost(b->hostPlan);
+    if (b->hostExt) cudaFreeHost(b->hostExt);
+    if (b->extEvent) cudaEventDestroy(b->extEvent);
+    if (b->mem) cudaFree(b->mem);
+    if (b->I) cc_destroy_instance(b->I);
+    delete b;
+}
+
+int cc_volume_batch_use_graph(cc_volume_batch* b, int enable) {
+    if (!b) { setError("cc_volume_batch_use_graph: null batch"); return CC_ERR_INVALID_ARGUMENT; }
+    b->useGraph = enable != 0;
+    return CC_OK;
+}
+
+int cc_volume_batch_compress(cc_volume_batch* b, const float* const* dVolumes) {
+    if (!b || !dVolumes) { setError("cc_volume_batch_compress: null argument"); return CC_ERR_INVALID_ARGUMENT; }
+    cudaSetDevice(b->I->device);
+    b->I->stream = b->user->stream;
+    b->I->timing = b->user->timing;
+    int rc = uploadTable(b, reinterpret_cast<const void* const*>(dVolumes), b->inTab);
+    if (rc) return rc;
+    return runMaybeGraph(b, batchEnqueueCompress, b->gCompress, b->launchesCompress);
+}
+
+int cc_volume_batch_decompress(cc_volume_batch* b, float* const* dVolumes) {
+    if (!b || !dVolumes) { setError("cc_volume_batch_decompress: null argument"); return CC_ERR_INVALID_ARGUMENT; }
+    cudaSetDevice(b->I->device);
+    b->I->stream = b->user->stream;
+    b->I->timing = b->user->timing;
+    int rc = uploadTable(b, reinterpret_cast<const void* const*>(dVolumes), b->outTab);
+    if (rc) return rc;
+    return runMaybeGraph(b, batchEnqueueDecompress, b->gDecompress, b->launchesDecompress);
+}
+
+int cc_volume_batch_stream(const cc_volume_batch* b, const uint32_t** dWords, const uint64_t** dWordOffsets,
+                           const uint64_t** dBitSizes, uint64_t* capacityWords) {
+    if (!b) { setError("cc_volume_batch_stream: null batch"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dWords) *dWords = b->I->out;
+    if (dWordOffsets) *dWordOffsets = b->wordOff;
+    if (dBitSizes) *dBitSizes = b->bitSize;
+    if (capacityWords) *capacityWords = b->I->outWordsMax;
+    return CC_OK;
+}
+
+int cc_volume_batch_read_stream(cc_volume_batch* b, uint32_t v, uint32_t* dst, uint64_t capacityWords,
+                                uint64_t* bitSize) {
+    if (!b || !bitSize || v >= b->count) { setError("cc_volume_batch_read_stream: bad argument"); return CC_ERR_INVALID_ARGUMENT; }
+    cudaSetDevice(b->I->device);
+    u64 ext[2] = {0, 0};
+    CC_TRY_CUDA(cudaMemcpyAsync(&ext[0], b->wordOff + v, sizeof(u64), cudaMemcpyDeviceToHost, b->I->stream), "read offset");
+    CC_TRY_CUDA(cudaMemcpyAsync(&ext[1], b->bitSize + v, sizeof(u64), cudaMemcpyDeviceToHost, b->I->stream), "read size");
+    CC_TRY_CUDA(cudaStreamSynchronize(b->I->stream), "read stream");
+    *bitSize = ext[1];
+    const u64 words = ceilDiv(ext[1], 32);
+    if (!dst) return CC_OK;
+    if (words > capacityWords) { setError("cc_volume_batch_read_stream: need %llu words", (unsigned long long)words); return CC_ERR_CAPACITY; }
+    CC_TRY_CUDA(cudaMemcpy(dst, b->I->out + ext[0], words * 4, cudaMemcpyDefault), "copy stream");
+    return CC_OK;
+}
+
+int cc_volume_batch_load_streams(cc_volume_batch* b, const uint32_t* const* words, const uint64_t* bitSizes) {
+    if (!b || !words || !bitSizes) { setError("cc_volume_batch_load_streams: null argument"); return CC_ERR_INVALID_ARGUMENT; }
+    cudaSetDevice(b->I->device);
+    cudaStream_t st = b->user->stream;
+    cudaEventSynchronize(b->extEvent);   // the previous load has read the pinned offsets
+    u64 at = 0;
+    for (u32 v = 0; v < b->count; ++v) {
+        const u64 nw = ceilDiv(bitSizes[v], 32);
+        if (at + nw > b->I->outWordsMax) { setError("cc_volume_batch_load_streams: streams exceed the batch buffer (%llu words)", (unsigned long long)b->I->outWordsMax); return CC_ERR_CAPACITY; }
+        b->hostExt[v] = at;
+        b->hostExt[b->count + v] = bitSizes[v];
+        if (nw) CC_TRY_CUDA(cudaMemcpyAsync(b->I->out + at, words[v], nw * 4, cudaMemcpyDefault, st), "load stream");
+        at += nw;
+    }
+    CC_TRY_CUDA(cudaMemcpyAsync(b->wordOff, b->hostExt, sizeof(u64) * b->count, cudaMemcpyHostToDevice, st), "load offsets");
+    CC_TRY_CUDA(cudaMemcpyAsync(b->bitSize, b->hostExt + b->count, sizeof(u64) * b->count, cudaMemcpyHostToDevice, st), "load sizes");
+    cudaEventRecord(b->extEvent, st);
+    return CC_OK;
+}
+
+int cc_volume_batch_status(cc_volume_batch* b) {
+    if (!b) return CC_ERR_INVALID_ARGUMENT;
+    u32 flags[8] = {};
+    CC_TRY_CUDA(cudaMemcpyAsync(flags, b->I->errors, sizeof(flags), cudaMemcpyDeviceToHost, b->I->stream), "batch status");
+    CC_TRY_CUDA(cudaStreamSynchronize(b->I->stream), "batch status");
+    if (flags[0]) return deviceErrorStatus(flags[0], "batch compress");
+    return deviceErrorStatus(flags[4], "batch decompress");
+}
+
+// Resolves and folds the batch's internal timing sections into the user
+// instance (cc_timing_* report both).
+void cc_volume_batch_collect_timings(cc_volume_batch* b) {
+    if (!b) return;
+    b->I->resolveTimings();
+    for (auto& kv : b->I->timings) {
+        auto& acc = b->user->timings[kv.first];
+        acc.first += kv.second.first;
+        acc.second += kv.second.second;
+    }
+    b->I->timings.clear();
+}
+
+}  // extern "C"

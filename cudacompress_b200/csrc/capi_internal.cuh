@@ -16,6 +16,16 @@ void countLaunch(unsigned n = 1);
 void setError(const char* fmt, ...);
 int cudaFail(cudaError_t e, const char* what);
 
+// Capacities of an instance made for a batch of volumes (instead of the
+// reference's streamCountMax x elemCountPerStreamMax contract).
+struct InstanceCaps {
+    u32 streams;      // streams of one call
+    u64 symbols;      // run-length symbols of one call
+    u64 histBins;     // histogram bins of one call
+};
+int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 elemCountPerStreamMax,
+                   u32 codingBlockSize, u32 log2Max, const InstanceCaps* caps);
+
 // Maps the device error flags of a call to a status (and message).
 inline int deviceErrorStatus(u32 flags, const char* what) {
     if (!flags) return CC_OK;
@@ -45,10 +55,66 @@ struct EncOutput {
 };
 int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutput& out, bool download,
                  u64* totalWords = nullptr);
+// The same in two steps, for callers that keep the descriptors on the device
+// and replay the launches (batches, CUDA graphs): encodePrepare writes the
+// descriptors to a host buffer; the caller copies them to plan.dev; then
+// encodeLaunch enqueues only kernels and device memsets.
+struct EncPlan {
+    u32 S = 0, T = 0, tiles = 0, blocks = 0, maxCount = 0;
+    u64 compact = 0;
+    size_t offTables = 0, bytes = 0;
+    const void* dev = nullptr;
+};
+int encodePrepare(cc_instance* I, const EncStream* streams, u32 S, char* slot, size_t slotBytes, EncPlan& plan);
+int encodeLaunch(cc_instance* I, const EncPlan& plan, u32* out, u64 outCap);
 // Grows the instance's pipeline workspace to at least `bytes` (allocates only when it must grow).
 int ensurePipelineWork(cc_instance* I, size_t bytes);
 int decodeDevice(cc_instance* I, int kind, const u32* const* words, const u32* bitSizes, u32* bitPos, u32 bsCount,
                  const u32* bsIndex, void* const* outs, u32 S, u32 n);
+
+// Decode of device-resident bit streams walked on the device, in two steps
+// like the encoder: decodePrepare writes the descriptors of stream i (kind,
+// n symbols into out) read from source streams[i].source - the streams of one
+// source consecutive and in stream order from its startBit - into a host
+// buffer; decodeLaunch enqueues the walk and the decode (kernels and device
+// memsets only).  A source's words are words + wordOff[k] with bitSize[k]
+// bits when the plan gives device arrays for them (the output of a batched
+// encode), else the pointer and size given here.  Errors surface through the
+// instance's decode status.
+struct DecStreamSpec {
+    u32 kind;
+    u32 n;
+    void* out;
+    u32 source;
+};
+struct DecSourceSpec {
+    const u32* words;
+    u64 bitSize;
+    u64 startBit;
+};
+struct DecPlan {
+    u32 S = 0, T = 0, B = 0, nRl = 0, nH = 0, rlBlocks = 0, hBlocks = 0;
+    size_t bytes = 0;
+    void* dev = nullptr;
+    const u32* wordsBase = nullptr;   // with wordOff / bitSize: indirect sources
+    const u64* wordOff = nullptr;
+    const u64* bitSize = nullptr;
+};
+int decodePrepare(cc_instance* I, const DecStreamSpec* streams, u32 S, const DecSourceSpec* sources, u32 B,
+                  char* slot, size_t slotBytes, DecPlan& plan);
+int decodeLaunch(cc_instance* I, const DecPlan& plan);
+
+// Per-device cache of the dynamic shared memory limits set on kernels (so
+// that repeated launches, and launches recorded in a stream capture, do not
+// set them again): returns cudaSuccess once the kernel allows `bytes`.
+enum SmemAttrKernel { kAttrTableBuild = 0, kAttrDecHuff16 = 1, kAttrDecHuff32 = 2, kAttrCount = 3 };
+cudaError_t ensureSmemAttribute(const void* kernel, int which, int device, size_t bytes);
+// Sets the largest shared memory the encoder and decoder kernels may ask for
+// on the instance's device.
+int prepareKernelAttributes(cc_instance* I);
+// Batched encode: per volume (streams first[v] .. first[v+1]-1) its word
+// offset and bit size in the output, from the device layout.
+void volumeExtents(cc_instance* I, const u32* first, u32 count, u64* wordOff, u64* bitSize, cudaStream_t st);
 
 // Records a named, event-timed section on the instance stream when the
 // instance has timing enabled (setTimingDetail / cc_set_timing).

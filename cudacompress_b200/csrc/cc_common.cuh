@@ -82,6 +82,15 @@ __device__ __forceinline__ u32 blockExclusiveSum(u32 v, u32* scratch, u32* total
     return r;
 }
 
+// Quantize.cuh:26-35: symbol = 2|v| for v >= 0, 2|v| - 1 for v < 0, and back.
+__device__ __forceinline__ u32 symbolizeI(int v) { return 2u * u32(abs(v)) + u32(v >> 31); }
+__device__ __forceinline__ int unsymbolizeI(u32 s) {
+    int neg = int(s & 1u);
+    return (1 - 2 * neg) * int((s + u32(neg)) >> 1);
+}
+__device__ __forceinline__ float signF(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+__device__ __forceinline__ float signI(int q) { return q > 0 ? 1.0f : (q < 0 ? -1.0f : 0.0f); }
+
 // Warp-aggregated increment of `bins[key]`: lanes with equal keys are merged
 // with match_any so each distinct key issues one shared/global atomic.
 __device__ __forceinline__ void aggregatedIncrement(u32* bins, u32 key, bool active) {

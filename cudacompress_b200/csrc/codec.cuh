@@ -122,23 +122,44 @@ struct SegmentLayout {
     u32 countWord;        // relative word of compactCount (RLHuff)
 };
 
-// Decode-side table descriptor (filled by the host walk of the bit stream).
+// Decode-side table descriptor, filled by the host walk of a caller's bit
+// stream (cc_decode) or by the device walk of a device-resident one.
 struct DecTableDesc {
-    u64 hdrBit;       // absolute bit of the table header in the staged words
+    u64 hdrBit;       // absolute bit of the table header in its stream's words
     u64 cwWord;       // first codeword word
+    u64 offWord;      // first word of the u16 offset increments
     u32 cwBits;       // codeword bits
     u32 count;        // symbols to decode
-    u64 offWord;      // first word of the u16 offset increments
     u32 symbolBits;   // bits per symbol in the header
     u32 nLen;         // number of codeword lengths
     u32 nSym;         // symbols in the table
-    u32 pad;
+    u32 stream;       // owning stream
+    u32 blockOff;     // first of its coding blocks in the call's block arrays
+    u32 symOff;       // first of its symbols in the decode symbol array
+};
+
+// A bit stream a decode call reads.  Device walk: words may be given as a
+// base pointer plus a device array of word offsets (results of a batched
+// encode), resolved by the walk.
+struct DecSource {
+    const u32* words;
+    u64 wordCount;
+    u64 bitSize;      // readable bits
+    u64 startBit;     // device walk: where its first stream starts
+    u64 endBit;       // device walk: where its last stream ends
+    u32 firstStream;  // device walk: its streams, in stream order
+    u32 streamCount;
 };
 
 struct DecStreamDesc {
     void* out;        // device output symbols
+    u64 zcOff;        // RLHuff: offset of its decoded zero counts
     u32 n;            // output symbol count
     u32 m;            // compact count (RLHuff) / n (Huff)
+    u32 kind;         // KIND_RLHUFF or KIND_HUFF
+    u32 tableFirst;   // its first table (RLHuff: symbols, then zero counts)
+    u32 source;       // index of its DecSource
+    u32 blockFirst;   // first of its blocks among the streams of its kind
 };
 
 // Decode tables in device memory: canonical description + fast lookup.
@@ -206,15 +227,13 @@ struct cc_instance {
     ccb::u32* parentWork = nullptr;    // [2 capLeaves]
     ccb::u32* orderWork = nullptr;     // [capLeaves]
     ccb::u32* leafSymWork = nullptr;   // [capLeaves]
-    // decode
-    ccb::DecTableDesc* dDecTables = nullptr;  // [2S]
-    ccb::DecStreamDesc* dDecStreams = nullptr; // [S]
-    ccb::DecTable* decTables = nullptr;       // [2S]
-    ccb::u32* decSyms = nullptr;              // [2S][leavesMax]
-    ccb::u32* decLut = nullptr;               // [2S][1 << kLutBits]
-    ccb::u32* stagedWords = nullptr;          // decode input words
+    // decode (descriptors live in dPlan)
+    ccb::DecTable* decTables = nullptr;       // [capTables]
+    ccb::u32* decSyms = nullptr;              // [capLeaves]
+    ccb::u32* decLut = nullptr;               // [capTables][1 << kLutBits]
+    ccb::u32* stagedWords = nullptr;          // decode input words (host bit streams)
     ccb::u64 stagedWordsMax = 0;
-    ccb::u32* blockSum = nullptr;             // [S][blocksMax]
+    ccb::u32* blockSum = nullptr;             // [capBlocks]
 
     // host staging: ring of slots for uploads, one buffer for downloads
     static constexpr int kRing = 8;

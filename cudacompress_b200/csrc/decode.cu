@@ -2,12 +2,21 @@
 // (Encode.cpp:473-646, :792-917; Huffman.cu:189-279; HuffmanTable.cu:117-266;
 // RunLength.cu:257-328).
 //
-// The host only walks the stream headers to find where each table, codeword
-// block and offset block lies (O(table size field count) per table); all
-// table parsing, offset prefix sums, Huffman decoding and zero-run expansion
-// run on the device.  Every read of the staged words is bounds-checked, and
-// malformed tables or codes raise CC_ERR_CORRUPT_STREAM instead of reading or
-// writing out of bounds.
+// One call decodes a batch of streams of any sizes and of both kinds.  Two
+// front ends fill the same descriptors:
+//  * cc_decode (the reference's decode entry points, caller's host bit
+//    streams): the host walks the stream headers - the reference's own
+//    decode parses them on the host too and returns before the GPU work is
+//    done - and stages the touched words once;
+//  * decodePrepare / decodeLaunch (batched volume codec, device-resident bit
+//    streams): one thread per bit stream walks its headers on the device, so
+//    nothing goes through the host and the launches can be replayed.
+// Back end, one launch per stage over the whole batch (coding blocks are
+// numbered across the streams of a kind and found back by binary search):
+//   symPlan -> tables -> huffman (Huff) | zero counts -> run scan -> symbols
+// Every read of the bit stream is bounds-checked, and malformed tables or
+// codes raise CC_ERR_CORRUPT_STREAM instead of reading or writing out of
+// bounds.
 #include <cstring>
 
 #include "capi_internal.cuh"
@@ -15,52 +24,201 @@
 namespace ccb {
 
 struct DecParams {
-    int kind;
-    u32 S;
-    u32 cb;
-    u32 log2Max;
-    u32 symBytes;
-    u32 leavesMax;
-    u32 blocksMax;
-    u64 nStride;
-    const u32* words;        // staged bit-stream words
-    u64 wordCount;
-    const DecTableDesc* tables;
-    const DecStreamDesc* streams;
+    u32 S, T, nSrc, nRl, nH;
+    u32 rlBlocks, hBlocks;     // coding blocks (upper bounds) of the RLHuff / Huff streams
+    u32 cb, log2Max, symBytes, leavesMax;
+    u64 capLeaves;
+    DecStreamDesc* streams;
+    DecTableDesc* tables;
+    DecSource* sources;
+    const u32* rlList;         // RLHuff stream indices (by blockFirst)
+    const u32* hList;          // Huff stream indices (by blockFirst)
+    const u32* wordsBase;      // indirect sources (device walk): base + wordOff[k], bitSize[k]
+    const u64* wordOff;
+    const u64* bitSize;
     DecTable* dec;
-    u32* syms;               // [T][leavesMax]
-    u32* lut;                // [T][1 << kLutBits]
-    u32* blockOff;           // [T][blocksMax]  absolute bit offsets
-    u32* blockSum;           // [S][blocksMax]
-    char* zc;                // decoded zero counts [S][nStride]
+    u32* syms;                 // [capLeaves]
+    u32* lut;                  // [T][1 << kLutBits]
+    u32* blockOff;             // coding-block bit offsets, by table blockOff
+    u32* blockSum;             // RLHuff: per zero-count block output lengths
+    char* zc;                  // decoded zero counts, by stream zcOff
     u32* errors;
 };
 
-__device__ __forceinline__ u32 wordAt(const DecParams& p, u64 w) { return w < p.wordCount ? p.words[w] : 0u; }
+// Bounds-checked view of one bit stream's words.
+struct WordSrc {
+    const u32* w;
+    u64 n;
+    __device__ __forceinline__ u32 at(u64 i) const { return i < n ? w[i] : 0u; }
+    __device__ __forceinline__ u32 bits(u64 bit, u32 count) const {
+        if (count == 0) return 0;
+        const u64 wi = bit >> 5;
+        const u32 b = u32(bit & 31u);
+        const u64 window = (u64(at(wi)) << 32) | at(wi + 1);
+        return u32((window << b) >> (64 - count));
+    }
+};
 
-__device__ __forceinline__ u32 readBitsAt(const DecParams& p, u64 bit, u32 count) {
-    if (count == 0) return 0;
-    const u64 w = bit >> 5;
-    const u32 b = u32(bit & 31u);
-    const u64 window = (u64(wordAt(p, w)) << 32) | wordAt(p, w + 1);
-    return u32((window << b) >> (64 - count));
+__device__ __forceinline__ WordSrc srcOf(const DecParams& p, u32 stream) {
+    const DecSource& s = p.sources[p.streams[stream].source];
+    return WordSrc{s.words, s.wordCount};
 }
 
+__device__ __forceinline__ bool capacityFailed(const DecParams& p) {
+    return (*reinterpret_cast<volatile const u32*>(p.errors) & DEV_ERR_TABLE_CAPACITY) != 0;
+}
+
+// Stream owning flattened block `b` of the RLHuff (or Huff) list.
+__device__ __forceinline__ u32 streamOfBlock(const DecParams& p, const u32* list, u32 count, u32 b) {
+    u32 lo = 0, hi = count;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (p.streams[list[mid]].blockFirst <= b) lo = mid; else hi = mid;
+    }
+    return list[lo];
+}
+
+// ---------------------------------------------------------------------------
+// Device walk (HuffmanTable.cu:117-151 header fields, Encode.cpp:473-646 /
+// 792-917 stream layout, BitStream.h:290-308 alignment).
+// ---------------------------------------------------------------------------
+struct DevReader {
+    const u32* w;
+    u64 nWords, size, pos;
+    bool ok;
+    __device__ u32 read(u32 n) {
+        if (n == 0) return 0;
+        if (pos + n > size) { ok = false; pos = size; return 0; }
+        const u64 wi = pos >> 5;
+        const u32 b = u32(pos & 31u);
+        const u64 window = (u64(wi < nWords ? w[wi] : 0u) << 32) | (wi + 1 < nWords ? w[wi + 1] : 0u);
+        pos += n;
+        return u32((window << b) >> (64 - n));
+    }
+    __device__ void align() {
+        const u64 a = (pos + 31) / 32 * 32;
+        pos = a < size ? a : size;
+    }
+    __device__ void skip(u64 n) { pos = pos + n < size ? pos + n : size; }
+};
+
+__device__ bool walkTableDev(DevReader& r, u32 log2Max, u32 leavesMax, DecTableDesc& d) {
+    d.hdrBit = r.pos;
+    d.nLen = r.read(5);
+    r.skip(u64(d.nLen) * log2Max);
+    d.nSym = r.read(log2Max);
+    const bool longSym = log2Max > 16;
+    d.symbolBits = r.read(longSym ? 5 : 4);
+    if (!longSym && d.symbolBits == 0 && d.nSym > 1) d.symbolBits = 16;   // HuffmanTable.cu:138-139
+    r.skip(u64(d.nSym) * d.symbolBits);
+    return r.ok && d.nSym <= leavesMax && d.nLen <= 31;
+}
+
+__device__ bool walkPayloadDev(DevReader& r, u32 count, u32 cb, DecTableDesc& d) {
+    r.align();
+    d.cwBits = r.read(32);
+    d.cwWord = r.pos / 32;
+    r.skip(ceilDiv(d.cwBits, 32) * 32);
+    r.align();
+    d.offWord = r.pos / 32;
+    r.skip(ceilDiv(count, cb) * 16);
+    r.align();
+    d.count = count;
+    return r.ok;
+}
+
+__global__ void __launch_bounds__(64) k_decWalk(DecParams p) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.nSrc) return;
+    DecSource& src = p.sources[i];
+    if (p.wordOff) {
+        const u64 bits = p.bitSize[i];
+        src.words = p.wordsBase + p.wordOff[i];
+        src.bitSize = bits;
+        src.wordCount = ceilDiv(bits, 32);
+    }
+    const u64 wordBits = src.wordCount * 32ull;
+    DevReader r{src.words, src.wordCount, src.bitSize < wordBits ? src.bitSize : wordBits, src.startBit, true};
+    bool ok = true;
+    for (u32 k = 0; k < src.streamCount && ok; ++k) {
+        const u32 s = src.firstStream + k;
+        DecStreamDesc& sd = p.streams[s];
+        DecTableDesc& t0 = p.tables[sd.tableFirst];
+        if (sd.kind == KIND_RLHUFF) {
+            r.align();
+            const u32 m = r.read(32);
+            ok = r.ok && m <= sd.n;
+            sd.m = ok ? m : 0u;
+            DecTableDesc& t1 = p.tables[sd.tableFirst + 1];
+            ok = ok && walkTableDev(r, p.log2Max, p.leavesMax, t0) && walkPayloadDev(r, m, p.cb, t0);
+            ok = ok && walkTableDev(r, p.log2Max, p.leavesMax, t1) && walkPayloadDev(r, m, p.cb, t1);
+        } else {
+            sd.m = sd.n;
+            ok = walkTableDev(r, p.log2Max, p.leavesMax, t0) && walkPayloadDev(r, sd.n, p.cb, t0);
+        }
+    }
+    if (!ok) {
+        atomicOr(p.errors, DEV_ERR_CORRUPT);
+        // nothing of this source is decoded
+        for (u32 k = 0; k < src.streamCount; ++k) {
+            DecStreamDesc& sd = p.streams[src.firstStream + k];
+            sd.m = 0;
+            const u32 parts = sd.kind == KIND_RLHUFF ? 2u : 1u;
+            for (u32 w = 0; w < parts; ++w) {
+                DecTableDesc& t = p.tables[sd.tableFirst + w];
+                t.count = 0;
+                t.nSym = 0;
+                t.nLen = 0;
+                t.hdrBit = t.cwWord = t.offWord = 0;
+                t.cwBits = 0;
+                t.symbolBits = 0;
+            }
+        }
+    }
+    src.endBit = r.pos;
+}
+
+// Symbol array offsets of the tables (prefix of nSym) and capacity check.
+__global__ void __launch_bounds__(1024) k_decSymPlan(DecParams p) {
+    __shared__ u32 scratch[40];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (u32 base = 0; base < p.T; base += 1024) {
+        const u32 t = base + threadIdx.x;
+        u32 v = 0;
+        if (t < p.T) v = min(p.tables[t].nSym, p.leavesMax);
+        u32 tot;
+        const u32 ex = blockExclusiveSum<1024>(v, scratch, &tot);
+        if (t < p.T) p.tables[t].symOff = u32(carry + ex);
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && carry > p.capLeaves) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+}
+
+// ---------------------------------------------------------------------------
 // Table parse and decode structures (HuffmanTable.cu:117-151, :205-266).
+// ---------------------------------------------------------------------------
 constexpr u32 kDecThreads = 256;
 
 __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
     __shared__ u32 cpl[32];
     __shared__ int sFirst[32], sMin[32], sMax[32];
     __shared__ u32 sScan[40];
-    __shared__ u32 sCarry;
+    __shared__ u32 sCarry, sFail;
     const u32 t = blockIdx.x;
+    if (threadIdx.x == 0) sFail = capacityFailed(p) ? 1u : 0u;
+    __syncthreads();
+    if (sFail) return;
     const DecTableDesc d = p.tables[t];
+    const WordSrc ws = srcOf(p, d.stream);
     DecTable* D = p.dec + t;
-    u32* syms = p.syms + u64(t) * p.leavesMax;
+    u32* syms = p.syms + d.symOff;
     u32* lut = p.lut + (u64(t) << kLutBits);
     const u64 cntBit = d.hdrBit + 5;
-    if (threadIdx.x < 32) cpl[threadIdx.x] = threadIdx.x < d.nLen ? readBitsAt(p, cntBit + u64(threadIdx.x) * p.log2Max, p.log2Max) : 0u;
+    if (threadIdx.x < 32) cpl[threadIdx.x] = threadIdx.x < d.nLen ? ws.bits(cntBit + u64(threadIdx.x) * p.log2Max, p.log2Max) : 0u;
     __syncthreads();
     if (threadIdx.x == 0) {
         // canonical codes: codeword[i] = (codeword[i-1]+1) << (len_i - len_{i-1})
@@ -92,10 +250,13 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
         sCarry = ok ? 1u : 0u;
     }
     __syncthreads();
-    if (!sCarry) return;
+    if (!sCarry) {
+        if (threadIdx.x == 0) D->nSym = 0xFFFFFFFFu;   // marks the table unusable
+        return;
+    }
     const u64 symBit = cntBit + u64(d.nLen) * p.log2Max + p.log2Max + (p.log2Max > 16 ? 5u : 4u);
     for (u32 i = threadIdx.x; i < d.nSym; i += kDecThreads) {
-        u32 v = readBitsAt(p, symBit + u64(i) * d.symbolBits, d.symbolBits);
+        u32 v = ws.bits(symBit + u64(i) * d.symbolBits, d.symbolBits);
         syms[i] = p.symBytes == 2 ? (v & 0xFFFFu) : v;
     }
     // lookup table: first length l <= kLutBits whose prefix fits the canonical range
@@ -117,18 +278,19 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
     }
     if (threadIdx.x == 0) {
         D->nSym = d.nSym;
-        D->single = d.nSym >= 1 ? (p.symBytes == 2 ? readBitsAt(p, symBit, d.symbolBits) & 0xFFFFu : readBitsAt(p, symBit, d.symbolBits)) : 0u;
+        const u32 v0 = d.nSym >= 1 ? ws.bits(symBit, d.symbolBits) : 0u;
+        D->single = p.symBytes == 2 ? (v0 & 0xFFFFu) : v0;
         sCarry = 0;
     }
     // absolute block offsets: inclusive prefix of the u16 increments (PackInc.cu:220-229)
     const u32 blocks = u32(ceilDiv(d.count, p.cb));
-    u32* bo = p.blockOff + u64(t) * p.blocksMax;
+    u32* bo = p.blockOff + d.blockOff;
     __syncthreads();
     for (u32 base = 0; base < blocks; base += kDecThreads) {
         const u32 k = base + threadIdx.x;
         u32 inc = 0;
         if (k < blocks) {
-            const u32 w = wordAt(p, d.offWord + k / 2);
+            const u32 w = ws.at(d.offWord + k / 2);
             inc = (k & 1) ? (w >> 16) : (w & 0xFFFFu);
         }
         u32 tot;
@@ -147,15 +309,18 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
 // Decodes up to `cnt` symbols of one coding block starting at absolute bit
 // `bit`, calling emit(i, symbol).
 template <class Emit>
-__device__ __forceinline__ void decodeBlock(const DecParams& p, const DecTable& D, const u32* syms, const u32* lut,
+__device__ __forceinline__ void decodeBlock(const WordSrc& ws, const DecTable& D, const u32* syms, const u32* lut,
                                             u64 bit, u32 cnt, bool& corrupt, Emit emit) {
-    if (D.nSym <= 1) {
-        for (u32 i = 0; i < cnt; ++i) emit(i, D.single);
+    const u32 nSym = D.nSym;
+    if (nSym == 0xFFFFFFFFu) { corrupt = true; return; }
+    if (nSym <= 1) {
+        const u32 single = D.single;
+        for (u32 i = 0; i < cnt; ++i) emit(i, single);
         return;
     }
     u64 w = bit >> 5;
     u32 bpos = u32(bit & 31u);
-    u64 cache = (u64(wordAt(p, w)) << 32) | wordAt(p, w + 1);
+    u64 cache = (u64(ws.at(w)) << 32) | ws.at(w + 1);
     w += 2;
     for (u32 i = 0; i < cnt; ++i) {
         const u32 v = u32((cache << bpos) >> 32);
@@ -170,48 +335,60 @@ __device__ __forceinline__ void decodeBlock(const DecParams& p, const DecTable& 
             if (len > 31) { corrupt = true; return; }
             idx = u32(D.firstIndex[len - 1] + int(v >> (32 - len)) - D.minCode[len - 1]);
         }
-        if (idx >= D.nSym) { corrupt = true; return; }
+        if (idx >= nSym) { corrupt = true; return; }
         emit(i, syms[idx]);
         bpos += len;
         if (bpos >= 32) {
-            cache = (cache << 32) | wordAt(p, w);
+            cache = (cache << 32) | ws.at(w);
             ++w;
             bpos -= 32;
         }
     }
 }
 
-// decodeHuff: one thread per coding block, output staged through shared
-// memory so each warp writes its 32 blocks coalesced.
+// decodeHuff: one thread per coding block; when a warp's 32 blocks belong to
+// one stream its output is staged through shared memory and written coalesced.
 template <class Sym>
 __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
     extern __shared__ __align__(16) unsigned char stage[];
-    const u32 s = blockIdx.y;
+    if (__any_sync(0xffffffffu, capacityFailed(p))) return;
     const u32 lane = threadIdx.x;
-    const DecStreamDesc sd = p.streams[s];
-    const u32 blocks = u32(ceilDiv(sd.n, p.cb));
     const u32 b0 = blockIdx.x * 32;
-    if (b0 >= blocks) return;
-    const u32 b = b0 + lane;
+    const u32 gb = b0 + lane;
+    const bool valid = gb < p.hBlocks;
+    const u32 s = streamOfBlock(p, p.hList, p.nH, valid ? gb : p.hBlocks - 1);
+    const u32 s0 = __shfl_sync(0xffffffffu, s, 0);
+    const bool uniform = __all_sync(0xffffffffu, !valid || s == s0);
+    const DecStreamDesc sd = p.streams[s];
+    const u32 b = gb - sd.blockFirst;
+    const u32 blocks = u32(ceilDiv(sd.n, p.cb));
     const u32 rowPitch = p.cb + (sizeof(Sym) == 2 ? 2 : 1);
     Sym* rows = reinterpret_cast<Sym*>(stage);
+    Sym* out = reinterpret_cast<Sym*>(sd.out);
     bool corrupt = false;
-    __shared__ DecTable D;
-    if (lane == 0) D = p.dec[s];
-    __syncwarp();
-    const u32* syms = p.syms + u64(s) * p.leavesMax;
-    const u32* lut = p.lut + (u64(s) << kLutBits);
-    if (b < blocks) {
-        const u32 i0 = b * p.cb;
+    const bool mine = valid && b < blocks;
+    const u32 i0 = b * p.cb;
+    if (mine) {
+        const u32 t = sd.tableFirst;
+        const DecTableDesc& td = p.tables[t];
+        const WordSrc ws = srcOf(p, s);
         const u32 cnt = min(p.cb, sd.n - i0);
-        const u64 bit = p.tables[s].cwWord * 32ull + p.blockOff[u64(s) * p.blocksMax + b];
-        decodeBlock(p, D, syms, lut, bit, cnt, corrupt, [&](u32 i, u32 v) { rows[lane * rowPitch + i] = Sym(v); });
+        const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
+        if (uniform)
+            decodeBlock(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+                        [&](u32 i, u32 v) { rows[lane * rowPitch + i] = Sym(v); });
+        else
+            decodeBlock(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+                        [&](u32 i, u32 v) { out[i0 + i] = Sym(v); });
     }
     if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
+    if (!uniform) return;
     __syncwarp();
-    Sym* out = reinterpret_cast<Sym*>(sd.out);
-    const u32 nb = min(32u, blocks - b0);
-    const u64 base = u64(b0) * p.cb;
+    // every lane's sd is the stream of block b0 here
+    const u32 bFirst = b0 - sd.blockFirst;
+    if (bFirst >= blocks) return;
+    const u32 nb = min(32u, blocks - bFirst);
+    const u64 base = u64(bFirst) * p.cb;
     const u64 lim = u64(sd.n) - base;
     const u64 total = u64(nb) * p.cb < lim ? u64(nb) * p.cb : lim;
     for (u64 k = lane; k < total; k += 32) out[base + k] = rows[(k / p.cb) * rowPitch + (k % p.cb)];
@@ -220,33 +397,34 @@ __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
 // decodeRLHuff, zero counts: decode and store them, and sum (zc + 1) per block.
 template <class Sym>
 __global__ void __launch_bounds__(128) k_decZc(DecParams p) {
-    const u32 s = blockIdx.y;
-    const u32 b = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 gb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gb >= p.rlBlocks || capacityFailed(p)) return;
+    const u32 s = streamOfBlock(p, p.rlList, p.nRl, gb);
     const DecStreamDesc sd = p.streams[s];
-    const u32 blocks = u32(ceilDiv(sd.m, p.cb));
-    if (b >= blocks) return;
-    const u32 t = p.S + s;
-    const DecTable& D = p.dec[t];
+    const u32 b = gb - sd.blockFirst;
+    if (b >= u32(ceilDiv(sd.m, p.cb))) return;
+    const u32 t = sd.tableFirst + 1;
+    const DecTableDesc& td = p.tables[t];
     const u32 i0 = b * p.cb;
     const u32 cnt = min(p.cb, sd.m - i0);
-    const u64 bit = p.tables[t].cwWord * 32ull + p.blockOff[u64(t) * p.blocksMax + b];
-    Sym* zc = reinterpret_cast<Sym*>(p.zc) + u64(s) * p.nStride + i0;
+    const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
+    Sym* zc = reinterpret_cast<Sym*>(p.zc) + sd.zcOff + i0;
     u32 sum = 0;
     bool corrupt = false;
-    decodeBlock(p, D, p.syms + u64(t) * p.leavesMax, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+    decodeBlock(srcOf(p, s), p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
                 [&](u32 i, u32 v) { zc[i] = Sym(v); sum += v + 1; });
     if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
-    p.blockSum[u64(s) * p.blocksMax + b] = sum;
+    p.blockSum[td.blockOff + b] = sum;
 }
 
-// Exclusive scan of the per-block output lengths (one block per stream).
+// Exclusive scan of the per-block output lengths (one block per RLHuff stream).
 __global__ void __launch_bounds__(1024) k_decScan(DecParams p) {
     __shared__ u32 scratch[40];
     __shared__ u32 carry;
-    const u32 s = blockIdx.x;
+    const u32 s = p.rlList[blockIdx.x];
     const DecStreamDesc sd = p.streams[s];
     const u32 blocks = u32(ceilDiv(sd.m, p.cb));
-    u32* bs = p.blockSum + u64(s) * p.blocksMax;
+    u32* bs = p.blockSum + p.tables[sd.tableFirst + 1].blockOff;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (u32 base = 0; base < blocks; base += 1024) {
@@ -259,31 +437,30 @@ __global__ void __launch_bounds__(1024) k_decScan(DecParams p) {
         if (threadIdx.x == 0) carry += tot;
         __syncthreads();
     }
-    if (threadIdx.x == 0 && carry > sd.n + (sd.m ? 0u : 0u)) {
-        // the last symbol's position must be < n: total length <= n
-        if (carry > sd.n) atomicOr(p.errors, DEV_ERR_CORRUPT);
-    }
+    // the last symbol's position must be < n: total length <= n
+    if (threadIdx.x == 0 && carry > sd.n) atomicOr(p.errors, DEV_ERR_CORRUPT);
 }
 
 // decodeRLHuff, symbols: decode and scatter out[scan(zc)+i] = symbol
 // (RunLengthKernels.cui:56-66).
 template <class Sym>
 __global__ void __launch_bounds__(128) k_decSymScatter(DecParams p) {
-    const u32 s = blockIdx.y;
-    const u32 b = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 gb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gb >= p.rlBlocks || capacityFailed(p)) return;
+    const u32 s = streamOfBlock(p, p.rlList, p.nRl, gb);
     const DecStreamDesc sd = p.streams[s];
-    const u32 blocks = u32(ceilDiv(sd.m, p.cb));
-    if (b >= blocks) return;
-    const u32 t = s;
-    const DecTable& D = p.dec[t];
+    const u32 b = gb - sd.blockFirst;
+    if (b >= u32(ceilDiv(sd.m, p.cb))) return;
+    const u32 t = sd.tableFirst;
+    const DecTableDesc& td = p.tables[t];
     const u32 i0 = b * p.cb;
     const u32 cnt = min(p.cb, sd.m - i0);
-    const u64 bit = p.tables[t].cwWord * 32ull + p.blockOff[u64(t) * p.blocksMax + b];
-    const Sym* zc = reinterpret_cast<const Sym*>(p.zc) + u64(s) * p.nStride + i0;
+    const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
+    const Sym* zc = reinterpret_cast<const Sym*>(p.zc) + sd.zcOff + i0;
     Sym* out = reinterpret_cast<Sym*>(sd.out);
-    u32 pos = p.blockSum[u64(s) * p.blocksMax + b];
+    u32 pos = p.blockSum[p.tables[t + 1].blockOff + b];
     bool corrupt = false;
-    decodeBlock(p, D, p.syms + u64(t) * p.leavesMax, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+    decodeBlock(srcOf(p, s), p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
                 [&](u32 i, u32 v) {
                     pos += u32(zc[i]);
                     if (pos < sd.n) out[pos] = Sym(v);
@@ -294,7 +471,7 @@ __global__ void __launch_bounds__(128) k_decSymScatter(DecParams p) {
 }
 
 // ---------------------------------------------------------------------------
-// Host side: header walk over the caller's bit streams.
+// Host side.
 // ---------------------------------------------------------------------------
 struct HostReader {
     const u32* w;
@@ -349,65 +526,192 @@ static bool walkPayload(HostReader& r, u32 count, u32 cb, DecTableDesc& d) {
     return r.ok;
 }
 
+// Descriptor layout of one call in a host buffer and in device memory.
+struct DecLayout {
+    size_t offStreams = 0, offTables, offSources, offRl, offH, bytes;
+    DecLayout(u32 S, u32 T, u32 B) {
+        offTables = alignUp(sizeof(DecStreamDesc) * S, 64);
+        offSources = alignUp(offTables + sizeof(DecTableDesc) * T, 64);
+        offRl = alignUp(offSources + sizeof(DecSource) * B, 64);
+        offH = alignUp(offRl + sizeof(u32) * S, 64);
+        bytes = offH + sizeof(u32) * S;
+    }
+};
+
+// Fills the stream/table skeleton (kinds, sizes, table and block offsets)
+// and the RLHuff / Huff lists of a call.
+static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* const* outs, const u32* sourceOf, u32 S,
+                      u32 B, char* slot, size_t slotBytes, DecPlan& dc) {
+    dc = DecPlan{};
+    u32 T = 0;
+    for (u32 s = 0; s < S; ++s) T += kinds[s] == KIND_RLHUFF ? 2u : 1u;
+    const DecLayout L(S, T, B);
+    if (S > I->capStreams || T > I->capTables || L.bytes > slotBytes) {
+        setError("decode: call exceeds the instance capacity (%u streams)", S);
+        return CC_ERR_CAPACITY;
+    }
+    DecStreamDesc* sd = reinterpret_cast<DecStreamDesc*>(slot + L.offStreams);
+    DecTableDesc* td = reinterpret_cast<DecTableDesc*>(slot + L.offTables);
+    u32* rl = reinterpret_cast<u32*>(slot + L.offRl);
+    u32* hl = reinterpret_cast<u32*>(slot + L.offH);
+    u32 t = 0;
+    u64 blocks = 0, zc = 0, rlBlocks = 0, hBlocks = 0;
+    for (u32 s = 0; s < S; ++s) {
+        const u32 nb = u32(ceilDiv(ns[s], I->codingBlockSize));
+        DecStreamDesc d{};
+        d.out = outs[s];
+        d.n = ns[s];
+        d.m = ns[s];
+        d.kind = kinds[s];
+        d.tableFirst = t;
+        d.source = sourceOf[s];
+        const u32 parts = d.kind == KIND_RLHUFF ? 2u : 1u;
+        for (u32 w = 0; w < parts; ++w) {
+            DecTableDesc tt{};
+            tt.stream = s;
+            tt.blockOff = u32(blocks);
+            blocks += nb;
+            td[t++] = tt;
+        }
+        if (d.kind == KIND_RLHUFF) {
+            d.zcOff = zc;
+            zc += ns[s];
+            d.blockFirst = u32(rlBlocks);
+            rlBlocks += nb;
+            rl[dc.nRl++] = s;
+        } else {
+            d.blockFirst = u32(hBlocks);
+            hBlocks += nb;
+            hl[dc.nH++] = s;
+        }
+        sd[s] = d;
+    }
+    if (blocks > I->capBlocks || zc > I->capCompact) {
+        setError("decode: call exceeds the instance capacity (%llu coding blocks, %llu run-length symbols)",
+                 (unsigned long long)blocks, (unsigned long long)zc);
+        return CC_ERR_CAPACITY;
+    }
+    dc.S = S;
+    dc.T = T;
+    dc.B = B;
+    dc.rlBlocks = u32(rlBlocks);
+    dc.hBlocks = u32(hBlocks);
+    dc.bytes = L.bytes;
+    return CC_OK;
+}
+
 template <class Sym>
-static int launchDecode(cc_instance* I, const DecParams& p, u32 nMax, u32 mMax) {
+static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
     cudaStream_t st = I->stream;
-    const u32 T = p.kind == KIND_RLHUFF ? 2 * p.S : p.S;
-    { SectionTimer t(I, "dec.tables", st); k_decTables<<<T, kDecThreads, 0, st>>>(p); countLaunch(); }
-    if (p.kind == KIND_HUFF) {
-        const u32 blocks = std::max<u32>(1u, u32(ceilDiv(nMax, p.cb)));
+    { SectionTimer t(I, "dec.sym_plan", st); k_decSymPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "dec.tables", st); k_decTables<<<p.T, kDecThreads, 0, st>>>(p); countLaunch(); }
+    if (p.hBlocks) {
         const size_t smem = size_t(32) * (p.cb + 2) * sizeof(Sym);
-        CC_TRY_CUDA(cudaFuncSetAttribute(k_decHuff<Sym>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "decHuff smem");
-        { SectionTimer t(I, "dec.huffman", st); k_decHuff<Sym><<<dim3(u32(ceilDiv(blocks, 32)), p.S), 32, smem, st>>>(p); countLaunch(); }
-    } else {
-        const u32 blocks = std::max<u32>(1u, u32(ceilDiv(mMax, p.cb)));
-        dim3 g(u32(ceilDiv(blocks, 128)), p.S);
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<Sym>),
+                                        sizeof(Sym) == 2 ? kAttrDecHuff16 : kAttrDecHuff32, I->device, smem),
+                    "decHuff smem");
+        SectionTimer t(I, "dec.huffman", st);
+        k_decHuff<Sym><<<u32(ceilDiv(p.hBlocks, 32)), 32, smem, st>>>(p);
+        countLaunch();
+    }
+    if (p.rlBlocks) {
+        const u32 g = u32(ceilDiv(p.rlBlocks, 128));
         { SectionTimer t(I, "dec.zero_counts", st); k_decZc<Sym><<<g, 128, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.nRl, 1024, 0, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.symbols_scatter", st); k_decSymScatter<Sym><<<g, 128, 0, st>>>(p); countLaunch(); }
     }
     CC_TRY_CUDA(cudaGetLastError(), "decode launch");
     return CC_OK;
 }
 
+int prepareDecodeAttributes(cc_instance* I) {
+    const size_t smem = size_t(32) * (I->codingBlockSize + 2) * I->symBytes;
+    if (I->symBytes == 2)
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u16>), kAttrDecHuff16, I->device, smem), "decHuff smem");
+    else
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u32>), kAttrDecHuff32, I->device, smem), "decHuff smem");
+    return CC_OK;
+}
+
+static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
+    const DecLayout L(dc.S, dc.T, dc.B);
+    char* d = static_cast<char*>(dc.dev);
+    DecParams p{};
+    p.S = dc.S;
+    p.T = dc.T;
+    p.nSrc = dc.B;
+    p.nRl = dc.nRl;
+    p.nH = dc.nH;
+    p.rlBlocks = dc.rlBlocks;
+    p.hBlocks = dc.hBlocks;
+    p.cb = I->codingBlockSize;
+    p.log2Max = I->log2Max;
+    p.symBytes = I->symBytes;
+    p.leavesMax = I->leavesMax;
+    p.capLeaves = I->capLeaves;
+    p.streams = reinterpret_cast<DecStreamDesc*>(d + L.offStreams);
+    p.tables = reinterpret_cast<DecTableDesc*>(d + L.offTables);
+    p.sources = reinterpret_cast<DecSource*>(d + L.offSources);
+    p.rlList = reinterpret_cast<const u32*>(d + L.offRl);
+    p.hList = reinterpret_cast<const u32*>(d + L.offH);
+    p.wordsBase = dc.wordsBase;
+    p.wordOff = dc.wordOff;
+    p.bitSize = dc.bitSize;
+    p.dec = I->decTables;
+    p.syms = I->decSyms;
+    p.lut = I->decLut;
+    p.blockOff = I->blockOff;
+    p.blockSum = I->blockSum;
+    p.zc = static_cast<char*>(I->zc);
+    p.errors = I->errors + 4;
+    return p;
+}
+
+// Host-walk front end (cc_decode): the reference's decode entry points.
 int decodeDevice(cc_instance* I, int kind, const u32* const* words, const u32* bitSizes, u32* bitPos, u32 bsCount,
                  const u32* bsIndex, void* const* outs, u32 S, u32 n) {
     if (S == 0) return CC_OK;
     if (S > I->streamCountMax) { setError("stream count %u exceeds instance limit %u", S, I->streamCountMax); return CC_ERR_CAPACITY; }
     if (n > I->elemCountPerStreamMax) { setError("symbol count %u exceeds instance limit %u", n, I->elemCountPerStreamMax); return CC_ERR_CAPACITY; }
-    const u32 T = kind == KIND_RLHUFF ? 2 * S : S;
+    std::vector<u32> kinds(S, u32(kind)), ns(S, n), srcOf(S);
+    for (u32 s = 0; s < S; ++s) {
+        srcOf[s] = bsIndex ? bsIndex[s] : 0u;
+        if (srcOf[s] >= bsCount) { setError("decode: bit stream index out of range"); return CC_ERR_INVALID_ARGUMENT; }
+    }
     char* slot = I->takeRingSlot();
-    DecTableDesc* td = reinterpret_cast<DecTableDesc*>(slot);
-    DecStreamDesc* sd = reinterpret_cast<DecStreamDesc*>(slot + alignUp(sizeof(DecTableDesc) * T, 64));
+    DecPlan dc;
+    int rc = planDecode(I, kinds.data(), ns.data(), outs, srcOf.data(), S, bsCount, slot, I->hostRingBytes, dc);
+    if (rc) return rc;
+    const DecLayout L(dc.S, dc.T, dc.B);
+    DecStreamDesc* sd = reinterpret_cast<DecStreamDesc*>(slot + L.offStreams);
+    DecTableDesc* td = reinterpret_cast<DecTableDesc*>(slot + L.offTables);
+    DecSource* src = reinterpret_cast<DecSource*>(slot + L.offSources);
     // walk the headers
     std::vector<u64> lo(bsCount, ~0ull), hi(bsCount, 0);
     std::vector<HostReader> rd(bsCount);
     for (u32 k = 0; k < bsCount; ++k) rd[k] = HostReader{words[k], bitSizes[k], bitPos[k]};
-    u32 mMax = 0;
     for (u32 s = 0; s < S; ++s) {
-        const u32 k = bsIndex ? bsIndex[s] : 0u;
-        if (k >= bsCount) { setError("decode: bit stream index out of range"); return CC_ERR_INVALID_ARGUMENT; }
+        const u32 k = srcOf[s];
         HostReader& r = rd[k];
         u64 start = r.pos;
         bool ok = true;
         u32 m = n;
+        DecTableDesc& t0 = td[sd[s].tableFirst];
         if (kind == KIND_RLHUFF) {
             r.align();
             start = r.pos;
             m = r.readBits(32);
             ok = r.ok && m <= n;
-            ok = ok && walkTable(r, I->log2Max, I->leavesMax, td[s]) && walkPayload(r, m, I->codingBlockSize, td[s]);
-            ok = ok && walkTable(r, I->log2Max, I->leavesMax, td[S + s]) && walkPayload(r, m, I->codingBlockSize, td[S + s]);
+            DecTableDesc& t1 = td[sd[s].tableFirst + 1];
+            ok = ok && walkTable(r, I->log2Max, I->leavesMax, t0) && walkPayload(r, m, I->codingBlockSize, t0);
+            ok = ok && walkTable(r, I->log2Max, I->leavesMax, t1) && walkPayload(r, m, I->codingBlockSize, t1);
         } else {
-            ok = walkTable(r, I->log2Max, I->leavesMax, td[s]) && walkPayload(r, n, I->codingBlockSize, td[s]);
+            ok = walkTable(r, I->log2Max, I->leavesMax, t0) && walkPayload(r, n, I->codingBlockSize, t0);
         }
         if (!ok) { setError("decode: corrupt or truncated bit stream (stream %u)", s); return CC_ERR_CORRUPT_STREAM; }
         lo[k] = std::min<u64>(lo[k], start / 32);
         hi[k] = std::max<u64>(hi[k], ceilDiv(r.pos, 32));
-        sd[s].out = outs[s];
-        sd[s].n = n;
         sd[s].m = m;
-        mMax = std::max(mMax, m);
     }
     // stage the touched words of every bit stream and rebase the positions
     std::vector<u64> base(bsCount, 0);
@@ -420,47 +724,65 @@ int decodeDevice(cc_instance* I, int kind, const u32* const* words, const u32* b
     if (total > I->stagedWordsMax) { setError("decode: bit stream larger than the instance staging (%llu words)", (unsigned long long)total); return CC_ERR_CAPACITY; }
     cudaStream_t st = I->stream;
     for (u32 k = 0; k < bsCount; ++k) {
+        const u64 span = hi[k] > lo[k] ? hi[k] - lo[k] + 2 : 0;
+        src[k] = DecSource{I->stagedWords + base[k], span, span * 32, 0, 0, 0, 0};
         if (hi[k] <= lo[k]) continue;
         const u64 nw = std::min<u64>(hi[k], ceilDiv(bitSizes[k], 32)) - lo[k];
         CC_TRY_CUDA(cudaMemcpyAsync(I->stagedWords + base[k], words[k] + lo[k], nw * 4, cudaMemcpyHostToDevice, st), "stage bit stream");
-        CC_TRY_CUDA(cudaMemsetAsync(I->stagedWords + base[k] + nw, 0, (hi[k] - lo[k] + 2 - nw) * 4, st), "pad staging");
+        CC_TRY_CUDA(cudaMemsetAsync(I->stagedWords + base[k] + nw, 0, (span - nw) * 4, st), "pad staging");
     }
-    for (u32 t = 0; t < T; ++t) {
-        const u32 s = t < S ? t : t - S;
-        const u32 k = bsIndex ? bsIndex[s] : 0u;
-        const u64 shiftBits = (lo[k] - base[k]) * 32;
-        td[t].hdrBit -= shiftBits;
-        td[t].cwWord -= lo[k] - base[k];
-        td[t].offWord -= lo[k] - base[k];
+    for (u32 t = 0; t < dc.T; ++t) {
+        const u32 k = srcOf[td[t].stream];
+        td[t].hdrBit -= lo[k] * 32;
+        td[t].cwWord -= lo[k];
+        td[t].offWord -= lo[k];
     }
-    CC_TRY_CUDA(cudaMemcpyAsync(I->dDecTables, td, sizeof(DecTableDesc) * T, cudaMemcpyHostToDevice, st), "upload tables");
-    CC_TRY_CUDA(cudaMemcpyAsync(I->dDecStreams, sd, sizeof(DecStreamDesc) * S, cudaMemcpyHostToDevice, st), "upload streams");
+    dc.dev = I->dPlan;
+    CC_TRY_CUDA(cudaMemcpyAsync(I->dPlan, slot, L.bytes, cudaMemcpyHostToDevice, st), "upload decode plan");
     cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
     CC_TRY_CUDA(cudaMemsetAsync(I->errors + 4, 0, sizeof(u32), st), "memset errors");
-    DecParams p{};
-    p.kind = kind;
-    p.S = S;
-    p.cb = I->codingBlockSize;
-    p.log2Max = I->log2Max;
-    p.symBytes = I->symBytes;
-    p.leavesMax = I->leavesMax;
-    p.blocksMax = I->blocksMax;
-    p.nStride = I->elemCountPerStreamMax;
-    p.words = I->stagedWords;
-    p.wordCount = total;
-    p.tables = I->dDecTables;
-    p.streams = I->dDecStreams;
-    p.dec = I->decTables;
-    p.syms = I->decSyms;
-    p.lut = I->decLut;
-    p.blockOff = I->blockOff;
-    p.blockSum = I->blockSum;
-    p.zc = static_cast<char*>(I->zc);
-    p.errors = I->errors + 4;
-    int rc = I->symBytes == 2 ? launchDecode<u16>(I, p, n, mMax) : launchDecode<u32>(I, p, n, mMax);
+    const DecParams p = makeDecParams(I, dc);
+    rc = I->symBytes == 2 ? launchDecodeBackEnd<u16>(I, p) : launchDecodeBackEnd<u32>(I, p);
     if (rc) return rc;
     for (u32 k = 0; k < bsCount; ++k) bitPos[k] = u32(rd[k].pos);
     return CC_OK;
+}
+
+// Device-walk front end, step 1: descriptors into `slot`.
+int decodePrepare(cc_instance* I, const DecStreamSpec* streams, u32 S, const DecSourceSpec* sources, u32 B,
+                  char* slot, size_t slotBytes, DecPlan& dc) {
+    std::vector<u32> kinds(S), ns(S), srcOf(S);
+    std::vector<void*> outs(S);
+    for (u32 s = 0; s < S; ++s) {
+        kinds[s] = streams[s].kind;
+        ns[s] = streams[s].n;
+        outs[s] = streams[s].out;
+        srcOf[s] = streams[s].source;
+        if (srcOf[s] >= B) { setError("decode: source index out of range"); return CC_ERR_INVALID_ARGUMENT; }
+        if (s > 0 && srcOf[s] < srcOf[s - 1]) { setError("decode: streams must be grouped by source"); return CC_ERR_INVALID_ARGUMENT; }
+    }
+    int rc = planDecode(I, kinds.data(), ns.data(), outs.data(), srcOf.data(), S, B, slot, slotBytes, dc);
+    if (rc) return rc;
+    const DecLayout L(dc.S, dc.T, dc.B);
+    DecSource* src = reinterpret_cast<DecSource*>(slot + L.offSources);
+    for (u32 k = 0; k < B; ++k)
+        src[k] = DecSource{sources[k].words, ceilDiv(sources[k].bitSize, 32), sources[k].bitSize, sources[k].startBit, 0, 0, 0};
+    for (u32 s = 0; s < S; ++s) {
+        DecSource& d = src[srcOf[s]];
+        if (d.streamCount == 0) d.firstStream = s;
+        ++d.streamCount;
+    }
+    return CC_OK;
+}
+
+// Device-walk front end, step 2: the launches (descriptors at dc.dev).
+int decodeLaunch(cc_instance* I, const DecPlan& dc) {
+    if (dc.S == 0) return CC_OK;
+    cudaStream_t st = I->stream;
+    CC_TRY_CUDA(cudaMemsetAsync(I->errors + 4, 0, sizeof(u32), st), "memset errors");
+    const DecParams p = makeDecParams(I, dc);
+    { SectionTimer t(I, "dec.walk", st); k_decWalk<<<u32(ceilDiv(dc.B, 64)), 64, 0, st>>>(p); countLaunch(); }
+    return I->symBytes == 2 ? launchDecodeBackEnd<u16>(I, p) : launchDecodeBackEnd<u32>(I, p);
 }
 
 }  // namespace ccb

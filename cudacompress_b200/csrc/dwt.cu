@@ -13,7 +13,7 @@
 // Int: CDF 5/3 lifting on shorts (DWTIntKernels.cui:14-1188) with the
 // reference's rounding (DWTCommon.cuh:133-142), including the narrowing of
 // every intermediate to 16 bits.
-#include "capi_internal.cuh"
+#include "batch.cuh"
 
 namespace ccb {
 
@@ -322,6 +322,155 @@ static int dwtScratchFor(int device, float** out) {
     }
     *out = p;
     return CC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched passes (batch.cuh): the same arithmetic as k_firRows / k_firCols /
+// k_quantize, over all volumes of a batch in one launch.
+// ---------------------------------------------------------------------------
+template <class Desc>
+__device__ __forceinline__ u32 findDesc(const Desc* d, u32 nd, u32 cta) {
+    u32 lo = 0, hi = nd;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (d[mid].ctaOff <= cta) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <bool kInverse>
+__global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ descs, u32 nd,
+                                               const float* const* inTab, float* const* outTab) {
+    __shared__ float s[1024 + 64];
+    __shared__ u32 sDesc;
+    if (threadIdx.x == 0) sDesc = findDesc(descs, nd, blockIdx.x);
+    __syncthreads();
+    const BRowDesc D = descs[sDesc];
+    const float* src = D.src ? D.src : inTab[D.vol];
+    float* dst = D.dst ? D.dst : outTab[D.vol];
+    const u32 local = blockIdx.x - D.ctaOff;
+    const int xt = int(local % u32(D.tilesX)), rg = int(local / u32(D.tilesX));
+    const int x0 = xt * D.W, Wp = D.W + 8, rows = D.ny * D.nz;
+    for (int k = threadIdx.x; k < D.R * Wp; k += 256) {
+        const int j = k / Wp, kk = k - j * Wp, r = rg * D.R + j;
+        const int xx = x0 - 4 + kk;
+        if (r < rows && xx < D.nx + 4) {
+            const int m = mirrorIdx(xx, D.nx);
+            const int y = r % D.ny, z = r / D.ny;
+            s[k] = src[size_t(z) * D.srcSlice + size_t(y) * D.srcRow + (kInverse ? splitPos(m, D.nx) : m)];
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < D.R * D.W; k += 256) {
+        const int j = k / D.W, kk = k - j * D.W, r = rg * D.R + j, x = x0 + kk;
+        if (r < rows && x < D.nx) {
+            const int y = r % D.ny, z = r / D.ny;
+            const float v = fir9<kInverse>(s + j * Wp + kk, x & 1);
+            dst[size_t(z) * D.dstSlice + size_t(y) * D.dstRow + (kInverse ? x : splitPos(x, D.nx))] = v;
+        }
+    }
+}
+
+template <bool kInverse, bool kSymbols>
+__global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ descs, u32 nd) {
+    __shared__ float s[kColTile + 8][33];
+    __shared__ u32 sDesc;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (tx == 0 && ty == 0) sDesc = findDesc(descs, nd, blockIdx.x);
+    __syncthreads();
+    const BColDesc& D = descs[sDesc];
+    const u32 local = blockIdx.x - D.ctaOff;
+    const u32 xt = local % D.tilesX, rest = local / D.tilesX;
+    const int at = int(rest % D.tilesA), c = int(rest / D.tilesA);
+    const int nx = D.nx, na = D.na;
+    const int x = int(xt) * 32 + tx;
+    const int a0 = at * kColTile;
+    if (x < nx) {
+        for (int k = ty; k < kColTile + 8; k += 8) {
+            const int j = a0 - 4 + k;
+            if (j < na + 4) {
+                const int m = mirrorIdx(j, na);
+                const int a = kInverse ? splitPos(m, na) : m;
+                float v;
+                if (kSymbols) {
+                    // axis Z: a = z, c = y (DWTFloatFromSymbolsKernels.cui:18-464)
+                    const int y = c, z = a;
+                    const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
+                    const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
+                    const int b = bx + 2 * by + 4 * bz;
+                    if (b == 0) {
+                        v = D.src[size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx];
+                    } else {
+                        const u32 sym = D.bands[u64(b - 1) * D.bandStride + (u64(lz) * D.hy + ly) * D.hx + lx];
+                        const int q = unsymbolizeI(sym);
+                        v = (float(q) + signI(q) * 0.5f) * D.step;
+                    }
+                } else {
+                    v = D.src[size_t(x) * D.sx + size_t(a) * D.sa + size_t(c) * D.sc];
+                }
+                s[k][tx] = v;
+            }
+        }
+    }
+    __syncthreads();
+    if (x >= nx) return;
+    for (int k = ty; k < kColTile; k += 8) {
+        const int a = a0 + k;
+        if (a >= na) break;
+        float v[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) v[i] = s[k + i][tx];
+        const float r = fir9<kInverse>(v, a & 1);
+        const int o = kInverse ? a : splitPos(a, na);
+        D.dst[size_t(x) * D.dx + size_t(o) * D.da + size_t(c) * D.dc] = r;
+    }
+}
+
+template <bool kDequantize>
+__global__ void __launch_bounds__(256) k_bQuant(const BQuantDesc* __restrict__ descs, u32 nd) {
+    __shared__ u32 sDesc;
+    if (threadIdx.x == 0) sDesc = findDesc(descs, nd, blockIdx.x);
+    __syncthreads();
+    const BQuantDesc& D = descs[sDesc];
+    const u64 plane = u64(D.nx) * D.ny, total = plane * D.nz;
+    const u64 e0 = u64(blockIdx.x - D.ctaOff) * kBQuantPerCta;
+    for (u32 k = threadIdx.x; k < u32(kBQuantPerCta); k += 256) {
+        const u64 e = e0 + k;
+        if (e >= total) break;
+        if (kDequantize) {
+            const int q = unsymbolizeI(u32(D.sym[e]));
+            D.dstF[e] = (float(q) + signI(q) * 0.5f) * D.step;   // Quantize.cuh:104-110
+        } else {
+            const u32 z = u32(e / plane), r = u32(e - u64(z) * plane);
+            const u32 y = r / u32(D.nx), xx = r - y * u32(D.nx);
+            const float v = D.src[size_t(z) * D.slice + size_t(y) * D.row + xx];
+            D.sym[e] = u16(symbolizeI(int(v * D.inv)));            // Quantize.cuh:55-59 deadzone
+        }
+    }
+}
+
+void launchBatchRows(const BRowDesc* d, u32 nd, u32 ctas, bool inverse, const float* const* inTab,
+                     float* const* outTab, cudaStream_t st) {
+    if (!ctas) return;
+    if (inverse) k_bRows<true><<<ctas, 256, 0, st>>>(d, nd, inTab, outTab);
+    else k_bRows<false><<<ctas, 256, 0, st>>>(d, nd, inTab, outTab);
+    countLaunch();
+}
+
+void launchBatchCols(const BColDesc* d, u32 nd, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st) {
+    if (!ctas) return;
+    const dim3 blk(32, 8);
+    if (fromSymbols) k_bCols<true, true><<<ctas, blk, 0, st>>>(d, nd);
+    else if (inverse) k_bCols<true, false><<<ctas, blk, 0, st>>>(d, nd);
+    else k_bCols<false, false><<<ctas, blk, 0, st>>>(d, nd);
+    countLaunch();
+}
+
+void launchBatchQuant(const BQuantDesc* d, u32 nd, u32 ctas, bool dequantize, cudaStream_t st) {
+    if (!ctas) return;
+    if (dequantize) k_bQuant<true><<<ctas, 256, 0, st>>>(d, nd);
+    else k_bQuant<false><<<ctas, 256, 0, st>>>(d, nd);
+    countLaunch();
 }
 
 }  // namespace ccb

@@ -816,17 +816,28 @@ __global__ void __launch_bounds__(128) k_headers(EncParams p) {
     }
 }
 
+// Word offset and bit size of each volume's stream in a batched encode's
+// output: volume v owns streams first[v] .. first[v+1]-1, written back to back.
+__global__ void k_volumeExtents(const SegmentLayout* layout, const u32* first, u32 count, u64* wordOff,
+                                u64* bitSize, const u32* errors) {
+    const u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= count) return;
+    if (*errors) { wordOff[v] = 0; bitSize[v] = 0; return; }
+    const u32 a = first[v], b = first[v + 1];
+    const u64 off = layout[a].startWord;
+    const u64 end = layout[b - 1].startWord + layout[b - 1].words;
+    wordOff[v] = off;
+    bitSize[v] = (end - off) * 32ull;
+}
+
 // ---------------------------------------------------------------------------
 // Host orchestration.
 // ---------------------------------------------------------------------------
-struct HostPlan {
-    u32 T = 0, tiles = 0, blocks = 0, maxCount = 0;
-    u64 compact = 0;
-    size_t offTables = 0, bytes = 0;
-};
-
-// Writes the stream and table descriptors of a call into `slot` (pinned).
-static int buildPlan(cc_instance* I, const EncStream* streams, u32 S, char* slot, HostPlan& hp) {
+// Writes the stream and table descriptors of a call into `slot` (host) and
+// returns its summary; slotBytes bounds the descriptors.
+int encodePrepare(cc_instance* I, const EncStream* streams, u32 S, char* slot, size_t slotBytes, EncPlan& hp) {
+    hp = EncPlan{};
+    hp.S = S;
     for (u32 s = 0; s < S; ++s) {
         const EncStream& e = streams[s];
         const u64 nb = ceilDiv(e.n, I->codingBlockSize);
@@ -844,7 +855,7 @@ static int buildPlan(cc_instance* I, const EncStream* streams, u32 S, char* slot
     }
     hp.offTables = alignUp(sizeof(EncStreamDev) * S, 64);
     hp.bytes = hp.offTables + sizeof(EncTableDev) * hp.T;
-    if (hp.bytes > I->hostRingBytes) { setError("encode: descriptors exceed the staging slot"); return CC_ERR_CAPACITY; }
+    if (hp.bytes > slotBytes) { setError("encode: descriptors exceed the staging slot"); return CC_ERR_CAPACITY; }
     EncStreamDev* sd = reinterpret_cast<EncStreamDev*>(slot);
     EncTableDev* td = reinterpret_cast<EncTableDev*>(slot + hp.offTables);
     u32 tile = 0, table = 0, block = 0;
@@ -885,7 +896,8 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) { SectionTimer t(I, "enc.rle_write_hist", st); k_write<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
     const size_t buildSmem = sizeof(u64) * (p.heapCap + 2) + 3 * sizeof(u32) * size_t(p.heapCap);
-    CC_TRY_CUDA(cudaFuncSetAttribute(k_tableBuild, cudaFuncAttributeMaxDynamicSharedMemorySize, int(buildSmem)), "tableBuild smem");
+    CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
+                "tableBuild smem");
     { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
     if (p.totalBlocks) {
         const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
@@ -905,20 +917,28 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     return CC_OK;
 }
 
-int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutput& outSpec, bool download,
-                 u64* totalWords) {
-    if (totalWords) *totalWords = 0;
-    if (S == 0) { I->lastLayout.clear(); return CC_OK; }
-    cudaStream_t st = I->stream;
-    char* slot = I->takeRingSlot();
-    HostPlan hp;
-    int rc = buildPlan(I, streams, S, slot, hp);
-    if (rc) return rc;
-    char* dPlan = reinterpret_cast<char*>(I->dPlan);
-    CC_TRY_CUDA(cudaMemcpyAsync(dPlan, slot, hp.bytes, cudaMemcpyHostToDevice, st), "upload plan");
-    cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
+int prepareDecodeAttributes(cc_instance* I);
+
+int prepareKernelAttributes(cc_instance* I) {
+    const u32 heapCap = std::min<u32>(I->leavesMax, kBuildSmemLeaves);
+    const size_t buildSmem = sizeof(u64) * (heapCap + 2) + 3 * sizeof(u32) * size_t(heapCap);
+    CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
+                "tableBuild smem");
+    return prepareDecodeAttributes(I);
+}
+
+void volumeExtents(cc_instance* I, const u32* first, u32 count, u64* wordOff, u64* bitSize, cudaStream_t st) {
+    k_volumeExtents<<<u32(ceilDiv(count, 256)), 256, 0, st>>>(I->layout, first, count, wordOff, bitSize, I->errors);
+    countLaunch();
+}
+
+// Launches the encode of a prepared call whose descriptors are at
+// plan.dev (device); writes the segments to out (at most outCap words).
+// Only kernel launches and device-side memsets.
+int encodeLaunch(cc_instance* I, const EncPlan& hp, u32* out, u64 outCap) {
+    const char* dPlan = static_cast<const char*>(hp.dev);
     EncParams p{};
-    p.S = S;
+    p.S = hp.S;
     p.T = hp.T;
     p.totalTiles = hp.tiles;
     p.totalBlocks = hp.blocks;
@@ -941,8 +961,8 @@ int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutpu
     p.blockBits = I->blockBits;
     p.blockOff = I->blockOff;
     p.layout = I->layout;
-    p.out = outSpec.words ? outSpec.words : I->out;
-    p.outWordsMax = outSpec.words ? outSpec.capacity : I->outWordsMax;
+    p.out = out;
+    p.outWordsMax = outCap;
     p.capHist = I->capHist;
     p.capLeaves = I->capLeaves;
     p.capHdr = I->capHdr;
@@ -953,7 +973,23 @@ int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutpu
     p.orderWork = I->orderWork;
     p.leafSymWork = I->leafSymWork;
     p.heapCap = std::min<u32>(std::min<u32>(I->leavesMax, kBuildSmemLeaves), hp.maxCount + 1u);
-    rc = I->symBytes == 2 ? launchEncode<u16>(I, p) : launchEncode<u32>(I, p);
+    return I->symBytes == 2 ? launchEncode<u16>(I, p) : launchEncode<u32>(I, p);
+}
+
+int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutput& outSpec, bool download,
+                 u64* totalWords) {
+    if (totalWords) *totalWords = 0;
+    if (S == 0) { I->lastLayout.clear(); return CC_OK; }
+    cudaStream_t st = I->stream;
+    char* slot = I->takeRingSlot();
+    EncPlan hp;
+    int rc = encodePrepare(I, streams, S, slot, I->hostRingBytes, hp);
+    if (rc) return rc;
+    hp.dev = I->dPlan;
+    CC_TRY_CUDA(cudaMemcpyAsync(I->dPlan, slot, hp.bytes, cudaMemcpyHostToDevice, st), "upload plan");
+    cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
+    u32* out = outSpec.words ? outSpec.words : I->out;
+    rc = encodeLaunch(I, hp, out, outSpec.words ? outSpec.capacity : I->outWordsMax);
     if (rc) return rc;
     // results: layout, total words, error flags
     char* down = I->hostDown;
@@ -969,7 +1005,7 @@ int encodeDevice(cc_instance* I, const EncStream* streams, u32 S, const EncOutpu
     if (totalWords) *totalWords = total;
     if (download && total) {
         if (total > I->hostWordsMax) { setError("encode: result larger than the host staging"); return CC_ERR_CAPACITY; }
-        CC_TRY_CUDA(cudaMemcpyAsync(I->hostWords, p.out, total * 4, cudaMemcpyDeviceToHost, st), "download words");
+        CC_TRY_CUDA(cudaMemcpyAsync(I->hostWords, out, total * 4, cudaMemcpyDeviceToHost, st), "download words");
         CC_TRY_CUDA(cudaStreamSynchronize(st), "download words");
     }
     return CC_OK;

@@ -34,6 +34,20 @@ int cudaFail(cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? CC_ERR_OUT_OF_MEMORY : CC_ERR_CUDA;
 }
 
+static std::atomic<size_t> g_smemSet[64][kAttrCount];
+
+cudaError_t ensureSmemAttribute(const void* kernel, int which, int device, size_t bytes) {
+    if (device < 0 || device >= 64) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    std::atomic<size_t>& cur = g_smemSet[device][which];
+    if (cur.load() >= bytes) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e == cudaSuccess) {
+        size_t c = cur.load();
+        while (c < bytes && !cur.compare_exchange_weak(c, bytes)) {}
+    }
+    return e;
+}
+
 int ensurePipelineWork(cc_instance* I, size_t bytes) {
     if (I->pipeWorkBytes >= bytes) return CC_OK;
     cudaStreamSynchronize(I->stream);
@@ -96,8 +110,6 @@ struct Carver {
 
 void layoutArena(cc_instance* I, char* base, size_t* total) {
     Carver c{base};
-    const u32 S = I->streamCountMax, T = 2 * S;
-    const u64 SN = u64(S) * I->elemCountPerStreamMax;
     I->compact = c.take<char>(I->capCompact * I->symBytes + 64);
     I->zc = c.take<char>(I->capCompact * I->symBytes + 64);
     I->tiles = c.take<RunSum>(I->capTiles);
@@ -120,31 +132,33 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->orderWork = c.take<u32>(I->capLeaves);
     I->leafSymWork = c.take<u32>(I->capLeaves);
     // decode (one call of at most streamCountMax streams)
-    I->dDecTables = c.take<DecTableDesc>(T);
-    I->dDecStreams = c.take<DecStreamDesc>(S);
-    I->decTables = c.take<DecTable>(T);
-    I->decSyms = c.take<u32>(u64(T) * I->leavesMax);
-    I->decLut = c.take<u32>(u64(T) << kLutBits);
-    I->stagedWordsMax = I->outWordsMax + 64;
+    // decode
+    I->decTables = c.take<DecTable>(I->capTables);
+    I->decSyms = c.take<u32>(I->capLeaves + 1);
+    I->decLut = c.take<u32>(u64(I->capTables) << kLutBits);
+    I->stagedWordsMax = I->hostWordsMax + 64;
     I->stagedWords = c.take<u32>(I->stagedWordsMax);
-    I->blockSum = c.take<u32>(SN / I->codingBlockSize + S + 1);
+    I->blockSum = c.take<u32>(I->capBlocks + 1);
     *total = alignUp(c.off, 256);
 }
 
-// Capacities of one encode call.  The instance promises streamCountMax
-// streams of elemCountPerStreamMax symbols; internally a call may split the
-// same symbol budget over up to capStreams streams of any sizes.
-void sizeCapacities(cc_instance* I) {
+// Capacities of one encode or decode call.  The instance promises
+// streamCountMax streams of elemCountPerStreamMax symbols; internally a call
+// may split the same symbol budget over up to capStreams streams of any
+// sizes.  An instance made for a batch of volumes gets its capacities from
+// `caps` instead.
+void sizeCapacities(cc_instance* I, const InstanceCaps* caps) {
     const u32 S = I->streamCountMax;
-    const u64 SN = u64(S) * I->elemCountPerStreamMax;
-    I->capStreams = std::max<u32>(S, 1024u);
+    const u64 SN = caps ? caps->symbols : u64(S) * I->elemCountPerStreamMax;
+    I->capStreams = caps ? caps->streams : std::max<u32>(S, 1024u);
     I->capTables = 2 * I->capStreams;
     I->capCompact = SN;
     I->capTiles = u32(ceilDiv(SN, kRleTile) + I->capStreams);
     I->capBlocks = u32(2 * (ceilDiv(SN, I->codingBlockSize) + I->capStreams));
     // histograms: at most 2^log2Max bins for symbols and 256 for zero counts
-    // per stream of a full call
-    I->capHist = u64(S) * I->bins + u64(S) * std::min<u32>(256u, I->bins);
+    // per stream of a full call (a batch gives a bin budget instead; the
+    // device plan checks every call against it)
+    I->capHist = caps ? caps->histBins : u64(S) * I->bins + u64(S) * std::min<u32>(256u, I->bins);
     I->capLeaves = std::min<u64>(I->capHist, 2 * SN + I->capTables);
     const u64 symBits = I->log2Max > 16 ? 24 : 16;
     I->capHdr = u64(I->capTables) * (headerWordsFor(0, I->log2Max) + 1) + ceilDiv(I->capLeaves * symBits, 32);
@@ -153,11 +167,11 @@ void sizeCapacities(cc_instance* I) {
     // count) + 16-bit offsets
     I->outWordsMax = I->capHdr + 16ull * I->capStreams + ceilDiv(SN * (I->log2Max + 8), 32) +
                      ceilDiv(SN, I->codingBlockSize) + 64;
-    I->hostRingBytes = alignUp(std::max<u64>(u64(I->capStreams) * sizeof(EncStreamDev) + 64 +
-                                                 u64(I->capTables) * sizeof(EncTableDev),
-                                             2ull * S * sizeof(DecTableDesc) + u64(S) * sizeof(DecStreamDesc) + 64) +
-                                   4096,
-                               4096);
+    I->hostWordsMax = caps ? 1024 : I->outWordsMax;   // batches keep their results on the device
+    const u64 encPlan = u64(I->capStreams) * sizeof(EncStreamDev) + 64 + u64(I->capTables) * sizeof(EncTableDev);
+    const u64 decPlan = u64(I->capStreams) * (sizeof(DecStreamDesc) + sizeof(DecSource) + 2 * sizeof(u32)) +
+                        u64(I->capTables) * sizeof(DecTableDesc) + 5 * 64;
+    I->hostRingBytes = alignUp(std::max(encPlan, decPlan) + 4096, 4096);
 }
 
 }  // namespace
@@ -170,6 +184,15 @@ const char* cc_version(void) { return "cudacompress_b200 0.1 (sm_100a)"; }
 
 int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMax, uint32_t elemCountPerStreamMax,
                        uint32_t codingBlockSize, uint32_t log2Max) {
+    return ccb::createInstance(out, cudaDevice, streamCountMax, elemCountPerStreamMax, codingBlockSize, log2Max, nullptr);
+}
+
+}  // extern "C"
+
+namespace ccb {
+
+int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 elemCountPerStreamMax,
+                   u32 codingBlockSize, u32 log2Max, const InstanceCaps* caps) {
     if (!out) { setError("cc_create_instance: out is NULL"); return CC_ERR_INVALID_ARGUMENT; }
     *out = nullptr;
     if (codingBlockSize == 0) codingBlockSize = 128;          // InstanceImpl.cpp:65-69
@@ -203,7 +226,7 @@ int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMa
         setError("streamCountMax * elemCountPerStreamMax must be <= 2^36");
         return CC_ERR_INVALID_ARGUMENT;
     }
-    sizeCapacities(I);
+    sizeCapacities(I, caps);
 
     size_t bytes = 0;
     layoutArena(I, nullptr, &bytes);
@@ -225,7 +248,6 @@ int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMa
         cc_destroy_instance(I);
         return cudaFail(e, "cudaHostAlloc(down)");
     }
-    I->hostWordsMax = I->outWordsMax;
     if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostWords), I->hostWordsMax * 4, cudaHostAllocDefault)) != cudaSuccess) {
         cc_destroy_instance(I);
         return cudaFail(e, "cudaHostAlloc(words)");
@@ -234,6 +256,10 @@ int cc_create_instance(cc_instance** out, int cudaDevice, uint32_t streamCountMa
     *out = I;
     return CC_OK;
 }
+
+}  // namespace ccb
+
+extern "C" {
 
 void cc_destroy_instance(cc_instance* I) {
     if (!I) return;

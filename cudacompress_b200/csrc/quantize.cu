@@ -11,13 +11,6 @@
 
 namespace ccb {
 
-__device__ __forceinline__ u32 symbolizeI(int v) { return 2u * u32(abs(v)) + u32(v >> 31); }
-__device__ __forceinline__ int unsymbolizeI(u32 s) {
-    int neg = int(s & 1u);
-    return (1 - 2 * neg) * int((s + u32(neg)) >> 1);
-}
-__device__ __forceinline__ float signF(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
-__device__ __forceinline__ float signI(int q) { return q > 0 ? 1.0f : (q < 0 ? -1.0f : 0.0f); }
 
 __device__ __forceinline__ int quantizeV(float v, float inv, int type) {
     if (type == 0) return int(v * inv);

@@ -196,6 +196,42 @@ int cc_compress_heightfield(cc_instance* inst, const int16_t* d_image, uint32_t 
 int cc_decompress_heightfield(cc_instance* inst, int16_t* d_image, uint32_t size_x, uint32_t size_y,
                               uint32_t levels, const uint32_t* d_words, uint32_t bit_size);
 
+/* ---- batched volume codec (B200 addition; callers: CompressVolume.cpp:312-516) ----
+ * Compresses and decompresses `count` float32 volumes of any sizes (each
+ * divisible by 2^levels, coarsest level >= 8) with one launch per stage for
+ * the whole batch.  Each volume's stream is byte-identical to
+ * cc_compress_volume_float's with its own quantization step.  Planned once
+ * at creation (its own device memory; the instance gives device, stream,
+ * coding block size and symbol range, which must be 16-bit); compress and
+ * decompress only enqueue work on the instance stream (no host
+ * synchronization) and, with cc_volume_batch_use_graph, replay it as one
+ * CUDA graph.  sizes: x, y, z per volume. */
+typedef struct cc_volume_batch cc_volume_batch;
+int cc_volume_batch_create(cc_instance* inst, uint32_t count, const uint32_t* sizes, uint32_t levels,
+                           const float* quant_steps, cc_volume_batch** out);
+void cc_volume_batch_destroy(cc_volume_batch* batch);
+int cc_volume_batch_use_graph(cc_volume_batch* batch, int enable);
+/* d_volumes: `count` device pointers (dense x-fastest volumes). */
+int cc_volume_batch_compress(cc_volume_batch* batch, const float* const* d_volumes);
+/* Decodes the batch's own streams (those of the last compress, or streams
+ * written into the buffer cc_volume_batch_stream returns). */
+int cc_volume_batch_decompress(cc_volume_batch* batch, float* const* d_volumes);
+/* Device views of the streams: words, per-volume word offset and bit size. */
+int cc_volume_batch_stream(const cc_volume_batch* batch, const uint32_t** d_words, const uint64_t** d_word_offsets,
+                           const uint64_t** d_bit_sizes, uint64_t* capacity_words);
+/* Synchronizes and copies volume v's stream (host or device dst; NULL dst:
+ * size only). */
+int cc_volume_batch_read_stream(cc_volume_batch* batch, uint32_t volume, uint32_t* dst, uint64_t capacity_words,
+                                uint64_t* bit_size);
+/* Loads `count` streams (host or device words, bit sizes) back to back into
+ * the batch's buffer for cc_volume_batch_decompress (e.g. streams of
+ * cc_compress_volume_float or of another batch with the same shapes). */
+int cc_volume_batch_load_streams(cc_volume_batch* batch, const uint32_t* const* words, const uint64_t* bit_sizes);
+/* Synchronizes the instance stream; reports device errors of the last calls. */
+int cc_volume_batch_status(cc_volume_batch* batch);
+/* Adds the batch's timing sections to the instance's (cc_timing_*). */
+void cc_volume_batch_collect_timings(cc_volume_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

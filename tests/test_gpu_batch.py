@@ -1,0 +1,104 @@
+"""Batched volume codec (cc_volume_batch_*): uneven bricks in one batch, each
+stream byte-identical to the CPU oracle's (and so to the plain codec's), each
+reconstruction bit-identical to the oracle's; the same with the whole
+sequence replayed as a CUDA graph, on repeated calls and with new inputs."""
+import numpy as np
+import pytest
+
+from helpers import Oracle
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import cudacompress_b200 as cc  # noqa: E402
+from cudacompress_b200 import fields  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    return Oracle()
+
+
+def bricks(count, levels, seed):
+    rng = np.random.default_rng(seed)
+    src = fields.turbulence_field(64, 128, 16, seed=seed)
+    f = 1 << levels
+    edges = [e for e in (16, 24, 32, 48, 64) if e % f == 0 and (e >> (levels - 1)) >= 8]
+    out, steps = [], []
+    for _ in range(count):
+        nz, ny, nx = (int(rng.choice(edges)) for _ in range(3))
+        z0, y0, x0 = (int(rng.integers(0, 64 - n + 1)) for n in (nz, ny, nx))
+        out.append(np.ascontiguousarray(src[z0:z0 + nz, y0:y0 + ny, x0:x0 + nx]))
+        steps.append(float(np.exp(rng.uniform(np.log(0.002), np.log(0.05)))) * float(src.std()))
+    return out, steps
+
+
+def check_batch(oracle, vols, steps, levels, graph, rounds=2):
+    inst = cc.Instance(0, 7, 1 << 12, 128, 14)
+    with cc.VolumeBatch(inst, [v.shape for v in vols], levels, steps, graph=graph) as b:
+        ref = [oracle.compress_volume(v, levels, q) for v, q in zip(vols, steps)]
+        recs = [oracle.decompress_volume(w, bits, v.shape, levels, q) for (w, bits), v, q in zip(ref, vols, steps)]
+        dev = [torch.from_numpy(v).cuda() for v in vols]
+        outs = [torch.full(v.shape, float("nan"), dtype=torch.float32, device="cuda") for v in vols]
+        for r in range(rounds):
+            b.compress(dev)
+            b.decompress(outs)
+            b.status()
+            for i, v in enumerate(vols):
+                words, bits = b.read_stream(i)
+                assert bits == ref[i][1], (r, i, bits, ref[i][1])
+                assert np.array_equal(words, ref[i][0]), (r, i)
+                got = outs[i].cpu().numpy()
+                assert np.array_equal(got.view(np.uint32), recs[i].view(np.uint32)), (r, i)
+            for o in outs:
+                o.fill_(float("nan"))
+    inst.close()
+
+
+def test_batch_uneven_bricks_match_oracle(oracle):
+    vols, steps = bricks(12, 2, seed=1005)
+    check_batch(oracle, vols, steps, 2, graph=False)
+
+
+def test_batch_graph_replay_matches_oracle(oracle):
+    vols, steps = bricks(9, 2, seed=1006)
+    check_batch(oracle, vols, steps, 2, graph=True, rounds=3)
+
+
+def test_batch_three_levels_and_new_inputs(oracle):
+    vols, steps = bricks(4, 3, seed=77)
+    check_batch(oracle, vols, steps, 3, graph=True)
+    # same shapes, other data through the same (graph) batch
+    vols2 = [np.ascontiguousarray(v[::-1]) for v in vols]
+    check_batch(oracle, vols2, steps, 3, graph=True)
+
+
+def test_batch_rejects_bad_sizes():
+    inst = cc.Instance(0, 7, 1 << 12, 128, 14)
+    with pytest.raises(cc.CudaCompressError):
+        cc.VolumeBatch(inst, [(16, 16, 18)], 2, [0.1])
+    inst.close()
+
+
+def test_batch_decodes_streams_of_the_plain_codec(oracle):
+    """Streams written by cc_compress_volume_float, loaded into a batch and
+    decoded there, give the oracle's reconstruction."""
+    vols, steps = bricks(5, 2, seed=31)
+    inst = cc.Instance(0, 7, 32 ** 3, 128, 14)
+    words, bits = [], []
+    for v, q in zip(vols, steps):
+        w, b = cc.compress_volume_float(inst, torch.from_numpy(v).cuda(), 2, q)
+        words.append(w[: (b + 31) // 32].cpu().numpy().view(np.uint32).copy())
+        bits.append(b)
+    with cc.VolumeBatch(inst, [v.shape for v in vols], 2, steps) as bt:
+        bt.load_streams(words, bits)
+        outs = [torch.empty(v.shape, dtype=torch.float32, device="cuda") for v in vols]
+        bt.decompress(outs)
+        bt.status()
+        for i, (v, q) in enumerate(zip(vols, steps)):
+            ref = oracle.decompress_volume(words[i], bits[i], v.shape, 2, q)
+            assert np.array_equal(outs[i].cpu().numpy().view(np.uint32), ref.view(np.uint32)), i
+    inst.close()
