@@ -65,6 +65,8 @@ _SIGS = {
     "cc_volume_batch_create": (c_int, [c_vp, c_u32, c_u32p, c_u32, ctypes.POINTER(c_float), ctypes.POINTER(c_vp)]),
     "cc_volume_batch_destroy": (None, [c_vp]),
     "cc_volume_batch_use_graph": (c_int, [c_vp, c_int]),
+    "cc_volume_batch_set_active": (c_int, [c_vp, c_u32]),
+    "cc_volume_batch_set_stream": (c_int, [c_vp, c_vp]),
     "cc_volume_batch_compress": (c_int, [c_vp, c_vpp]),
     "cc_volume_batch_decompress": (c_int, [c_vp, c_vpp]),
     "cc_volume_batch_stream": (c_int, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), ctypes.POINTER(c_vp),

@@ -366,12 +366,23 @@ class VolumeBatch:
     def __exit__(self, *exc):
         self.close()
 
+    def set_active(self, k: int) -> None:
+        check(lib().cc_volume_batch_set_active(self.handle, k), "cc_volume_batch_set_active")
+        self.active = k
+
+    def set_stream(self, stream) -> None:
+        check(lib().cc_volume_batch_set_stream(self.handle, _stream(stream)), "cc_volume_batch_set_stream")
+
     def compress(self, volumes) -> None:
-        arr = (ctypes.c_void_p * self.count)(*[v.data_ptr() for v in volumes])
+        if len(volumes) < getattr(self, "active", self.count):
+            raise ValueError("one volume per active slot is needed")
+        arr = (ctypes.c_void_p * max(len(volumes), 1))(*[v.data_ptr() for v in volumes])
         check(lib().cc_volume_batch_compress(self.handle, arr), "cc_volume_batch_compress")
 
     def decompress(self, outs) -> None:
-        arr = (ctypes.c_void_p * self.count)(*[o.data_ptr() for o in outs])
+        if len(outs) < getattr(self, "active", self.count):
+            raise ValueError("one output per active slot is needed")
+        arr = (ctypes.c_void_p * max(len(outs), 1))(*[o.data_ptr() for o in outs])
         check(lib().cc_volume_batch_decompress(self.handle, arr), "cc_volume_batch_decompress")
 
     def status(self) -> None:
@@ -392,8 +403,8 @@ class VolumeBatch:
         ptrs = []
         for w in words:
             ptrs.append(w.data_ptr() if isinstance(w, torch.Tensor) else np.ascontiguousarray(w, np.uint32).ctypes.data)
-        arr = (ctypes.c_void_p * self.count)(*ptrs)
-        bits = (ctypes.c_uint64 * self.count)(*[int(b) for b in bit_sizes])
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        bits = (ctypes.c_uint64 * len(ptrs))(*[int(b) for b in bit_sizes])
         check(lib().cc_volume_batch_load_streams(self.handle, arr, bits), "cc_volume_batch_load_streams")
 
     def collect_timings(self) -> None:

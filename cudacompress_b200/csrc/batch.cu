@@ -21,6 +21,7 @@
 // descriptors, and per brick the word offset and bit size of its stream in
 // the batch's output words.
 #include <cstring>
+#include <map>
 
 #include "batch.cuh"
 
@@ -45,19 +46,27 @@ struct cc_volume_batch {
     ccb::u64* bitSize = nullptr;
     ccb::u32* volFirstStream = nullptr;   // [count + 1]
     // launch lists
-    struct Rows { const ccb::BRowDesc* d; ccb::u32 n, ctas; };
-    struct Cols { const ccb::BColDesc* d; ccb::u32 n, ctas; };
-    struct Quant { const ccb::BQuantDesc* d; ccb::u32 n, ctas; };
+    // per volume v: descriptors and CTAs of volumes 0..v (prefix launches)
+    struct Rows { const ccb::BRowDesc* d; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    struct Cols { const ccb::BColDesc* d; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    struct Quant { const ccb::BQuantDesc* d; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
     std::vector<Rows> fwdRows, invRows;        // per level
     std::vector<Cols> fwdY, fwdZ, invZ, invY;  // per level
     Quant quant{}, dequantLP{};
     ccb::EncPlan enc;
     ccb::DecPlan dec;
+    // per volume v: encoder / decoder counts of volumes 0..v
+    std::vector<ccb::u32> encS, encT, encTiles, encBlocks;
+    std::vector<ccb::u32> decT, decRl, decH, decRlBlocks, decHBlocks;
+    std::vector<ccb::u64> symEnd;       // symbols of volumes 0..v
+    ccb::u32 active = 0;                // volumes a call processes (the first `active`)
+    cudaStream_t ownStream = nullptr;   // set: the batch's work goes here instead of the instance stream
+    bool hasOwnStream = false;
     // graphs
     bool useGraph = false;
-    cudaGraphExec_t gCompress = nullptr, gDecompress = nullptr;
+    std::map<ccb::u32, cudaGraphExec_t> gCompress, gDecompress;   // by active count
     cudaStream_t captureStream = nullptr;
-    unsigned launchesCompress = 0, launchesDecompress = 0;
+    std::map<ccb::u32, unsigned> launchesCompress, launchesDecompress;
 };
 
 namespace ccb {
@@ -125,19 +134,36 @@ SymLayout symLayout(u32 nx, u32 ny, u32 nz, u32 L) {
 
 }  // namespace
 
+template <class List>
+static void prefixOf(const List& li, u32 k, u32& nd, u32& ctas) {
+    nd = li.descEnd[k - 1];
+    ctas = li.ctaEnd[k - 1];
+}
+
 static int batchEnqueueCompress(cc_volume_batch* b) {
     cc_instance* I = b->I;
     cudaStream_t st = I->stream;
+    const u32 k = b->active;
+    u32 nd, ctas;
     for (u32 l = 0; l < b->levels; ++l) {
         SectionTimer t(I, "batch.dwt_forward", st);
-        launchBatchRows(b->fwdRows[l].d, b->fwdRows[l].n, b->fwdRows[l].ctas, false, b->inTab, b->outTab, st);
-        launchBatchCols(b->fwdY[l].d, b->fwdY[l].n, b->fwdY[l].ctas, false, false, st);
-        launchBatchCols(b->fwdZ[l].d, b->fwdZ[l].n, b->fwdZ[l].ctas, false, false, st);
+        prefixOf(b->fwdRows[l], k, nd, ctas);
+        launchBatchRows(b->fwdRows[l].d, nd, ctas, false, b->inTab, b->outTab, st);
+        prefixOf(b->fwdY[l], k, nd, ctas);
+        launchBatchCols(b->fwdY[l].d, nd, ctas, false, false, st);
+        prefixOf(b->fwdZ[l], k, nd, ctas);
+        launchBatchCols(b->fwdZ[l].d, nd, ctas, false, false, st);
     }
-    { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, b->quant.n, b->quant.ctas, false, st); }
-    int rc = encodeLaunch(I, b->enc, I->out, I->outWordsMax);
+    prefixOf(b->quant, k, nd, ctas);
+    { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, nd, ctas, false, st); }
+    EncPlan ep = b->enc;
+    ep.S = b->encS[k - 1];
+    ep.T = b->encT[k - 1];
+    ep.tiles = b->encTiles[k - 1];
+    ep.blocks = b->encBlocks[k - 1];
+    int rc = encodeLaunch(I, ep, I->out, I->outWordsMax);
     if (rc) return rc;
-    volumeExtents(I, b->volFirstStream, b->count, b->wordOff, b->bitSize, st);
+    volumeExtents(I, b->volFirstStream, k, b->wordOff, b->bitSize, st);
     CC_TRY_CUDA(cudaGetLastError(), "batch compress");
     return CC_OK;
 }
@@ -145,15 +171,29 @@ static int batchEnqueueCompress(cc_volume_batch* b) {
 static int batchEnqueueDecompress(cc_volume_batch* b) {
     cc_instance* I = b->I;
     cudaStream_t st = I->stream;
-    CC_TRY_CUDA(cudaMemsetAsync(b->syms, 0, b->symBytes, st), "zero symbols");
-    int rc = decodeLaunch(I, b->dec);
+    const u32 k = b->active;
+    u32 nd, ctas;
+    CC_TRY_CUDA(cudaMemsetAsync(b->syms, 0, b->symEnd[k - 1] * sizeof(u16), st), "zero symbols");
+    DecPlan dp = b->dec;
+    dp.S = b->encS[k - 1];
+    dp.T = b->decT[k - 1];
+    dp.B = k;
+    dp.nRl = b->decRl[k - 1];
+    dp.nH = b->decH[k - 1];
+    dp.rlBlocks = b->decRlBlocks[k - 1];
+    dp.hBlocks = b->decHBlocks[k - 1];
+    int rc = decodeLaunch(I, dp);
     if (rc) return rc;
-    { SectionTimer t(I, "batch.dequantize", st); launchBatchQuant(b->dequantLP.d, b->dequantLP.n, b->dequantLP.ctas, true, st); }
+    prefixOf(b->dequantLP, k, nd, ctas);
+    { SectionTimer t(I, "batch.dequantize", st); launchBatchQuant(b->dequantLP.d, nd, ctas, true, st); }
     for (int l = int(b->levels) - 1; l >= 0; --l) {
         SectionTimer t(I, "batch.dwt_inverse", st);
-        launchBatchCols(b->invZ[l].d, b->invZ[l].n, b->invZ[l].ctas, true, true, st);
-        launchBatchCols(b->invY[l].d, b->invY[l].n, b->invY[l].ctas, true, false, st);
-        launchBatchRows(b->invRows[l].d, b->invRows[l].n, b->invRows[l].ctas, true, b->inTab, b->outTab, st);
+        prefixOf(b->invZ[l], k, nd, ctas);
+        launchBatchCols(b->invZ[l].d, nd, ctas, true, true, st);
+        prefixOf(b->invY[l], k, nd, ctas);
+        launchBatchCols(b->invY[l].d, nd, ctas, true, false, st);
+        prefixOf(b->invRows[l], k, nd, ctas);
+        launchBatchRows(b->invRows[l].d, nd, ctas, true, b->inTab, b->outTab, st);
     }
     CC_TRY_CUDA(cudaGetLastError(), "batch decompress");
     return CC_OK;
@@ -162,8 +202,8 @@ static int batchEnqueueDecompress(cc_volume_batch* b) {
 // Copies a volume pointer table to the device (outside any captured graph).
 static int uploadTable(cc_volume_batch* b, const void* const* ptrs, void* dTable) {
     cudaEventSynchronize(b->tabEvent);   // the previous upload has read the pinned buffer
-    std::memcpy(b->hostPlan, ptrs, sizeof(void*) * b->count);
-    CC_TRY_CUDA(cudaMemcpyAsync(dTable, b->hostPlan, sizeof(void*) * b->count, cudaMemcpyHostToDevice, b->I->stream),
+    std::memcpy(b->hostPlan, ptrs, sizeof(void*) * b->active);
+    CC_TRY_CUDA(cudaMemcpyAsync(dTable, b->hostPlan, sizeof(void*) * b->active, cudaMemcpyHostToDevice, b->I->stream),
                 "upload volume pointers");
     cudaEventRecord(b->tabEvent, b->I->stream);
     return CC_OK;
@@ -173,9 +213,12 @@ using Enqueue = int (*)(cc_volume_batch*);
 
 // Runs an enqueue function directly, or through its CUDA graph (captured on
 // the first use; later calls replay it).
-static int runMaybeGraph(cc_volume_batch* b, Enqueue fn, cudaGraphExec_t& exec, unsigned& launches) {
+static int runMaybeGraph(cc_volume_batch* b, Enqueue fn, std::map<u32, cudaGraphExec_t>& graphs,
+                         std::map<u32, unsigned>& counts) {
     cc_instance* I = b->I;
     if (!b->useGraph) return fn(b);
+    cudaGraphExec_t& exec = graphs[b->active];
+    unsigned& launches = counts[b->active];
     if (!exec) {
         // Capture on the batch's own stream (the instance stream may be the
         // legacy default stream, which cannot be captured); the graph is then
@@ -491,6 +534,51 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     }
     b->quant = {reinterpret_cast<const BQuantDesc*>(base + qAt), u32(qd.size()), qC};
     b->dequantLP = {reinterpret_cast<const BQuantDesc*>(base + dqAt), u32(dq.size()), dqC};
+    // prefixes by volume
+    auto prefix = [&](auto& li, const auto& host, u32 perVolume) {
+        li.descEnd.resize(count);
+        li.ctaEnd.resize(count);
+        for (u32 v = 0; v < count; ++v) {
+            const u32 e = (v + 1) * perVolume;
+            li.descEnd[v] = e;
+            li.ctaEnd[v] = e < host.size() ? host[e].ctaOff : li.ctas;
+        }
+    };
+    for (u32 l = 0; l < L; ++l) {
+        prefix(b->fwdRows[l], fr[l], 1);
+        prefix(b->invRows[l], ir[l], 1);
+        prefix(b->fwdY[l], fy[l], 1);
+        prefix(b->fwdZ[l], fz[l], 1);
+        prefix(b->invZ[l], iz[l], 1);
+        prefix(b->invY[l], iy[l], 1);
+    }
+    prefix(b->quant, qd, 1 + 7 * L);
+    prefix(b->dequantLP, dq, 1);
+    {
+        const u32 cb = I->codingBlockSize;
+        u32 S = 0, T = 0, tiles = 0, blocks = 0, nRl = 0, nH = 0, rlB = 0, hB = 0;
+        for (u32 v = 0; v < count; ++v) {
+            for (u32 st = firstStream[v]; st < firstStream[v + 1]; ++st) {
+                const EncStream& e = es[st];
+                const u32 nb = u32(ceilDiv(e.n, cb));
+                ++S;
+                tiles += u32(ceilDiv(e.n, kRleTile));
+                if (e.kind == KIND_RLHUFF) { T += 2; blocks += 2 * nb; ++nRl; rlB += nb; }
+                else { T += 1; blocks += nb; ++nH; hB += nb; }
+            }
+            b->encS.push_back(S);
+            b->encT.push_back(T);
+            b->encTiles.push_back(tiles);
+            b->encBlocks.push_back(blocks);
+            b->decT.push_back(T);
+            b->decRl.push_back(nRl);
+            b->decH.push_back(nH);
+            b->decRlBlocks.push_back(rlB);
+            b->decHBlocks.push_back(hB);
+            b->symEnd.push_back(symOff[v] + sl[v].total);
+        }
+    }
+    b->active = count;
     *out = b;
     return CC_OK;
 }
@@ -499,8 +587,8 @@ void cc_volume_batch_destroy(cc_volume_batch* b) {
     if (!b) return;
     if (b->I) cudaSetDevice(b->I->device);
     cudaDeviceSynchronize();
-    if (b->gCompress) cudaGraphExecDestroy(b->gCompress);
-    if (b->gDecompress) cudaGraphExecDestroy(b->gDecompress);
+    for (auto& kv : b->gCompress) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : b->gDecompress) cudaGraphExecDestroy(kv.second);
     if (b->captureStream) cudaStreamDestroy(b->captureStream);
     if (b->tabEvent) cudaEventDestroy(b->tabEvent);
     if (b->hostPlan) cudaFreeHost(b->hostPlan);
@@ -509,6 +597,19 @@ void cc_volume_batch_destroy(cc_volume_batch* b) {
     if (b->mem) cudaFree(b->mem);
     if (b->I) cc_destroy_instance(b->I);
     delete b;
+}
+
+int cc_volume_batch_set_active(cc_volume_batch* b, uint32_t active) {
+    if (!b || active == 0 || active > b->count) { setError("cc_volume_batch_set_active: active must be 1..count"); return CC_ERR_INVALID_ARGUMENT; }
+    b->active = active;
+    return CC_OK;
+}
+
+int cc_volume_batch_set_stream(cc_volume_batch* b, void* stream) {
+    if (!b) { setError("cc_volume_batch_set_stream: null batch"); return CC_ERR_INVALID_ARGUMENT; }
+    b->ownStream = static_cast<cudaStream_t>(stream);
+    b->hasOwnStream = true;
+    return CC_OK;
 }
 
 int cc_volume_batch_use_graph(cc_volume_batch* b, int enable) {
@@ -520,7 +621,7 @@ int cc_volume_batch_use_graph(cc_volume_batch* b, int enable) {
 int cc_volume_batch_compress(cc_volume_batch* b, const float* const* dVolumes) {
     if (!b || !dVolumes) { setError("cc_volume_batch_compress: null argument"); return CC_ERR_INVALID_ARGUMENT; }
     cudaSetDevice(b->I->device);
-    b->I->stream = b->user->stream;
+    b->I->stream = b->hasOwnStream ? b->ownStream : b->user->stream;
     b->I->timing = b->user->timing;
     int rc = uploadTable(b, reinterpret_cast<const void* const*>(dVolumes), b->inTab);
     if (rc) return rc;
@@ -530,7 +631,7 @@ int cc_volume_batch_compress(cc_volume_batch* b, const float* const* dVolumes) {
 int cc_volume_batch_decompress(cc_volume_batch* b, float* const* dVolumes) {
     if (!b || !dVolumes) { setError("cc_volume_batch_decompress: null argument"); return CC_ERR_INVALID_ARGUMENT; }
     cudaSetDevice(b->I->device);
-    b->I->stream = b->user->stream;
+    b->I->stream = b->hasOwnStream ? b->ownStream : b->user->stream;
     b->I->timing = b->user->timing;
     int rc = uploadTable(b, reinterpret_cast<const void* const*>(dVolumes), b->outTab);
     if (rc) return rc;
@@ -566,19 +667,20 @@ int cc_volume_batch_read_stream(cc_volume_batch* b, uint32_t v, uint32_t* dst, u
 int cc_volume_batch_load_streams(cc_volume_batch* b, const uint32_t* const* words, const uint64_t* bitSizes) {
     if (!b || !words || !bitSizes) { setError("cc_volume_batch_load_streams: null argument"); return CC_ERR_INVALID_ARGUMENT; }
     cudaSetDevice(b->I->device);
-    cudaStream_t st = b->user->stream;
+    cudaStream_t st = b->hasOwnStream ? b->ownStream : b->user->stream;
+    b->I->stream = st;
     cudaEventSynchronize(b->extEvent);   // the previous load has read the pinned offsets
     u64 at = 0;
-    for (u32 v = 0; v < b->count; ++v) {
+    for (u32 v = 0; v < b->active; ++v) {
         const u64 nw = ceilDiv(bitSizes[v], 32);
         if (at + nw > b->I->outWordsMax) { setError("cc_volume_batch_load_streams: streams exceed the batch buffer (%llu words)", (unsigned long long)b->I->outWordsMax); return CC_ERR_CAPACITY; }
         b->hostExt[v] = at;
-        b->hostExt[b->count + v] = bitSizes[v];
+        b->hostExt[b->active + v] = bitSizes[v];
         if (nw) CC_TRY_CUDA(cudaMemcpyAsync(b->I->out + at, words[v], nw * 4, cudaMemcpyDefault, st), "load stream");
         at += nw;
     }
-    CC_TRY_CUDA(cudaMemcpyAsync(b->wordOff, b->hostExt, sizeof(u64) * b->count, cudaMemcpyHostToDevice, st), "load offsets");
-    CC_TRY_CUDA(cudaMemcpyAsync(b->bitSize, b->hostExt + b->count, sizeof(u64) * b->count, cudaMemcpyHostToDevice, st), "load sizes");
+    CC_TRY_CUDA(cudaMemcpyAsync(b->wordOff, b->hostExt, sizeof(u64) * b->active, cudaMemcpyHostToDevice, st), "load offsets");
+    CC_TRY_CUDA(cudaMemcpyAsync(b->bitSize, b->hostExt + b->active, sizeof(u64) * b->active, cudaMemcpyHostToDevice, st), "load sizes");
     cudaEventRecord(b->extEvent, st);
     return CC_OK;
 }

@@ -95,6 +95,7 @@ struct DecSourceSpec {
 struct DecPlan {
     u32 S = 0, T = 0, B = 0, nRl = 0, nH = 0, rlBlocks = 0, hBlocks = 0;
     size_t bytes = 0;
+    size_t offStreams = 0, offTables = 0, offSources = 0, offRl = 0, offH = 0;   // within dev
     void* dev = nullptr;
     const u32* wordsBase = nullptr;   // with wordOff / bitSize: indirect sources
     const u64* wordOff = nullptr;

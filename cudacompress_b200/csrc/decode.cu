@@ -597,6 +597,11 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
     dc.rlBlocks = u32(rlBlocks);
     dc.hBlocks = u32(hBlocks);
     dc.bytes = L.bytes;
+    dc.offStreams = L.offStreams;
+    dc.offTables = L.offTables;
+    dc.offSources = L.offSources;
+    dc.offRl = L.offRl;
+    dc.offH = L.offH;
     return CC_OK;
 }
 
@@ -634,7 +639,6 @@ int prepareDecodeAttributes(cc_instance* I) {
 }
 
 static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
-    const DecLayout L(dc.S, dc.T, dc.B);
     char* d = static_cast<char*>(dc.dev);
     DecParams p{};
     p.S = dc.S;
@@ -649,11 +653,11 @@ static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
     p.symBytes = I->symBytes;
     p.leavesMax = I->leavesMax;
     p.capLeaves = I->capLeaves;
-    p.streams = reinterpret_cast<DecStreamDesc*>(d + L.offStreams);
-    p.tables = reinterpret_cast<DecTableDesc*>(d + L.offTables);
-    p.sources = reinterpret_cast<DecSource*>(d + L.offSources);
-    p.rlList = reinterpret_cast<const u32*>(d + L.offRl);
-    p.hList = reinterpret_cast<const u32*>(d + L.offH);
+    p.streams = reinterpret_cast<DecStreamDesc*>(d + dc.offStreams);
+    p.tables = reinterpret_cast<DecTableDesc*>(d + dc.offTables);
+    p.sources = reinterpret_cast<DecSource*>(d + dc.offSources);
+    p.rlList = reinterpret_cast<const u32*>(d + dc.offRl);
+    p.hList = reinterpret_cast<const u32*>(d + dc.offH);
     p.wordsBase = dc.wordsBase;
     p.wordOff = dc.wordOff;
     p.bitSize = dc.bitSize;

@@ -211,6 +211,12 @@ int cc_volume_batch_create(cc_instance* inst, uint32_t count, const uint32_t* si
                            const float* quant_steps, cc_volume_batch** out);
 void cc_volume_batch_destroy(cc_volume_batch* batch);
 int cc_volume_batch_use_graph(cc_volume_batch* batch, int enable);
+/* Later calls process only the first `active` volumes (1..count); pointer
+ * arrays and loaded streams then cover those volumes. */
+int cc_volume_batch_set_active(cc_volume_batch* batch, uint32_t active);
+/* Runs the batch's work on `stream` (cudaStream_t) instead of the instance
+ * stream, so that several batches can overlap on the device. */
+int cc_volume_batch_set_stream(cc_volume_batch* batch, void* stream);
 /* d_volumes: `count` device pointers (dense x-fastest volumes). */
 int cc_volume_batch_compress(cc_volume_batch* batch, const float* const* d_volumes);
 /* Decodes the batch's own streams (those of the last compress, or streams
