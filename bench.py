@@ -5,13 +5,20 @@ Workload (default): the 3-component 256^3 float32 vector field - each
 component a seeded k^(-5/3) random-phase field (1024 modes, |k| <= 64, unit
 std) - compressed with the lossy volume codec (3-level CDF 9/7 DWT, deadzone
 quantization with step 0.01*std, zero-run RLE + Huffman, coding block 128)
-and decompressed again.  One step = encode + decode of all 3 components.
+and decompressed again.  One step = encode + decode of all 3 components
+through the batched codec (one batch of 3 volumes, each stream byte-identical
+to the plain single-volume codec's, replayed as CUDA graphs).
 
   value   raw field bytes / step time, inputs and outputs resident in HBM
-          (GB/s raw, encode+decode); encode_gbs / decode_gbs split it
-  e2e     the same through the public API with host buffers: H2D of the field,
-          D2H of the stream, H2D of the stream, D2H of the reconstruction
-          inside the timed region
+          (GB/s raw, encode+decode); encode_gbs / decode_gbs split it;
+          plain_path_ms_per_step times the per-component plain codec
+  e2e     the same through the public API with host buffers: H2D of the
+          fields, D2H of the streams, H2D of the streams, D2H of the
+          reconstructions inside the timed region
+  batched_vs_per_brick  1024 uneven bricks (edges {16..64} per axis, q0
+          log-uniform [0.002, 0.05]) in one batch vs one plain call per brick
+  serving the continuous-batching brick service at 10k req/s (Poisson, 90%
+          decode, edges {32, 64, 128}): p50 / p99 latency, bricks/s
   roofline  the dominant kernel section (CUDA-event timed inside the library)
           against the measured HBM copy bandwidth
   cpu_baseline  the reference's own CPU coder (src/CPU RunLengthCPU /
@@ -19,7 +26,9 @@ and decompressed again.  One step = encode + decode of all 3 components.
           oracle/_ref) plus the oracle's CPU DWT/quantize port (the reference
           has no CPU DWT), on one component, all host threads
 
-`--impl reference` times that CPU path as the reference arm.  Multi-GPU runs
+Other workloads: --workload bricks-4096 (the full batched-bricks config),
+--workload serving (1k / 10k / 50k req/s), --workload volume-128.
+`--impl reference` times the CPU path as the reference arm.  Multi-GPU runs
 (torchrun) are weak-scaling replicas: every rank codes its own field, no
 collective on the data path; the time is the max over ranks.
 """
@@ -49,6 +58,10 @@ WORKLOADS = {
 WORKLOADS["bricks-4096"] = dict(count=4096, levels=2, seed=1005, plain_sample=256,
                                 desc="4096 float32 bricks, edges {16,24,32,48,64} per axis, q0 log-uniform "
                                      "[0.002,0.05]*std, 2-level CDF 9/7, RLE+Huffman cb=128, per-brick tables")
+WORKLOADS["serving"] = dict(rates=(1000.0, 10000.0, 50000.0), requests=3000, edges=(32, 64, 128), decode_frac=0.9,
+                           q0=0.01, levels=3, slots={32: 64, 64: 16, 128: 4}, bricks_per_edge=16, seed=1006,
+                           desc="open-loop Poisson brick requests, 90% decode / 10% encode, cubic edge {32,64,128}, "
+                                "q0=0.01*std, 3-level CDF 9/7, 4 GB HBM admission budget")
 FALLBACK_HBM_GBS = 6650.0
 L2_BYTES = 126 * 1024 * 1024
 
@@ -302,6 +315,60 @@ def measure_bricks(count, levels, seed, steps, warmup, plain_sample, local):
     }
 
 
+def measure_serving(wl, local, requests=None, rates=None):
+    """Open-loop Poisson runs of the continuous-batching brick service at
+    each rate (p50/p99 arrival -> result latency, bricks/s) and an offline
+    run of the same requests all arriving at once (batched throughput)."""
+    import torch
+    from cudacompress_b200 import fields, serving
+    rng = np.random.default_rng(wl["seed"])
+    src = fields.turbulence_field(128, 1024, 64, wl["seed"])
+    sources = {}
+    for e in wl["edges"]:
+        bl = []
+        for _ in range(wl["bricks_per_edge"]):
+            o = [int(rng.integers(0, 128 - e + 1)) for _ in range(3)]
+            bl.append(torch.from_numpy(np.ascontiguousarray(src[o[0]:o[0] + e, o[1]:o[1] + e, o[2]:o[2] + e]))
+                      .cuda(local))
+        sources[e] = bl
+    srv = serving.BrickServer(local, sources, wl["slots"], wl["levels"], wl["q0"], budget_bytes=4 << 30)
+    n = requests or wl["requests"]
+    out = {"requests_per_rate": n, "store_bytes": srv.store_bytes}
+    warm = serving.poisson_requests(200, 1e9, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"], wl["seed"] + 1)
+    srv.run(warm)                     # captures the graphs of the common fill levels
+    offline = serving.poisson_requests(n, 1e12, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"], wl["seed"] + 2)
+    out["offline"] = serving.latency_stats(srv.run(offline))
+    for rate in (rates or wl["rates"]):
+        reqs = serving.poisson_requests(n, rate, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"],
+                                        wl["seed"] + int(rate))
+        st = serving.latency_stats(srv.run(reqs))
+        dec = [r for r in reqs if r.op == serving.DECODE and r.edge == min(wl["edges"])]
+        if dec:
+            lat = np.array([r.done - r.arrival for r in dec]) * 1e3
+            st["p99_ms_single_brick_decode_edge%d" % min(wl["edges"])] = float(np.percentile(lat, 99))
+        out["rate_%d" % int(rate)] = st
+    srv.close()
+    return out
+
+
+def run_serving(args, wl):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    sampler = ClockSampler(local)
+    r = measure_serving(wl, local)
+    clocks = sampler.stop()
+    best = max(v["bricks_per_s"] for k, v in r.items() if k.startswith("rate_"))
+    line = {
+        "metric": METRIC, "value": best, "unit": "bricks/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded k^-5/3 random-phase fields)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": "replicas1"},
+        "serving": r, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_bricks(args, wl):
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -494,6 +561,9 @@ def run_ours(args, wl):
     bricks = None
     if rank == 0 and world == 1 and not args.no_bricks:
         bricks = measure_bricks(1024, 2, 1005, max(2, args.steps // 2), 2, 128, local)
+    serve = None
+    if rank == 0 and world == 1 and not args.no_bricks:
+        serve = measure_serving(WORKLOADS["serving"], local, requests=1500, rates=(10000.0,))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -512,7 +582,7 @@ def run_ours(args, wl):
             "decode_gbs": world * raw_step / (dec_ms / 1e3) / 1e9,
             "compression_ratio": raw_step / max(coded_bytes, 1), "psnr_db": psnr,
             "plain_path_ms_per_step": plain_ms, "streams_identical_to_plain_codec": bool(same_as_plain),
-            "batched_vs_per_brick": bricks,
+            "batched_vs_per_brick": bricks, "serving": serve,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roofline, "pipeline_roofline": pipeline,
@@ -541,6 +611,8 @@ def main():
         run_reference(args, wl)
     elif args.workload.startswith("bricks"):
         run_bricks(args, wl)
+    elif args.workload == "serving":
+        run_serving(args, wl)
     else:
         run_ours(args, wl)
 
