@@ -32,6 +32,24 @@ __device__ __forceinline__ int mirrorIdx(int i, int n) {
 // position of interleaved index j (inverse domain) in the [L|H] layout
 __device__ __forceinline__ int splitPos(int j, int n) { return (j & 1) ? (n >> 1) + (j >> 1) : (j >> 1); }
 
+// The same taps as compile-time constants: with the parity known at compile
+// time the coefficients become instruction immediates (no divergent
+// constant-cache reads when neighbouring threads hold outputs of both
+// parities).  Identical fmaf chain, so identical results.
+template <bool kInverse, int kParity>
+__device__ __forceinline__ float fir9c(const float* v) {
+    constexpr float kF[2][9] = {
+        {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+        {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+    constexpr float kI[2][9] = {
+        {0.0f, 0.0337282f, -0.0575435f, -0.5337281f, 1.1150871f, -0.5337281f, -0.0575435f, 0.0337282f, 0.0f},
+        {0.0534975f, -0.0912718f, -0.1564465f, 0.5912718f, 1.2058980f, 0.5912718f, -0.1564465f, -0.0912718f, 0.0534975f}};
+    float sum = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) sum = __fmaf_rn(kInverse ? kI[kParity][i] : kF[kParity][i], v[i], sum);
+    return sum;
+}
+
 template <bool kInverse>
 __device__ __forceinline__ float fir9(const float* v, int parity) {
     const float* c = kInverse ? c_inv[parity] : c_fwd[parity];
@@ -71,12 +89,14 @@ __global__ void __launch_bounds__(256) k_firRows(TOut* __restrict__ dst, const T
         }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < kRowTile; k += 256) {
-        int x = x0 + k;
+    // one (even, odd) output pair per thread: parity-free taps
+    for (int p = threadIdx.x; p < kRowTile / 2; p += 256) {
+        const int x = x0 + 2 * p;
         if (x >= nx) break;
-        float r = fir9<kInverse>(s + k, x & 1);
-        int o = kInverse ? x : splitPos(x, nx);
-        out[size_t(o) * dstElem] = fromF<TOut>(r);
+        const float e = fir9c<kInverse, 0>(s + 2 * p), o = fir9c<kInverse, 1>(s + 2 * p + 1);
+        const int oe = kInverse ? x : (x >> 1), oo = kInverse ? x + 1 : (nx >> 1) + (x >> 1);
+        out[size_t(oe) * dstElem] = fromF<TOut>(e);
+        out[size_t(oo) * dstElem] = fromF<TOut>(o);
     }
 }
 
@@ -351,22 +371,43 @@ __global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ desc
     const u32 local = blockIdx.x - D.ctaOff;
     const int xt = int(local % u32(D.tilesX)), rg = int(local / u32(D.tilesX));
     const int x0 = xt * D.W, Wp = D.W + 8, rows = D.ny * D.nz;
-    for (int k = threadIdx.x; k < D.R * Wp; k += 256) {
+    // all of a thread's loads are issued before any is used (R * Wp <= 1088)
+    float vals[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const int k = threadIdx.x + 256 * i;
         const int j = k / Wp, kk = k - j * Wp, r = rg * D.R + j;
         const int xx = x0 - 4 + kk;
-        if (r < rows && xx < D.nx + 4) {
+        vals[i] = 0.0f;
+        if (k < D.R * Wp && r < rows && xx < D.nx + 4) {
             const int m = mirrorIdx(xx, D.nx);
             const int y = r % D.ny, z = r / D.ny;
-            s[k] = src[size_t(z) * D.srcSlice + size_t(y) * D.srcRow + (kInverse ? splitPos(m, D.nx) : m)];
+            vals[i] = src[size_t(z) * D.srcSlice + size_t(y) * D.srcRow + (kInverse ? splitPos(m, D.nx) : m)];
         }
     }
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const int k = threadIdx.x + 256 * i;
+        if (k < D.R * Wp) s[k] = vals[i];
+    }
     __syncthreads();
-    for (int k = threadIdx.x; k < D.R * D.W; k += 256) {
-        const int j = k / D.W, kk = k - j * D.W, r = rg * D.R + j, x = x0 + kk;
+    // each thread computes an (even, odd) output pair: coalesced stores to
+    // both halves (forward) or one float2 (inverse), parity-free taps
+    const int hw = D.W / 2;
+    for (int k = threadIdx.x; k < D.R * hw; k += 256) {
+        const int j = k / hw, p = k - j * hw, r = rg * D.R + j, x = x0 + 2 * p;
         if (r < rows && x < D.nx) {
             const int y = r % D.ny, z = r / D.ny;
-            const float v = fir9<kInverse>(s + j * Wp + kk, x & 1);
-            dst[size_t(z) * D.dstSlice + size_t(y) * D.dstRow + (kInverse ? x : splitPos(x, D.nx))] = v;
+            const float* w = s + j * Wp + 2 * p;
+            const float e = fir9c<kInverse, 0>(w), o = fir9c<kInverse, 1>(w + 1);
+            float* row = dst + size_t(z) * D.dstSlice + size_t(y) * D.dstRow;
+            if (kInverse) {
+                row[x] = e;
+                row[x + 1] = o;
+            } else {
+                row[x >> 1] = e;
+                row[(D.nx >> 1) + (x >> 1)] = o;
+            }
         }
     }
 }
@@ -385,33 +426,37 @@ __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ desc
     const int nx = D.nx, na = D.na;
     const int x = int(xt) * 32 + tx;
     const int a0 = at * kColTile;
-    if (x < nx) {
-        for (int k = ty; k < kColTile + 8; k += 8) {
-            const int j = a0 - 4 + k;
-            if (j < na + 4) {
-                const int m = mirrorIdx(j, na);
-                const int a = kInverse ? splitPos(m, na) : m;
-                float v;
-                if (kSymbols) {
-                    // axis Z: a = z, c = y (DWTFloatFromSymbolsKernels.cui:18-464)
-                    const int y = c, z = a;
-                    const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
-                    const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
-                    const int b = bx + 2 * by + 4 * bz;
-                    if (b == 0) {
-                        v = D.src[size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx];
-                    } else {
-                        const u32 sym = D.bands[u64(b - 1) * D.bandStride + (u64(lz) * D.hy + ly) * D.hx + lx];
-                        const int q = unsymbolizeI(sym);
-                        v = (float(q) + signI(q) * 0.5f) * D.step;
-                    }
+    // all of a thread's column loads are issued before any is used
+    constexpr int kLoads = (kColTile + 8) / 8;
+    float vals[kLoads];
+#pragma unroll
+    for (int i = 0; i < kLoads; ++i) {
+        const int k = ty + 8 * i;
+        const int j = a0 - 4 + k;
+        vals[i] = 0.0f;
+        if (x < nx && j < na + 4) {
+            const int m = mirrorIdx(j, na);
+            const int a = kInverse ? splitPos(m, na) : m;
+            if (kSymbols) {
+                // axis Z: a = z, c = y (DWTFloatFromSymbolsKernels.cui:18-464)
+                const int y = c, z = a;
+                const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
+                const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
+                const int b = bx + 2 * by + 4 * bz;
+                if (b == 0) {
+                    vals[i] = D.src[size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx];
                 } else {
-                    v = D.src[size_t(x) * D.sx + size_t(a) * D.sa + size_t(c) * D.sc];
+                    const u32 sym = D.bands[u64(b - 1) * D.bandStride + (u64(lz) * D.hy + ly) * D.hx + lx];
+                    const int q = unsymbolizeI(sym);
+                    vals[i] = (float(q) + signI(q) * 0.5f) * D.step;
                 }
-                s[k][tx] = v;
+            } else {
+                vals[i] = D.src[size_t(x) * D.sx + size_t(a) * D.sa + size_t(c) * D.sc];
             }
         }
     }
+#pragma unroll
+    for (int i = 0; i < kLoads; ++i) s[ty + 8 * i][tx] = vals[i];
     __syncthreads();
     if (x >= nx) return;
     for (int k = ty; k < kColTile; k += 8) {
@@ -434,9 +479,10 @@ __global__ void __launch_bounds__(256) k_bQuant(const BQuantDesc* __restrict__ d
     const BQuantDesc& D = descs[sDesc];
     const u64 plane = u64(D.nx) * D.ny, total = plane * D.nz;
     const u64 e0 = u64(blockIdx.x - D.ctaOff) * kBQuantPerCta;
+#pragma unroll
     for (u32 k = threadIdx.x; k < u32(kBQuantPerCta); k += 256) {
         const u64 e = e0 + k;
-        if (e >= total) break;
+        if (e >= total) continue;
         if (kDequantize) {
             const int q = unsymbolizeI(u32(D.sym[e]));
             D.dstF[e] = (float(q) + signI(q) * 0.5f) * D.step;   // Quantize.cuh:104-110
