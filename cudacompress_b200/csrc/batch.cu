@@ -20,6 +20,7 @@
 // bands of each level coarse -> fine, every band 16-byte aligned), the
 // descriptors, and per brick the word offset and bit size of its stream in
 // the batch's output words.
+#include <algorithm>
 #include <cstring>
 #include <map>
 
@@ -47,9 +48,9 @@ struct cc_volume_batch {
     ccb::u32* volFirstStream = nullptr;   // [count + 1]
     // launch lists
     // per volume v: descriptors and CTAs of volumes 0..v (prefix launches)
-    struct Rows { const ccb::BRowDesc* d; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
-    struct Cols { const ccb::BColDesc* d; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
-    struct Quant { const ccb::BQuantDesc* d; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    struct Rows { const ccb::BRowDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    struct Cols { const ccb::BColDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    struct Quant { const ccb::BQuantDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
     std::vector<Rows> fwdRows, invRows;        // per level
     std::vector<Cols> fwdY, fwdZ, invZ, invY;  // per level
     Quant quant{}, dequantLP{};
@@ -88,17 +89,30 @@ u64 vol3(u32 x, u32 y, u32 z) { return u64(x) * y * z; }
 void addRows(std::vector<BRowDesc>& v, u32& ctas, BRowDesc d) {
     batchRowTiling(d.nx, d.W, d.R);
     d.tilesX = int(ceilDiv(d.nx, d.W));
+    d.vec = (d.nx % 8 == 0 && d.W % 8 == 0 && d.srcRow % 4 == 0 && d.srcSlice % 4 == 0 && d.dstRow % 4 == 0 &&
+             d.dstSlice % 4 == 0) ? 1 : 0;
     d.ctaOff = ctas;
     ctas += u32(d.tilesX) * u32(ceilDiv(u64(d.ny) * d.nz, d.R));
     v.push_back(d);
 }
 
 void addCols(std::vector<BColDesc>& v, u32& ctas, BColDesc d) {
-    d.tilesX = u32(ceilDiv(d.nx, 32));
-    d.tilesA = u32(ceilDiv(d.na, 64));
+    d.tilesX = u32(ceilDiv(d.nx, kBColTileX));
+    d.tilesA = u32(ceilDiv(d.na, kBColTileA));
     d.ctaOff = ctas;
     ctas += d.tilesX * d.tilesA * u32(d.nc);
     v.push_back(d);
+}
+
+// CTA -> descriptor index of one launch (descriptors are in CTA order)
+template <class Desc>
+std::vector<u32> ctaMapOf(const std::vector<Desc>& v, u32 ctas) {
+    std::vector<u32> m(ctas);
+    for (size_t i = 0; i < v.size(); ++i) {
+        const u32 end = i + 1 < v.size() ? v[i + 1].ctaOff : ctas;
+        std::fill(m.begin() + v[i].ctaOff, m.begin() + end, u32(i));
+    }
+    return m;
 }
 
 void addQuant(std::vector<BQuantDesc>& v, u32& ctas, BQuantDesc d) {
@@ -148,14 +162,14 @@ static int batchEnqueueCompress(cc_volume_batch* b) {
     for (u32 l = 0; l < b->levels; ++l) {
         SectionTimer t(I, "batch.dwt_forward", st);
         prefixOf(b->fwdRows[l], k, nd, ctas);
-        launchBatchRows(b->fwdRows[l].d, nd, ctas, false, b->inTab, b->outTab, st);
+        launchBatchRows(b->fwdRows[l].d, b->fwdRows[l].map, ctas, false, b->inTab, b->outTab, st);
         prefixOf(b->fwdY[l], k, nd, ctas);
-        launchBatchCols(b->fwdY[l].d, nd, ctas, false, false, st);
+        launchBatchCols(b->fwdY[l].d, b->fwdY[l].map, ctas, false, false, st);
         prefixOf(b->fwdZ[l], k, nd, ctas);
-        launchBatchCols(b->fwdZ[l].d, nd, ctas, false, false, st);
+        launchBatchCols(b->fwdZ[l].d, b->fwdZ[l].map, ctas, false, false, st);
     }
     prefixOf(b->quant, k, nd, ctas);
-    { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, nd, ctas, false, st); }
+    { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, b->quant.map, ctas, false, st); }
     EncPlan ep = b->enc;
     ep.S = b->encS[k - 1];
     ep.T = b->encT[k - 1];
@@ -185,15 +199,15 @@ static int batchEnqueueDecompress(cc_volume_batch* b) {
     int rc = decodeLaunch(I, dp);
     if (rc) return rc;
     prefixOf(b->dequantLP, k, nd, ctas);
-    { SectionTimer t(I, "batch.dequantize", st); launchBatchQuant(b->dequantLP.d, nd, ctas, true, st); }
+    { SectionTimer t(I, "batch.dequantize", st); launchBatchQuant(b->dequantLP.d, b->dequantLP.map, ctas, true, st); }
     for (int l = int(b->levels) - 1; l >= 0; --l) {
         SectionTimer t(I, "batch.dwt_inverse", st);
         prefixOf(b->invZ[l], k, nd, ctas);
-        launchBatchCols(b->invZ[l].d, nd, ctas, true, true, st);
+        launchBatchCols(b->invZ[l].d, b->invZ[l].map, ctas, true, true, st);
         prefixOf(b->invY[l], k, nd, ctas);
-        launchBatchCols(b->invY[l].d, nd, ctas, true, false, st);
+        launchBatchCols(b->invY[l].d, b->invY[l].map, ctas, true, false, st);
         prefixOf(b->invRows[l], k, nd, ctas);
-        launchBatchRows(b->invRows[l].d, nd, ctas, true, b->inTab, b->outTab, st);
+        launchBatchRows(b->invRows[l].d, b->invRows[l].map, ctas, true, b->inTab, b->outTab, st);
     }
     CC_TRY_CUDA(cudaGetLastError(), "batch decompress");
     return CC_OK;
@@ -275,6 +289,10 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             return CC_ERR_INVALID_ARGUMENT;
         }
         if (!(quantSteps[v] > 0.0f)) { setError("cc_volume_batch_create: volume %u: quantization step must be > 0", v); return CC_ERR_INVALID_ARGUMENT; }
+        if (vol3(x, y, z) >= (u64(1) << 31)) {
+            setError("cc_volume_batch_create: volume %u (%u x %u x %u): at most 2^31 - 1 elements per volume", v, x, y, z);
+            return CC_ERR_INVALID_ARGUMENT;
+        }
         N0sum += vol3(x, y, z);
         maxStream = std::max<u32>(maxStream, u32(vol3(x >> 1, y >> 1, z >> 1)));
     }
@@ -368,8 +386,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             BColDesc c{};
             c.src = t1(v); c.dst = t2(v);
             c.nx = sx; c.na = syz; c.nc = sz;
-            c.sx = 1; c.sa = sx; c.sc = sx * syz;
-            c.dx = 1; c.da = sx; c.dc = sx * syz;
+            c.sa = sx; c.sc = sx * syz;
+            c.da = sx; c.dc = sx * syz;
             addCols(fy[l], fyC[l], c);
             // Z: t2 -> level l coefficients
             BColDesc cz = c;
@@ -383,7 +401,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             ic.src = lev(l + 1, v);
             ic.dst = t2(v);
             ic.nx = sx; ic.na = sz; ic.nc = syz;
-            ic.dx = 1; ic.da = sx * syz; ic.dc = sx;
+            ic.da = sx * syz; ic.dc = sx;
             ic.bands = sy(v) + sl[v].level[l];
             ic.bandStride = sl[v].bandStride[l];
             ic.step = b->q0[v] / float(1u << l);
@@ -393,8 +411,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             BColDesc iyd{};
             iyd.src = t2(v); iyd.dst = t1(v);
             iyd.nx = sx; iyd.na = syz; iyd.nc = sz;
-            iyd.sx = 1; iyd.sa = sx; iyd.sc = sx * syz;
-            iyd.dx = 1; iyd.da = sx; iyd.dc = sx * syz;
+            iyd.sa = sx; iyd.sc = sx * syz;
+            iyd.da = sx; iyd.dc = sx * syz;
             addCols(iy[l], iyC[l], iyd);
             BRowDesc irw{};
             irw.vol = int(v);
@@ -458,6 +476,24 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     }
     const size_t qAt = A.take(bytesOf(qd.size(), sizeof(BQuantDesc)), 64);
     const size_t dqAt = A.take(bytesOf(dq.size(), sizeof(BQuantDesc)), 64);
+    // CTA maps, one per launch
+    std::vector<std::vector<u32>> maps;
+    std::vector<size_t> mapAt;
+    auto addMap = [&](std::vector<u32> m) {
+        mapAt.push_back(A.take(bytesOf(m.size(), sizeof(u32)), 64));
+        maps.push_back(std::move(m));
+        return maps.size() - 1;
+    };
+    std::vector<size_t> frMap(L), irMap(L), fyMap(L), fzMap(L), izMap(L), iyMap(L);
+    for (u32 l = 0; l < L; ++l) {
+        frMap[l] = addMap(ctaMapOf(fr[l], frC[l]));
+        irMap[l] = addMap(ctaMapOf(ir[l], irC[l]));
+        fyMap[l] = addMap(ctaMapOf(fy[l], fyC[l]));
+        fzMap[l] = addMap(ctaMapOf(fz[l], fzC[l]));
+        izMap[l] = addMap(ctaMapOf(iz[l], izC[l]));
+        iyMap[l] = addMap(ctaMapOf(iy[l], iyC[l]));
+    }
+    const size_t qMap = addMap(ctaMapOf(qd, qC)), dqMap = addMap(ctaMapOf(dq, dqC));
     // encoder / decoder descriptors: sized by preparing into a host buffer
     const size_t planMax = size_t(I->hostRingBytes);
     std::vector<char> encHost(planMax), decHost(planMax);
@@ -512,6 +548,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
         if (e == cudaSuccess) e = up(izAt[l], iz[l].data(), iz[l].size() * sizeof(BColDesc));
         if (e == cudaSuccess) e = up(iyAt[l], iy[l].data(), iy[l].size() * sizeof(BColDesc));
     }
+    for (size_t m = 0; m < maps.size() && e == cudaSuccess; ++m) e = up(mapAt[m], maps[m].data(), maps[m].size() * sizeof(u32));
     if (e == cudaSuccess) e = up(qAt, qd.data(), qd.size() * sizeof(BQuantDesc));
     if (e == cudaSuccess) e = up(dqAt, dq.data(), dq.size() * sizeof(BQuantDesc));
     if (e == cudaSuccess) e = up(encAt, encHost.data(), b->enc.bytes);
@@ -524,16 +561,17 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { cc_volume_batch_destroy(b); return cudaFail(e, "volume batch set-up"); }
     b->fwdRows.resize(L); b->invRows.resize(L); b->fwdY.resize(L); b->fwdZ.resize(L); b->invZ.resize(L); b->invY.resize(L);
+    auto mapPtr = [&](size_t m) { return reinterpret_cast<const u32*>(base + mapAt[m]); };
     for (u32 l = 0; l < L; ++l) {
-        b->fwdRows[l] = {reinterpret_cast<const BRowDesc*>(base + frAt[l]), u32(fr[l].size()), frC[l]};
-        b->invRows[l] = {reinterpret_cast<const BRowDesc*>(base + irAt[l]), u32(ir[l].size()), irC[l]};
-        b->fwdY[l] = {reinterpret_cast<const BColDesc*>(base + fyAt[l]), u32(fy[l].size()), fyC[l]};
-        b->fwdZ[l] = {reinterpret_cast<const BColDesc*>(base + fzAt[l]), u32(fz[l].size()), fzC[l]};
-        b->invZ[l] = {reinterpret_cast<const BColDesc*>(base + izAt[l]), u32(iz[l].size()), izC[l]};
-        b->invY[l] = {reinterpret_cast<const BColDesc*>(base + iyAt[l]), u32(iy[l].size()), iyC[l]};
+        b->fwdRows[l] = {reinterpret_cast<const BRowDesc*>(base + frAt[l]), mapPtr(frMap[l]), u32(fr[l].size()), frC[l]};
+        b->invRows[l] = {reinterpret_cast<const BRowDesc*>(base + irAt[l]), mapPtr(irMap[l]), u32(ir[l].size()), irC[l]};
+        b->fwdY[l] = {reinterpret_cast<const BColDesc*>(base + fyAt[l]), mapPtr(fyMap[l]), u32(fy[l].size()), fyC[l]};
+        b->fwdZ[l] = {reinterpret_cast<const BColDesc*>(base + fzAt[l]), mapPtr(fzMap[l]), u32(fz[l].size()), fzC[l]};
+        b->invZ[l] = {reinterpret_cast<const BColDesc*>(base + izAt[l]), mapPtr(izMap[l]), u32(iz[l].size()), izC[l]};
+        b->invY[l] = {reinterpret_cast<const BColDesc*>(base + iyAt[l]), mapPtr(iyMap[l]), u32(iy[l].size()), iyC[l]};
     }
-    b->quant = {reinterpret_cast<const BQuantDesc*>(base + qAt), u32(qd.size()), qC};
-    b->dequantLP = {reinterpret_cast<const BQuantDesc*>(base + dqAt), u32(dq.size()), dqC};
+    b->quant = {reinterpret_cast<const BQuantDesc*>(base + qAt), mapPtr(qMap), u32(qd.size()), qC};
+    b->dequantLP = {reinterpret_cast<const BQuantDesc*>(base + dqAt), mapPtr(dqMap), u32(dq.size()), dqC};
     // prefixes by volume
     auto prefix = [&](auto& li, const auto& host, u32 perVolume) {
         li.descEnd.resize(count);

@@ -1,7 +1,7 @@
 // batch.cuh - descriptors and launchers of the batched volume codec's
 // transform kernels (dwt.cu).  Every launch covers one pass of one level for
-// all volumes of a batch: its CTAs are numbered across the volumes and each
-// CTA finds its volume's descriptor by binary search over ctaOff.
+// all volumes of a batch: its CTAs are numbered across the volumes and a
+// per-launch CTA map (u32 per CTA) gives each CTA its descriptor's index.
 #pragma once
 
 #include "capi_internal.cuh"
@@ -16,10 +16,12 @@ struct BRowDesc {
     int nx, ny, nz;
     int srcRow, srcSlice, dstRow, dstSlice;
     int W, R, tilesX;       // tile width, rows per CTA, tiles per row
+    int vec;                // nx, W and all pitches allow float4 rows (pointers are checked per CTA)
     u32 ctaOff;
 };
 
-// Y or Z pass: 32 x-columns by 64 axis positions per CTA.  With `bands`
+// Y or Z pass: kBColTileX x-columns (unit stride, float2 pairs) by
+// kBColTileA axis positions per CTA.  With `bands`
 // set it is the first inverse pass of dwtFloat3DInverseFromSymbols: the
 // lowpass octant comes from src (lpRow, lpSlice pitches), the other seven
 // from dequantized symbol bands (band b-1 at bands + (b-1) * bandStride).
@@ -27,8 +29,8 @@ struct BColDesc {
     const float* src;
     float* dst;
     int nx, na, nc;
-    int sx, sa, sc;         // source strides (x, axis, other)
-    int dx, da, dc;         // destination strides
+    int sa, sc;             // source strides (axis, other); x has unit stride
+    int da, dc;             // destination strides
     const u16* bands;
     u64 bandStride;
     float step;
@@ -45,24 +47,29 @@ struct BQuantDesc {
     float* dstF;
     int nx, ny, nz, row, slice;
     float step, inv;
-    u32 ctaOff;             // 1024 elements per CTA
+    u32 ctaOff;             // kBQuantPerCta elements per CTA
 };
 
-constexpr int kBRowOutputs = 512;
-constexpr int kBQuantPerCta = 1024;
+constexpr int kBRowOutputs = 4096;    // outputs per row-pass CTA
+constexpr int kBRowMaxWidth = 2048;   // row tile width
+constexpr int kBRowMaxRows = 128;     // rows per row-pass CTA
+constexpr int kBRowSmem = kBRowOutputs + 8 * kBRowMaxRows;   // floats: R rows of W + 8
+constexpr int kBColTileX = 64;
+constexpr int kBColTileA = 64;
+constexpr int kBQuantPerCta = 4096;
 
-// Descriptor arrays are device pointers; ctas = total CTA count.
-void launchBatchRows(const BRowDesc* d, u32 nd, u32 ctas, bool inverse, const float* const* inTab,
+// Descriptor arrays and CTA maps are device pointers; ctas = CTA count.
+void launchBatchRows(const BRowDesc* d, const u32* map, u32 ctas, bool inverse, const float* const* inTab,
                      float* const* outTab, cudaStream_t st);
-void launchBatchCols(const BColDesc* d, u32 nd, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st);
-void launchBatchQuant(const BQuantDesc* d, u32 nd, u32 ctas, bool dequantize, cudaStream_t st);
+void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st);
+void launchBatchQuant(const BQuantDesc* d, const u32* map, u32 ctas, bool dequantize, cudaStream_t st);
 
 // Row tiling of an X pass over an nx-wide level: tile width, rows per CTA.
 inline void batchRowTiling(int nx, int& W, int& R) {
-    W = nx < kBRowOutputs ? nx : kBRowOutputs;
+    W = nx < kBRowMaxWidth ? nx : kBRowMaxWidth;
     R = kBRowOutputs / W;
     if (R < 1) R = 1;
-    if (R > 64) R = 64;
+    if (R > kBRowMaxRows) R = kBRowMaxRows;
 }
 
 }  // namespace ccb

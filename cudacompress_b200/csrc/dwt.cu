@@ -346,112 +346,234 @@ static int dwtScratchFor(int device, float** out) {
 
 // ---------------------------------------------------------------------------
 // Batched passes (batch.cuh): the same arithmetic as k_firRows / k_firCols /
-// k_quantize, over all volumes of a batch in one launch.
+// k_quantize, over all volumes of a batch in one launch.  A CTA reads its
+// descriptor index from the launch's CTA map (one load) and the descriptor.
 // ---------------------------------------------------------------------------
-template <class Desc>
-__device__ __forceinline__ u32 findDesc(const Desc* d, u32 nd, u32 cta) {
-    u32 lo = 0, hi = nd;
-    while (hi - lo > 1) {
-        const u32 mid = (lo + hi) >> 1;
-        if (d[mid].ctaOff <= cta) lo = mid; else hi = mid;
+template <bool kInverse>
+__device__ __forceinline__ void rowPairs4(const float* w, float4& a, float4& b) {
+    // four (even, odd) output pairs from the 16-sample window w[0..15]
+    const float e0 = fir9c<kInverse, 0>(w), o0 = fir9c<kInverse, 1>(w + 1);
+    const float e1 = fir9c<kInverse, 0>(w + 2), o1 = fir9c<kInverse, 1>(w + 3);
+    const float e2 = fir9c<kInverse, 0>(w + 4), o2 = fir9c<kInverse, 1>(w + 5);
+    const float e3 = fir9c<kInverse, 0>(w + 6), o3 = fir9c<kInverse, 1>(w + 7);
+    if (kInverse) {
+        a = make_float4(e0, o0, e1, o1);
+        b = make_float4(e2, o2, e3, o3);
+    } else {
+        a = make_float4(e0, e1, e2, e3);
+        b = make_float4(o0, o1, o2, o3);
     }
-    return lo;
 }
 
+// Row (X) pass.  A CTA transforms R rows of one W-wide tile of a row
+// (R * W <= kBRowOutputs): the rows and their 4-sample mirrored halos are
+// staged in shared memory, then every thread computes output pairs.  Fast
+// path (descriptor flag `vec` and 16-byte aligned pointers): float4 loads of
+// the tile body - the inverse reads the low and high halves separately and
+// interleaves them on the way into shared memory - and float4 stores of four
+// pairs per thread.  Otherwise scalar loads and stores.
 template <bool kInverse>
-__global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ descs, u32 nd,
+__global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ descs, const u32* __restrict__ map,
                                                const float* const* inTab, float* const* outTab) {
-    __shared__ float s[1024 + 64];
-    __shared__ u32 sDesc;
-    if (threadIdx.x == 0) sDesc = findDesc(descs, nd, blockIdx.x);
-    __syncthreads();
-    const BRowDesc D = descs[sDesc];
+    __shared__ __align__(16) float s[kBRowSmem];
+    const BRowDesc D = descs[map[blockIdx.x]];
     const float* src = D.src ? D.src : inTab[D.vol];
     float* dst = D.dst ? D.dst : outTab[D.vol];
     const u32 local = blockIdx.x - D.ctaOff;
     const int xt = int(local % u32(D.tilesX)), rg = int(local / u32(D.tilesX));
-    const int x0 = xt * D.W, Wp = D.W + 8, rows = D.ny * D.nz;
-    // all of a thread's loads are issued before any is used (R * Wp <= 1088)
-    float vals[5];
+    const int nx = D.nx, hn = nx >> 1;
+    const int x0 = xt * D.W, Wt = min(D.W, nx - x0), Wp = Wt + 8;
+    const int rows = D.ny * D.nz, r0 = rg * D.R, R = min(D.R, rows - r0);
+    auto srcRow = [&](int j) {
+        const int r = r0 + j, z = r / D.ny, y = r - z * D.ny;
+        return src + size_t(z) * D.srcSlice + size_t(y) * D.srcRow;
+    };
+    auto dstRow = [&](int j) {
+        const int r = r0 + j, z = r / D.ny, y = r - z * D.ny;
+        return dst + size_t(z) * D.dstSlice + size_t(y) * D.dstRow;
+    };
+    const int tid = threadIdx.x;
+    const bool vec = D.vec && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+    if (vec) {
+        // body: forward U = Wt/4 float4 per row; inverse U = Wt/8 (low, high) float4 pairs per row
+        constexpr int kBody = kBRowOutputs / 1024;   // float4 loads per thread
+        float4 body[kBody];
+        float halo[kBody];
+        const int U = kInverse ? Wt >> 3 : Wt >> 2;
 #pragma unroll
-    for (int i = 0; i < 5; ++i) {
-        const int k = threadIdx.x + 256 * i;
-        const int j = k / Wp, kk = k - j * Wp, r = rg * D.R + j;
-        const int xx = x0 - 4 + kk;
-        vals[i] = 0.0f;
-        if (k < D.R * Wp && r < rows && xx < D.nx + 4) {
-            const int m = mirrorIdx(xx, D.nx);
-            const int y = r % D.ny, z = r / D.ny;
-            vals[i] = src[size_t(z) * D.srcSlice + size_t(y) * D.srcRow + (kInverse ? splitPos(m, D.nx) : m)];
+        for (int i = 0; i < kBody; ++i) {
+            const int k = tid + 256 * (kInverse ? (i >> 1) : i);
+            body[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < R * U) {
+                const int j = k / U, q = k - j * U;
+                const float* row = srcRow(j);
+                if (kInverse) body[i] = *reinterpret_cast<const float4*>(row + (i & 1) * hn + (x0 >> 1) + 4 * q);
+                else body[i] = *reinterpret_cast<const float4*>(row + x0 + 4 * q);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kBody; ++i) {
+            const int k = tid + 256 * i;
+            halo[i] = 0.0f;
+            if (k < R * 8) {
+                const int j = k >> 3, h = k & 7;
+                const int m = mirrorIdx(h < 4 ? x0 - 4 + h : x0 + Wt + h - 4, nx);
+                halo[i] = srcRow(j)[kInverse ? splitPos(m, nx) : m];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kBody; ++i) {
+            const int k = tid + 256 * (kInverse ? (i >> 1) : i);
+            if (k < R * U) {
+                const int j = k / U, q = k - j * U;
+                if (kInverse) {
+                    if (i & 1) {
+                        const float4 l = body[i - 1], h = body[i];
+                        float4* o = reinterpret_cast<float4*>(s + j * Wp + 4 + 8 * q);
+                        o[0] = make_float4(l.x, h.x, l.y, h.y);
+                        o[1] = make_float4(l.z, h.z, l.w, h.w);
+                    }
+                } else {
+                    *reinterpret_cast<float4*>(s + j * Wp + 4 + 4 * q) = body[i];
+                }
+            }
+            if (tid + 256 * i < R * 8) {
+                const int k2 = tid + 256 * i, j = k2 >> 3, h = k2 & 7;
+                s[j * Wp + (h < 4 ? h : Wt + h)] = halo[i];
+            }
+        }
+        __syncthreads();
+        // outputs: four pairs per thread-step
+        const int Q = Wt >> 3;
+#pragma unroll
+        for (int i = 0; i < kBRowOutputs / 2048; ++i) {
+            const int k = tid + 256 * i;
+            if (k < R * Q) {
+                const int j = k / Q, q = k - j * Q;
+                const float* w4 = s + j * Wp + 8 * q;
+                float w[16];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const float4 v = *reinterpret_cast<const float4*>(w4 + 4 * t);
+                    w[4 * t] = v.x; w[4 * t + 1] = v.y; w[4 * t + 2] = v.z; w[4 * t + 3] = v.w;
+                }
+                float4 a, b;
+                rowPairs4<kInverse>(w, a, b);
+                float* row = dstRow(j);
+                if (kInverse) {
+                    float4* o = reinterpret_cast<float4*>(row + x0 + 8 * q);
+                    o[0] = a;
+                    o[1] = b;
+                } else {
+                    *reinterpret_cast<float4*>(row + (x0 >> 1) + 4 * q) = a;
+                    *reinterpret_cast<float4*>(row + hn + (x0 >> 1) + 4 * q) = b;
+                }
+            }
+        }
+        return;
+    }
+    // scalar path: positions x0-4 .. x0+Wt+3 of each row, 8 loads in flight per thread
+    const int total = R * Wp;
+    for (int base = 0; base < total; base += 256 * 8) {
+        float v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int k = base + tid + 256 * i;
+            v[i] = 0.0f;
+            if (k < total) {
+                const int j = k / Wp, kk = k - j * Wp;
+                const int m = mirrorIdx(x0 - 4 + kk, nx);
+                v[i] = srcRow(j)[kInverse ? splitPos(m, nx) : m];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int k = base + tid + 256 * i;
+            if (k < total) s[k] = v[i];
         }
     }
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-        const int k = threadIdx.x + 256 * i;
-        if (k < D.R * Wp) s[k] = vals[i];
-    }
     __syncthreads();
-    // each thread computes an (even, odd) output pair: coalesced stores to
-    // both halves (forward) or one float2 (inverse), parity-free taps
-    const int hw = D.W / 2;
-    for (int k = threadIdx.x; k < D.R * hw; k += 256) {
-        const int j = k / hw, p = k - j * hw, r = rg * D.R + j, x = x0 + 2 * p;
-        if (r < rows && x < D.nx) {
-            const int y = r % D.ny, z = r / D.ny;
-            const float* w = s + j * Wp + 2 * p;
-            const float e = fir9c<kInverse, 0>(w), o = fir9c<kInverse, 1>(w + 1);
-            float* row = dst + size_t(z) * D.dstSlice + size_t(y) * D.dstRow;
-            if (kInverse) {
-                row[x] = e;
-                row[x + 1] = o;
-            } else {
-                row[x >> 1] = e;
-                row[(D.nx >> 1) + (x >> 1)] = o;
-            }
+    const int P = Wt >> 1;
+    for (int k = tid; k < R * P; k += 256) {
+        const int j = k / P, p = k - j * P, x = x0 + 2 * p;
+        const float* w = s + j * Wp + 2 * p;
+        const float e = fir9c<kInverse, 0>(w), o = fir9c<kInverse, 1>(w + 1);
+        float* row = dstRow(j);
+        if (kInverse) {
+            row[x] = e;
+            row[x + 1] = o;
+        } else {
+            row[x >> 1] = e;
+            row[hn + (x >> 1)] = o;
         }
     }
 }
 
+// One sample of the first inverse pass of dwtFloat3DInverseFromSymbols:
+// (x, y, z) in the level's interleaved-band layout; the lowpass octant comes
+// from src, the other seven from dequantized symbol bands
+// (DWTFloatFromSymbolsKernels.cui:18-464).
+__device__ __forceinline__ float bandSample(const BColDesc& D, int x, int y, int z) {
+    const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
+    const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
+    const int b = bx + 2 * by + 4 * bz;
+    if (b == 0) return D.src[size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx];
+    const u32 sym = D.bands[u64(b - 1) * D.bandStride + (u64(lz) * D.hy + ly) * D.hx + lx];
+    const int q = unsymbolizeI(sym);
+    return (float(q) + signI(q) * 0.5f) * D.step;   // Quantize.cuh:104-110
+}
+
+template <bool kInverse, int kParity>
+__device__ __forceinline__ void colOutputs(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x, int c,
+                                           int a0) {
+    for (int k = ty; k < kBColTileA; k += 8) {
+        const int a = a0 + k;
+        if (a >= D.na) break;
+        float v0[9], v1[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const float2 t = s[k + i][tx];
+            v0[i] = t.x;
+            v1[i] = t.y;
+        }
+        const float2 r = make_float2(fir9c<kInverse, kParity>(v0), fir9c<kInverse, kParity>(v1));
+        const int o = kInverse ? a : splitPos(a, D.na);
+        *reinterpret_cast<float2*>(D.dst + size_t(x) + size_t(o) * D.da + size_t(c) * D.dc) = r;
+    }
+}
+
+// Y or Z pass: 64 x-columns (a column pair per thread, float2 accesses; all
+// level extents are even and x is the unit-stride axis) by kBColTileA axis
+// positions per CTA.  The output parity of a thread is fixed (kBColTileA and
+// the row step 8 are even), so its taps are compile-time immediates.
+static_assert(kBColTileX == 64, "a column-pass CTA has 32 threads of column pairs per row");
+
 template <bool kInverse, bool kSymbols>
-__global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ descs, u32 nd) {
-    __shared__ float s[kColTile + 8][33];
-    __shared__ u32 sDesc;
+__global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ descs, const u32* __restrict__ map) {
+    __shared__ float2 s[kBColTileA + 8][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
-    if (tx == 0 && ty == 0) sDesc = findDesc(descs, nd, blockIdx.x);
-    __syncthreads();
-    const BColDesc& D = descs[sDesc];
+    const BColDesc& D = descs[map[blockIdx.x]];
     const u32 local = blockIdx.x - D.ctaOff;
     const u32 xt = local % D.tilesX, rest = local / D.tilesX;
     const int at = int(rest % D.tilesA), c = int(rest / D.tilesA);
     const int nx = D.nx, na = D.na;
-    const int x = int(xt) * 32 + tx;
-    const int a0 = at * kColTile;
+    const int x = int(xt) * kBColTileX + 2 * tx;
+    const int a0 = at * kBColTileA;
     // all of a thread's column loads are issued before any is used
-    constexpr int kLoads = (kColTile + 8) / 8;
-    float vals[kLoads];
+    constexpr int kLoads = (kBColTileA + 8) / 8;
+    float2 vals[kLoads];
 #pragma unroll
     for (int i = 0; i < kLoads; ++i) {
-        const int k = ty + 8 * i;
-        const int j = a0 - 4 + k;
-        vals[i] = 0.0f;
+        const int j = a0 - 4 + ty + 8 * i;
+        vals[i] = make_float2(0.0f, 0.0f);
         if (x < nx && j < na + 4) {
             const int m = mirrorIdx(j, na);
             const int a = kInverse ? splitPos(m, na) : m;
             if (kSymbols) {
-                // axis Z: a = z, c = y (DWTFloatFromSymbolsKernels.cui:18-464)
-                const int y = c, z = a;
-                const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
-                const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
-                const int b = bx + 2 * by + 4 * bz;
-                if (b == 0) {
-                    vals[i] = D.src[size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx];
-                } else {
-                    const u32 sym = D.bands[u64(b - 1) * D.bandStride + (u64(lz) * D.hy + ly) * D.hx + lx];
-                    const int q = unsymbolizeI(sym);
-                    vals[i] = (float(q) + signI(q) * 0.5f) * D.step;
-                }
+                // axis Z: a = z, c = y
+                vals[i] = make_float2(bandSample(D, x, c, a), bandSample(D, x + 1, c, a));
             } else {
-                vals[i] = D.src[size_t(x) * D.sx + size_t(a) * D.sa + size_t(c) * D.sc];
+                vals[i] = *reinterpret_cast<const float2*>(D.src + size_t(x) + size_t(a) * D.sa + size_t(c) * D.sc);
             }
         }
     }
@@ -459,63 +581,100 @@ __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ desc
     for (int i = 0; i < kLoads; ++i) s[ty + 8 * i][tx] = vals[i];
     __syncthreads();
     if (x >= nx) return;
-    for (int k = ty; k < kColTile; k += 8) {
-        const int a = a0 + k;
-        if (a >= na) break;
-        float v[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) v[i] = s[k + i][tx];
-        const float r = fir9<kInverse>(v, a & 1);
-        const int o = kInverse ? a : splitPos(a, na);
-        D.dst[size_t(x) * D.dx + size_t(o) * D.da + size_t(c) * D.dc] = r;
-    }
+    if ((a0 + ty) & 1) colOutputs<kInverse, 1>(D, s, tx, ty, x, c, a0);
+    else colOutputs<kInverse, 0>(D, s, tx, ty, x, c, a0);
 }
 
+// Quantization of one band to u16 symbols (deadzone, Quantize.cuh:55-59), or
+// dequantization of dense symbols (Quantize.cuh:104-110).  A CTA covers
+// kBQuantPerCta elements of one band in groups of four consecutive elements;
+// a group inside one row with 16-byte aligned source moves as one float4
+// and one 8-byte symbol store.
 template <bool kDequantize>
-__global__ void __launch_bounds__(256) k_bQuant(const BQuantDesc* __restrict__ descs, u32 nd) {
-    __shared__ u32 sDesc;
-    if (threadIdx.x == 0) sDesc = findDesc(descs, nd, blockIdx.x);
-    __syncthreads();
-    const BQuantDesc& D = descs[sDesc];
-    const u64 plane = u64(D.nx) * D.ny, total = plane * D.nz;
-    const u64 e0 = u64(blockIdx.x - D.ctaOff) * kBQuantPerCta;
+__global__ void __launch_bounds__(256) k_bQuant(const BQuantDesc* __restrict__ descs, const u32* __restrict__ map) {
+    const BQuantDesc& D = descs[map[blockIdx.x]];
+    const u32 nx = u32(D.nx), plane = nx * u32(D.ny), total = plane * u32(D.nz);
+    const u32 e0 = (blockIdx.x - D.ctaOff) * u32(kBQuantPerCta);
+    constexpr int kGroups = kBQuantPerCta / 1024;
+    if (kDequantize) {
 #pragma unroll
-    for (u32 k = threadIdx.x; k < u32(kBQuantPerCta); k += 256) {
-        const u64 e = e0 + k;
-        if (e >= total) continue;
-        if (kDequantize) {
-            const int q = unsymbolizeI(u32(D.sym[e]));
-            D.dstF[e] = (float(q) + signI(q) * 0.5f) * D.step;   // Quantize.cuh:104-110
+        for (int g = 0; g < kGroups; ++g) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const u32 e = e0 + u32(g) * 1024u + u32(t) * 256u + threadIdx.x;
+                if (e < total) {
+                    const int q = unsymbolizeI(u32(D.sym[e]));
+                    D.dstF[e] = (float(q) + signI(q) * 0.5f) * D.step;
+                }
+            }
+        }
+        return;
+    }
+    const bool vec = (nx & 3) == 0 && ((D.row | D.slice) & 3) == 0 && (reinterpret_cast<uintptr_t>(D.src) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(D.sym) & 7) == 0;
+    float4 v[kGroups];
+    u32 eg[kGroups];
+#pragma unroll
+    for (int g = 0; g < kGroups; ++g) {
+        eg[g] = e0 + u32(g) * 1024u + 4u * threadIdx.x;
+        v[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (eg[g] < total) {
+            const u32 z = eg[g] / plane, r = eg[g] - z * plane, y = r / nx, xx = r - y * nx;
+            const float* p = D.src + size_t(z) * D.slice + size_t(y) * D.row + xx;
+            if (vec) {
+                v[g] = *reinterpret_cast<const float4*>(p);
+            } else {
+                // element by element (the group may cross rows or be unaligned)
+                float t[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const u32 e = eg[g] + u32(i);
+                    if (e < total) {
+                        const u32 zi = e / plane, ri = e - zi * plane, yi = ri / nx, xi = ri - yi * nx;
+                        t[i] = D.src[size_t(zi) * D.slice + size_t(yi) * D.row + xi];
+                    }
+                }
+                v[g] = make_float4(t[0], t[1], t[2], t[3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < kGroups; ++g) {
+        if (eg[g] >= total) continue;
+        const u16 s0 = u16(symbolizeI(int(v[g].x * D.inv))), s1 = u16(symbolizeI(int(v[g].y * D.inv)));
+        const u16 s2 = u16(symbolizeI(int(v[g].z * D.inv))), s3 = u16(symbolizeI(int(v[g].w * D.inv)));
+        if (vec) {
+            *reinterpret_cast<uint2*>(D.sym + eg[g]) = make_uint2(u32(s0) | (u32(s1) << 16), u32(s2) | (u32(s3) << 16));
         } else {
-            const u32 z = u32(e / plane), r = u32(e - u64(z) * plane);
-            const u32 y = r / u32(D.nx), xx = r - y * u32(D.nx);
-            const float v = D.src[size_t(z) * D.slice + size_t(y) * D.row + xx];
-            D.sym[e] = u16(symbolizeI(int(v * D.inv)));            // Quantize.cuh:55-59 deadzone
+            const u16 sv[4] = {s0, s1, s2, s3};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (eg[g] + u32(i) < total) D.sym[eg[g] + u32(i)] = sv[i];
         }
     }
 }
 
-void launchBatchRows(const BRowDesc* d, u32 nd, u32 ctas, bool inverse, const float* const* inTab,
+void launchBatchRows(const BRowDesc* d, const u32* map, u32 ctas, bool inverse, const float* const* inTab,
                      float* const* outTab, cudaStream_t st) {
     if (!ctas) return;
-    if (inverse) k_bRows<true><<<ctas, 256, 0, st>>>(d, nd, inTab, outTab);
-    else k_bRows<false><<<ctas, 256, 0, st>>>(d, nd, inTab, outTab);
+    if (inverse) k_bRows<true><<<ctas, 256, 0, st>>>(d, map, inTab, outTab);
+    else k_bRows<false><<<ctas, 256, 0, st>>>(d, map, inTab, outTab);
     countLaunch();
 }
 
-void launchBatchCols(const BColDesc* d, u32 nd, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st) {
+void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st) {
     if (!ctas) return;
     const dim3 blk(32, 8);
-    if (fromSymbols) k_bCols<true, true><<<ctas, blk, 0, st>>>(d, nd);
-    else if (inverse) k_bCols<true, false><<<ctas, blk, 0, st>>>(d, nd);
-    else k_bCols<false, false><<<ctas, blk, 0, st>>>(d, nd);
+    if (fromSymbols) k_bCols<true, true><<<ctas, blk, 0, st>>>(d, map);
+    else if (inverse) k_bCols<true, false><<<ctas, blk, 0, st>>>(d, map);
+    else k_bCols<false, false><<<ctas, blk, 0, st>>>(d, map);
     countLaunch();
 }
 
-void launchBatchQuant(const BQuantDesc* d, u32 nd, u32 ctas, bool dequantize, cudaStream_t st) {
+void launchBatchQuant(const BQuantDesc* d, const u32* map, u32 ctas, bool dequantize, cudaStream_t st) {
     if (!ctas) return;
-    if (dequantize) k_bQuant<true><<<ctas, 256, 0, st>>>(d, nd);
-    else k_bQuant<false><<<ctas, 256, 0, st>>>(d, nd);
+    if (dequantize) k_bQuant<true><<<ctas, 256, 0, st>>>(d, map);
+    else k_bQuant<false><<<ctas, 256, 0, st>>>(d, map);
     countLaunch();
 }
 

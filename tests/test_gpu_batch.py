@@ -36,13 +36,22 @@ def bricks(count, levels, seed):
     return out, steps
 
 
-def check_batch(oracle, vols, steps, levels, graph, rounds=2):
+def shifted(shape, shift):
+    """A contiguous device float32 volume whose data starts `shift` elements
+    into its allocation (shift 1: 4-byte but not 16-byte aligned)."""
+    n = int(np.prod(shape))
+    return torch.empty(n + shift, dtype=torch.float32, device="cuda")[shift:].view(shape)
+
+
+def check_batch(oracle, vols, steps, levels, graph, rounds=2, shift=0):
     inst = cc.Instance(0, 7, 1 << 12, 128, 14)
     with cc.VolumeBatch(inst, [v.shape for v in vols], levels, steps, graph=graph) as b:
         ref = [oracle.compress_volume(v, levels, q) for v, q in zip(vols, steps)]
         recs = [oracle.decompress_volume(w, bits, v.shape, levels, q) for (w, bits), v, q in zip(ref, vols, steps)]
-        dev = [torch.from_numpy(v).cuda() for v in vols]
-        outs = [torch.full(v.shape, float("nan"), dtype=torch.float32, device="cuda") for v in vols]
+        dev = [shifted(v.shape, shift) for v in vols]
+        for d, v in zip(dev, vols):
+            d.copy_(torch.from_numpy(v))
+        outs = [shifted(v.shape, shift).fill_(float("nan")) for v in vols]
         for r in range(rounds):
             b.compress(dev)
             b.decompress(outs)
@@ -74,6 +83,26 @@ def test_batch_three_levels_and_new_inputs(oracle):
     # same shapes, other data through the same (graph) batch
     vols2 = [np.ascontiguousarray(v[::-1]) for v in vols]
     check_batch(oracle, vols2, steps, 3, graph=True)
+
+
+def test_batch_unaligned_volume_pointers(oracle):
+    """Inputs and outputs 4 bytes past a 16-byte boundary take the scalar
+    row path; results are unchanged."""
+    vols, steps = bricks(6, 2, seed=4242)
+    check_batch(oracle, vols, steps, 2, graph=True, shift=1)
+    check_batch(oracle, vols, steps, 2, graph=False, shift=3)
+
+
+def test_batch_wide_rows(oracle):
+    """Rows wider than one row tile (2048): a full and a partial tile per
+    row, with the vector path (x % 8 == 0) and the scalar one."""
+    rng = np.random.default_rng(99)
+    vols = []
+    for nx in (2200, 2058):
+        v = np.cumsum(rng.standard_normal((8, 8, nx)).astype(np.float32), axis=2) * np.float32(0.05)
+        vols.append(np.ascontiguousarray(v.astype(np.float32)))
+    steps = [0.02 * float(v.std()) for v in vols]
+    check_batch(oracle, vols, steps, 1, graph=False)
 
 
 def test_batch_rejects_bad_sizes():
