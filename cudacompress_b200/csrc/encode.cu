@@ -503,6 +503,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     __syncthreads();
     // 3. tree, depths and sort
     if (inSmem) {
+        if (L >= 2) tb::blockMakeHeap(H, int(L));
         if (threadIdx.x == 0 && L >= 2) tb::buildTree(H, parentS, int(L));
         __syncthreads();
         const u32 root = L >= 2 ? 2 * L - 2 : 0;

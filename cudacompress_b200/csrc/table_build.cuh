@@ -3,9 +3,10 @@
 // 487-596, libstdc++ priority_queue + std::sort) with the work a block can
 // share done by the block.
 //
-//  * tree: the priority-queue merge stays sequential (one thread), on a
-//    shared-memory heap laid out 1-based so that the two children of a node
-//    are one aligned 16-byte load;
+//  * tree: make_heap runs level by level over the block; the merge loop
+//    stays sequential (one thread) on a shared-memory heap laid out 1-based
+//    so that the two children of a node are one aligned 16-byte load, with
+//    the grandchildren loaded speculatively beside them;
 //  * depths: one thread per leaf walks to the root;
 //  * sort: std::sort's introsort is replayed exactly, but every partition
 //    step runs on a warp: the left scan stops at the k-th element not less
@@ -26,65 +27,122 @@ namespace tb {
 // ---------------------------------------------------------------------------
 // Tree (HuffmanTable.cu:507-529).  H[i + 1] holds heap element i, i.e. the
 // heap is 1-based inside H; H must be 16-byte aligned and hold L + 2 entries.
-// Elements: (probability << 32) | node id.  Writes parent[id] for every node
-// except the root.
+// Elements: (probability << 32) | node id; "less(a, b)" is b.prob < a.prob
+// (the top is the smallest probability; ties are not broken by id, so the
+// result depends on the exact libstdc++ heap moves, which are replayed).
+// Writes parent[id] for every node except the root.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ u32 probOf(u64 v) { return u32(v >> 32); }
 
-// libstdc++ __adjust_heap from the root with value v over `len` elements,
-// then __push_heap; "less(a, b)" is b.prob < a.prob.
-__device__ __forceinline__ void siftFromRoot(u64* H, int len, u64 v) {
-    int hole = 0, child = 0;
-    const int lim = (len - 1) / 2;
-    while (child < lim) {
-        child = 2 * (child + 1);                                     // right child (0-based)
-        const ulonglong2 pr = *reinterpret_cast<const ulonglong2*>(H + child);   // elements child-1, child
-        const bool takeLeft = probOf(pr.x) < probOf(pr.y);           // less(right, left)
-        child -= takeLeft ? 1 : 0;
-        H[hole + 1] = takeLeft ? pr.x : pr.y;
-        hole = child;
+// make_heap (libstdc++ __make_heap): __adjust_heap of every parent from
+// (len-2)/2 down to 0.  Parents at one depth have disjoint subtrees and all
+// deeper parents come first in that order, so the parents of one depth are
+// adjusted in parallel, deepest depth first, with the same result.  All
+// threads of the block.
+__device__ void blockMakeHeap(u64* H, int len) {
+    if (len < 2) return;
+    const int lastParent = (len - 2) / 2;
+    for (int d = 31 - __clz(lastParent + 1); d >= 0; --d) {
+        const int first = (1 << d) - 1, last = min(2 * first, lastParent);
+        for (int p = first + int(threadIdx.x); p <= last; p += int(blockDim.x))
+            hb::adjustHeap(H + 1, p, len, H[p + 1], hb::ProbInvLess());
+        __syncthreads();
     }
-    if ((len & 1) == 0 && child == (len - 2) / 2) {
-        child = 2 * (child + 1);
-        H[hole + 1] = H[child];                                      // element child - 1
-        hole = child - 1;
-    }
-    const u32 pv = probOf(v);
-    while (hole > 0) {
-        const int parent = (hole - 1) / 2;
-        const u64 pe = H[parent + 1];
-        if (!(pv < probOf(pe))) break;                               // less(a[parent], v)
-        H[hole + 1] = pe;
-        hole = parent;
-    }
-    H[hole + 1] = v;
 }
 
+__device__ __forceinline__ ulonglong2 ld2(const u64* H, int i) { return *reinterpret_cast<const ulonglong2*>(H + i); }
+
+// pop_heap on H[1..n+1] (libstdc++ __pop_heap: the last element v goes
+// through __adjust_heap(first, 0, n, v) and __push_heap); returns the top.
+// One thread.  The sift-down resolves two levels per step: the children and
+// both grandchild pairs are loaded together (capEven: the largest even index
+// e with H[e + 1] inside the array clamps the speculative loads).  The
+// push-up compares v with the last two values moved up, still in registers.
+__device__ __forceinline__ u64 popTop(u64* H, int n, int capEven) {
+    const u64 top = H[1];
+    if (n <= 0) return top;
+    const u64 v = H[n + 1];
+    const u32 pv = probOf(v);
+    const int lim = (n - 1) / 2;
+    int hole = 0;
+    u64 w1 = 0, w2 = 0;   // values moved into the hole's parent and grandparent
+    while (hole < lim) {
+        const int c = 2 * hole + 2;   // right child; the pair (c-1, c) is H[c], H[c+1]
+        const ulonglong2 pr = ld2(H, c);
+        const ulonglong2 gl = ld2(H, min(2 * c, capEven));
+        const ulonglong2 gr = ld2(H, min(2 * c + 2, capEven));
+        const bool left = probOf(pr.x) < probOf(pr.y);   // less(right, left)
+        const u64 cv = left ? pr.x : pr.y;
+        H[hole + 1] = cv;
+        hole = left ? c - 1 : c;
+        w2 = w1;
+        w1 = cv;
+        if (hole >= lim) break;
+        const ulonglong2 q = left ? gl : gr;
+        const bool left2 = probOf(q.x) < probOf(q.y);
+        const u64 cv2 = left2 ? q.x : q.y;
+        H[hole + 1] = cv2;
+        hole = 2 * hole + (left2 ? 1 : 2);
+        w2 = w1;
+        w1 = cv2;
+    }
+    if ((n & 1) == 0 && hole == (n - 2) / 2) {
+        const u64 cv = H[2 * hole + 2];
+        H[hole + 1] = cv;
+        hole = 2 * hole + 1;
+        w2 = w1;
+        w1 = cv;
+    }
+    if (hole > 0 && pv < probOf(w1)) {
+        H[hole + 1] = w1;
+        hole = (hole - 1) / 2;
+        if (hole > 0 && pv < probOf(w2)) {
+            H[hole + 1] = w2;
+            hole = (hole - 1) / 2;
+            while (hole > 0) {
+                const int parent = (hole - 1) / 2;
+                const u64 pe = H[parent + 1];
+                if (!(pv < probOf(pe))) break;
+                H[hole + 1] = pe;
+                hole = parent;
+            }
+        }
+    }
+    H[hole + 1] = v;
+    return top;
+}
+
+// push_heap of v as element len-1 (__push_heap); three ancestors per step are
+// loaded together.
 __device__ __forceinline__ void pushLast(u64* H, int len, u64 v) {
     int hole = len - 1;
     const u32 pv = probOf(v);
     while (hole > 0) {
-        const int parent = (hole - 1) / 2;
-        const u64 pe = H[parent + 1];
-        if (!(pv < probOf(pe))) break;
-        H[hole + 1] = pe;
-        hole = parent;
+        const int p1 = (hole - 1) / 2, p2 = p1 > 0 ? (p1 - 1) / 2 : 0, p3 = p2 > 0 ? (p2 - 1) / 2 : 0;
+        const u64 e1 = H[p1 + 1], e2 = H[p2 + 1], e3 = H[p3 + 1];
+        if (!(pv < probOf(e1))) break;
+        H[hole + 1] = e1;
+        hole = p1;
+        if (hole == 0 || !(pv < probOf(e2))) break;
+        H[hole + 1] = e2;
+        hole = p2;
+        if (hole == 0 || !(pv < probOf(e3))) break;
+        H[hole + 1] = e3;
+        hole = p3;
     }
     H[hole + 1] = v;
 }
 
-// One thread.  H[1..L] holds the leaves (prob << 32 | leaf index) in symbol
-// order.
+// The merge loop (HuffmanTable.cu:512-529) on a heap made by blockMakeHeap.
+// One thread; H holds L + 2 entries.
 __device__ void buildTree(u64* H, u32* parent, int L) {
-    hb::makeHeap(H + 1, L, hb::ProbInvLess());
+    const int capEven = L & ~1;
     int len = L;
     u32 next = u32(L);
     while (len > 1) {
-        const u64 a = H[1];
-        siftFromRoot(H, len - 1, H[len]);
+        const u64 a = popTop(H, len - 1, capEven);
         --len;
-        const u64 b = H[1];
-        siftFromRoot(H, len - 1, H[len]);
+        const u64 b = popTop(H, len - 1, capEven);
         --len;
         parent[u32(a)] = next;
         parent[u32(b)] = next;
