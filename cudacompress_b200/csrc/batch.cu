@@ -18,8 +18,15 @@
 // brick (forward coefficients, and the reconstructions on the way back),
 // two transform temporaries, the symbols (per brick: lowpass, then the 7
 // bands of each level coarse -> fine, every band 16-byte aligned), the
-// descriptors, and per brick the word offset and bit size of its stream in
-// the batch's output words.
+// descriptors, the bricks' streams, and per brick the word offset and bit
+// size of its stream there.
+//
+// Compress runs as two encodes: the lowpass streams (one Huffman stream per
+// brick; its table is the largest of the brick, and its sequential tree
+// build the longest single step) on a side stream with an instance of its
+// own, concurrently with the highpass streams on the main stream.  After
+// both, every brick's stream is assembled as [lowpass segment][highpass
+// segments] - segments are whole words, so this is a word copy.
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -27,7 +34,12 @@
 #include "batch.cuh"
 
 struct cc_volume_batch {
-    cc_instance* I = nullptr;          // own instance, sized for the batch
+    cc_instance* I = nullptr;          // own instance, sized for the batch (highpass encode, decode)
+    cc_instance* ILP = nullptr;        // own instance of the lowpass encode
+    cudaStream_t sideStream = nullptr; // the lowpass encode's stream
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    ccb::u32* words = nullptr;         // device: the bricks' streams
+    ccb::u64 wordsCap = 0;
     cc_instance* user = nullptr;
     ccb::u32 count = 0, levels = 0;
     std::vector<ccb::u32> nx, ny, nz;
@@ -45,7 +57,6 @@ struct cc_volume_batch {
     float** outTab = nullptr;
     ccb::u64* wordOff = nullptr;
     ccb::u64* bitSize = nullptr;
-    ccb::u32* volFirstStream = nullptr;   // [count + 1]
     // launch lists
     // per volume v: descriptors and CTAs of volumes 0..v (prefix launches)
     struct Rows { const ccb::BRowDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
@@ -54,10 +65,12 @@ struct cc_volume_batch {
     std::vector<Rows> fwdRows, invRows;        // per level
     std::vector<Cols> fwdY, fwdZ, invZ, invY;  // per level
     Quant quant{}, dequantLP{};
-    ccb::EncPlan enc;
+    ccb::EncPlan enc, encLP;           // highpass streams (I), lowpass streams (ILP)
     ccb::DecPlan dec;
     // per volume v: encoder / decoder counts of volumes 0..v
     std::vector<ccb::u32> encS, encT, encTiles, encBlocks;
+    std::vector<ccb::u32> lpTiles, lpBlocks;
+    std::vector<ccb::u32> decS;
     std::vector<ccb::u32> decT, decRl, decH, decRlBlocks, decHBlocks;
     std::vector<ccb::u64> symEnd;       // symbols of volumes 0..v
     ccb::u32 active = 0;                // volumes a call processes (the first `active`)
@@ -148,6 +161,51 @@ SymLayout symLayout(u32 nx, u32 ny, u32 nz, u32 L) {
 
 }  // namespace
 
+// Per brick: words of its lowpass segment plus its highpass segments, and
+// the exclusive scan of those totals (its offset in the stream words).
+__global__ void __launch_bounds__(1024) k_brickOffsets(const SegmentLayout* lp, const SegmentLayout* hp, u32 hpPer,
+                                                       u32 count, u64* wordOff, u64* bitSize, const u32* errLP,
+                                                       const u32* errHP) {
+    __shared__ u32 scratch[40];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const bool failed = *errLP != 0 || *errHP != 0;
+    for (u32 base = 0; base < count; base += 1024) {
+        const u32 v = base + threadIdx.x;
+        u32 words = 0;
+        if (v < count && !failed) {
+            const SegmentLayout& f = hp[u64(v) * hpPer];
+            const SegmentLayout& l = hp[u64(v) * hpPer + hpPer - 1];
+            words = lp[v].words + u32(l.startWord + l.words - f.startWord);
+        }
+        u32 tot;
+        const u32 ex = blockExclusiveSum<1024>(words, scratch, &tot);
+        if (v < count) {
+            wordOff[v] = carry + ex;
+            bitSize[v] = u64(words) * 32ull;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+}
+
+// Brick v's stream: its lowpass words, then its highpass words; `parts` CTAs
+// per brick.
+__global__ void __launch_bounds__(256) k_brickConcat(const u32* lpOut, const u32* hpOut, const SegmentLayout* lp,
+                                                     const SegmentLayout* hp, u32 hpPer, u32 parts, const u64* wordOff,
+                                                     const u64* bitSize, u32* dst) {
+    const u32 v = blockIdx.x / parts, part = blockIdx.x - v * parts;
+    const u64 total = bitSize[v] / 32u;
+    if (total == 0) return;
+    const u64 lpW = lp[v].words, lpS = lp[v].startWord, hpS = hp[u64(v) * hpPer].startWord;
+    const u64 chunk = (total + parts - 1) / parts;
+    const u64 w0 = u64(part) * chunk, w1 = min(total, w0 + chunk);
+    u32* out = dst + wordOff[v];
+    for (u64 w = w0 + threadIdx.x; w < w1; w += blockDim.x) out[w] = w < lpW ? lpOut[lpS + w] : hpOut[hpS + (w - lpW)];
+}
+
 template <class List>
 static void prefixOf(const List& li, u32 k, u32& nd, u32& ctas) {
     nd = li.descEnd[k - 1];
@@ -170,14 +228,42 @@ static int batchEnqueueCompress(cc_volume_batch* b) {
     }
     prefixOf(b->quant, k, nd, ctas);
     { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, b->quant.map, ctas, false, st); }
+    // fork: the lowpass streams on the side stream
+    cc_instance* ILP = b->ILP;
+    ILP->stream = b->sideStream;
+    CC_TRY_CUDA(cudaEventRecord(b->evFork, st), "fork");
+    CC_TRY_CUDA(cudaStreamWaitEvent(b->sideStream, b->evFork, 0), "fork");
+    EncPlan lp = b->encLP;
+    lp.S = k;
+    lp.T = k;
+    lp.tiles = b->lpTiles[k - 1];
+    lp.blocks = b->lpBlocks[k - 1];
+    int rc;
+    {
+        SectionTimer t(I, "batch.lowpass_encode", b->sideStream);
+        rc = encodeLaunch(ILP, lp, ILP->out, ILP->outWordsMax);
+    }
+    if (rc) return rc;
+    CC_TRY_CUDA(cudaEventRecord(b->evJoin, b->sideStream), "join");
+    // the highpass streams here
     EncPlan ep = b->enc;
     ep.S = b->encS[k - 1];
     ep.T = b->encT[k - 1];
     ep.tiles = b->encTiles[k - 1];
     ep.blocks = b->encBlocks[k - 1];
-    int rc = encodeLaunch(I, ep, I->out, I->outWordsMax);
+    rc = encodeLaunch(I, ep, I->out, I->outWordsMax);
     if (rc) return rc;
-    volumeExtents(I, b->volFirstStream, k, b->wordOff, b->bitSize, st);
+    CC_TRY_CUDA(cudaStreamWaitEvent(st, b->evJoin, 0), "join");
+    {
+        SectionTimer t(I, "batch.assemble", st);
+        const u32 hpPer = 7 * b->levels;
+        k_brickOffsets<<<1, 1024, 0, st>>>(ILP->layout, I->layout, hpPer, k, b->wordOff, b->bitSize, ILP->errors,
+                                           I->errors);
+        const u32 parts = std::max<u32>(1, std::min<u32>(64, u32(ceilDiv(4 * 148, k))));
+        k_brickConcat<<<k * parts, 256, 0, st>>>(ILP->out, I->out, ILP->layout, I->layout, hpPer, parts, b->wordOff,
+                                                 b->bitSize, b->words);
+        countLaunch(2);
+    }
     CC_TRY_CUDA(cudaGetLastError(), "batch compress");
     return CC_OK;
 }
@@ -189,7 +275,7 @@ static int batchEnqueueDecompress(cc_volume_batch* b) {
     u32 nd, ctas;
     CC_TRY_CUDA(cudaMemsetAsync(b->syms, 0, b->symEnd[k - 1] * sizeof(u16), st), "zero symbols");
     DecPlan dp = b->dec;
-    dp.S = b->encS[k - 1];
+    dp.S = b->decS[k - 1];
     dp.T = b->decT[k - 1];
     dp.B = k;
     dp.nRl = b->decRl[k - 1];
@@ -279,8 +365,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     }
     if (user->symBytes != 2) { setError("cc_volume_batch_create: needs a 16-bit-symbol instance (log2 symbol count <= 16)"); return CC_ERR_INVALID_ARGUMENT; }
     const u32 L = levels, f = 1u << L;
-    u64 N0sum = 0, histBins = 0;
-    u32 maxStream = 1;
+    u64 N0sum = 0, histBins = 0, LPsum = 0;
+    u32 maxStream = 1, maxLP = 1;
     for (u32 v = 0; v < count; ++v) {
         const u32 x = sizes[3 * v], y = sizes[3 * v + 1], z = sizes[3 * v + 2];
         if (x % f || y % f || z % f || (x >> (L - 1)) < 8 || (y >> (L - 1)) < 8 || (z >> (L - 1)) < 8) {
@@ -294,7 +380,9 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             return CC_ERR_INVALID_ARGUMENT;
         }
         N0sum += vol3(x, y, z);
+        LPsum += vol3(x >> L, y >> L, z >> L);
         maxStream = std::max<u32>(maxStream, u32(vol3(x >> 1, y >> 1, z >> 1)));
+        maxLP = std::max<u32>(maxLP, u32(vol3(x >> L, y >> L, z >> L)));
     }
     const u32 S = count * (1 + 7 * L);
     // histogram bins: every table at most 2^log2Max; budget 2^26 bins (the
@@ -318,9 +406,20 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     cc_instance* I = b->I;
     I->stream = user->stream;
     I->timing = user->timing;
+    // the lowpass encode's instance: one stream, one table per brick
+    InstanceCaps capsLP{count, std::max<u64>(LPsum, 1), std::min<u64>(u64(2 * count) * user->bins, u64(1) << 26)};
+    rc = createInstance(&b->ILP, user->device, count, maxLP, user->codingBlockSize, user->log2Max, &capsLP);
+    if (rc) { cc_volume_batch_destroy(b); return rc; }
+    b->ILP->timing = false;
     // kernel attributes set once here, so that captured launches do not set them
     rc = prepareKernelAttributes(I);
-    if (rc) { cc_destroy_instance(I); delete b; return rc; }
+    if (!rc) rc = prepareKernelAttributes(b->ILP);
+    if (rc) { cc_volume_batch_destroy(b); return rc; }
+    cudaError_t ce = cudaStreamCreateWithFlags(&b->sideStream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming);
+    if (ce != cudaSuccess) { cc_volume_batch_destroy(b); return cudaFail(ce, "volume batch streams"); }
+    b->wordsCap = I->outWordsMax + b->ILP->outWordsMax;
 
     // ---- layout of the work areas ----
     // Descriptors hold offsets until the allocation exists, and a null
@@ -352,7 +451,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     const size_t symAt = A.take((symTot + 64) * sizeof(u16));
     const size_t inTabAt = A.take(sizeof(void*) * count), outTabAt = A.take(sizeof(void*) * count);
     const size_t wordOffAt = A.take(sizeof(u64) * count), bitSizeAt = A.take(sizeof(u64) * count);
-    const size_t firstAt = A.take(sizeof(u32) * (count + 1));
+    const size_t wordsAt = A.take(b->wordsCap * sizeof(u32));
 
     // ---- descriptors (host) ----
     auto lev = [&](u32 l, u32 v) { return reinterpret_cast<float*>(levAt[l]) + levOff[l][v]; };   // offsets, rebased below
@@ -494,16 +593,29 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
         iyMap[l] = addMap(ctaMapOf(iy[l], iyC[l]));
     }
     const size_t qMap = addMap(ctaMapOf(qd, qC)), dqMap = addMap(ctaMapOf(dq, dqC));
+    // the encodes' streams: the lowpass streams, and the highpass streams with
+    // their group indices rebased to the highpass list
+    std::vector<EncStream> esLP, esHP;
+    for (u32 v = 0; v < count; ++v) {
+        esLP.push_back(es[firstStream[v]]);
+        for (u32 t = firstStream[v] + 1; t < firstStream[v + 1]; ++t) {
+            EncStream e = es[t];
+            e.groupFirst -= v + 1;
+            esHP.push_back(e);
+        }
+    }
     // encoder / decoder descriptors: sized by preparing into a host buffer
-    const size_t planMax = size_t(I->hostRingBytes);
-    std::vector<char> encHost(planMax), decHost(planMax);
-    rc = encodePrepare(I, es.data(), u32(es.size()), encHost.data(), planMax, b->enc);
+    const size_t planMax = size_t(I->hostRingBytes), planLPMax = size_t(b->ILP->hostRingBytes);
+    std::vector<char> encHost(planMax), encLPHost(planLPMax), decHost(planMax);
+    rc = encodePrepare(I, esHP.data(), u32(esHP.size()), encHost.data(), planMax, b->enc);
+    if (!rc) rc = encodePrepare(b->ILP, esLP.data(), u32(esLP.size()), encLPHost.data(), planLPMax, b->encLP);
     if (!rc) rc = decodePrepare(I, ds.data(), u32(ds.size()), dsrc.data(), count, decHost.data(), planMax, b->dec);
-    if (rc) { cc_destroy_instance(I); delete b; return rc; }
-    const size_t encAt = A.take(b->enc.bytes, 256), decAt = A.take(b->dec.bytes, 256);
+    if (rc) { cc_volume_batch_destroy(b); return rc; }
+    const size_t encAt = A.take(b->enc.bytes, 256), encLPAt = A.take(b->encLP.bytes, 256);
+    const size_t decAt = A.take(b->dec.bytes, 256);
     b->memBytes = alignUp(A.off, 256);
     cudaError_t e = cudaMalloc(&b->mem, b->memBytes);
-    if (e != cudaSuccess) { cc_destroy_instance(I); delete b; return cudaFail(e, "cudaMalloc(volume batch)"); }
+    if (e != cudaSuccess) { b->mem = nullptr; cc_volume_batch_destroy(b); return cudaFail(e, "cudaMalloc(volume batch)"); }
     char* base = b->mem;
     // rebase the device pointers written as offsets
     auto rebaseF = [&](const float* p) -> float* { return p ? reinterpret_cast<float*>(base + reinterpret_cast<uintptr_t>(p)) : nullptr; };
@@ -520,6 +632,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     {
         EncStreamDev* sdv = reinterpret_cast<EncStreamDev*>(encHost.data());
         for (u32 s = 0; s < b->enc.S; ++s) sdv[s].in = base + reinterpret_cast<uintptr_t>(sdv[s].in);
+        EncStreamDev* ldv = reinterpret_cast<EncStreamDev*>(encLPHost.data());
+        for (u32 s = 0; s < b->encLP.S; ++s) ldv[s].in = base + reinterpret_cast<uintptr_t>(ldv[s].in);
         DecStreamDesc* ddv = reinterpret_cast<DecStreamDesc*>(decHost.data());
         for (u32 s = 0; s < b->dec.S; ++s) ddv[s].out = base + reinterpret_cast<uintptr_t>(ddv[s].out);
     }
@@ -529,10 +643,11 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     b->outTab = reinterpret_cast<float**>(base + outTabAt);
     b->wordOff = reinterpret_cast<u64*>(base + wordOffAt);
     b->bitSize = reinterpret_cast<u64*>(base + bitSizeAt);
-    b->volFirstStream = reinterpret_cast<u32*>(base + firstAt);
+    b->words = reinterpret_cast<u32*>(base + wordsAt);
     b->enc.dev = base + encAt;
+    b->encLP.dev = base + encLPAt;
     b->dec.dev = base + decAt;
-    b->dec.wordsBase = I->out;
+    b->dec.wordsBase = b->words;
     b->dec.wordOff = b->wordOff;
     b->dec.bitSize = b->bitSize;
     // upload everything once
@@ -552,8 +667,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     if (e == cudaSuccess) e = up(qAt, qd.data(), qd.size() * sizeof(BQuantDesc));
     if (e == cudaSuccess) e = up(dqAt, dq.data(), dq.size() * sizeof(BQuantDesc));
     if (e == cudaSuccess) e = up(encAt, encHost.data(), b->enc.bytes);
+    if (e == cudaSuccess) e = up(encLPAt, encLPHost.data(), b->encLP.bytes);
     if (e == cudaSuccess) e = up(decAt, decHost.data(), b->dec.bytes);
-    if (e == cudaSuccess) e = up(firstAt, firstStream.data(), sizeof(u32) * (count + 1));
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&b->hostPlan), sizeof(void*) * count, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->tabEvent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&b->hostExt), 2 * sizeof(u64) * count, cudaHostAllocDefault);
@@ -595,19 +710,28 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     {
         const u32 cb = I->codingBlockSize;
         u32 S = 0, T = 0, tiles = 0, blocks = 0, nRl = 0, nH = 0, rlB = 0, hB = 0;
+        u32 hS = 0, hT = 0, hTiles = 0, hBlocks = 0, lTiles = 0, lBlocks = 0;
         for (u32 v = 0; v < count; ++v) {
             for (u32 st = firstStream[v]; st < firstStream[v + 1]; ++st) {
                 const EncStream& e = es[st];
-                const u32 nb = u32(ceilDiv(e.n, cb));
+                const u32 nb = u32(ceilDiv(e.n, cb)), nt = u32(ceilDiv(e.n, kRleTile));
                 ++S;
-                tiles += u32(ceilDiv(e.n, kRleTile));
-                if (e.kind == KIND_RLHUFF) { T += 2; blocks += 2 * nb; ++nRl; rlB += nb; }
-                else { T += 1; blocks += nb; ++nH; hB += nb; }
+                tiles += nt;
+                if (e.kind == KIND_RLHUFF) {
+                    T += 2; blocks += 2 * nb; ++nRl; rlB += nb;
+                    ++hS; hT += 2; hTiles += nt; hBlocks += 2 * nb;
+                } else {
+                    T += 1; blocks += nb; ++nH; hB += nb;
+                    lTiles += nt; lBlocks += nb;
+                }
             }
-            b->encS.push_back(S);
-            b->encT.push_back(T);
-            b->encTiles.push_back(tiles);
-            b->encBlocks.push_back(blocks);
+            b->encS.push_back(hS);
+            b->encT.push_back(hT);
+            b->encTiles.push_back(hTiles);
+            b->encBlocks.push_back(hBlocks);
+            b->lpTiles.push_back(lTiles);
+            b->lpBlocks.push_back(lBlocks);
+            b->decS.push_back(S);
             b->decT.push_back(T);
             b->decRl.push_back(nRl);
             b->decH.push_back(nH);
@@ -628,11 +752,15 @@ void cc_volume_batch_destroy(cc_volume_batch* b) {
     for (auto& kv : b->gCompress) cudaGraphExecDestroy(kv.second);
     for (auto& kv : b->gDecompress) cudaGraphExecDestroy(kv.second);
     if (b->captureStream) cudaStreamDestroy(b->captureStream);
+    if (b->sideStream) cudaStreamDestroy(b->sideStream);
+    if (b->evFork) cudaEventDestroy(b->evFork);
+    if (b->evJoin) cudaEventDestroy(b->evJoin);
     if (b->tabEvent) cudaEventDestroy(b->tabEvent);
     if (b->hostPlan) cudaFreeHost(b->hostPlan);
     if (b->hostExt) cudaFreeHost(b->hostExt);
     if (b->extEvent) cudaEventDestroy(b->extEvent);
     if (b->mem) cudaFree(b->mem);
+    if (b->ILP) cc_destroy_instance(b->ILP);
     if (b->I) cc_destroy_instance(b->I);
     delete b;
 }
@@ -679,10 +807,10 @@ int cc_volume_batch_decompress(cc_volume_batch* b, float* const* dVolumes) {
 int cc_volume_batch_stream(const cc_volume_batch* b, const uint32_t** dWords, const uint64_t** dWordOffsets,
                            const uint64_t** dBitSizes, uint64_t* capacityWords) {
     if (!b) { setError("cc_volume_batch_stream: null batch"); return CC_ERR_INVALID_ARGUMENT; }
-    if (dWords) *dWords = b->I->out;
+    if (dWords) *dWords = b->words;
     if (dWordOffsets) *dWordOffsets = b->wordOff;
     if (dBitSizes) *dBitSizes = b->bitSize;
-    if (capacityWords) *capacityWords = b->I->outWordsMax;
+    if (capacityWords) *capacityWords = b->wordsCap;
     return CC_OK;
 }
 
@@ -698,7 +826,7 @@ int cc_volume_batch_read_stream(cc_volume_batch* b, uint32_t v, uint32_t* dst, u
     const u64 words = ceilDiv(ext[1], 32);
     if (!dst) return CC_OK;
     if (words > capacityWords) { setError("cc_volume_batch_read_stream: need %llu words", (unsigned long long)words); return CC_ERR_CAPACITY; }
-    CC_TRY_CUDA(cudaMemcpy(dst, b->I->out + ext[0], words * 4, cudaMemcpyDefault), "copy stream");
+    CC_TRY_CUDA(cudaMemcpy(dst, b->words + ext[0], words * 4, cudaMemcpyDefault), "copy stream");
     return CC_OK;
 }
 
@@ -711,10 +839,10 @@ int cc_volume_batch_load_streams(cc_volume_batch* b, const uint32_t* const* word
     u64 at = 0;
     for (u32 v = 0; v < b->active; ++v) {
         const u64 nw = ceilDiv(bitSizes[v], 32);
-        if (at + nw > b->I->outWordsMax) { setError("cc_volume_batch_load_streams: streams exceed the batch buffer (%llu words)", (unsigned long long)b->I->outWordsMax); return CC_ERR_CAPACITY; }
+        if (at + nw > b->wordsCap) { setError("cc_volume_batch_load_streams: streams exceed the batch buffer (%llu words)", (unsigned long long)b->wordsCap); return CC_ERR_CAPACITY; }
         b->hostExt[v] = at;
         b->hostExt[b->active + v] = bitSizes[v];
-        if (nw) CC_TRY_CUDA(cudaMemcpyAsync(b->I->out + at, words[v], nw * 4, cudaMemcpyDefault, st), "load stream");
+        if (nw) CC_TRY_CUDA(cudaMemcpyAsync(b->words + at, words[v], nw * 4, cudaMemcpyDefault, st), "load stream");
         at += nw;
     }
     CC_TRY_CUDA(cudaMemcpyAsync(b->wordOff, b->hostExt, sizeof(u64) * b->active, cudaMemcpyHostToDevice, st), "load offsets");
@@ -725,9 +853,11 @@ int cc_volume_batch_load_streams(cc_volume_batch* b, const uint32_t* const* word
 
 int cc_volume_batch_status(cc_volume_batch* b) {
     if (!b) return CC_ERR_INVALID_ARGUMENT;
-    u32 flags[8] = {};
+    u32 flags[8] = {}, lp = 0;
     CC_TRY_CUDA(cudaMemcpyAsync(flags, b->I->errors, sizeof(flags), cudaMemcpyDeviceToHost, b->I->stream), "batch status");
+    CC_TRY_CUDA(cudaMemcpyAsync(&lp, b->ILP->errors, sizeof(lp), cudaMemcpyDeviceToHost, b->I->stream), "batch status");
     CC_TRY_CUDA(cudaStreamSynchronize(b->I->stream), "batch status");
+    if (lp) return deviceErrorStatus(lp, "batch compress (lowpass streams)");
     if (flags[0]) return deviceErrorStatus(flags[0], "batch compress");
     return deviceErrorStatus(flags[4], "batch decompress");
 }
