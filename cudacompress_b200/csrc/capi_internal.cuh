@@ -108,7 +108,16 @@ int decodeLaunch(cc_instance* I, const DecPlan& plan);
 // Per-device cache of the dynamic shared memory limits set on kernels (so
 // that repeated launches, and launches recorded in a stream capture, do not
 // set them again): returns cudaSuccess once the kernel allows `bytes`.
-enum SmemAttrKernel { kAttrTableBuild = 0, kAttrDecHuff16 = 1, kAttrDecHuff32 = 2, kAttrCount = 3 };
+enum SmemAttrKernel {
+    kAttrTableBuild = 0,
+    kAttrDecHuff16,
+    kAttrDecHuff32,
+    kAttrDecZc16,
+    kAttrDecZc32,
+    kAttrDecSc16,
+    kAttrDecSc32,
+    kAttrCount
+};
 cudaError_t ensureSmemAttribute(const void* kernel, int which, int device, size_t bytes);
 // Sets the largest shared memory the encoder and decoder kernels may ask for
 // on the instance's device.

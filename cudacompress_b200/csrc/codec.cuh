@@ -234,6 +234,7 @@ struct cc_instance {
     ccb::u32* stagedWords = nullptr;          // decode input words (host bit streams)
     ccb::u64 stagedWordsMax = 0;
     ccb::u32* blockSum = nullptr;             // [capBlocks]
+    ccb::u64* decRlTasks = nullptr;           // [capBlocks / 32 + capStreams + 1]: run-length decode warp tasks, then their count
 
     // host staging: ring of slots for uploads, one buffer for downloads
     static constexpr int kRing = 8;

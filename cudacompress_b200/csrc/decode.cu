@@ -17,6 +17,7 @@
 // Every read of the bit stream is bounds-checked, and malformed tables or
 // codes raise CC_ERR_CORRUPT_STREAM instead of reading or writing out of
 // bounds.
+#include <algorithm>
 #include <cstring>
 
 #include "capi_internal.cuh"
@@ -27,6 +28,7 @@ struct DecParams {
     u32 S, T, nSrc, nRl, nH;
     u32 rlBlocks, hBlocks;     // coding blocks (upper bounds) of the RLHuff / Huff streams
     u32 cb, log2Max, symBytes, leavesMax;
+    u32 stageWords;            // run-length decode: staged code words per warp
     u64 capLeaves;
     DecStreamDesc* streams;
     DecTableDesc* tables;
@@ -41,6 +43,8 @@ struct DecParams {
     u32* lut;                  // [T][1 << kLutBits]
     u32* blockOff;             // coding-block bit offsets, by table blockOff
     u32* blockSum;             // RLHuff: per zero-count block output lengths
+    u64* rlTasks;              // RLHuff decode warp tasks (stream << 32 | first block); count at rlTasks[rlTaskCap]
+    u32 rlTaskCap;
     char* zc;                  // decoded zero counts, by stream zcOff
     u32* errors;
 };
@@ -56,6 +60,18 @@ struct WordSrc {
         const u32 b = u32(bit & 31u);
         const u64 window = (u64(at(wi)) << 32) | at(wi + 1);
         return u32((window << b) >> (64 - count));
+    }
+};
+
+// Code words of a warp's coding blocks staged in shared memory; indices
+// outside the staged range read 0 like WordSrc past its end.
+struct StagedWords {
+    const u32* w;
+    u64 base;
+    u32 n;
+    __device__ __forceinline__ u32 at(u64 i) const {
+        const u64 k = i - base;
+        return k < n ? w[k] : 0u;
     }
 };
 
@@ -259,13 +275,18 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
         u32 v = ws.bits(symBit + u64(i) * d.symbolBits, d.symbolBits);
         syms[i] = p.symBytes == 2 ? (v & 0xFFFFu) : v;
     }
-    // lookup table: first length l <= kLutBits whose prefix fits the canonical range
+    // lookup table: first length l <= kLutBits whose prefix fits the canonical
+    // range; the entry holds (l << 24) | the symbol's value for 16-bit
+    // symbols, | its index otherwise
+    const bool valueLut = p.symBytes == 2;
+    if (valueLut) __syncthreads();   // syms[] of this table written above
     for (u32 e = threadIdx.x; e < (1u << kLutBits); e += kDecThreads) {
         u32 entry = 0;
         for (u32 l = 1; l <= kLutBits; ++l) {
             int pref = int(e >> (kLutBits - l));
             if (sMax[l - 1] >= 0 && pref <= sMax[l - 1]) {
-                entry = (l << 24) | u32(sFirst[l - 1] + pref - sMin[l - 1]);
+                const u32 idx = u32(sFirst[l - 1] + pref - sMin[l - 1]);
+                entry = (l << 24) | (valueLut ? syms[idx] : idx);
                 break;
             }
         }
@@ -307,9 +328,11 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
 }
 
 // Decodes up to `cnt` symbols of one coding block starting at absolute bit
-// `bit`, calling emit(i, symbol).
-template <class Emit>
-__device__ __forceinline__ void decodeBlock(const WordSrc& ws, const DecTable& D, const u32* syms, const u32* lut,
+// `bit`, calling emit(i, symbol).  kValueLut: lookup entries hold symbol
+// values (16-bit symbols), else symbol indices.  The 64-bit window is two
+// words, read with a funnel shift.
+template <bool kValueLut, class Src, class Emit>
+__device__ __forceinline__ void decodeBlock(const Src& ws, const DecTable& D, const u32* syms, const u32* lut,
                                             u64 bit, u32 cnt, bool& corrupt, Emit emit) {
     const u32 nSym = D.nSym;
     if (nSym == 0xFFFFFFFFu) { corrupt = true; return; }
@@ -320,26 +343,32 @@ __device__ __forceinline__ void decodeBlock(const WordSrc& ws, const DecTable& D
     }
     u64 w = bit >> 5;
     u32 bpos = u32(bit & 31u);
-    u64 cache = (u64(ws.at(w)) << 32) | ws.at(w + 1);
+    u32 hi = ws.at(w), lo = ws.at(w + 1);
     w += 2;
     for (u32 i = 0; i < cnt; ++i) {
-        const u32 v = u32((cache << bpos) >> 32);
+        const u32 v = __funnelshift_l(lo, hi, bpos);
         const u32 e = lut[v >> (32 - kLutBits)];
-        u32 len, idx;
+        u32 len, val;
         if (e) {
             len = e >> 24;
-            idx = e & 0xFFFFFFu;
+            val = e & 0xFFFFFFu;
+            if (!kValueLut) {
+                if (val >= nSym) { corrupt = true; return; }
+                val = syms[val];
+            }
         } else {
             len = kLutBits + 1;
             while (len <= 31 && int(v >> (32 - len)) > D.maxCode[len - 1]) ++len;
             if (len > 31) { corrupt = true; return; }
-            idx = u32(D.firstIndex[len - 1] + int(v >> (32 - len)) - D.minCode[len - 1]);
+            const u32 idx = u32(D.firstIndex[len - 1] + int(v >> (32 - len)) - D.minCode[len - 1]);
+            if (idx >= nSym) { corrupt = true; return; }
+            val = syms[idx];
         }
-        if (idx >= nSym) { corrupt = true; return; }
-        emit(i, syms[idx]);
+        emit(i, val);
         bpos += len;
         if (bpos >= 32) {
-            cache = (cache << 32) | ws.at(w);
+            hi = lo;
+            lo = ws.at(w);
             ++w;
             bpos -= 32;
         }
@@ -375,10 +404,10 @@ __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
         const u32 cnt = min(p.cb, sd.n - i0);
         const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
         if (uniform)
-            decodeBlock(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+            decodeBlock<sizeof(Sym) == 2>(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
                         [&](u32 i, u32 v) { rows[lane * rowPitch + i] = Sym(v); });
         else
-            decodeBlock(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+            decodeBlock<sizeof(Sym) == 2>(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
                         [&](u32 i, u32 v) { out[i0 + i] = Sym(v); });
     }
     if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
@@ -394,27 +423,190 @@ __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
     for (u64 k = lane; k < total; k += 32) out[base + k] = rows[(k / p.cb) * rowPitch + (k % p.cb)];
 }
 
-// decodeRLHuff, zero counts: decode and store them, and sum (zc + 1) per block.
+// Copies n words from ws (from word lo) to shared memory, eight loads in
+// flight per lane.
+__device__ __forceinline__ void stageWordsIn(u32* dst, const WordSrc& ws, u64 lo, u32 n, u32 lane) {
+    for (u32 base = 0; base < n; base += 256) {
+        u32 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const u32 k = base + lane + 32u * i;
+            v[i] = k < n ? ws.at(lo + k) : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const u32 k = base + lane + 32u * i;
+            if (k < n) dst[k] = v[i];
+        }
+    }
+}
+
+// Copies n elements of type Sym to shared memory (16-byte vectors when src
+// is 16-byte aligned), eight loads in flight per lane.
 template <class Sym>
-__global__ void __launch_bounds__(128) k_decZc(DecParams p) {
-    const u32 gb = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gb >= p.rlBlocks || capacityFailed(p)) return;
-    const u32 s = streamOfBlock(p, p.rlList, p.nRl, gb);
+__device__ __forceinline__ void stageSymsIn(Sym* dst, const Sym* src, u32 n, u32 lane) {
+    constexpr u32 kPer = 16 / sizeof(Sym);
+    u32 done = 0;
+    if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+        const u32 nv = n / kPer;
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        for (u32 base = 0; base < nv; base += 256) {
+            uint4 v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const u32 k = base + lane + 32u * i;
+                if (k < nv) v[i] = s4[k];
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const u32 k = base + lane + 32u * i;
+                if (k < nv) d4[k] = v[i];
+            }
+        }
+        done = nv * kPer;
+    }
+    for (u32 base = done; base < n; base += 256) {
+        Sym v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const u32 k = base + lane + 32u * i;
+            if (k < n) v[i] = src[k];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const u32 k = base + lane + 32u * i;
+            if (k < n) dst[k] = v[i];
+        }
+    }
+}
+
+// Coding blocks of RLHuff stream s that a decode covers: its run-length
+// symbol count in blocks, within the blocks planned for its length.
+__device__ __forceinline__ u32 rlBlocksOf(const DecParams& p, const DecStreamDesc& sd) {
+    return u32(min(ceilDiv(u64(sd.m), p.cb), ceilDiv(u64(sd.n), p.cb)));
+}
+
+// Warp tasks of the run-length decode, once the headers are walked: every
+// RLHuff stream's coding blocks in groups of 32, so that a warp's blocks
+// belong to one stream and warps without blocks are not started.
+__global__ void __launch_bounds__(1024) k_decRlTasks(DecParams p) {
+    __shared__ u32 scratch[40];
+    __shared__ u32 carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (u32 base = 0; base < p.nRl; base += 1024) {
+        const u32 k = base + threadIdx.x;
+        u32 s = 0, warps = 0;
+        if (k < p.nRl) {
+            s = p.rlList[k];
+            warps = u32(ceilDiv(rlBlocksOf(p, p.streams[s]), 32));
+        }
+        u32 tot;
+        const u32 ex = blockExclusiveSum<1024>(warps, scratch, &tot);
+        for (u32 i = 0; i < warps; ++i)
+            if (carry + ex + i < p.rlTaskCap) p.rlTasks[carry + ex + i] = (u64(s) << 32) | (32u * i);
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) reinterpret_cast<u32*>(p.rlTasks + p.rlTaskCap)[0] = min(carry, p.rlTaskCap);
+}
+
+// decodeRLHuff (RunLengthKernels.cui:56-66 for the scatter): one lane per
+// coding block, 32 consecutive blocks of one stream per warp (k_decRlTasks).
+// Zero counts (kSymbols false): decode, store, and sum (zc + 1) per block.
+// Symbols: decode and scatter out[scan(zc) + i] = symbol.  The blocks' code
+// words are staged in shared memory with coalesced loads, the decoded values go to
+// shared rows, zero counts are written out row by row, and the scatter runs
+// block by block on the blocks' zero counts (staged over the code words
+// once decoded): every lane takes cb/32 consecutive elements and a warp scan
+// of their (zc + 1) sums gives the positions.
+template <class Sym, bool kSymbols>
+__global__ void __launch_bounds__(128) k_decRl(DecParams p) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const u32 rowPitch = p.cb + (sizeof(Sym) == 2 ? 2 : 1);
+    const u32 warpBytes = p.stageWords * 4u + u32(alignUp(u64(32) * rowPitch * sizeof(Sym), 16));
+    u32* words = reinterpret_cast<u32*>(dyn + warp * warpBytes);
+    Sym* rows = reinterpret_cast<Sym*>(dyn + warp * warpBytes + p.stageWords * 4u);
+    if (__any_sync(0xffffffffu, capacityFailed(p))) return;
+    const u32 wt = blockIdx.x * 4u + warp;
+    if (wt >= reinterpret_cast<const u32*>(p.rlTasks + p.rlTaskCap)[0]) return;
+    const u64 task = p.rlTasks[wt];
+    const u32 s = u32(task >> 32), bFirst = u32(task);
     const DecStreamDesc sd = p.streams[s];
-    const u32 b = gb - sd.blockFirst;
-    if (b >= u32(ceilDiv(sd.m, p.cb))) return;
-    const u32 t = sd.tableFirst + 1;
+    const u32 b = bFirst + lane;
+    const u32 blocks = rlBlocksOf(p, sd);
+    const bool mine = b < blocks;
+    const u32 t = sd.tableFirst + (kSymbols ? 0u : 1u);
     const DecTableDesc& td = p.tables[t];
-    const u32 i0 = b * p.cb;
-    const u32 cnt = min(p.cb, sd.m - i0);
-    const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
-    Sym* zc = reinterpret_cast<Sym*>(p.zc) + sd.zcOff + i0;
-    u32 sum = 0;
+    const WordSrc ws = srcOf(p, s);
+    const u32* lut = p.lut + (u64(t) << kLutBits);
+    const u32* symv = p.syms + td.symOff;
+    const u32 cnt = mine ? min(p.cb, sd.m - b * p.cb) : 0u;
+    const u64 bit = mine ? td.cwWord * 32ull + p.blockOff[td.blockOff + b] : 0ull;
     bool corrupt = false;
-    decodeBlock(srcOf(p, s), p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
-                [&](u32 i, u32 v) { zc[i] = Sym(v); sum += v + 1; });
+    u32 sum = 0;
+    const u32 nMine = __popc(__ballot_sync(0xffffffffu, mine));   // lanes 0 .. nMine-1
+    if (nMine == 0) return;
+    const u64 cw0 = td.cwWord * 32ull;
+    const u64 startBit = cw0 + p.blockOff[td.blockOff + bFirst];
+    const u64 endBit = cw0 + (bFirst + nMine < blocks ? p.blockOff[td.blockOff + bFirst + nMine] : td.cwBits);
+    const u64 wLo = startBit >> 5, wHi = ((endBit + 31) >> 5) + 2;
+    const bool staged = endBit >= startBit && wHi - wLo <= p.stageWords;
+    if (staged) stageWordsIn(words, ws, wLo, u32(wHi - wLo), lane);
+    __syncwarp();
+    if (mine) {
+        auto emit = [&](u32 i, u32 v) {
+            rows[lane * rowPitch + i] = Sym(v);
+            if (!kSymbols) sum += v + 1;
+        };
+        if (staged) decodeBlock<sizeof(Sym) == 2>(StagedWords{words, wLo, u32(wHi - wLo)}, p.dec[t], symv, lut, bit, cnt, corrupt, emit);
+        else decodeBlock<sizeof(Sym) == 2>(ws, p.dec[t], symv, lut, bit, cnt, corrupt, emit);
+    }
+    __syncwarp();
+    if (!kSymbols) {
+        if (mine) p.blockSum[td.blockOff + b] = sum;
+        Sym* zc = reinterpret_cast<Sym*>(p.zc) + sd.zcOff;
+        for (u32 j = 0; j < nMine; ++j) {
+            const u32 c = min(p.cb, sd.m - (bFirst + j) * p.cb);
+            for (u32 k = lane; k < c; k += 32) zc[u64(bFirst + j) * p.cb + k] = rows[j * rowPitch + k];
+        }
+    } else {
+        // the blocks' zero counts, over the code words
+        Sym* zs = reinterpret_cast<Sym*>(words);
+        const u32 zn = min(nMine * p.cb, sd.m - bFirst * p.cb);
+        stageSymsIn(zs, reinterpret_cast<const Sym*>(p.zc) + sd.zcOff + u64(bFirst) * p.cb, zn, lane);
+        __syncwarp();
+        const u32 zcBlockOff = p.tables[t + 1].blockOff;
+        const u32 myStart = mine ? p.blockSum[zcBlockOff + b] : 0u;   // block starts: one load for all 32
+        Sym* out = reinterpret_cast<Sym*>(sd.out);
+        const u32 E = (p.cb + 31) / 32;
+        for (u32 j = 0; j < nMine; ++j) {
+            const u32 start = __shfl_sync(0xffffffffu, myStart, j);
+            const u32 bj = bFirst + j;
+            const u32 c = min(p.cb, sd.m - bj * p.cb);
+            const u32 e0 = min(lane * E, c), e1 = min(e0 + E, c);
+            const Sym* z = zs + j * p.cb;
+            u32 local = 0;
+            for (u32 e = e0; e < e1; ++e) local += u32(z[e]) + 1u;
+            u32 incl = local;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const u32 y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (int(lane) >= d) incl += y;
+            }
+            u32 pos = start + incl - local;
+            for (u32 e = e0; e < e1; ++e) {
+                pos += u32(z[e]);
+                if (pos < sd.n) out[pos] = rows[j * rowPitch + e];
+                else corrupt = true;
+                ++pos;
+            }
+        }
+    }
     if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
-    p.blockSum[td.blockOff + b] = sum;
 }
 
 // Exclusive scan of the per-block output lengths (one block per RLHuff stream).
@@ -439,35 +631,6 @@ __global__ void __launch_bounds__(1024) k_decScan(DecParams p) {
     }
     // the last symbol's position must be < n: total length <= n
     if (threadIdx.x == 0 && carry > sd.n) atomicOr(p.errors, DEV_ERR_CORRUPT);
-}
-
-// decodeRLHuff, symbols: decode and scatter out[scan(zc)+i] = symbol
-// (RunLengthKernels.cui:56-66).
-template <class Sym>
-__global__ void __launch_bounds__(128) k_decSymScatter(DecParams p) {
-    const u32 gb = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gb >= p.rlBlocks || capacityFailed(p)) return;
-    const u32 s = streamOfBlock(p, p.rlList, p.nRl, gb);
-    const DecStreamDesc sd = p.streams[s];
-    const u32 b = gb - sd.blockFirst;
-    if (b >= u32(ceilDiv(sd.m, p.cb))) return;
-    const u32 t = sd.tableFirst;
-    const DecTableDesc& td = p.tables[t];
-    const u32 i0 = b * p.cb;
-    const u32 cnt = min(p.cb, sd.m - i0);
-    const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
-    const Sym* zc = reinterpret_cast<const Sym*>(p.zc) + sd.zcOff + i0;
-    Sym* out = reinterpret_cast<Sym*>(sd.out);
-    u32 pos = p.blockSum[p.tables[t + 1].blockOff + b];
-    bool corrupt = false;
-    decodeBlock(srcOf(p, s), p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
-                [&](u32 i, u32 v) {
-                    pos += u32(zc[i]);
-                    if (pos < sd.n) out[pos] = Sym(v);
-                    else corrupt = true;
-                    ++pos;
-                });
-    if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
 }
 
 // ---------------------------------------------------------------------------
@@ -575,7 +738,7 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
         }
         if (d.kind == KIND_RLHUFF) {
             d.zcOff = zc;
-            zc += ns[s];
+            zc = alignUp(zc + ns[s], 8);   // 16-byte aligned zero counts of every stream
             d.blockFirst = u32(rlBlocks);
             rlBlocks += nb;
             rl[dc.nRl++] = s;
@@ -586,7 +749,7 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
         }
         sd[s] = d;
     }
-    if (blocks > I->capBlocks || zc > I->capCompact) {
+    if (blocks > I->capBlocks || zc > I->capCompact + 8ull * I->capStreams) {
         setError("decode: call exceeds the instance capacity (%llu coding blocks, %llu run-length symbols)",
                  (unsigned long long)blocks, (unsigned long long)zc);
         return CC_ERR_CAPACITY;
@@ -605,6 +768,18 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
     return CC_OK;
 }
 
+// Run-length decode staging: code words per warp (12 bits per symbol on
+// average fit; longer blocks decode from global memory) and the dynamic
+// shared memory of a 4-warp block.
+// (the area also holds the 32 blocks' zero counts in the scatter).
+static u32 decRlStageWords(u32 cb, size_t symBytes) {
+    return u32(alignUp(std::max<u64>(u64(12) * cb + 4, u64(32) * cb * symBytes / 4), 4));
+}
+static size_t decRlSmem(u32 cb, u32 stageWords, size_t symBytes) {
+    const u64 rowPitch = cb + (symBytes == 2 ? 2 : 1);
+    return 4 * (size_t(stageWords) * 4 + size_t(alignUp(u64(32) * rowPitch * symBytes, 16)));
+}
+
 template <class Sym>
 static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
     cudaStream_t st = I->stream;
@@ -620,10 +795,18 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
         countLaunch();
     }
     if (p.rlBlocks) {
-        const u32 g = u32(ceilDiv(p.rlBlocks, 128));
-        { SectionTimer t(I, "dec.zero_counts", st); k_decZc<Sym><<<g, 128, 0, st>>>(p); countLaunch(); }
+        const u32 g = u32(ceilDiv(u64(p.rlBlocks) / 32 + p.nRl, 4));   // warp tasks <= rlBlocks / 32 + nRl
+        const size_t smem = decRlSmem(p.cb, p.stageWords, sizeof(Sym));
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<Sym, false>),
+                                        sizeof(Sym) == 2 ? kAttrDecZc16 : kAttrDecZc32, I->device, smem),
+                    "decRl smem");
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<Sym, true>),
+                                        sizeof(Sym) == 2 ? kAttrDecSc16 : kAttrDecSc32, I->device, smem),
+                    "decRl smem");
+        { SectionTimer t(I, "dec.rl_tasks", st); k_decRlTasks<<<1, 1024, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.zero_counts", st); k_decRl<Sym, false><<<g, 128, smem, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.nRl, 1024, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "dec.symbols_scatter", st); k_decSymScatter<Sym><<<g, 128, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.symbols_scatter", st); k_decRl<Sym, true><<<g, 128, smem, st>>>(p); countLaunch(); }
     }
     CC_TRY_CUDA(cudaGetLastError(), "decode launch");
     return CC_OK;
@@ -631,10 +814,17 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
 
 int prepareDecodeAttributes(cc_instance* I) {
     const size_t smem = size_t(32) * (I->codingBlockSize + 2) * I->symBytes;
-    if (I->symBytes == 2)
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u16>), kAttrDecHuff16, I->device, smem), "decHuff smem");
-    else
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u32>), kAttrDecHuff32, I->device, smem), "decHuff smem");
+    const size_t rl = decRlSmem(I->codingBlockSize, decRlStageWords(I->codingBlockSize, I->symBytes), I->symBytes);
+    const int dev = I->device;
+    if (I->symBytes == 2) {
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u16>), kAttrDecHuff16, dev, smem), "decHuff smem");
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u16, false>), kAttrDecZc16, dev, rl), "decRl smem");
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u16, true>), kAttrDecSc16, dev, rl), "decRl smem");
+    } else {
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u32>), kAttrDecHuff32, dev, smem), "decHuff smem");
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u32, false>), kAttrDecZc32, dev, rl), "decRl smem");
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u32, true>), kAttrDecSc32, dev, rl), "decRl smem");
+    }
     return CC_OK;
 }
 
@@ -649,6 +839,7 @@ static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
     p.rlBlocks = dc.rlBlocks;
     p.hBlocks = dc.hBlocks;
     p.cb = I->codingBlockSize;
+    p.stageWords = decRlStageWords(I->codingBlockSize, I->symBytes);
     p.log2Max = I->log2Max;
     p.symBytes = I->symBytes;
     p.leavesMax = I->leavesMax;
@@ -666,6 +857,8 @@ static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
     p.lut = I->decLut;
     p.blockOff = I->blockOff;
     p.blockSum = I->blockSum;
+    p.rlTasks = I->decRlTasks;
+    p.rlTaskCap = u32(u64(I->capBlocks) / 32 + I->capStreams);
     p.zc = static_cast<char*>(I->zc);
     p.errors = I->errors + 4;
     return p;

@@ -111,7 +111,7 @@ struct Carver {
 void layoutArena(cc_instance* I, char* base, size_t* total) {
     Carver c{base};
     I->compact = c.take<char>(I->capCompact * I->symBytes + 64);
-    I->zc = c.take<char>(I->capCompact * I->symBytes + 64);
+    I->zc = c.take<char>((I->capCompact + 8ull * I->capStreams) * I->symBytes + 64);   // per stream 16-byte aligned
     I->tiles = c.take<RunSum>(I->capTiles);
     I->tileStart = c.take<TileStart>(I->capTiles);
     I->streamMax = c.take<u32>(I->capStreams);
@@ -139,6 +139,7 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->stagedWordsMax = I->hostWordsMax + 64;
     I->stagedWords = c.take<u32>(I->stagedWordsMax);
     I->blockSum = c.take<u32>(I->capBlocks + 1);
+    I->decRlTasks = c.take<u64>(u64(I->capBlocks) / 32 + I->capStreams + 2);
     *total = alignUp(c.off, 256);
 }
 
