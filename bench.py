@@ -128,23 +128,36 @@ class ClockSampler:
 # ------------------------------------------------------------------ fields
 def make_fields(wl, rank=0):
     from cudacompress_b200 import fields
-    return [fields.turbulence_field(wl["n"], wl["modes"], wl["kmax"], s + 100 * rank) for s in wl["seeds"]]
+    from cudacompress_b200.replicas import rank_seeds
+    return [fields.turbulence_field(wl["n"], wl["modes"], wl["kmax"], s) for s in rank_seeds(wl["seeds"], rank)]
 
 
 # -------------------------------------------------------------- CPU paths
 def cpu_reference_step(vol, wl, threads):
-    """Reference CPU coder on one component: oracle DWT + quantize (the
-    reference has no CPU DWT), the reference's own src/CPU RLE+Huffman for
-    every band stream, then the inverse.  Returns (encode_s, decode_s, kind)."""
+    """Reference CPU coder on one component of the workload."""
+    return cpu_reference_volume(vol, wl["levels"], wl["q0"], threads)
+
+
+_ORACLE = []
+
+
+def cpu_reference_volume(vol, L, q0, threads):
+    """Reference CPU coder on one float32 volume (any z, y, x sizes): oracle
+    DWT + quantize (the reference has no CPU DWT), the reference's own src/CPU
+    RLE+Huffman for every band stream, then the inverse.  Returns
+    (encode_s, decode_s, kind)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import Oracle
-    orc = Oracle()
-    n, L, q0 = wl["n"], wl["levels"], wl["q0"]
-    total = n ** 3
+    if not _ORACLE:
+        _ORACLE.append(Oracle())
+    orc = _ORACLE[0]
+    vol = np.ascontiguousarray(vol, np.float32)
+    nz, ny, nx = vol.shape
+    total = vol.size
     refcpu_path = os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")
     t0 = time.perf_counter()
     syms = np.zeros(total, np.uint16)
-    orc.lib.orc_volume_symbols(vol, n, n, n, L, q0, syms)
+    orc.lib.orc_volume_symbols(vol, nx, ny, nz, L, q0, syms)
     if os.path.exists(refcpu_path):
         kind = "reference"
         ref = ctypes.CDLL(refcpu_path)
@@ -156,10 +169,12 @@ def cpu_reference_step(vol, wl, threads):
         ref.refcpu_decode_rlhuff.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
         # stream groups as the codec calls them: LP (1 stream), then per level
         # coarse->fine the 7 bands (equal sizes, contiguous)
-        groups = [(0, 1, (n >> L) ** 3)]
-        off = (n >> L) ** 3
+        def band(shift):
+            return (nx >> shift) * (ny >> shift) * (nz >> shift)
+        groups = [(0, 1, band(L))]
+        off = band(L)
         for l in range(L - 1, -1, -1):
-            bn = (n >> (l + 1)) ** 3
+            bn = band(l + 1)
             groups.append((off, 7, bn))
             off += 7 * bn
         outs = []
@@ -176,7 +191,7 @@ def cpu_reference_step(vol, wl, threads):
         for (words, sw, o, S, cnt) in outs:
             ref.refcpu_decode_rlhuff(words.ctypes.data, sw.ctypes.data, S, cnt, 128, threads, dec[o:].ctypes.data)
         rec = np.zeros(vol.shape, np.float32)
-        orc.lib.orc_volume_from_symbols(dec, rec, n, n, n, L, q0)
+        orc.lib.orc_volume_from_symbols(dec, rec, nx, ny, nz, L, q0)
         t2 = time.perf_counter()
         assert np.array_equal(dec, syms), "reference CPU coder round trip mismatch"
         return t1 - t0, t2 - t1, kind
@@ -188,11 +203,97 @@ def cpu_reference_step(vol, wl, threads):
     return t1 - t0, t2 - t1, kind
 
 
+def reference_line(args, wl, value, unit, step_s, kind, threads, sample):
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": wl["desc"], "sample": sample},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def run_reference_bricks(args, wl, threads):
+    """The reference CPU coder over a bounded sample of the brick set: each
+    step codes the next 64 bricks one after another (encode + decode)."""
+    from cudacompress_b200 import fields
+    bricks, q = fields.brick_set(wl["count"], wl["seed"])
+    per = 64
+    kind = "port"
+    k = 0
+
+    def one_step():
+        nonlocal k, kind
+        t = 0.0
+        raw = 0
+        for _ in range(per):
+            b = bricks[k % len(bricks)]
+            e, d, kind = cpu_reference_volume(b, wl["levels"], float(q[k % len(bricks)]), threads)
+            t += e + d
+            raw += b.size * 4
+            k += 1
+        return t, raw
+
+    for _ in range(args.warmup):
+        one_step()
+    tt, rr = 0.0, 0
+    for _ in range(args.steps):
+        t, r = one_step()
+        tt += t
+        rr += r
+    value = rr / tt / 1e9
+    print(json.dumps(reference_line(args, wl, value, "GB/s", tt / args.steps, kind, threads,
+                                    f"{per} bricks per step, encode+decode one brick at a time")), flush=True)
+
+
+def run_reference_serving(args, wl, threads):
+    """The reference CPU coder serving the same request mix one request at a
+    time (encode: code the source brick; decode: decode its stream), bricks/s
+    over a bounded sample of 200 requests per step."""
+    from cudacompress_b200 import fields, serving
+    rng = np.random.default_rng(wl["seed"])
+    src = fields.turbulence_field(128, 1024, 64, wl["seed"])
+    sources = {}
+    for e in wl["edges"]:
+        bl = []
+        for _ in range(wl["bricks_per_edge"]):
+            o = [int(rng.integers(0, 128 - e + 1)) for _ in range(3)]
+            bl.append(np.ascontiguousarray(src[o[0]:o[0] + e, o[1]:o[1] + e, o[2]:o[2] + e]))
+        sources[e] = bl
+    per = 200
+    reqs = serving.poisson_requests(per * (args.steps + args.warmup), 1e12, wl["edges"], wl["decode_frac"],
+                                    wl["bricks_per_edge"], wl["seed"] + 2)
+    kind = "port"
+
+    def one_step(chunk):
+        nonlocal kind
+        t = 0.0
+        for r in chunk:
+            e, d, kind = cpu_reference_volume(sources[r.edge][r.brick], wl["levels"], wl["q0"], threads)
+            t += e if r.op == serving.ENCODE else d
+        return t
+
+    for w in range(args.warmup):
+        one_step(reqs[w * per:(w + 1) * per])
+    tt = 0.0
+    for st in range(args.steps):
+        a = (args.warmup + st) * per
+        tt += one_step(reqs[a:a + per])
+    value = per * args.steps / tt
+    print(json.dumps(reference_line(args, wl, value, "bricks/s", tt / args.steps, kind, threads,
+                                    f"{per} requests per step, one at a time")), flush=True)
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if args.workload.startswith("bricks"):
+        return run_reference_bricks(args, wl, threads)
+    if args.workload == "serving":
+        return run_reference_serving(args, wl, threads)
     vol = make_fields(wl)[0]
     for _ in range(args.warmup):
         cpu_reference_step(vol, wl, threads)
@@ -403,7 +504,7 @@ def run_bricks(args, wl):
 def run_ours(args, wl):
     import torch
     import cudacompress_b200 as cc
-    from cudacompress_b200 import fields
+    from cudacompress_b200 import fields, replicas
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -467,12 +568,9 @@ def run_ours(args, wl):
     ms = start.elapsed_time(end) / args.steps
     enc_ms = sum(evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)) / args.steps
     dec_ms = sum(evs[k][1].elapsed_time(evs[k][2]) for k in range(args.steps)) / args.steps
-    if dist:
-        t = torch.tensor([ms, enc_ms, dec_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, enc_ms, dec_ms = t.tolist()
+    ms, enc_ms, dec_ms = replicas.max_over_ranks([ms, enc_ms, dec_ms], dist, dev)
     raw_step = C * n ** 3 * 4
-    value = world * raw_step / (ms / 1e3) / 1e9
+    value = replicas.job_gbs(world, raw_step, ms)
 
     # the plain per-component path (cc_compress_volume_float / decompress), for comparison
     plain_out = torch.empty_like(vols[0])
@@ -525,11 +623,8 @@ def run_ours(args, wl):
     e2.record()
     torch.cuda.synchronize()
     e2e_ms = s2.elapsed_time(e2) / args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
-    e2e_value = world * raw_step / (e2e_ms / 1e3) / 1e9
+    e2e_ms = replicas.max_over_ranks([e2e_ms], dist, dev)[0]
+    e2e_value = replicas.job_gbs(world, raw_step, e2e_ms)
 
     # per-kernel sections (one extra step with event timing on)
     lib = cc.lib()
@@ -596,8 +691,8 @@ def run_ours(args, wl):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded k^-5/3 random-phase fields)",
             "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": f"replicas{world}",
                        "l2": f"inputs {C * n ** 3 * 4 >> 20} MiB per step > L2 126 MiB"},
-            "encode_gbs": world * raw_step / (enc_ms / 1e3) / 1e9,
-            "decode_gbs": world * raw_step / (dec_ms / 1e3) / 1e9,
+            "encode_gbs": replicas.job_gbs(world, raw_step, enc_ms),
+            "decode_gbs": replicas.job_gbs(world, raw_step, dec_ms),
             "compression_ratio": raw_step / max(coded_bytes, 1), "psnr_db": psnr,
             "plain_path_ms_per_step": plain_ms, "streams_identical_to_plain_codec": bool(same_as_plain),
             "batched_vs_per_brick": bricks, "serving": serve,
