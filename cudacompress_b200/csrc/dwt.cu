@@ -523,6 +523,21 @@ __device__ __forceinline__ float bandSample(const BColDesc& D, int x, int y, int
     return (float(q) + signI(q) * 0.5f) * D.step;   // Quantize.cuh:104-110
 }
 
+// The samples (x, x + 1), x even, of that pass.  With an even half width hx
+// both lie in one band at an even offset: one 4-byte symbol pair, or one
+// float2 of the lowpass (all pitches even, bases 16-byte aligned).
+__device__ __forceinline__ float2 bandPair(const BColDesc& D, int x, int y, int z) {
+    if (D.hx & 1) return make_float2(bandSample(D, x, y, z), bandSample(D, x + 1, y, z));
+    const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
+    const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
+    const int b = bx + 2 * by + 4 * bz;
+    if (b == 0) return *reinterpret_cast<const float2*>(D.src + size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx);
+    const u32 pair =
+        *reinterpret_cast<const u32*>(D.bands + u64(b - 1) * D.bandStride + (u64(lz) * D.hy + ly) * D.hx + lx);
+    const int q0 = unsymbolizeI(pair & 0xFFFFu), q1 = unsymbolizeI(pair >> 16);
+    return make_float2((float(q0) + signI(q0) * 0.5f) * D.step, (float(q1) + signI(q1) * 0.5f) * D.step);
+}
+
 template <bool kInverse, int kParity>
 __device__ __forceinline__ void colOutputs(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x, int c,
                                            int a0) {
@@ -571,7 +586,7 @@ __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ desc
             const int a = kInverse ? splitPos(m, na) : m;
             if (kSymbols) {
                 // axis Z: a = z, c = y
-                vals[i] = make_float2(bandSample(D, x, c, a), bandSample(D, x + 1, c, a));
+                vals[i] = bandPair(D, x, c, a);
             } else {
                 vals[i] = *reinterpret_cast<const float2*>(D.src + size_t(x) + size_t(a) * D.sa + size_t(c) * D.sc);
             }
