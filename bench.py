@@ -19,8 +19,14 @@ to the plain single-volume codec's, replayed as CUDA graphs).
           log-uniform [0.002, 0.05]) in one batch vs one plain call per brick
   serving the continuous-batching brick service at 10k req/s (Poisson, 90%
           decode, edges {32, 64, 128}): p50 / p99 latency, bricks/s
-  roofline  the dominant kernel section (CUDA-event timed inside the library)
-          against the measured HBM copy bandwidth
+  roofline  the dominant bandwidth-bound kernel section (CUDA-event timed
+          inside the library; the batched transform's passes, each counted
+          with its own input read once and output written once) against the
+          measured HBM copy bandwidth; its `traffic` is the section's DRAM
+          bytes from an ncu capture (profiles/traffic.json)
+  pipeline_roofline  the whole codec with algorithmic bytes = raw +
+          compressed (intermediate passes not counted), step, encode and
+          decode fractions of the same peak
   cpu_baseline  the reference's own CPU coder (src/CPU RunLengthCPU /
           HuffmanTableCPU / HuffmanCPU, built from the reference sources into
           oracle/_ref) plus the oracle's CPU DWT/quantize port (the reference
@@ -321,17 +327,26 @@ METRIC = "enc/dec GB/s raw (%HBM peak); batched vs per-brick GB/s at fixed PSNR;
 
 
 # ---------------------------------------------------------- section bytes
+# per-unit algorithmic bytes of the sections the roofline may pick
+SECTION_UNITS = {
+    "batch.dwt_forward": "per pass (k_bRows / k_bCols, 3 per level): its input read once + its output written "
+                         "once, 8 B/voxel",
+    "batch.dwt_inverse": "per pass (k_bCols from symbols, k_bCols, k_bRows per level): 2 B/symbol + 4 B/lowpass "
+                         "voxel in and 4 B/voxel out for the first, 8 B/voxel for the others",
+}
+
+
 def section_bytes(name, wl, coded_bytes, counts):
     """Compulsory HBM bytes of one timed section over one step (algorithmic:
-    each input read once, each output written once)."""
+    each launch's inputs read once, its outputs written once)."""
     n, L, C = wl["n"], wl["levels"], wl["comps"]
     vols = [(n >> l) ** 3 for l in range(L)]
     hp = sum(7 * v // 8 for v in vols)
     lp = vols[-1] // 8
     m = {
         "pipe.dwt_forward": sum(8 * v for v in vols) * C,
-        "batch.dwt_forward": sum(8 * v for v in vols) * C,
-        "batch.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
+        "batch.dwt_forward": sum(3 * 8 * v for v in vols) * C,
+        "batch.dwt_inverse": sum(4 * (v // 8) + 2 * (7 * v // 8) + 4 * v + 2 * 8 * v for v in vols) * C,
         "batch.quantize": (hp + lp) * 6 * C,
         "pipe.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
         "pipe.quantize": (hp + lp) * 6 * C,
@@ -662,14 +677,18 @@ def run_ours(args, wl):
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "traffic": traffic, "launches": dom[1][1], "share": dom[1][0] / total_sec,
-                "algorithmic_bytes_per_step": dom_bytes,
+                "algorithmic_bytes_per_step": dom_bytes, "per_unit": SECTION_UNITS.get(dom[0]),
                 "dominant_section": {"name": top[0], "ms": top[1][0], "share": top[1][0] / total_sec,
                                      "note": "enc.table_build is latency-bound (sequential libstdc++-order heap merge)"
                                      if top[0] == "enc.table_build" else None}}
+    # whole codec (algorithmic: raw + compressed bytes; intermediate passes do not count)
     step_alg = 2 * (raw_step + coded_bytes)
+    enc_gbs_alg = (raw_step + coded_bytes) / (enc_ms / 1e3) / 1e9
+    dec_gbs_alg = (raw_step + coded_bytes) / (dec_ms / 1e3) / 1e9
     pipeline = {"achieved": step_alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": step_alg / (ms / 1e3) / 1e9 / peak,
-                "algorithmic_bytes_per_step": step_alg}
+                "algorithmic_bytes_per_step": step_alg,
+                "encode_frac": enc_gbs_alg / peak, "decode_frac": dec_gbs_alg / peak}
 
     bricks = None
     if rank == 0 and world == 1 and not args.no_bricks:
