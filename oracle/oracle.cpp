@@ -817,8 +817,8 @@ int orc_decode(int kind, int symBytes, const u32* words, u32 bitSize, u32* bitPo
 // coarsest step), LP band encodeHuff, then per level coarse->fine the 7 HP
 // bands (index x+2y+4z) with encodeRLHuff.  Symbol16 streams.
 // ---------------------------------------------------------------------------
-int orc_compress_volume_float(const float* vol, long nx, long ny, long nz, int levels, float q0, u32 cb,
-                              u32 log2Max, u32* words, u32 cap, u32* bitSize) {
+int orc_compress_volume_float_ex(const float* vol, long nx, long ny, long nz, int levels, float q0, u32 cb,
+                                 u32 log2Max, int rleOnlyLevel0, u32* words, u32 cap, u32* bitSize) {
     std::vector<std::vector<float>> lv(levels);
     std::vector<float> cur(vol, vol + nx * ny * nz);
     long sx = nx, sy = ny, sz = nz;
@@ -851,15 +851,22 @@ int orc_compress_volume_float(const float* vol, long nx, long ny, long nz, int l
             quantizeBand(lv[l].data(), n0, n1, n2, b % 2, (b / 2) % 2, b / 4, step, bands.data() + (b - 1) * bandN);
             s[b - 1] = bands.data() + (b - 1) * bandN;
         }
-        int r = encodeRLHuff(bs, s, u32(bandN), cb, log2Max);
+        // CompressVolume.cpp:389-395: with doRLEOnlyOnLvl0 the levels above 0 skip the RLE
+        int r = (rleOnlyLevel0 && l > 0) ? encodeHuff(bs, s, u32(bandN), cb, log2Max)
+                                         : encodeRLHuff(bs, s, u32(bandN), cb, log2Max);
         if (r) return r;
     }
     u32 pos;
     return finishBits(bs, words, cap, bitSize, &pos);
 }
 
-int orc_decompress_volume_float(const u32* words, u32 bitSize, float* out, long nx, long ny, long nz, int levels,
-                                float q0, u32 cb, u32 log2Max) {
+int orc_compress_volume_float(const float* vol, long nx, long ny, long nz, int levels, float q0, u32 cb,
+                              u32 log2Max, u32* words, u32 cap, u32* bitSize) {
+    return orc_compress_volume_float_ex(vol, nx, ny, nz, levels, q0, cb, log2Max, 0, words, cap, bitSize);
+}
+
+int orc_decompress_volume_float_ex(const u32* words, u32 bitSize, float* out, long nx, long ny, long nz, int levels,
+                                   float q0, u32 cb, u32 log2Max, int rleOnlyLevel0) {
     BitReader br{words, bitSize, 0};
     long sx = nx >> levels, sy = ny >> levels, sz = nz >> levels;
     std::vector<u16> lp(sx * sy * sz);
@@ -873,7 +880,8 @@ int orc_decompress_volume_float(const u32* words, u32 bitSize, float* out, long 
         std::vector<u16> bands(7 * bandN);
         std::vector<u16*> ob(7);
         for (int b = 0; b < 7; ++b) ob[b] = bands.data() + b * bandN;
-        decodeRLHuff(br, ob, u32(bandN), cb, log2Max);
+        if (rleOnlyLevel0 && l > 0) decodeHuff(br, ob, u32(bandN), cb, log2Max);   // CompressVolume.cpp:491-495
+        else decodeRLHuff(br, ob, u32(bandN), cb, log2Max);
         float step = q0 / float(1 << l);
         std::vector<float> coef(n0 * n1 * n2);
         for (long z = 0; z < n2 / 2; ++z)
@@ -886,6 +894,110 @@ int orc_decompress_volume_float(const u32* words, u32 bitSize, float* out, long 
         dwtFloat(coef.data(), cur.data(), n0, n1, n2, true);
     }
     std::copy(cur.begin(), cur.end(), out);
+    return 0;
+}
+
+int orc_decompress_volume_float(const u32* words, u32 bitSize, float* out, long nx, long ny, long nz, int levels,
+                                float q0, u32 cb, u32 log2Max) {
+    return orc_decompress_volume_float_ex(words, bitSize, out, nx, ny, nz, levels, q0, cb, log2Max, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Quantize-first lossy volume codec (examples CompressVolume.cpp:651-757 /
+// :759-856): uniform quantization of the whole volume to short
+// (Quantize.cuh:86-93, int(v * (1/step) + sign(v) * 0.5), restated with the
+// product contracted into one fma), then an integer 5/3 DWT per level on the
+// LLL region of the previous level, the final lowpass symbolized and
+// encodeHuff'd, and per level coarse -> fine the 7 highpass bands (index
+// x+2y+4z) symbolized and encodeRLHuff'd (encodeHuff above level 0 with
+// doRLEOnlyOnLvl0).  Decoding inverts the levels coarse -> fine and
+// unquantizes q * step (Quantize.cuh:113-119).
+// ---------------------------------------------------------------------------
+static inline i16 quantUniform(float v, float inv) {
+    const float s = v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f);
+    return i16(int(std::fmaf(v, inv, s * 0.5f)));
+}
+
+int orc_compress_volume_quantfirst(const float* vol, long nx, long ny, long nz, int levels, float step, u32 cb,
+                                   u32 log2Max, int rleOnlyLevel0, u32* words, u32 cap, u32* bitSize) {
+    const float inv = 1.0f / step;   // Quantize.cu:236: reciprocal on the host
+    std::vector<i16> cur(nx * ny * nz);
+    for (long i = 0; i < nx * ny * nz; ++i) cur[i] = quantUniform(vol[i], inv);
+    std::vector<std::vector<i16>> lv(levels);
+    long sx = nx, sy = ny, sz = nz;
+    for (int l = 0; l < levels; ++l) {
+        lv[l].resize(sx * sy * sz);
+        dwtInt(cur.data(), lv[l].data(), sx, sy, sz, false);
+        long hx = sx / 2, hy = sy / 2, hz = sz / 2;
+        cur.resize(hx * hy * hz);
+        for (long z = 0; z < hz; ++z)
+            for (long y = 0; y < hy; ++y)
+                for (long x = 0; x < hx; ++x) cur[(z * hy + y) * hx + x] = lv[l][(z * sy + y) * sx + x];
+        sx = hx; sy = hy; sz = hz;
+    }
+    BitStream bs;
+    {
+        std::vector<u16> lp(cur.size());
+        for (size_t i = 0; i < cur.size(); ++i) lp[i] = u16(symbolize(cur[i]));
+        std::vector<const u16*> s(1, lp.data());
+        int r = encodeHuff(bs, s, u32(lp.size()), cb, log2Max);
+        if (r) return r;
+    }
+    for (int l = levels - 1; l >= 0; --l) {
+        long n0 = nx >> l, n1 = ny >> l, n2 = nz >> l;
+        long hx = n0 / 2, hy = n1 / 2, hz = n2 / 2, bandN = hx * hy * hz;
+        std::vector<u16> bands(7 * bandN);
+        std::vector<const u16*> s(7);
+        for (int b = 1; b < 8; ++b) {
+            const long bx = b % 2, by = (b / 2) % 2, bz = b / 4;
+            u16* o = bands.data() + (b - 1) * bandN;
+            for (long z = 0; z < hz; ++z)
+                for (long y = 0; y < hy; ++y)
+                    for (long x = 0; x < hx; ++x)
+                        o[(z * hy + y) * hx + x] = u16(symbolize(lv[l][((z + bz * hz) * n1 + (y + by * hy)) * n0 + x + bx * hx]));
+            s[b - 1] = o;
+        }
+        int r = (rleOnlyLevel0 && l > 0) ? encodeHuff(bs, s, u32(bandN), cb, log2Max)
+                                         : encodeRLHuff(bs, s, u32(bandN), cb, log2Max);
+        if (r) return r;
+    }
+    u32 pos;
+    return finishBits(bs, words, cap, bitSize, &pos);
+}
+
+int orc_decompress_volume_quantfirst(const u32* words, u32 bitSize, float* out, long nx, long ny, long nz,
+                                     int levels, float step, u32 cb, u32 log2Max, int rleOnlyLevel0) {
+    BitReader br{words, bitSize, 0};
+    long sx = nx >> levels, sy = ny >> levels, sz = nz >> levels;
+    std::vector<u16> lp(sx * sy * sz);
+    std::vector<u16*> o(1, lp.data());
+    decodeHuff(br, o, u32(lp.size()), cb, log2Max);
+    std::vector<i16> cur(lp.size());
+    for (size_t i = 0; i < lp.size(); ++i) cur[i] = i16(unsymbolize(lp[i]));
+    for (int l = levels - 1; l >= 0; --l) {
+        long n0 = nx >> l, n1 = ny >> l, n2 = nz >> l;
+        long hx = n0 / 2, hy = n1 / 2, hz = n2 / 2, bandN = hx * hy * hz;
+        std::vector<u16> bands(7 * bandN);
+        std::vector<u16*> ob(7);
+        for (int b = 0; b < 7; ++b) ob[b] = bands.data() + b * bandN;
+        if (rleOnlyLevel0 && l > 0) decodeHuff(br, ob, u32(bandN), cb, log2Max);
+        else decodeRLHuff(br, ob, u32(bandN), cb, log2Max);
+        std::vector<i16> coef(n0 * n1 * n2);
+        for (long z = 0; z < hz; ++z)
+            for (long y = 0; y < hy; ++y)
+                for (long x = 0; x < hx; ++x) coef[(z * n1 + y) * n0 + x] = cur[(z * hy + y) * hx + x];
+        for (int b = 1; b < 8; ++b) {
+            const long bx = b % 2, by = (b / 2) % 2, bz = b / 4;
+            for (long z = 0; z < hz; ++z)
+                for (long y = 0; y < hy; ++y)
+                    for (long x = 0; x < hx; ++x)
+                        coef[((z + bz * hz) * n1 + (y + by * hy)) * n0 + x + bx * hx] =
+                            i16(unsymbolize(ob[b - 1][(z * hy + y) * hx + x]));
+        }
+        cur.resize(coef.size());
+        dwtInt(coef.data(), cur.data(), n0, n1, n2, true);
+    }
+    for (long i = 0; i < nx * ny * nz; ++i) out[i] = float(cur[i]) * step;
     return 0;
 }
 

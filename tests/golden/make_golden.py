@@ -12,8 +12,15 @@ ref_streams.npz  encodeRLHuff / encodeHuff bit streams (Encode.cpp:207-471,
                  648-790) of seeded symbol streams, with their inputs.
 ref_dwt.npz      util::dwtFloat3DForward/Inverse, dwtIntForward/Inverse and
                  quantizeToSymbols outputs with their inputs.
+ref_volume.npz   the reference's example volume codec (examples/CompressVolume.cpp):
+                 compressVolumeFloat / compressVolumeFloatQuantFirst streams with and
+                 without doRLEOnlyOnLvl0, their reconstructions, and the multi-channel
+                 decoders' outputs (python tests/golden/make_golden.py --gpu --only volume).
+                 Inputs are seeded fields (cudacompress_b200.fields), stored as seed +
+                 SHA-256 of the generated array.
 """
 import argparse
+import hashlib
 import ctypes
 import os
 import sys
@@ -191,17 +198,106 @@ def make_dwt(ref):
     print("ref_dwt.npz written")
 
 
+# Whole-volume cases of the reference's example codec (examples/CompressVolume.cpp):
+# (name, (nz, ny, nx), levels, step, rleOnlyLevel0, quantFirst, keep the reconstruction)
+VOLUME_CASES = [
+    ("f2", (16, 16, 32), 2, 0.01, 0, 0, True),
+    ("f2r", (16, 16, 32), 2, 0.01, 1, 0, True),
+    ("f3r", (32, 32, 32), 3, 0.01, 1, 0, True),
+    ("q2", (16, 16, 32), 2, 0.05, 0, 1, True),
+    ("q2r", (16, 16, 32), 2, 0.05, 1, 1, True),
+    ("q3", (32, 32, 32), 3, 0.05, 0, 1, False),   # odd levels: the reference's decompress reads the other buffer
+]
+# multi-channel decodes: (name, (nz, ny, nx), levels, steps per channel, rleOnlyLevel0, quantFirst)
+MULTI_CASES = [
+    ("mf", (16, 16, 32), 2, (0.01, 0.02, 0.005), 0, 0),
+    ("mfr", (16, 16, 32), 2, (0.01, 0.02, 0.005), 1, 0),
+    ("mq", (16, 16, 32), 2, (0.05, 0.1, 0.03), 0, 1),
+]
+
+
+def make_volume(ref, out_dir):
+    import torch
+    from cudacompress_b200 import fields
+    u32p = c.POINTER(c.c_uint32)
+    ref.ref_volume_compress.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float,
+                                        c.c_int, c.c_int, u32p, c.c_uint32, u32p]
+    ref.ref_volume_decompress.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float,
+                                          c.c_int, c.c_int, u32p, c.c_uint32]
+    ref.ref_volume_decompress_multichannel.argtypes = [c.c_void_p, c.c_void_p, u32p, c.POINTER(c.c_float), c.c_uint32,
+                                                       c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_int, c.c_int]
+    P = lambda t: c.c_void_p(t.data_ptr())  # noqa: E731
+
+    def vol_for(shape, seed):
+        nz, ny, nx = shape
+        return fields.turbulence_field(max(shape), 64, 8, seed=seed)[:nz, :ny, :nx].copy()
+
+    def compress(v, levels, q, rle, qf):
+        nz, ny, nx = v.shape
+        cap = v.size * 4 + 65536
+        words = np.zeros(cap, np.uint32)
+        nw = c.c_uint32()
+        r = ref.ref_volume_compress(P(torch.from_numpy(v).cuda()), nx, ny, nz, levels, q, rle, qf,
+                                    words.ctypes.data_as(u32p), cap, c.byref(nw))
+        assert r == 0, r
+        return words[: nw.value].copy()
+
+    def sha(v):
+        return np.frombuffer(hashlib.sha256(v.tobytes()).digest(), np.uint8)
+
+    # inputs are not stored: they are regenerated from their seeds (the hash guards the generator)
+    out = {}
+    for i, (name, shape, levels, q, rle, qf, keep) in enumerate(VOLUME_CASES):
+        v = vol_for(shape, 500 + i)
+        w = compress(v, levels, q, rle, qf)
+        out[f"{name}_seed"], out[f"{name}_insha"], out[f"{name}_words"] = np.array([500 + i], np.int64), sha(v), w
+        out[f"{name}_meta"] = np.array([levels, rle, qf], np.int32)
+        out[f"{name}_q"] = np.array([q], np.float32)
+        if keep:
+            nz, ny, nx = shape
+            rec = torch.full(shape, float("nan"), dtype=torch.float32, device="cuda")
+            r = ref.ref_volume_decompress(P(rec), nx, ny, nz, levels, q, rle, qf, w.ctypes.data_as(u32p), len(w))
+            assert r == 0, r
+            out[f"{name}_rec"] = rec.cpu().numpy()
+    for i, (name, shape, levels, qs, rle, qf) in enumerate(MULTI_CASES):
+        nz, ny, nx = shape
+        seeds = [600 + 10 * i + k for k in range(len(qs))]
+        vols = [vol_for(shape, sd) for sd in seeds]
+        ws = [compress(v, levels, q, rle, qf) for v, q in zip(vols, qs)]
+        recs = [torch.full(shape, float("nan"), dtype=torch.float32, device="cuda") for _ in qs]
+        ptrs = (c.c_void_p * len(qs))(*[r.data_ptr() for r in recs])
+        wp = (u32p * len(qs))(*[w.ctypes.data_as(u32p) for w in ws])
+        nws = (c.c_uint32 * len(qs))(*[len(w) for w in ws])
+        qa = (c.c_float * len(qs))(*qs)
+        r = ref.ref_volume_decompress_multichannel(ptrs, wp, nws, qa, len(qs), nx, ny, nz, levels, rle, qf)
+        assert r == 0, r
+        out[f"{name}_meta"] = np.array([levels, rle, qf, len(qs)], np.int32)
+        out[f"{name}_q"] = np.array(qs, np.float32)
+        for k in range(len(qs)):
+            out[f"{name}_seed{k}"], out[f"{name}_insha{k}"] = np.array([seeds[k]], np.int64), sha(vols[k])
+            out[f"{name}_words{k}"] = ws[k]
+            out[f"{name}_rec{k}"] = recs[k].cpu().numpy()
+    np.savez_compressed(os.path.join(out_dir, "ref_volume.npz"), **out)
+    print("ref_volume.npz written")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpu", action="store_true", help="also run the reference's GPU code")
+    ap.add_argument("--only", choices=["volume"], help="only the whole-volume fixtures (GPU)")
+    ap.add_argument("--out", default=HERE, help="output directory")
     args = ap.parse_args()
     ref = load_ref_gpu_lib()
     if ref is None:
         sys.exit("oracle/_ref/libref_gpu.so missing: run `make -C oracle/ref` first")
+    if args.only == "volume":
+        make_volume(ref, args.out)
+        return
     make_tables(ref)
     if args.gpu:
         make_streams(ref)
         make_dwt(ref)
+        make_volume(ref, args.out)
 
 
 if __name__ == "__main__":

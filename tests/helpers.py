@@ -115,6 +115,16 @@ class Oracle:
                                                 c.c_uint32, U32P, c.c_uint32, c.POINTER(c.c_uint32)]
         L.orc_decompress_volume_float.argtypes = [U32P, c.c_uint32, F32P, c.c_long, c.c_long, c.c_long, c.c_int,
                                                   c.c_float, c.c_uint32, c.c_uint32]
+        L.orc_compress_volume_float_ex.argtypes = [F32P, c.c_long, c.c_long, c.c_long, c.c_int, c.c_float,
+                                                   c.c_uint32, c.c_uint32, c.c_int, U32P, c.c_uint32,
+                                                   c.POINTER(c.c_uint32)]
+        L.orc_decompress_volume_float_ex.argtypes = [U32P, c.c_uint32, F32P, c.c_long, c.c_long, c.c_long, c.c_int,
+                                                     c.c_float, c.c_uint32, c.c_uint32, c.c_int]
+        L.orc_compress_volume_quantfirst.argtypes = [F32P, c.c_long, c.c_long, c.c_long, c.c_int, c.c_float,
+                                                     c.c_uint32, c.c_uint32, c.c_int, U32P, c.c_uint32,
+                                                     c.POINTER(c.c_uint32)]
+        L.orc_decompress_volume_quantfirst.argtypes = [U32P, c.c_uint32, F32P, c.c_long, c.c_long, c.c_long,
+                                                       c.c_int, c.c_float, c.c_uint32, c.c_uint32, c.c_int]
         L.orc_volume_symbols.argtypes = [F32P, c.c_long, c.c_long, c.c_long, c.c_int, c.c_float, U16P]
         L.orc_volume_from_symbols.argtypes = [U16P, F32P, c.c_long, c.c_long, c.c_long, c.c_int, c.c_float]
         L.orc_compress_heightfield.argtypes = [I16P, c.c_long, c.c_long, c.c_int, c.c_uint32, c.c_uint32, U32P,
@@ -180,21 +190,23 @@ class Oracle:
                             ctypes.byref(p), out.ctypes.data, S, n, cb, log2max)
         return out, p.value
 
-    def compress_volume(self, vol, levels, q0, cb=128, log2max=14):
+    def compress_volume(self, vol, levels, q0, cb=128, log2max=14, rle_only_level0=False, quant_first=False):
         vol = np.ascontiguousarray(vol, np.float32)
         nz, ny, nx = vol.shape
         cap = vol.size * 2 + 65536
         words = np.zeros(cap, np.uint32)
         bits = ctypes.c_uint32()
-        r = self.lib.orc_compress_volume_float(vol, nx, ny, nz, levels, q0, cb, log2max, words, cap, ctypes.byref(bits))
+        f = self.lib.orc_compress_volume_quantfirst if quant_first else self.lib.orc_compress_volume_float_ex
+        r = f(vol, nx, ny, nz, levels, q0, cb, log2max, int(rle_only_level0), words, cap, ctypes.byref(bits))
         assert r == 0, r
         return words[: (bits.value + 31) // 32].copy(), bits.value
 
-    def decompress_volume(self, words, bits, shape, levels, q0, cb=128, log2max=14):
+    def decompress_volume(self, words, bits, shape, levels, q0, cb=128, log2max=14, rle_only_level0=False,
+                          quant_first=False):
         nz, ny, nx = shape
         out = np.zeros(shape, np.float32)
-        self.lib.orc_decompress_volume_float(np.ascontiguousarray(words, np.uint32), bits, out, nx, ny, nz, levels,
-                                             q0, cb, log2max)
+        f = self.lib.orc_decompress_volume_quantfirst if quant_first else self.lib.orc_decompress_volume_float_ex
+        f(np.ascontiguousarray(words, np.uint32), bits, out, nx, ny, nz, levels, q0, cb, log2max, int(rle_only_level0))
         return out
 
     def compress_heightfield(self, img, levels, cb=128, log2max=14):

@@ -1,0 +1,87 @@
+"""The oracle's whole-volume codecs against the reference's own example codec
+(examples/CompressVolume.cpp, run on a B200 into tests/golden/ref_volume.npz
+by tests/golden/make_golden.py): compressVolumeFloat with and without
+doRLEOnlyOnLvl0, compressVolumeFloatQuantFirst, their decompressors and the
+multi-channel decompressors.  Streams must be word-identical and
+reconstructions bit-identical.  The quant-first decoder of the reference
+starts its inverse transform from the wrong ping-pong buffer when the level
+count is odd; its fixtures therefore hold the stream only for 3 levels."""
+import hashlib
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from helpers import Oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+GOLD = os.path.join(ROOT, "tests", "golden", "ref_volume.npz")
+
+VOLUME = ["f2", "f2r", "f3r", "q2", "q2r", "q3"]
+MULTI = ["mf", "mfr", "mq"]
+SHAPES = {"f2": (16, 16, 32), "f2r": (16, 16, 32), "f3r": (32, 32, 32), "q2": (16, 16, 32), "q2r": (16, 16, 32),
+          "q3": (32, 32, 32), "mf": (16, 16, 32), "mfr": (16, 16, 32), "mq": (16, 16, 32)}
+
+
+@pytest.fixture(scope="module")
+def gold():
+    if not os.path.exists(GOLD):
+        pytest.skip("ref_volume.npz missing")
+    return np.load(GOLD)
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    return Oracle()
+
+
+def regen(shape, seed, sha):
+    from cudacompress_b200 import fields
+    nz, ny, nx = shape
+    v = fields.turbulence_field(max(shape), 64, 8, seed=int(seed))[:nz, :ny, :nx].copy()
+    assert hashlib.sha256(v.tobytes()).digest() == bytes(sha), "field generator changed"
+    return v
+
+
+@pytest.mark.parametrize("name", VOLUME)
+def test_oracle_volume_codec_matches_reference(gold, oracle, name):
+    levels, rle, qf = (int(x) for x in gold[f"{name}_meta"])
+    q = float(gold[f"{name}_q"][0])
+    v = regen(SHAPES[name], gold[f"{name}_seed"][0], gold[f"{name}_insha"])
+    words, bits = oracle.compress_volume(v, levels, q, rle_only_level0=rle, quant_first=qf)
+    ref = gold[f"{name}_words"]
+    assert bits == ref.size * 32 and np.array_equal(words, ref)
+    if f"{name}_rec" in gold.files:
+        rec = oracle.decompress_volume(ref, ref.size * 32, v.shape, levels, q, rle_only_level0=rle, quant_first=qf)
+        assert np.array_equal(rec.view(np.uint32), gold[f"{name}_rec"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", MULTI)
+def test_oracle_multichannel_matches_reference(gold, oracle, name):
+    levels, rle, qf, count = (int(x) for x in gold[f"{name}_meta"])
+    qs = gold[f"{name}_q"]
+    for k in range(count):
+        v = regen(SHAPES[name], gold[f"{name}_seed{k}"][0], gold[f"{name}_insha{k}"])
+        w = gold[f"{name}_words{k}"]
+        words, _ = oracle.compress_volume(v, levels, float(qs[k]), rle_only_level0=rle, quant_first=qf)
+        assert np.array_equal(words, w), k
+        rec = oracle.decompress_volume(w, w.size * 32, v.shape, levels, float(qs[k]), rle_only_level0=rle,
+                                       quant_first=qf)
+        assert np.array_equal(rec.view(np.uint32), gold[f"{name}_rec{k}"].view(np.uint32)), k
+
+
+def test_quant_first_round_trip_bound(oracle):
+    """Size-independent property of quant-first for any level count (the
+    integer transform is reversible): every output is k * step, and within
+    step / 2 of the input (midtread quantization)."""
+    from cudacompress_b200 import fields
+    v = fields.turbulence_field(64, 64, 8, seed=77)[:32, :32, :64].copy()
+    step = 0.04
+    for levels in (1, 2, 3):
+        words, bits = oracle.compress_volume(v, levels, step, quant_first=True)
+        rec = oracle.decompress_volume(words, bits, v.shape, levels, step, quant_first=True)
+        k = rec / np.float32(step)
+        assert np.array_equal(k, np.round(k)), levels
+        assert np.abs(rec - v).max() <= step / 2 * (1 + 1e-5), levels
