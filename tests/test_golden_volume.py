@@ -82,6 +82,6 @@ def test_quant_first_round_trip_bound(oracle):
     for levels in (1, 2, 3):
         words, bits = oracle.compress_volume(v, levels, step, quant_first=True)
         rec = oracle.decompress_volume(words, bits, v.shape, levels, step, quant_first=True)
-        k = rec / np.float32(step)
-        assert np.array_equal(k, np.round(k)), levels
+        k = np.round(rec / np.float32(step)).astype(np.float32)
+        assert np.array_equal(rec, k * np.float32(step)), levels
         assert np.abs(rec - v).max() <= step / 2 * (1 + 1e-5), levels
