@@ -60,6 +60,16 @@ _SIGS = {
     "cc_get_max_abs": (c_int, [c_vp, c_vp, c_u32, c_vp]),
     "cc_compress_volume_float": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_vp, c_u64, c_u32p]),
     "cc_decompress_volume_float": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_vp, c_u32]),
+    "cc_compress_volume_float_ex": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_u32, c_vp, c_u64,
+                                            c_u32p]),
+    "cc_decompress_volume_float_ex": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_u32, c_vp, c_u32]),
+    "cc_decompress_volume_float_multichannel": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32, c_u32]),
+    "cc_compress_volume_float_quant_first": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_u32, c_vp,
+                                                     c_u64, c_u32p]),
+    "cc_decompress_volume_float_quant_first": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_float, c_u32, c_vp,
+                                                       c_u32]),
+    "cc_decompress_volume_float_quant_first_multichannel": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32,
+                                                                    c_u32]),
     "cc_compress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u64, c_u32p]),
     "cc_decompress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u32]),
     "cc_volume_batch_create": (c_int, [c_vp, c_u32, c_u32p, c_u32, ctypes.POINTER(c_float), ctypes.POINTER(c_vp)]),

@@ -288,25 +288,80 @@ def volume_stream_capacity_words(nx, ny, nz, log2max=14) -> int:
     return int(n * (log2max + 8) // 32 + 64 * 1024)
 
 
+RLE_ONLY_LEVEL0 = 1   # CC_VOLUME_RLE_ONLY_LEVEL0 (doRLEOnlyOnLvl0)
+
+
 def compress_volume_float(inst: Instance, volume: torch.Tensor, levels: int, q0: float,
-                          out_words: Optional[torch.Tensor] = None):
+                          out_words: Optional[torch.Tensor] = None, rle_only_level0: bool = False):
     """Lossy volume codec (CompressVolume.cpp:312-409).  volume: (z, y, x)
-    float32 CUDA tensor.  Returns (words tensor on the device, bit size)."""
+    float32 CUDA tensor.  rle_only_level0: doRLEOnlyOnLvl0 (levels above 0
+    with encodeHuff).  Returns (words tensor on the device, bit size)."""
     nz, ny, nx = volume.shape
     if out_words is None:
         out_words = torch.empty(volume_stream_capacity_words(nx, ny, nz), dtype=torch.int32, device=volume.device)
     bits = ctypes.c_uint32()
-    check(lib().cc_compress_volume_float(inst.handle, volume.data_ptr(), nx, ny, nz, levels, q0,
-                                         out_words.data_ptr(), out_words.numel(), ctypes.byref(bits)),
-          "compressVolumeFloat")
+    check(lib().cc_compress_volume_float_ex(inst.handle, volume.data_ptr(), nx, ny, nz, levels, q0,
+                                            RLE_ONLY_LEVEL0 if rle_only_level0 else 0, out_words.data_ptr(),
+                                            out_words.numel(), ctypes.byref(bits)), "compressVolumeFloat")
     return out_words, bits.value
 
 
 def decompress_volume_float(inst: Instance, out: torch.Tensor, levels: int, q0: float, words: torch.Tensor,
-                            bit_size: int) -> None:
+                            bit_size: int, rle_only_level0: bool = False) -> None:
     nz, ny, nx = out.shape
-    check(lib().cc_decompress_volume_float(inst.handle, out.data_ptr(), nx, ny, nz, levels, q0, words.data_ptr(),
-                                           bit_size), "decompressVolumeFloat")
+    check(lib().cc_decompress_volume_float_ex(inst.handle, out.data_ptr(), nx, ny, nz, levels, q0,
+                                              RLE_ONLY_LEVEL0 if rle_only_level0 else 0, words.data_ptr(), bit_size),
+          "decompressVolumeFloat")
+
+
+def compress_volume_float_quant_first(inst: Instance, volume: torch.Tensor, levels: int, step: float,
+                                      out_words: Optional[torch.Tensor] = None, rle_only_level0: bool = False):
+    """Quantize-first lossy codec (CompressVolume.cpp:651-757): uniform
+    quantization to short, integer DWT, symbols; error <= step / 2."""
+    nz, ny, nx = volume.shape
+    if out_words is None:
+        out_words = torch.empty(volume_stream_capacity_words(nx, ny, nz, 16), dtype=torch.int32,
+                                device=volume.device)
+    bits = ctypes.c_uint32()
+    check(lib().cc_compress_volume_float_quant_first(inst.handle, volume.data_ptr(), nx, ny, nz, levels, step,
+                                                     RLE_ONLY_LEVEL0 if rle_only_level0 else 0,
+                                                     out_words.data_ptr(), out_words.numel(), ctypes.byref(bits)),
+          "compressVolumeFloatQuantFirst")
+    return out_words, bits.value
+
+
+def decompress_volume_float_quant_first(inst: Instance, out: torch.Tensor, levels: int, step: float,
+                                        words: torch.Tensor, bit_size: int, rle_only_level0: bool = False) -> None:
+    nz, ny, nx = out.shape
+    check(lib().cc_decompress_volume_float_quant_first(inst.handle, out.data_ptr(), nx, ny, nz, levels, step,
+                                                       RLE_ONLY_LEVEL0 if rle_only_level0 else 0, words.data_ptr(),
+                                                       bit_size), "decompressVolumeFloatQuantFirst")
+
+
+class _Channel(ctypes.Structure):
+    _fields_ = [("d_volume", ctypes.c_void_p), ("d_words", ctypes.c_void_p), ("bit_size", ctypes.c_uint32),
+                ("quant_step", ctypes.c_float)]
+
+
+def decompress_volume_float_multichannel(inst: Instance, outs, words, bit_sizes, steps, levels: int,
+                                         rle_only_level0: bool = False, quant_first: bool = False) -> None:
+    """decompressVolumeFloat(QuantFirst)MultiChannel (CompressVolume.cpp:518-648,
+    863-988): outs, words (device tensors), bit sizes and steps per channel;
+    all channels the same shape."""
+    n = len(outs)
+    if not (len(words) == len(bit_sizes) == len(steps) == n) or n == 0:
+        raise ValueError("one stream, bit size and step per channel")
+    shape = tuple(outs[0].shape)
+    if any(tuple(o.shape) != shape for o in outs):
+        raise ValueError("all channels must have the same shape")
+    nz, ny, nx = shape
+    ch = (_Channel * n)(*[_Channel(o.data_ptr(), w.data_ptr(), int(b), float(s))
+                          for o, w, b, s in zip(outs, words, bit_sizes, steps)])
+    flags = RLE_ONLY_LEVEL0 if rle_only_level0 else 0
+    f = lib().cc_decompress_volume_float_quant_first_multichannel if quant_first \
+        else lib().cc_decompress_volume_float_multichannel
+    check(f(inst.handle, ctypes.cast(ch, ctypes.c_void_p), n, nx, ny, nz, levels, flags),
+          "decompressVolumeFloatMultiChannel")
 
 
 def compress_heightfield(inst: Instance, image: torch.Tensor, levels: int, out_words: Optional[torch.Tensor] = None):

@@ -191,6 +191,46 @@ int cc_compress_volume_float(cc_instance* inst, const float* d_volume, uint32_t 
 int cc_decompress_volume_float(cc_instance* inst, float* d_volume, uint32_t size_x, uint32_t size_y,
                                uint32_t size_z, uint32_t levels, float quant_step_level0, const uint32_t* d_words,
                                uint32_t bit_size);
+/* Variants of examples/CompressVolume.h:60-79.  flags: CC_VOLUME_RLE_ONLY_LEVEL0
+ * (doRLEOnlyOnLvl0: the levels above 0 code their bands with encodeHuff
+ * instead of encodeRLHuff, CompressVolume.cpp:389-395, 491-495). */
+#define CC_VOLUME_RLE_ONLY_LEVEL0 1u
+int cc_compress_volume_float_ex(cc_instance* inst, const float* d_volume, uint32_t size_x, uint32_t size_y,
+                                uint32_t size_z, uint32_t levels, float quant_step_level0, uint32_t flags,
+                                uint32_t* d_words, uint64_t capacity_words, uint32_t* bit_size);
+int cc_decompress_volume_float_ex(cc_instance* inst, float* d_volume, uint32_t size_x, uint32_t size_y,
+                                  uint32_t size_z, uint32_t levels, float quant_step_level0, uint32_t flags,
+                                  const uint32_t* d_words, uint32_t bit_size);
+/* One channel of a multi-channel decode (VolumeChannel, CompressVolume.h:36-42):
+ * its output volume, its device bit stream and its quantization step. */
+typedef struct cc_volume_channel {
+    float* d_volume;
+    const uint32_t* d_words;
+    uint32_t bit_size;
+    float quant_step;
+} cc_volume_channel;
+/* decompressVolumeFloatMultiChannel (CompressVolume.cpp:518-648): `count`
+ * volumes of the same sizes; all lowpass streams in one decode call, each
+ * level's bands of all channels in one call.  The instance needs
+ * 7 * count streams.  Results equal `count` single-channel decodes. */
+int cc_decompress_volume_float_multichannel(cc_instance* inst, const cc_volume_channel* channels, uint32_t count,
+                                            uint32_t size_x, uint32_t size_y, uint32_t size_z, uint32_t levels,
+                                            uint32_t flags);
+/* compressVolumeFloatQuantFirst / decompressVolumeFloatQuantFirst(MultiChannel)
+ * (CompressVolume.cpp:651-988): uniform quantization to short, integer DWT,
+ * symbolize, then the same stream layout; error <= quant_step / 2.  The
+ * reference's decoder reads the wrong ping-pong buffer for odd level counts;
+ * this one inverts every level count correctly (streams are identical). */
+int cc_compress_volume_float_quant_first(cc_instance* inst, const float* d_volume, uint32_t size_x,
+                                         uint32_t size_y, uint32_t size_z, uint32_t levels, float quant_step,
+                                         uint32_t flags, uint32_t* d_words, uint64_t capacity_words,
+                                         uint32_t* bit_size);
+int cc_decompress_volume_float_quant_first(cc_instance* inst, float* d_volume, uint32_t size_x, uint32_t size_y,
+                                           uint32_t size_z, uint32_t levels, float quant_step, uint32_t flags,
+                                           const uint32_t* d_words, uint32_t bit_size);
+int cc_decompress_volume_float_quant_first_multichannel(cc_instance* inst, const cc_volume_channel* channels,
+                                                        uint32_t count, uint32_t size_x, uint32_t size_y,
+                                                        uint32_t size_z, uint32_t levels, uint32_t flags);
 int cc_compress_heightfield(cc_instance* inst, const int16_t* d_image, uint32_t size_x, uint32_t size_y,
                             uint32_t levels, uint32_t* d_words, uint64_t capacity_words, uint32_t* bit_size);
 int cc_decompress_heightfield(cc_instance* inst, int16_t* d_image, uint32_t size_x, uint32_t size_y,
