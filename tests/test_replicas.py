@@ -1,7 +1,8 @@
-"""The multi-GPU path is replicas only (no exchange step): two gloo ranks on
-the CPU check the host-side pieces bench.py uses for N > 1 - every rank draws
-distinct inputs, the job's step time is the maximum over ranks, and the
-whole-job throughput counts all ranks' bytes over that maximum."""
+"""The multi-GPU path has no exchange step: two gloo ranks on the CPU check
+the host-side pieces bench.py uses for N > 1 - every rank draws distinct
+inputs (replicas), bricks are partitioned by byte size and their results
+gathered on the host (partition), the job's step time is the maximum over
+ranks, and the whole-job throughput counts all ranks' bytes over it."""
 import os
 import socket
 import sys
@@ -40,6 +41,12 @@ def rank_main(rank, world, port, out_dir):
         gbs = replicas.job_gbs(world, 1 << 20, got[0])
         np.save(os.path.join(out_dir, f"rank{rank}.npy"), np.array(got + [gbs], np.float64))
         np.save(os.path.join(out_dir, f"vol{rank}.npy"), vols[0])
+        # partition of a brick set; each rank "codes" its bricks (a stand-in
+        # result: the brick's byte size + 1), then the host-side gather
+        sizes = [int(s) for s in np.random.default_rng(3).integers(1, 1000, 37)]
+        mine_idx = replicas.partition_by_bytes(sizes, world)[rank]
+        got_all = replicas.gather_on_host({i: sizes[i] + 1 for i in mine_idx}, dist)
+        np.save(os.path.join(out_dir, f"gather{rank}.npy"), np.array([got_all[i] for i in range(len(sizes))]))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -55,6 +62,21 @@ def test_two_rank_replicas(tmp_path):
     assert r0[2] == pytest.approx(2 * (1 << 20) / 15e-3 / 1e9)
     v0, v1 = np.load(tmp_path / "vol0.npy"), np.load(tmp_path / "vol1.npy")
     assert v0.shape == v1.shape and not np.array_equal(v0, v1)   # distinct inputs per rank
+    sizes = [int(s) for s in np.random.default_rng(3).integers(1, 1000, 37)]
+    for r in range(world):   # every rank holds every brick's result after the gather
+        assert list(np.load(tmp_path / f"gather{r}.npy")) == [s + 1 for s in sizes]
+
+
+def test_partition_by_bytes():
+    rng = np.random.default_rng(11)
+    for world in (1, 2, 3, 8):
+        sizes = [int(s) for s in rng.integers(1, 10 ** 6, 500)]
+        parts = replicas.partition_by_bytes(sizes, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(sizes)))                 # each brick exactly once
+        loads = [sum(sizes[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(sizes)           # balanced to within one brick
+    assert replicas.partition_by_bytes([5, 5, 5], 4) == [[0], [1], [2], []]
 
 
 def test_single_process_identity():
