@@ -325,18 +325,25 @@ static int runMaybeGraph(cc_volume_batch* b, Enqueue fn, std::map<u32, cudaGraph
         // launched on the instance stream.
         if (!b->captureStream)
             CC_TRY_CUDA(cudaStreamCreateWithFlags(&b->captureStream, cudaStreamNonBlocking), "capture stream");
-        const bool timing = I->timing;
+        const bool timing = I->timing, timingLP = b->ILP->timing;
         cudaStream_t userStream = I->stream;
         I->timing = false;   // no event records inside the graph
+        b->ILP->timing = false;
         I->stream = b->captureStream;
         cudaError_t e = cudaStreamBeginCapture(I->stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) { I->stream = userStream; I->timing = timing; return cudaFail(e, "begin capture"); }
+        if (e != cudaSuccess) {
+            I->stream = userStream;
+            I->timing = timing;
+            b->ILP->timing = timingLP;
+            return cudaFail(e, "begin capture");
+        }
         const unsigned long long c0 = cc_kernel_launches();
         int rc = fn(b);
         cudaGraph_t g = nullptr;
         e = cudaStreamEndCapture(I->stream, &g);
         I->stream = userStream;
         I->timing = timing;
+        b->ILP->timing = timingLP;
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return cudaFail(e, "end capture");
         launches = unsigned(cc_kernel_launches() - c0);
@@ -410,7 +417,10 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     InstanceCaps capsLP{count, std::max<u64>(LPsum, 1), std::min<u64>(u64(2 * count) * user->bins, u64(1) << 26)};
     rc = createInstance(&b->ILP, user->device, count, maxLP, user->codingBlockSize, user->log2Max, &capsLP);
     if (rc) { cc_volume_batch_destroy(b); return rc; }
-    b->ILP->timing = false;
+    b->ILP->timing = false;   // follows the user instance's timing on each compress call
+    // the lowpass tables are built while the highpass encode runs: one SM each
+    b->ILP->tableBuildSoloSM = true;
+    cudaDeviceGetAttribute(&b->ILP->smCount, cudaDevAttrMultiProcessorCount, user->device);
     // kernel attributes set once here, so that captured launches do not set them
     rc = prepareKernelAttributes(I);
     if (!rc) rc = prepareKernelAttributes(b->ILP);
@@ -789,6 +799,7 @@ int cc_volume_batch_compress(cc_volume_batch* b, const float* const* dVolumes) {
     cudaSetDevice(b->I->device);
     b->I->stream = b->hasOwnStream ? b->ownStream : b->user->stream;
     b->I->timing = b->user->timing;
+    b->ILP->timing = b->user->timing;
     int rc = uploadTable(b, reinterpret_cast<const void* const*>(dVolumes), b->inTab);
     if (rc) return rc;
     return runMaybeGraph(b, batchEnqueueCompress, b->gCompress, b->launchesCompress);
@@ -863,7 +874,8 @@ int cc_volume_batch_status(cc_volume_batch* b) {
 }
 
 // Resolves and folds the batch's internal timing sections into the user
-// instance (cc_timing_* report both).
+// instance (cc_timing_* report both); the lowpass encode's own sections
+// (on the side stream) get the prefix "lp.".
 void cc_volume_batch_collect_timings(cc_volume_batch* b) {
     if (!b) return;
     b->I->resolveTimings();
@@ -873,6 +885,13 @@ void cc_volume_batch_collect_timings(cc_volume_batch* b) {
         acc.second += kv.second.second;
     }
     b->I->timings.clear();
+    b->ILP->resolveTimings();
+    for (auto& kv : b->ILP->timings) {
+        auto& acc = b->user->timings[std::string("lp.") + kv.first];
+        acc.first += kv.second.first;
+        acc.second += kv.second.second;
+    }
+    b->ILP->timings.clear();
 }
 
 }  // extern "C"

@@ -234,6 +234,8 @@ struct cc_instance {
     ccb::u32* stagedWords = nullptr;          // decode input words (host bit streams)
     ccb::u64 stagedWordsMax = 0;
     ccb::u32* blockSum = nullptr;             // [capBlocks]
+    bool tableBuildSoloSM = false;            // table-build CTAs ask for a whole SM (calls of <= smCount tables)
+    int smCount = 148;
     ccb::u64* decRlTasks = nullptr;           // [capBlocks / 32 + capStreams + 1]: run-length decode warp tasks, then their count
 
     // host staging: ring of slots for uploads, one buffer for downloads

@@ -601,6 +601,22 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     }
 }
 
+// Dynamic shared memory that leaves no room on an SM for another table-build
+// CTA or most other kernels' CTAs: the device's per-block opt-in limit minus
+// the kernel's static shared memory.
+static size_t tableBuildSoloSmem(int device) {
+    static size_t cached[64] = {};
+    if (device < 0 || device >= 64) return 0;
+    if (!cached[device]) {
+        int optin = 0;
+        cudaFuncAttributes fa{};
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+        cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(k_tableBuild));
+        cached[device] = optin > int(fa.sharedSizeBytes) ? size_t(optin) - fa.sharedSizeBytes : 0;
+    }
+    return cached[device];
+}
+
 // ---------------------------------------------------------------------------
 // Huffman encode (Huffman.cu:73-187): per coding block bit totals, per table
 // scan to block offsets, then packing.  One warp per coding block.
@@ -896,7 +912,11 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) { SectionTimer t(I, "enc.rle_write_hist", st); k_write<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
-    const size_t buildSmem = sizeof(u64) * (p.heapCap + 2) + 3 * sizeof(u32) * size_t(p.heapCap);
+    size_t buildSmem = sizeof(u64) * (p.heapCap + 2) + 3 * sizeof(u32) * size_t(p.heapCap);
+    // an instance whose tables run beside other kernels (the batched codec's
+    // lowpass encode) may ask for an SM of its own per table: the sequential
+    // heap merge is latency-bound and loses issue slots to co-resident CTAs
+    if (I->tableBuildSoloSM && p.T <= u32(I->smCount)) buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
     CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
     { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
@@ -922,7 +942,8 @@ int prepareDecodeAttributes(cc_instance* I);
 
 int prepareKernelAttributes(cc_instance* I) {
     const u32 heapCap = std::min<u32>(I->leavesMax, kBuildSmemLeaves);
-    const size_t buildSmem = sizeof(u64) * (heapCap + 2) + 3 * sizeof(u32) * size_t(heapCap);
+    size_t buildSmem = sizeof(u64) * (heapCap + 2) + 3 * sizeof(u32) * size_t(heapCap);
+    if (I->tableBuildSoloSM) buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
     CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
     return prepareDecodeAttributes(I);
