@@ -236,6 +236,32 @@ int cc_compress_heightfield(cc_instance* inst, const int16_t* d_image, uint32_t 
 int cc_decompress_heightfield(cc_instance* inst, int16_t* d_image, uint32_t size_x, uint32_t size_y,
                               uint32_t levels, const uint32_t* d_words, uint32_t bit_size);
 
+/* ---- stream container (B200 addition; no counterpart in the reference) ----
+ * The reference's example stores a stream as raw concatenated u32 words
+ * (examples.cpp:527-536), leaving codec, levels, sizes and steps to the
+ * caller.  This container keeps them with the streams (layout in
+ * cudacompress_b200/csrc/container.cu).  Host memory only. */
+typedef struct cc_container_info {
+    uint32_t codec;               /* 0 float volume, 1 quant-first volume, 2 heightfield */
+    uint32_t flags;               /* CC_VOLUME_RLE_ONLY_LEVEL0 */
+    uint32_t levels;
+    uint32_t coding_block_size;
+    uint32_t log2_symbol_count;
+} cc_container_info;
+typedef struct cc_container_entry {
+    uint32_t size_x, size_y, size_z;
+    float quant_step;
+    uint64_t bit_size;
+    const uint32_t* words;        /* host; on read: points into the container */
+} cc_container_entry;
+/* Bytes of a container holding `count` streams of the given bit sizes. */
+uint64_t cc_container_bytes(uint32_t count, const uint64_t* bit_sizes);
+int cc_container_write(void* dst, uint64_t capacity, const cc_container_info* info, const cc_container_entry* entries,
+                       uint32_t count, uint64_t* written);
+/* entries NULL: *count receives the entry count only. */
+int cc_container_read(const void* src, uint64_t bytes, cc_container_info* info, cc_container_entry* entries,
+                      uint32_t capacity, uint32_t* count);
+
 /* ---- batched volume codec (B200 addition; callers: CompressVolume.cpp:312-516) ----
  * Compresses and decompresses `count` float32 volumes of any sizes (each
  * divisible by 2^levels, coarsest level >= 8) with one launch per stage for

@@ -124,3 +124,22 @@ def test_unknown_flags_rejected(inst):
                                                 w.numel(), None)
     assert bits != 0
     assert "flags" in cc.last_error()
+
+
+def test_container_round_trip_decodes(oracle, inst):
+    """Streams written to a container with their sizes and steps decode from
+    the container alone to the same reconstruction."""
+    from cudacompress_b200 import container as ct
+    vols = [fields.turbulence_field(32, 64, 8, seed=s)[:16, :16, :32].copy() for s in (71, 72)]
+    steps = [0.05, 0.03]
+    ss = []
+    for v, q in zip(vols, steps):
+        w, bits = compress(inst, v, 2, q, 1, 1)
+        ss.append(ct.Stream(v.shape, q, bits, w))
+    info, back = ct.unpack(ct.pack(ct.ContainerInfo(ct.QUANT_FIRST, cc.RLE_ONLY_LEVEL0, 2, 128, 14), ss))
+    assert info.codec == ct.QUANT_FIRST and info.flags == cc.RLE_ONLY_LEVEL0 and info.levels == 2
+    for v, s in zip(vols, back):
+        rec = decompress(inst, s.words, s.shape, info.levels, s.quant_step, info.flags & 1, 1)
+        want = oracle.decompress_volume(s.words, s.bit_size, v.shape, 2, s.quant_step, rle_only_level0=True,
+                                        quant_first=True)
+        assert np.array_equal(rec.view(np.uint32), want.view(np.uint32))
