@@ -331,7 +331,8 @@ METRIC = "enc/dec GB/s raw (%HBM peak); batched vs per-brick GB/s at fixed PSNR;
 # per-unit algorithmic bytes of the sections the roofline may pick
 SECTION_UNITS = {
     "batch.dwt_forward": "per pass (k_bRows / k_bCols, 3 per level): its input read once + its output written "
-                         "once, 8 B/voxel",
+                         "once, 8 B/voxel; the Z pass stores the 7 highpass octants as 2-byte symbols (quantization "
+                         "fused) and the LLL octant as float, or as symbols at the coarsest level",
     "batch.dwt_inverse": "per pass (k_bCols from symbols, k_bCols, k_bRows per level): 2 B/symbol + 4 B/lowpass "
                          "voxel in and 4 B/voxel out for the first, 8 B/voxel for the others",
 }
@@ -346,7 +347,8 @@ def section_bytes(name, wl, coded_bytes, counts):
     lp = vols[-1] // 8
     m = {
         "pipe.dwt_forward": sum(8 * v for v in vols) * C,
-        "batch.dwt_forward": sum(3 * 8 * v for v in vols) * C,
+        "batch.dwt_forward": sum(2 * 8 * v + 4 * v + 2 * (7 * v // 8) + (2 if i == len(vols) - 1 else 4) * (v // 8)
+                                 for i, v in enumerate(vols)) * C,
         "batch.dwt_inverse": sum(4 * (v // 8) + 2 * (7 * v // 8) + 4 * v + 2 * 8 * v for v in vols) * C,
         "batch.quantize": (hp + lp) * 6 * C,
         "pipe.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,

@@ -224,10 +224,8 @@ static int batchEnqueueCompress(cc_volume_batch* b) {
         prefixOf(b->fwdY[l], k, nd, ctas);
         launchBatchCols(b->fwdY[l].d, b->fwdY[l].map, ctas, false, false, st);
         prefixOf(b->fwdZ[l], k, nd, ctas);
-        launchBatchCols(b->fwdZ[l].d, b->fwdZ[l].map, ctas, false, false, st);
+        launchBatchCols(b->fwdZ[l].d, b->fwdZ[l].map, ctas, false, false, st, true);   // + deadzone quantization
     }
-    prefixOf(b->quant, k, nd, ctas);
-    { SectionTimer t(I, "batch.quantize", st); launchBatchQuant(b->quant.d, b->quant.map, ctas, false, st); }
     // fork: the lowpass streams on the side stream
     cc_instance* ILP = b->ILP;
     ILP->stream = b->sideStream;
@@ -498,12 +496,21 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             c.sa = sx; c.sc = sx * syz;
             c.da = sx; c.dc = sx * syz;
             addCols(fy[l], fyC[l], c);
-            // Z: t2 -> level l coefficients
+            // Z: t2 -> level l coefficients, quantized in the store: the LLL
+            // octant stays float (next level's input) except at the coarsest
+            // level, where it is the lowpass band
             BColDesc cz = c;
             cz.src = t2(v); cz.dst = lev(l, v);
             cz.na = sz; cz.nc = syz;
             cz.sa = sx * syz; cz.sc = sx;
             cz.da = sx * syz; cz.dc = sx;
+            cz.symOut = sy(v) + sl[v].level[l];
+            cz.lpSymOut = sy(v) + sl[v].lp;
+            cz.bandStride = sl[v].bandStride[l];
+            cz.hx = sx / 2; cz.hy = syz / 2; cz.hz = sz / 2;
+            cz.inv = 1.0f / (b->q0[v] / float(1u << l));              // Quantize.cu:90: reciprocal on the host
+            cz.invLP = 1.0f / (b->q0[v] / float(1u << (L - 1)));
+            cz.lastLevel = l + 1 == L ? 1 : 0;
             addCols(fz[l], fzC[l], cz);
             // inverse of level l: Z from symbols (lowpass = level l+1 reconstruction) -> t2, Y -> t1, X -> level l
             BColDesc ic{};
@@ -634,7 +641,13 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
         for (auto& d : fr[l]) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); }
         for (auto& d : ir[l]) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); }
         for (auto* vv : {&fy[l], &fz[l], &iz[l], &iy[l]})
-            for (auto& d : *vv) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); d.bands = rebaseS(d.bands); }
+            for (auto& d : *vv) {
+                d.src = rebaseF(d.src);
+                d.dst = rebaseF(d.dst);
+                d.bands = rebaseS(d.bands);
+                d.symOut = rebaseS(d.symOut);
+                d.lpSymOut = rebaseS(d.lpSymOut);
+            }
     }
     for (auto& d : qd) { d.src = rebaseF(d.src); d.sym = rebaseS(d.sym); }
     for (auto& d : dq) { d.sym = rebaseS(d.sym); d.dstF = rebaseF(d.dstF); }

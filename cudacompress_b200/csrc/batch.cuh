@@ -35,6 +35,14 @@ struct BColDesc {
     u64 bandStride;
     float step;
     int hx, hy, hz, lpRow, lpSlice;
+    // last forward pass of a level (axis Z) with quantization fused into the
+    // store: the 7 highpass octants go to symOut (band b-1 at b-1 bandStride)
+    // quantized with inv; the LLL octant stays float in dst, or - at the
+    // coarsest level - goes to lpSymOut quantized with invLP
+    u16* symOut;
+    u16* lpSymOut;
+    float inv, invLP;
+    int lastLevel;
     u32 tilesX, tilesA;
     u32 ctaOff;
 };
@@ -61,7 +69,8 @@ constexpr int kBQuantPerCta = 4096;
 // Descriptor arrays and CTA maps are device pointers; ctas = CTA count.
 void launchBatchRows(const BRowDesc* d, const u32* map, u32 ctas, bool inverse, const float* const* inTab,
                      float* const* outTab, cudaStream_t st);
-void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st);
+void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st,
+                     bool quantizeStore = false);
 void launchBatchQuant(const BQuantDesc* d, const u32* map, u32 ctas, bool dequantize, cudaStream_t st);
 
 // Row tiling of an X pass over an nx-wide level: tile width, rows per CTA.

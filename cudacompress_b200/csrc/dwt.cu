@@ -538,7 +538,43 @@ __device__ __forceinline__ float2 bandPair(const BColDesc& D, int x, int y, int 
     return make_float2((float(q0) + signI(q0) * 0.5f) * D.step, (float(q1) + signI(q1) * 0.5f) * D.step);
 }
 
-template <bool kInverse, int kParity>
+// One sample of the fused store (see BColDesc::symOut): (x, y, z) in the
+// level's [L|H] layout.  Deadzone quantization as k_bQuant's
+// (Quantize.cuh:55-59, reciprocal from the host).
+__device__ __forceinline__ void quantStoreOne(const BColDesc& D, int x, int y, int z, float v) {
+    const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
+    const int b = bx + 2 * by + 4 * bz;
+    if (b == 0 && !D.lastLevel) {
+        D.dst[size_t(x) + size_t(z) * D.da + size_t(y) * D.dc] = v;
+        return;
+    }
+    const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
+    u16* base = b == 0 ? D.lpSymOut : D.symOut + u64(b - 1) * D.bandStride;
+    base[(u64(lz) * D.hy + ly) * D.hx + lx] = u16(symbolizeI(int(v * (b == 0 ? D.invLP : D.inv))));
+}
+
+// The samples (x, x + 1), x even; with an even half width both lie in one
+// octant at an even offset (one float2 or one 4-byte symbol pair).
+__device__ __forceinline__ void quantStorePair(const BColDesc& D, int x, int y, int z, float2 v) {
+    if (D.hx & 1) {
+        quantStoreOne(D, x, y, z, v.x);
+        quantStoreOne(D, x + 1, y, z, v.y);
+        return;
+    }
+    const int bx = x >= D.hx, by = y >= D.hy, bz = z >= D.hz;
+    const int b = bx + 2 * by + 4 * bz;
+    if (b == 0 && !D.lastLevel) {
+        *reinterpret_cast<float2*>(D.dst + size_t(x) + size_t(z) * D.da + size_t(y) * D.dc) = v;
+        return;
+    }
+    const int lx = x - bx * D.hx, ly = y - by * D.hy, lz = z - bz * D.hz;
+    u16* base = b == 0 ? D.lpSymOut : D.symOut + u64(b - 1) * D.bandStride;
+    const float inv = b == 0 ? D.invLP : D.inv;
+    const u32 s0 = symbolizeI(int(v.x * inv)) & 0xFFFFu, s1 = symbolizeI(int(v.y * inv)) & 0xFFFFu;
+    *reinterpret_cast<u32*>(base + (u64(lz) * D.hy + ly) * D.hx + lx) = s0 | (s1 << 16);
+}
+
+template <bool kInverse, int kParity, bool kQuantize = false>
 __device__ __forceinline__ void colOutputs(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x, int c,
                                            int a0) {
     for (int k = ty; k < kBColTileA; k += 8) {
@@ -553,7 +589,8 @@ __device__ __forceinline__ void colOutputs(const BColDesc& D, const float2 (*s)[
         }
         const float2 r = make_float2(fir9c<kInverse, kParity>(v0), fir9c<kInverse, kParity>(v1));
         const int o = kInverse ? a : splitPos(a, D.na);
-        *reinterpret_cast<float2*>(D.dst + size_t(x) + size_t(o) * D.da + size_t(c) * D.dc) = r;
+        if (kQuantize) quantStorePair(D, x, c, o, r);   // axis Z: a = z, c = y
+        else *reinterpret_cast<float2*>(D.dst + size_t(x) + size_t(o) * D.da + size_t(c) * D.dc) = r;
     }
 }
 
@@ -563,7 +600,7 @@ __device__ __forceinline__ void colOutputs(const BColDesc& D, const float2 (*s)[
 // the row step 8 are even), so its taps are compile-time immediates.
 static_assert(kBColTileX == 64, "a column-pass CTA has 32 threads of column pairs per row");
 
-template <bool kInverse, bool kSymbols>
+template <bool kInverse, bool kSymbols, bool kQuantize = false>
 __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ descs, const u32* __restrict__ map) {
     __shared__ float2 s[kBColTileA + 8][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -596,8 +633,8 @@ __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ desc
     for (int i = 0; i < kLoads; ++i) s[ty + 8 * i][tx] = vals[i];
     __syncthreads();
     if (x >= nx) return;
-    if ((a0 + ty) & 1) colOutputs<kInverse, 1>(D, s, tx, ty, x, c, a0);
-    else colOutputs<kInverse, 0>(D, s, tx, ty, x, c, a0);
+    if ((a0 + ty) & 1) colOutputs<kInverse, 1, kQuantize>(D, s, tx, ty, x, c, a0);
+    else colOutputs<kInverse, 0, kQuantize>(D, s, tx, ty, x, c, a0);
 }
 
 // Quantization of one band to u16 symbols (deadzone, Quantize.cuh:55-59), or
@@ -677,10 +714,12 @@ void launchBatchRows(const BRowDesc* d, const u32* map, u32 ctas, bool inverse, 
     countLaunch();
 }
 
-void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st) {
+void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st,
+                     bool quantizeStore) {
     if (!ctas) return;
     const dim3 blk(32, 8);
-    if (fromSymbols) k_bCols<true, true><<<ctas, blk, 0, st>>>(d, map);
+    if (quantizeStore) k_bCols<false, false, true><<<ctas, blk, 0, st>>>(d, map);
+    else if (fromSymbols) k_bCols<true, true><<<ctas, blk, 0, st>>>(d, map);
     else if (inverse) k_bCols<true, false><<<ctas, blk, 0, st>>>(d, map);
     else k_bCols<false, false><<<ctas, blk, 0, st>>>(d, map);
     countLaunch();
