@@ -72,6 +72,39 @@ _SIGS = {
                                                                     c_u32]),
     "cc_compress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u64, c_u32p]),
     "cc_decompress_heightfield": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_vp, c_u32]),
+    "cc_dwt_float_forward_from_byte": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int,
+                                               c_int, c_int, c_vp]),
+    "cc_dwt_float_inverse_to_byte": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
+                                             c_int, c_vp]),
+    "cc_dwt_float_inverse_from_symbols_to_byte": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_float, c_int, c_int,
+                                                          c_int, c_int, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_dwt_float2d_forward_lowpass_only_from_byte": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int,
+                                                              c_vp]),
+    "cc_dwt_int_forward_lowpass_only": (c_int, [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp]),
+    "cc_float_to_byte_2d": (c_int, [c_vp, c_u32, c_u32, c_vp, c_u32, c_u32, c_u32, c_vp]),
+    "cc_byte_to_float_2d": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32, c_vp]),
+    "cc_quantize_difference_to_symbols_2d": (c_int, [c_vp, c_vp, c_float, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32,
+                                                     c_int, c_vp]),
+    "cc_quantize_difference_to_symbols_roundtrip_2d": (c_int, [c_vp, c_vp, c_float, c_vp, c_u32, c_u32, c_u32, c_u32,
+                                                               c_u32, c_int, c_vp]),
+    "cc_unquantize_difference_from_symbols_2d": (c_int, [c_vp, c_vp, c_float, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32,
+                                                         c_int, c_vp]),
+    "cc_convert_rgb_to_ycocg": (c_int, [c_vp, c_vp, c_int, c_int, c_vp]),
+    "cc_convert_ycocg_to_rgb": (c_int, [c_vp, c_vp, c_int, c_int, c_vp]),
+    "cc_get_lsb": (c_int, [c_vp, c_vp, c_u32, c_vp]),
+    "cc_remove_lsb": (c_int, [c_vp, c_vp, c_u32, ctypes.c_int16, c_vp]),
+    "cc_append_lsb": (c_int, [c_vp, c_vp, c_u32, ctypes.c_int16, c_vp]),
+    "cc_shift_elems": (c_int, [c_vp, c_u32, ctypes.c_int16, c_vp]),
+    "cc_compress_heightfield_one_level": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp, ctypes.c_int16, c_vp, c_u64,
+                                                  c_u32p]),
+    "cc_decompress_heightfield_one_level": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp, ctypes.c_int16, c_vp, c_u32]),
+    "cc_get_lowpass_heightfield": (c_int, [c_vp, c_int, c_int, c_vp, ctypes.c_int16, c_vp]),
+    "cc_compress_image_one_level": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_vp, c_float, c_vp, c_u64,
+                                            c_u32p]),
+    "cc_decompress_image_one_level": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_vp, c_float, c_vp, c_u32]),
+    "cc_compress_images_one_level": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32]),
+    "cc_decompress_images_one_level": (c_int, [c_vp, c_vp, c_u32, c_u32, c_u32, c_u32, c_u32]),
+    "cc_get_lowpass_image": (c_int, [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp]),
     "cc_container_bytes": (c_u64, [c_u32, ctypes.POINTER(c_u64)]),
     "cc_container_write": (c_int, [c_vp, c_u64, c_vp, c_vp, c_u32, ctypes.POINTER(c_u64)]),
     "cc_container_read": (c_int, [c_vp, c_u64, c_vp, c_vp, c_u32, c_u32p]),

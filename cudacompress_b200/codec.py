@@ -221,6 +221,48 @@ def dwt_float_inverse_from_symbols(dst, buf2, buf1, lowpass, highpass_ptrs: torc
           "dwtFloatInverseFromSymbols")
 
 
+def dwt_float_forward_from_byte(dst, buf2, buf1, src, size_x, size_y, size_z=1, src_channel_count=1,
+                                dst_row_pitch=0, dst_slice_pitch=0, src_row_pitch=0, src_slice_pitch=0, stream=None):
+    """dwtFloat{2D,3D}ForwardFromByte: src is a uint8 tensor (or a view starting
+    at the wanted channel) with src_channel_count interleaved channels."""
+    check(lib().cc_dwt_float_forward_from_byte(_ptr(dst), _ptr(buf2), _ptr(buf1), _ptr(src), size_x, size_y, size_z,
+                                                src_channel_count, dst_row_pitch, dst_slice_pitch, src_row_pitch,
+                                                src_slice_pitch, _stream(stream)), "dwtFloatForwardFromByte")
+
+
+def dwt_float_inverse_to_byte(dst, buf2, buf1, src, size_x, size_y, size_z=1, dst_channel_count=1, dst_row_pitch=0,
+                              dst_slice_pitch=0, src_row_pitch=0, src_slice_pitch=0, stream=None):
+    check(lib().cc_dwt_float_inverse_to_byte(_ptr(dst), _ptr(buf2), _ptr(buf1), _ptr(src), size_x, size_y, size_z,
+                                              dst_channel_count, dst_row_pitch, dst_slice_pitch, src_row_pitch,
+                                              src_slice_pitch, _stream(stream)), "dwtFloatInverseToByte")
+
+
+def dwt_float_inverse_from_symbols_to_byte(dst, buf2, buf1, lowpass, highpass_ptrs: torch.Tensor, symbol_bytes,
+                                           quant_step, size_x, size_y, size_z=1, dst_channel_count=1,
+                                           dst_row_pitch=0, dst_slice_pitch=0, lowpass_row_pitch=0,
+                                           lowpass_slice_pitch=0, stream=None):
+    check(lib().cc_dwt_float_inverse_from_symbols_to_byte(_ptr(dst), _ptr(buf2), _ptr(buf1), _ptr(lowpass),
+                                                           _ptr(highpass_ptrs), symbol_bytes, quant_step, size_x,
+                                                           size_y, size_z, dst_channel_count, dst_row_pitch,
+                                                           dst_slice_pitch, lowpass_row_pitch, lowpass_slice_pitch,
+                                                           _stream(stream)), "dwtFloatInverseFromSymbolsToByte")
+
+
+def dwt_float2d_forward_lowpass_only_from_byte(dst, buf, src, size_x, size_y, src_channel_count=1, dst_row_pitch=0,
+                                               src_row_pitch=0, stream=None):
+    """dwtFloat2DForwardLowpassOnlyFromByte: the LL band only (buf unused)."""
+    check(lib().cc_dwt_float2d_forward_lowpass_only_from_byte(_ptr(dst), _ptr(buf), _ptr(src), size_x, size_y,
+                                                               src_channel_count, dst_row_pitch, src_row_pitch,
+                                                               _stream(stream)),
+          "dwtFloat2DForwardLowpassOnlyFromByte")
+
+
+def dwt_int_forward_lowpass_only(dst, buf, src, size_x, size_y, dst_row_pitch=0, src_row_pitch=0, stream=None):
+    """dwtIntForwardLowpassOnly: the LL band only (buf unused)."""
+    check(lib().cc_dwt_int_forward_lowpass_only(_ptr(dst), _ptr(buf), _ptr(src), size_x, size_y, dst_row_pitch,
+                                                src_row_pitch, _stream(stream)), "dwtIntForwardLowpassOnly")
+
+
 def dwt_int_forward(dst, buf, src, size_x, size_y, size_z=1, dst_row_pitch=0, dst_slice_pitch=0, src_row_pitch=0,
                     src_slice_pitch=0, stream=None):
     check(lib().cc_dwt_int_forward(_ptr(dst), _ptr(buf), _ptr(src), size_x, size_y, size_z, dst_row_pitch,

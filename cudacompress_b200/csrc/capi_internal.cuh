@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <vector>
 
 #include "../../include/cudacompress_b200.h"
 #include "codec.cuh"
@@ -69,6 +70,15 @@ int encodePrepare(cc_instance* I, const EncStream* streams, u32 S, char* slot, s
 int encodeLaunch(cc_instance* I, const EncPlan& plan, u32* out, u64 outCap);
 // Grows the instance's pipeline workspace to at least `bytes` (allocates only when it must grow).
 int ensurePipelineWork(cc_instance* I, size_t bytes);
+// One reference encode call of a codec pipeline: `count` streams from `first`.
+struct EncGroup {
+    u32 first, count;
+};
+// Encodes groups of streams back to back into dWords (pipeline.cu); with
+// groupStart, entry k receives the first word of group k and entry
+// groups.size() the end of the last.
+int encodeGroups(cc_instance* I, const std::vector<EncStream>& streams, const std::vector<EncGroup>& groups,
+                 u32* dWords, u64 cap, u64* wordsOut, std::vector<u64>* groupStart = nullptr);
 int decodeDevice(cc_instance* I, int kind, const u32* const* words, const u32* bitSizes, u32* bitPos, u32 bsCount,
                  const u32* bsIndex, void* const* outs, u32 S, u32 n);
 

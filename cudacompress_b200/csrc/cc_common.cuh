@@ -90,6 +90,16 @@ __device__ __forceinline__ int unsymbolizeI(u32 s) {
 }
 __device__ __forceinline__ float signF(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
 __device__ __forceinline__ float signI(int q) { return q > 0 ? 1.0f : (q < 0 ? -1.0f : 0.0f); }
+// Quantize.cuh:75-131: type 0 deadzone (truncation; centre of the bin back),
+// type 1 uniform (round half away from zero; bin value back).
+__device__ __forceinline__ int quantizeV(float v, float inv, int type) {
+    if (type == 0) return int(v * inv);
+    return int(__fmaf_rn(v, inv, signF(v) * 0.5f));
+}
+__device__ __forceinline__ float unquantizeV(int q, float step, int type) {
+    if (type == 0) return (float(q) + signI(q) * 0.5f) * step;
+    return float(q) * step;
+}
 
 // Warp-aggregated increment of `bins[key]`: lanes with equal keys are merged
 // with match_any so each distinct key issues one shared/global atomic.

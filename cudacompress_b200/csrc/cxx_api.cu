@@ -9,8 +9,10 @@
 #include <cudaCompress/Encode.h>
 #include <cudaCompress/Instance.h>
 #include <cudaCompress/Timing.h>
+#include <cudaCompress/util/Bits.h>
 #include <cudaCompress/util/DWT.h>
 #include <cudaCompress/util/Quantize.h>
+#include <cudaCompress/util/YCoCg.h>
 
 #include "../../include/cudacompress_b200.h"
 
@@ -233,6 +235,40 @@ void dwtFloat3DInverseFromSymbols(float* d, float* b2, float* b1, const float* l
     report(cc_dwt_float_inverse_from_symbols(d, b2, b1, lp, reinterpret_cast<const void* const*>(hp), 4, q, sx, sy, sz,
                                              ch, dr, ds, lr, ls, st), "dwtFloat3DInverseFromSymbols");
 }
+void dwtFloat2DForwardFromByte(float* d, float* b, const byte* s, int sx, int sy, int ch, int dr, int sr, cudaStream_t st) {
+    report(cc_dwt_float_forward_from_byte(d, nullptr, b, s, sx, sy, 1, ch, dr, 0, sr, 0, st), "dwtFloat2DForwardFromByte");
+}
+void dwtFloat3DForwardFromByte(float* d, float* b2, float* b1, const byte* s, int sx, int sy, int sz, int ch, int dr,
+                               int ds, int sr, int ss, cudaStream_t st) {
+    report(cc_dwt_float_forward_from_byte(d, b2, b1, s, sx, sy, sz, ch, dr, ds, sr, ss, st), "dwtFloat3DForwardFromByte");
+}
+void dwtFloat2DInverseToByte(byte* d, float* b, const float* s, int sx, int sy, int ch, int dr, int sr, cudaStream_t st) {
+    report(cc_dwt_float_inverse_to_byte(d, nullptr, b, s, sx, sy, 1, ch, dr, 0, sr, 0, st), "dwtFloat2DInverseToByte");
+}
+void dwtFloat3DInverseToByte(byte* d, float* b2, float* b1, const float* s, int sx, int sy, int sz, int ch, int dr,
+                             int ds, int sr, int ss, cudaStream_t st) {
+    report(cc_dwt_float_inverse_to_byte(d, b2, b1, s, sx, sy, sz, ch, dr, ds, sr, ss, st), "dwtFloat3DInverseToByte");
+}
+void dwtFloat2DInverseFromSymbolsToByte(byte* d, float* b, const float* lp, const ushort* const* hp, float q, int sx,
+                                        int sy, int ch, int dr, int lr, cudaStream_t st) {
+    report(cc_dwt_float_inverse_from_symbols_to_byte(d, nullptr, b, lp, reinterpret_cast<const void* const*>(hp), 2, q,
+                                                     sx, sy, 1, ch, dr, 0, lr, 0, st),
+           "dwtFloat2DInverseFromSymbolsToByte");
+}
+void dwtFloat3DInverseFromSymbolsToByte(byte* d, float* b2, float* b1, const float* lp, const ushort* const* hp, float q,
+                                        int sx, int sy, int sz, int ch, int dr, int ds, int lr, int ls, cudaStream_t st) {
+    report(cc_dwt_float_inverse_from_symbols_to_byte(d, b2, b1, lp, reinterpret_cast<const void* const*>(hp), 2, q, sx,
+                                                     sy, sz, ch, dr, ds, lr, ls, st),
+           "dwtFloat3DInverseFromSymbolsToByte");
+}
+void dwtFloat2DForwardLowpassOnlyFromByte(float* d, float* b, const byte* s, int sx, int sy, int ch, int dr, int sr,
+                                          cudaStream_t st) {
+    report(cc_dwt_float2d_forward_lowpass_only_from_byte(d, b, s, sx, sy, ch, dr, sr, st),
+           "dwtFloat2DForwardLowpassOnlyFromByte");
+}
+void dwtIntForwardLowpassOnly(short* d, short* b, const short* s, int sx, int sy, int dr, int sr, cudaStream_t st) {
+    report(cc_dwt_int_forward_lowpass_only(d, b, s, sx, sy, dr, sr, st), "dwtIntForwardLowpassOnly");
+}
 void dwtIntForward(short* d, short* b, const short* s, int sx, int sy, int sz, int dr, int ds, int sr, int ss,
                    cudaStream_t st) {
     report(cc_dwt_int_forward(d, b, s, sx, sy, sz, dr, ds, sr, ss, st), "dwtIntForward");
@@ -279,6 +315,50 @@ void unquantizeFromShort(float* o, const short* i, uint sx, uint sy, uint sz, fl
     report(cc_unquantize_from_short(o, i, sx, sy, sz, q, r, s, int(t), nullptr), "unquantizeFromShort");
 }
 void getMaxAbs(Instance* p, const float* d, uint n, float* m) { report(cc_get_max_abs(p->h, d, n, m), "getMaxAbs"); }
+
+void floatToByte2D(byte* o, uint cc, uint c, const float* i, uint sx, uint sy, uint r) {
+    report(cc_float_to_byte_2d(o, cc, c, i, sx, sy, r, nullptr), "floatToByte2D");
+}
+void byteToFloat2D(float* o, const byte* i, uint cc, uint c, uint sx, uint sy, uint r) {
+    report(cc_byte_to_float_2d(o, i, cc, c, sx, sy, r, nullptr), "byteToFloat2D");
+}
+void quantizeDifferenceToSymbols2D(ushort* o, const float* i, float q, const byte* ref, uint cc, uint c, uint sx, uint sy,
+                                   uint r, EQuantizeType t) {
+    report(cc_quantize_difference_to_symbols_2d(o, i, q, ref, cc, c, sx, sy, r, int(t), nullptr),
+           "quantizeDifferenceToSymbols2D");
+}
+void quantizeDifferenceToSymbolsRoundtrip2D(ushort* o, float* i, float q, const byte* ref, uint cc, uint c, uint sx,
+                                            uint sy, uint r, EQuantizeType t) {
+    report(cc_quantize_difference_to_symbols_roundtrip_2d(o, i, q, ref, cc, c, sx, sy, r, int(t), nullptr),
+           "quantizeDifferenceToSymbolsRoundtrip2D");
+}
+void unquantizeDifferenceFromSymbols2D(float* o, const ushort* i, float q, const byte* ref, uint cc, uint c, uint sx,
+                                       uint sy, uint r, EQuantizeType t, cudaStream_t st) {
+    report(cc_unquantize_difference_from_symbols_2d(o, i, q, ref, cc, c, sx, sy, r, int(t), st),
+           "unquantizeDifferenceFromSymbols2D");
+}
+
+void convertRGBtoYCoCg(uchar3* d, const uchar3* s, int n) {
+    report(cc_convert_rgb_to_ycocg(reinterpret_cast<uint8_t*>(d), reinterpret_cast<const uint8_t*>(s), n, 3, nullptr),
+           "convertRGBtoYCoCg");
+}
+void convertYCoCgtoRGB(uchar3* d, const uchar3* s, int n) {
+    report(cc_convert_ycocg_to_rgb(reinterpret_cast<uint8_t*>(d), reinterpret_cast<const uint8_t*>(s), n, 3, nullptr),
+           "convertYCoCgtoRGB");
+}
+void convertRGBtoYCoCg(uchar4* d, const uchar4* s, int n) {
+    report(cc_convert_rgb_to_ycocg(reinterpret_cast<uint8_t*>(d), reinterpret_cast<const uint8_t*>(s), n, 4, nullptr),
+           "convertRGBtoYCoCg");
+}
+void convertYCoCgtoRGB(uchar4* d, const uchar4* s, int n) {
+    report(cc_convert_ycocg_to_rgb(reinterpret_cast<uint8_t*>(d), reinterpret_cast<const uint8_t*>(s), n, 4, nullptr),
+           "convertYCoCgtoRGB");
+}
+
+bool getLSB(const short* d, uint* b, uint n) { return report(cc_get_lsb(d, b, n, nullptr), "getLSB"); }
+bool removeLSB(short* d, uint* b, uint n, short s) { return report(cc_remove_lsb(d, b, n, s, nullptr), "removeLSB"); }
+bool appendLSB(short* d, const uint* b, uint n, short s) { return report(cc_append_lsb(d, b, n, s, nullptr), "appendLSB"); }
+bool shiftElems(short* d, uint n, short s) { return report(cc_shift_elems(d, n, s, nullptr), "shiftElems"); }
 
 }  // namespace util
 }  // namespace cudaCompress

@@ -314,6 +314,179 @@ static bool checkSizes(int sx, int sy, int sz, const char* what) {
 }
 
 // ---------------------------------------------------------------------------
+// Float transforms of every element type (DWTFloat.cu:465-533): float or byte
+// source (byte b -> b - 128, DWTCommon.cuh:14-27) and float or byte
+// destination (v -> clamp(v + 128.5, 0, 255) truncated, DWTCommon.cuh:29-41).
+// The byte side carries the interleaved channels; intermediates are float.
+// ---------------------------------------------------------------------------
+template <class TIn>
+static int floatForward(float* dst, float* buf2, float* buf1, const TIn* src, int sx, int sy, int sz, int ch,
+                        int dstRow, int dstSlice, int srcRow, int srcSlice, cudaStream_t st, const char* what) {
+    if (!checkSizes(sx, sy, sz, what)) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx * ch;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    const bool do3D = sz > 1;
+    rowPass<TIn, float, false>(buf1, src, sx, sy, sz, ch, srcRow, srcSlice, 1, dstRow, dstSlice, st);
+    float* yDst = do3D ? buf2 : dst;
+    colPass<false>(yDst, pitchLoad(buf1, 1, dstRow, dstSlice), sx, sy, sz, 1, dstRow, dstSlice, st);
+    if (do3D) colPass<false>(dst, pitchLoad(buf2, 2, dstRow, dstSlice), sx, sy, sz, 2, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), what);
+    return CC_OK;
+}
+
+template <class TOut>
+static int floatInverse(TOut* dst, float* buf2, float* buf1, const float* src, int sx, int sy, int sz, int ch,
+                        int dstRow, int dstSlice, int srcRow, int srcSlice, cudaStream_t st, const char* what) {
+    if (!checkSizes(sx, sy, sz, what)) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx * ch;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (srcRow <= 0) srcRow = sx;
+    if (srcSlice <= 0) srcSlice = sy * srcRow;
+    const bool do3D = sz > 1;
+    const float* ySrc = src;
+    if (do3D) {
+        colPass<true>(buf2, pitchLoad(src, 2, srcRow, srcSlice), sx, sy, sz, 2, srcRow, srcSlice, st);
+        ySrc = buf2;
+    }
+    colPass<true>(buf1, pitchLoad(ySrc, 1, srcRow, srcSlice), sx, sy, sz, 1, srcRow, srcSlice, st);
+    rowPass<float, TOut, true>(dst, buf1, sx, sy, sz, 1, srcRow, srcSlice, ch, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), what);
+    return CC_OK;
+}
+
+template <class TOut>
+static int floatInverseFromSymbols(TOut* dst, float* buf2, float* buf1, const float* lowpass,
+                                   const void* const* highpass, int symBytes, float step, int sx, int sy, int sz,
+                                   int ch, int dstRow, int dstSlice, int lpRow, int lpSlice, cudaStream_t st,
+                                   const char* what) {
+    if (!checkSizes(sx, sy, sz, what)) return CC_ERR_INVALID_ARGUMENT;
+    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (symBytes != 2 && symBytes != 4) { setError("symbol size must be 2 or 4"); return CC_ERR_INVALID_ARGUMENT; }
+    if (dstRow <= 0) dstRow = sx * ch;
+    if (dstSlice <= 0) dstSlice = sy * dstRow;
+    if (lpRow <= 0) lpRow = sx;
+    if (lpSlice <= 0) lpSlice = sy * lpRow;
+    const bool do3D = sz > 1;
+    const int bRow = sx, bSlice = sx * sy;   // DWTFloat.cu:354-355: tight intermediates
+    auto first = [&](auto tag, float* out, int axis) {
+        using Sym = decltype(tag);
+        SymbolLoad<Sym> l;
+        l.lp = lowpass;
+        l.lpRow = lpRow;
+        l.lpSlice = lpSlice;
+        l.bands = reinterpret_cast<const Sym* const*>(highpass);
+        l.step = step;
+        l.hx = sx / 2;
+        l.hy = sy / 2;
+        l.hz = do3D ? sz / 2 : 1;
+        l.axisIsZ = axis == 2;
+        colPass<true>(out, l, sx, sy, sz, axis, bRow, bSlice, st);
+    };
+    if (do3D) {
+        if (symBytes == 2) first(u16(), buf2, 2); else first(u32(), buf2, 2);
+        colPass<true>(buf1, pitchLoad(buf2, 1, bRow, bSlice), sx, sy, sz, 1, bRow, bSlice, st);
+    } else {
+        if (symBytes == 2) first(u16(), buf1, 1); else first(u32(), buf1, 1);
+    }
+    rowPass<float, TOut, true>(dst, buf1, sx, sy, sz, 1, bRow, bSlice, ch, dstRow, dstSlice, st);
+    CC_TRY_CUDA(cudaGetLastError(), what);
+    return CC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lowpass-only forward transforms: the LL band of one 2D level and nothing
+// else, in ONE kernel (the reference runs an X and a Y kernel through a
+// buffer).  A CTA owns 32 x 32 LL outputs: it stages the (mirrored) source
+// window they depend on, filters its rows along X into shared memory (the
+// even outputs only), then the columns of that along Y.  Each LL sample is
+// the same arithmetic as the reference's two passes, so results are
+// bit-identical.
+// ---------------------------------------------------------------------------
+constexpr int kLpTile = 32;
+
+// CDF 9/7 (DWTFloat2DLowpassKernels.cui:14-300): window 2L-4 .. 2L+4 per axis.
+// Channel blockIdx.z of interleaved source / destination elements (element
+// strides srcElem / dstElem, in elements of their type).
+template <class TIn, class TOut>
+__global__ void __launch_bounds__(256) k_lowpass97(TOut* __restrict__ dst, const TIn* __restrict__ src, int nx, int ny,
+                                                   int srcElem, int srcRow, int dstElem, int dstRow) {
+    src += blockIdx.z;
+    dst += blockIdx.z;
+    constexpr int kIn = 2 * kLpTile + 7;
+    __shared__ float sIn[kIn][kIn + 1];
+    __shared__ float sX[kIn][kLpTile + 1];
+    const int lx0 = blockIdx.x * kLpTile, ly0 = blockIdx.y * kLpTile;
+    const int x0 = 2 * lx0 - 4, y0 = 2 * ly0 - 4;
+    // samples at or beyond n + 4 feed no output of this tile
+    const int rows = min(kIn, ny + 4 - y0), cols = min(kIn, nx + 4 - x0);
+    for (int k = threadIdx.x; k < rows * kIn; k += 256) {
+        const int j = k / kIn, i = k - j * kIn;
+        if (i < cols)
+            sIn[j][i] = toF<TIn>(src[size_t(mirrorIdx(y0 + j, ny)) * srcRow + size_t(mirrorIdx(x0 + i, nx)) * srcElem]);
+    }
+    __syncthreads();
+    const int ox = min(kLpTile, (nx >> 1) - lx0), oy = min(kLpTile, (ny >> 1) - ly0);
+    for (int k = threadIdx.x; k < rows * ox; k += 256) {
+        const int j = k / ox, c = k - j * ox;
+        sX[j][c] = fir9c<false, 0>(&sIn[j][2 * c]);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < oy * ox; k += 256) {
+        const int r = k / ox, c = k - r * ox;
+        float v[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) v[i] = sX[2 * r + i][c];
+        dst[(size_t(ly0 + r) * dstRow + lx0 + c) * dstElem] = fromF<TOut>(fir9c<false, 0>(v));
+    }
+}
+
+// CDF 5/3 lifting (DWTInt2DLowpassKernels.cui:14-196): the even sample 2L
+// updated by its two predicted odd neighbours, window 2L-2 .. 2L+2.
+__device__ __forceinline__ i16 lowpass53(i16 a, i16 b, i16 c, i16 d, i16 e) {
+    const i16 d1 = i16(b - div2(i16(a + c)));
+    const i16 d3 = i16(d - div2(i16(c + e)));
+    return i16(c + div4(i16(d1 + d3)));
+}
+
+// kRemoveLsb: each LL sample v is stored as (t + (t < 0 ? -1 : 0)) / 2 with
+// t = v + shift in 16 bits (removeLSB without bits, Bits.cu:62-96).
+template <bool kRemoveLsb>
+__global__ void __launch_bounds__(256) k_lowpass53(i16* __restrict__ dst, const i16* __restrict__ src, int nx, int ny,
+                                                   int srcRow, int dstRow, i16 shift) {
+    constexpr int kIn = 2 * kLpTile + 3;
+    __shared__ i16 sIn[kIn][kIn + 1];
+    __shared__ i16 sX[kIn][kLpTile + 1];
+    const int lx0 = blockIdx.x * kLpTile, ly0 = blockIdx.y * kLpTile;
+    const int x0 = 2 * lx0 - 2, y0 = 2 * ly0 - 2;
+    const int rows = min(kIn, ny + 2 - y0), cols = min(kIn, nx + 2 - x0);
+    for (int k = threadIdx.x; k < rows * kIn; k += 256) {
+        const int j = k / kIn, i = k - j * kIn;
+        if (i < cols) sIn[j][i] = src[size_t(mirrorIdx(y0 + j, ny)) * srcRow + mirrorIdx(x0 + i, nx)];
+    }
+    __syncthreads();
+    const int ox = min(kLpTile, (nx >> 1) - lx0), oy = min(kLpTile, (ny >> 1) - ly0);
+    for (int k = threadIdx.x; k < rows * ox; k += 256) {
+        const int j = k / ox, c = k - j * ox;
+        const i16* s = &sIn[j][2 * c];
+        sX[j][c] = lowpass53(s[0], s[1], s[2], s[3], s[4]);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < oy * ox; k += 256) {
+        const int r = k / ox, c = k - r * ox;
+        i16 v = lowpass53(sX[2 * r][c], sX[2 * r + 1][c], sX[2 * r + 2][c], sX[2 * r + 3][c], sX[2 * r + 4][c]);
+        if (kRemoveLsb) {
+            const i16 t = i16(v + shift);
+            v = i16((int(t) + (t < 0 ? -1 : 0)) / 2);
+        }
+        dst[size_t(ly0 + r) * dstRow + lx0 + c] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Fixed scratch of cc_dwt_float_forward_static: the two intermediate volumes
 // of the forward transform live in this file-scope device array instead of
 // caller buffers, for callers that cannot allocate device memory (code that
@@ -740,78 +913,77 @@ extern "C" {
 
 int cc_dwt_float_forward(float* dst, float* buf2, float* buf1, const float* src, int sx, int sy, int sz, int ch,
                          int dstRow, int dstSlice, int srcRow, int srcSlice, void* stream) {
-    if (!checkSizes(sx, sy, sz, "dwtFloatForward")) return CC_ERR_INVALID_ARGUMENT;
-    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
-    if (dstRow <= 0) dstRow = sx;
-    if (dstSlice <= 0) dstSlice = sy * dstRow;
-    if (srcRow <= 0) srcRow = sx * ch;
-    if (srcSlice <= 0) srcSlice = sy * srcRow;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const bool do3D = sz > 1;
-    rowPass<float, float, false>(buf1, src, sx, sy, sz, ch, srcRow, srcSlice, 1, dstRow, dstSlice, st);
-    float* yDst = do3D ? buf2 : dst;
-    colPass<false>(yDst, pitchLoad(buf1, 1, dstRow, dstSlice), sx, sy, sz, 1, dstRow, dstSlice, st);
-    if (do3D) colPass<false>(dst, pitchLoad(buf2, 2, dstRow, dstSlice), sx, sy, sz, 2, dstRow, dstSlice, st);
-    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatForward");
-    return CC_OK;
+    return floatForward(dst, buf2, buf1, src, sx, sy, sz, ch, dstRow, dstSlice, srcRow, srcSlice,
+                        static_cast<cudaStream_t>(stream), "dwtFloatForward");
+}
+
+int cc_dwt_float_forward_from_byte(float* dst, float* buf2, float* buf1, const uint8_t* src, int sx, int sy, int sz,
+                                   int ch, int dstRow, int dstSlice, int srcRow, int srcSlice, void* stream) {
+    return floatForward(dst, buf2, buf1, src, sx, sy, sz, ch, dstRow, dstSlice, srcRow, srcSlice,
+                        static_cast<cudaStream_t>(stream), "dwtFloatForwardFromByte");
 }
 
 int cc_dwt_float_inverse(float* dst, float* buf2, float* buf1, const float* src, int sx, int sy, int sz, int ch,
                          int dstRow, int dstSlice, int srcRow, int srcSlice, void* stream) {
-    if (!checkSizes(sx, sy, sz, "dwtFloatInverse")) return CC_ERR_INVALID_ARGUMENT;
-    if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
-    if (dstRow <= 0) dstRow = sx * ch;
-    if (dstSlice <= 0) dstSlice = sy * dstRow;
-    if (srcRow <= 0) srcRow = sx;
-    if (srcSlice <= 0) srcSlice = sy * srcRow;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const bool do3D = sz > 1;
-    const float* ySrc = src;
-    if (do3D) {
-        colPass<true>(buf2, pitchLoad(src, 2, srcRow, srcSlice), sx, sy, sz, 2, srcRow, srcSlice, st);
-        ySrc = buf2;
-    }
-    colPass<true>(buf1, pitchLoad(ySrc, 1, srcRow, srcSlice), sx, sy, sz, 1, srcRow, srcSlice, st);
-    rowPass<float, float, true>(dst, buf1, sx, sy, sz, 1, srcRow, srcSlice, ch, dstRow, dstSlice, st);
-    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatInverse");
-    return CC_OK;
+    return floatInverse(dst, buf2, buf1, src, sx, sy, sz, ch, dstRow, dstSlice, srcRow, srcSlice,
+                        static_cast<cudaStream_t>(stream), "dwtFloatInverse");
+}
+
+int cc_dwt_float_inverse_to_byte(uint8_t* dst, float* buf2, float* buf1, const float* src, int sx, int sy, int sz,
+                                 int ch, int dstRow, int dstSlice, int srcRow, int srcSlice, void* stream) {
+    return floatInverse(dst, buf2, buf1, src, sx, sy, sz, ch, dstRow, dstSlice, srcRow, srcSlice,
+                        static_cast<cudaStream_t>(stream), "dwtFloatInverseToByte");
 }
 
 int cc_dwt_float_inverse_from_symbols(float* dst, float* buf2, float* buf1, const float* lowpass,
                                       const void* const* highpass, int symBytes, float step, int sx, int sy, int sz,
                                       int ch, int dstRow, int dstSlice, int lpRow, int lpSlice, void* stream) {
-    if (!checkSizes(sx, sy, sz, "dwtFloatInverseFromSymbols")) return CC_ERR_INVALID_ARGUMENT;
+    return floatInverseFromSymbols(dst, buf2, buf1, lowpass, highpass, symBytes, step, sx, sy, sz, ch, dstRow,
+                                   dstSlice, lpRow, lpSlice, static_cast<cudaStream_t>(stream),
+                                   "dwtFloatInverseFromSymbols");
+}
+
+int cc_dwt_float_inverse_from_symbols_to_byte(uint8_t* dst, float* buf2, float* buf1, const float* lowpass,
+                                              const void* const* highpass, int symBytes, float step, int sx, int sy,
+                                              int sz, int ch, int dstRow, int dstSlice, int lpRow, int lpSlice,
+                                              void* stream) {
+    return floatInverseFromSymbols(dst, buf2, buf1, lowpass, highpass, symBytes, step, sx, sy, sz, ch, dstRow,
+                                   dstSlice, lpRow, lpSlice, static_cast<cudaStream_t>(stream),
+                                   "dwtFloatInverseFromSymbolsToByte");
+}
+
+// dwtFloatForwardLowpassOnly (DWTFloat.cu:17-83, 535-551): the LL band of one
+// 2D level; pitches default to size_x / 2 (destination) and size_x * channels
+// (source).  The buffer is not used (the reference leaves its X-lowpass
+// intermediate there).
+int cc_dwt_float2d_forward_lowpass_only_from_byte(float* dst, float* buf, const uint8_t* src, int sx, int sy, int ch,
+                                                  int dstRow, int srcRow, void* stream) {
+    (void)buf;
+    if (!checkSizes(sx, sy, 1, "dwtFloat2DForwardLowpassOnlyFromByte")) return CC_ERR_INVALID_ARGUMENT;
     if (ch < 1 || ch > 4) { setError("channel count must be 1..4"); return CC_ERR_INVALID_ARGUMENT; }
-    if (symBytes != 2 && symBytes != 4) { setError("symbol size must be 2 or 4"); return CC_ERR_INVALID_ARGUMENT; }
-    if (dstRow <= 0) dstRow = sx * ch;
-    if (dstSlice <= 0) dstSlice = sy * dstRow;
-    if (lpRow <= 0) lpRow = sx;
-    if (lpSlice <= 0) lpSlice = sy * lpRow;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const bool do3D = sz > 1;
-    const int bRow = sx, bSlice = sx * sy;   // DWTFloat.cu:354-355: tight intermediates
-    auto first = [&](auto tag, float* out, int axis) {
-        using Sym = decltype(tag);
-        SymbolLoad<Sym> l;
-        l.lp = lowpass;
-        l.lpRow = lpRow;
-        l.lpSlice = lpSlice;
-        l.bands = reinterpret_cast<const Sym* const*>(highpass);
-        l.step = step;
-        l.hx = sx / 2;
-        l.hy = sy / 2;
-        l.hz = do3D ? sz / 2 : 1;
-        l.axisIsZ = axis == 2;
-        colPass<true>(out, l, sx, sy, sz, axis, bRow, bSlice, st);
-    };
-    if (do3D) {
-        if (symBytes == 2) first(u16(), buf2, 2); else first(u32(), buf2, 2);
-        colPass<true>(buf1, pitchLoad(buf2, 1, bRow, bSlice), sx, sy, sz, 1, bRow, bSlice, st);
-    } else {
-        if (symBytes == 2) first(u16(), buf1, 1); else first(u32(), buf1, 1);
-    }
-    rowPass<float, float, true>(dst, buf1, sx, sy, sz, 1, bRow, bSlice, ch, dstRow, dstSlice, st);
-    CC_TRY_CUDA(cudaGetLastError(), "dwtFloatInverseFromSymbols");
+    if (dstRow <= 0) dstRow = sx / 2;
+    if (srcRow <= 0) srcRow = sx * ch;
+    const dim3 g(unsigned(ceilDiv(sx / 2, kLpTile)), unsigned(ceilDiv(sy / 2, kLpTile)));
+    k_lowpass97<u8, float><<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>(dst, src, sx, sy, ch, srcRow, 1, dstRow);
+    countLaunch();
+    CC_TRY_CUDA(cudaGetLastError(), "dwtFloat2DForwardLowpassOnlyFromByte");
+    return CC_OK;
+}
+
+// dwtIntForwardLowpassOnly (DWTInt.cu:14-77): the LL band of one 2D level of
+// the 5/3 lifting.  The reference transforms only whole blocks of 512 columns
+// and 64 rows and leaves the rest of the band unwritten; here every LL sample
+// is computed, equal to the reference's wherever it writes one.
+int cc_dwt_int_forward_lowpass_only(int16_t* dst, int16_t* buf, const int16_t* src, int sx, int sy, int dstRow,
+                                    int srcRow, void* stream) {
+    (void)buf;
+    if (!checkSizes(sx, sy, 1, "dwtIntForwardLowpassOnly")) return CC_ERR_INVALID_ARGUMENT;
+    if (dstRow <= 0) dstRow = sx / 2;
+    if (srcRow <= 0) srcRow = sx;
+    const dim3 g(unsigned(ceilDiv(sx / 2, kLpTile)), unsigned(ceilDiv(sy / 2, kLpTile)));
+    k_lowpass53<false><<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>(dst, src, sx, sy, srcRow, dstRow, 0);
+    countLaunch();
+    CC_TRY_CUDA(cudaGetLastError(), "dwtIntForwardLowpassOnly");
     return CC_OK;
 }
 
@@ -853,6 +1025,38 @@ int cc_dwt_int_inverse(int16_t* dst, int16_t* buf, const int16_t* src, int sx, i
     return CC_OK;
 }
 
+
+// getLowpassImage (examples CompressImage.cpp:342-365): for the first
+// `channels` of `channelCount` interleaved byte channels, the LL band of one
+// 9/7 level converted back to bytes (floatToByte), into a byte image of
+// size_x/2 x size_y/2 with the same interleaving.  One launch for all
+// channels; no float intermediate.
+int cc_get_lowpass_image(const uint8_t* src, int sx, int sy, int channelCount, int channels, uint8_t* dst,
+                         void* stream) {
+    if (!checkSizes(sx, sy, 1, "getLowpassImage")) return CC_ERR_INVALID_ARGUMENT;
+    if (channelCount < 1 || channelCount > 4 || channels < 1 || channels > channelCount) {
+        setError("getLowpassImage: channel counts must satisfy 1 <= channels <= channelCount <= 4");
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    const dim3 g(unsigned(ceilDiv(sx / 2, kLpTile)), unsigned(ceilDiv(sy / 2, kLpTile)), unsigned(channels));
+    k_lowpass97<u8, u8><<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>(dst, src, sx, sy, channelCount,
+                                                                           sx * channelCount, channelCount, sx / 2);
+    countLaunch();
+    CC_TRY_CUDA(cudaGetLastError(), "getLowpassImage");
+    return CC_OK;
+}
+
+// getLowpassHeightfield (examples CompressHeightfield.cpp:218-235): the LL
+// band of one 5/3 level with the lowpass shift added and the least
+// significant bit removed (removeLSB without bits), dense size_x/2 x size_y/2.
+int cc_get_lowpass_heightfield(const int16_t* src, int sx, int sy, int16_t* dst, int16_t shift, void* stream) {
+    if (!checkSizes(sx, sy, 1, "getLowpassHeightfield")) return CC_ERR_INVALID_ARGUMENT;
+    const dim3 g(unsigned(ceilDiv(sx / 2, kLpTile)), unsigned(ceilDiv(sy / 2, kLpTile)));
+    k_lowpass53<true><<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>(dst, src, sx, sy, sx, sx / 2, shift);
+    countLaunch();
+    CC_TRY_CUDA(cudaGetLastError(), "getLowpassHeightfield");
+    return CC_OK;
+}
 
 // Forward float DWT with its intermediates in the library's fixed device
 // scratch (no counterpart in the reference).  Same arguments and results as

@@ -34,18 +34,22 @@ u64 cube(u64 a, u64 b, u64 c) { return a * b * c; }
 
 }  // namespace
 
-// One reference encode call of a pipeline: `count` streams from `first`.
-struct EncGroup {
-    u32 first, count;
-};
-
 // Encodes the groups back to back into dWords (word aligned segments; the
 // reference's BitStream is word aligned at every group start here), batching
 // as many groups per device call as the instance's symbol and stream budget
 // allows.  A batch whose histograms exceed the instance's table capacity is
 // redone one group per call (the capacity every instance guarantees).
-static int encodeGroups(cc_instance* I, const std::vector<EncStream>& streams, const std::vector<EncGroup>& groups,
-                        u32* dWords, u64 cap, u64* wordsOut) {
+int encodeGroups(cc_instance* I, const std::vector<EncStream>& streams, const std::vector<EncGroup>& groups,
+                 u32* dWords, u64 cap, u64* wordsOut, std::vector<u64>* groupStart) {
+    if (groupStart) groupStart->assign(groups.size() + 1, 0);
+    // word range of group k of the batch just encoded at word `base`
+    auto record = [&](size_t k, u32 batchFirst, u64 base) {
+        if (!groupStart) return;
+        const SegmentLayout& a = I->lastLayout[groups[k].first - batchFirst];
+        const SegmentLayout& b = I->lastLayout[groups[k].first + groups[k].count - 1 - batchFirst];
+        (*groupStart)[k] = base + a.startWord;
+        (*groupStart)[k + 1] = base + b.startWord + b.words;
+    };
     u64 at = 0;
     size_t g = 0;
     while (g < groups.size()) {
@@ -81,11 +85,13 @@ static int encodeGroups(cc_instance* I, const std::vector<EncStream>& streams, c
                 for (EncStream& e : one) e.groupFirst -= groups[k].first;
                 if ((rc = encodeDevice(I, one.data(), groups[k].count, EncOutput{dWords + at, cap - at}, false, &words)))
                     return rc;
+                record(k, groups[k].first, at);
                 at += words;
             }
         } else if (rc) {
             return rc;
         } else {
+            for (size_t k = g; k < h; ++k) record(k, first, at);
             at += words;
         }
         g = h;

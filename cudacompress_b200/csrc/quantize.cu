@@ -12,15 +12,6 @@
 namespace ccb {
 
 
-__device__ __forceinline__ int quantizeV(float v, float inv, int type) {
-    if (type == 0) return int(v * inv);
-    return int(__fmaf_rn(v, inv, signF(v) * 0.5f));
-}
-__device__ __forceinline__ float unquantizeV(int q, float step, int type) {
-    if (type == 0) return (float(q) + signI(q) * 0.5f) * step;
-    return float(q) * step;
-}
-
 struct Box {
     u32 nx, ny, nz;
     u32 row, slice;    // pitches of the strided side

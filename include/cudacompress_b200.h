@@ -137,6 +137,28 @@ int cc_dwt_float_inverse_from_symbols(float* d_dst, float* d_buf2, float* d_buf1
                                       int size_x, int size_y, int size_z, int dst_channel_count,
                                       int dst_row_pitch, int dst_slice_pitch, int lowpass_row_pitch,
                                       int lowpass_slice_pitch, void* stream);
+/* Byte variants (DWT.h:79-123): dwtFloat{2D,3D}ForwardFromByte reads one
+ * channel of an interleaved byte image (b -> b - 128; d_src addresses the
+ * channel, src_channel_count 1..4); ...InverseToByte and
+ * ...InverseFromSymbolsToByte write one channel of one
+ * (v -> clamp(v + 128.5, 0, 255), truncated).  2D: size_z = 1, d_buf2 unused. */
+int cc_dwt_float_forward_from_byte(float* d_dst, float* d_buf2, float* d_buf1, const uint8_t* d_src, int size_x,
+                                   int size_y, int size_z, int src_channel_count, int dst_row_pitch,
+                                   int dst_slice_pitch, int src_row_pitch, int src_slice_pitch, void* stream);
+int cc_dwt_float_inverse_to_byte(uint8_t* d_dst, float* d_buf2, float* d_buf1, const float* d_src, int size_x,
+                                 int size_y, int size_z, int dst_channel_count, int dst_row_pitch, int dst_slice_pitch,
+                                 int src_row_pitch, int src_slice_pitch, void* stream);
+int cc_dwt_float_inverse_from_symbols_to_byte(uint8_t* d_dst, float* d_buf2, float* d_buf1, const float* d_lowpass,
+                                              const void* const* d_highpass, int symbol_bytes, float quant_step,
+                                              int size_x, int size_y, int size_z, int dst_channel_count,
+                                              int dst_row_pitch, int dst_slice_pitch, int lowpass_row_pitch,
+                                              int lowpass_slice_pitch, void* stream);
+/* dwtFloat2DForwardLowpassOnlyFromByte (DWT.h:126-131): only the LL band of
+ * one 2D level (size_x/2 x size_y/2, row pitch default size_x/2).  d_buf is
+ * accepted for the reference's signature and not used. */
+int cc_dwt_float2d_forward_lowpass_only_from_byte(float* d_dst, float* d_buf, const uint8_t* d_src, int size_x,
+                                                  int size_y, int src_channel_count, int dst_row_pitch,
+                                                  int src_row_pitch, void* stream);
 /* No counterpart in the reference (whose dwtFloat{2D,3D}Forward take two
  * caller-allocated buffers): cc_dwt_float_forward with both intermediates in
  * a fixed 8 MiB device array inside this library, for callers that cannot
@@ -154,6 +176,12 @@ int cc_dwt_int_forward(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int
                        int dst_row_pitch, int dst_slice_pitch, int src_row_pitch, int src_slice_pitch, void* stream);
 int cc_dwt_int_inverse(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int size_x, int size_y, int size_z,
                        int dst_row_pitch, int dst_slice_pitch, int src_row_pitch, int src_slice_pitch, void* stream);
+/* dwtIntForwardLowpassOnly (DWT.h:152-157): only the LL band of one 2D
+ * level of the 5/3 lifting (row pitch default size_x/2); d_buf not used.
+ * The reference fills only whole blocks of 512 columns x 64 rows; this
+ * computes every LL sample (identical where the reference writes one). */
+int cc_dwt_int_forward_lowpass_only(int16_t* d_dst, int16_t* d_buf, const int16_t* d_src, int size_x, int size_y,
+                                    int dst_row_pitch, int src_row_pitch, void* stream);
 
 /* ---- util::Quantize (include/cudaCompress/util/Quantize.h:25-65, src/cudaCompress/util/Quantize.cu) ----
  * quant_type 0 = QUANTIZE_DEADZONE, 1 = QUANTIZE_UNIFORM.  The reference
@@ -179,6 +207,49 @@ int cc_unquantize_from_short(float* d_data, const int16_t* d_quant, uint32_t siz
                              int quant_type, void* stream);
 /* getMaxAbs(pInstance, dpImage, elemCount, dpValMax): max |x| into d_max. */
 int cc_get_max_abs(cc_instance* inst, const float* d_data, uint32_t elem_count, float* d_max);
+/* Byte images (Quantize.h:24-26, 58-61): channel `channel` of a byte image
+ * with `channel_count` interleaved channels (dense, size_x per row).
+ * floatToByte: clamp(v + 128.5, 0, 255) truncated; byteToFloat: b - 128.
+ * quantizeDifference*: the float minus the byte reference (b - 128),
+ * quantized to 16-bit symbols; the round trip writes back reference + the
+ * stored symbol's value.  unquantizeDifference is its inverse.  The
+ * reference launches these on the default stream (unquantizeDifference
+ * takes a stream); `stream` NULL does the same. */
+int cc_float_to_byte_2d(uint8_t* d_quant, uint32_t channel_count, uint32_t channel, const float* d_data,
+                        uint32_t size_x, uint32_t size_y, uint32_t row_pitch_src, void* stream);
+int cc_byte_to_float_2d(float* d_data, const uint8_t* d_quant, uint32_t channel_count, uint32_t channel,
+                        uint32_t size_x, uint32_t size_y, uint32_t row_pitch_dst, void* stream);
+int cc_quantize_difference_to_symbols_2d(uint16_t* d_symbols, const float* d_data, float quant_step,
+                                         const uint8_t* d_reference, uint32_t channel_count, uint32_t channel,
+                                         uint32_t size_x, uint32_t size_y, uint32_t row_pitch_src, int quant_type,
+                                         void* stream);
+int cc_quantize_difference_to_symbols_roundtrip_2d(uint16_t* d_symbols, float* d_data, float quant_step,
+                                                   const uint8_t* d_reference, uint32_t channel_count,
+                                                   uint32_t channel, uint32_t size_x, uint32_t size_y,
+                                                   uint32_t row_pitch_src, int quant_type, void* stream);
+int cc_unquantize_difference_from_symbols_2d(float* d_data, const uint16_t* d_symbols, float quant_step,
+                                             const uint8_t* d_reference, uint32_t channel_count, uint32_t channel,
+                                             uint32_t size_x, uint32_t size_y, uint32_t row_pitch_dst,
+                                             int quant_type, void* stream);
+
+/* ---- util::YCoCg (include/cudaCompress/util/YCoCg.h:14-20) ----
+ * RGB <-> YCoCg of `pixel_count` pixels of `channels` bytes (3 = uchar3,
+ * 4 = uchar4, the 4th byte copied; uchar4 pixels 4-byte aligned); in place
+ * allowed.  Y = (R + 2G + B + 2) / 4, Co = (R - B + 1) / 2 + 127,
+ * Cg = (2G - R - B + 2) / 4 + 127 (integer division), inverse clamped. */
+int cc_convert_rgb_to_ycocg(uint8_t* d_target, const uint8_t* d_data, int pixel_count, int channels, void* stream);
+int cc_convert_ycocg_to_rgb(uint8_t* d_target, const uint8_t* d_data, int pixel_count, int channels, void* stream);
+
+/* ---- util::Bits (include/cudaCompress/util/Bits.h:14-27) ----
+ * Bit j of word w of d_bits belongs to element 32 w + j (ceil(n/32) words).
+ * removeLSB: v -> (v + shift) with its lowest bit removed (floor of half),
+ * the removed bits into d_bits when not NULL; appendLSB: v -> 2v + bit +
+ * shift.  The reference processes whole blocks of 4096 elements (its callers
+ * pad); these touch exactly elem_count elements, bits past it are 0. */
+int cc_get_lsb(const int16_t* d_data, uint32_t* d_bits, uint32_t elem_count, void* stream);
+int cc_remove_lsb(int16_t* d_data, uint32_t* d_bits, uint32_t elem_count, int16_t shift, void* stream);
+int cc_append_lsb(int16_t* d_data, const uint32_t* d_bits, uint32_t elem_count, int16_t shift, void* stream);
+int cc_shift_elems(int16_t* d_data, uint32_t elem_count, int16_t shift, void* stream);
 
 /* ---- Volume / heightfield codecs (examples CompressVolume.cpp:312-516, CompressHeightfield.cpp:82-216) ----
  * Whole-pipeline entry points: device-resident input, device-resident bit
@@ -235,6 +306,60 @@ int cc_compress_heightfield(cc_instance* inst, const int16_t* d_image, uint32_t 
                             uint32_t levels, uint32_t* d_words, uint64_t capacity_words, uint32_t* bit_size);
 int cc_decompress_heightfield(cc_instance* inst, int16_t* d_image, uint32_t size_x, uint32_t size_y,
                               uint32_t levels, const uint32_t* d_words, uint32_t bit_size);
+/* One heightfield level (examples CompressHeightfield.cpp:82-216): the stream
+ * holds the ceil(n/32) words of the least significant bits of (LL + shift),
+ * n = size_x/2 * size_y/2, then one encodeRLHuff call over the 3 symbolized
+ * highpass bands.  d_lowpass (n shorts) receives (LL + shift) without that
+ * bit; decompress restores it in place (appendLSB) and rebuilds the image.
+ * getLowpassHeightfield (:218-235): the same d_lowpass, without coding. */
+int cc_compress_heightfield_one_level(cc_instance* inst, const int16_t* d_image, uint32_t size_x, uint32_t size_y,
+                                      int16_t* d_lowpass, int16_t lowpass_shift, uint32_t* d_words,
+                                      uint64_t capacity_words, uint32_t* bit_size);
+int cc_decompress_heightfield_one_level(cc_instance* inst, int16_t* d_image, uint32_t size_x, uint32_t size_y,
+                                        int16_t* d_lowpass, int16_t lowpass_shift, const uint32_t* d_words,
+                                        uint32_t bit_size);
+int cc_get_lowpass_heightfield(const int16_t* d_image, int size_x, int size_y, int16_t* d_lowpass,
+                               int16_t lowpass_shift, void* stream);
+
+/* ---- one image level (examples CompressImage.h:36-71, CompressImage.cpp) ----
+ * Byte images with channel_count_total interleaved channels (1..4), of which
+ * the first channel_count_to_process are coded.  Per channel: 9/7 DWT, the
+ * LL band minus the lowpass reference (a size_x/2 x size_y/2 byte image with
+ * the same interleaving, normally the decoded next-coarser level) and the 3
+ * highpass bands round-trip quantized with quant_step; compress overwrites
+ * d_image with the reconstruction.  Stream: one encodeRLHuff call over the
+ * LL-difference streams of all channels, then each channel's 3 bands.
+ * Colour conversion is the caller's (cc_convert_rgb_to_ycocg). */
+int cc_compress_image_one_level(cc_instance* inst, uint8_t* d_image, uint32_t size_x, uint32_t size_y,
+                                uint32_t channel_count_total, uint32_t channel_count_to_process,
+                                const uint8_t* d_lowpass_reference, float quant_step, uint32_t* d_words,
+                                uint64_t capacity_words, uint32_t* bit_size);
+int cc_decompress_image_one_level(cc_instance* inst, uint8_t* d_image, uint32_t size_x, uint32_t size_y,
+                                  uint32_t channel_count_total, uint32_t channel_count_to_process,
+                                  const uint8_t* d_lowpass_reference, float quant_step, const uint32_t* d_words,
+                                  uint32_t bit_size);
+/* Many images of the same sizes (Image / ImageV, compressImagesOneLevel):
+ * one DWT/quantize sequence per image, one encode (decode) call for all.
+ * Compress fills bit_size; decompress reads d_words / bit_size.  Decompress
+ * needs an instance with 4 x channels x count streams. */
+typedef struct cc_image {
+    uint8_t* d_image;
+    const uint8_t* d_lowpass_reference;
+    uint32_t* d_words;
+    uint64_t capacity_words;      /* compress only */
+    uint32_t bit_size;
+    float quant_step;
+} cc_image;
+int cc_compress_images_one_level(cc_instance* inst, cc_image* images, uint32_t count, uint32_t size_x,
+                                 uint32_t size_y, uint32_t channel_count_total, uint32_t channel_count_to_process);
+int cc_decompress_images_one_level(cc_instance* inst, const cc_image* images, uint32_t count, uint32_t size_x,
+                                   uint32_t size_y, uint32_t channel_count_total,
+                                   uint32_t channel_count_to_process);
+/* getLowpassImage (CompressImage.cpp:342-365): the LL band of one 9/7 level
+ * of each processed channel, as bytes (floatToByte), into d_lowpass
+ * (size_x/2 x size_y/2, channel_count_total interleaved channels). */
+int cc_get_lowpass_image(const uint8_t* d_image, int size_x, int size_y, int channel_count_total,
+                         int channel_count_to_process, uint8_t* d_lowpass, void* stream);
 
 /* ---- stream container (B200 addition; no counterpart in the reference) ----
  * The reference's example stores a stream as raw concatenated u32 words

@@ -25,6 +25,7 @@
 typedef uint32_t u32;
 typedef uint16_t u16;
 typedef int16_t i16;
+typedef uint8_t u8;
 
 namespace orc {
 
@@ -1132,6 +1133,311 @@ int orc_decompress_heightfield(const u32* words, u32 bitSize, i16* out, long nx,
         dwtInt(c.data(), cur.data(), n0, n1, 1, true);
     }
     std::copy(cur.begin(), cur.end(), out);
+    return 0;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// The 2D image side: byte conversions, lowpass-only transforms, byte-image
+// quantizers, YCoCg, least-significant-bit planes, and the one-level image
+// and heightfield codecs of the reference's examples.
+// ===========================================================================
+
+// DWTCommon.cuh:14-41 and Quantize.cuh:15-23
+static inline float byteToFloatO(u8 b) { return float(b) - 128.0f; }
+static inline u8 floatToByteO(float v) { return u8(std::min(std::max(v + 128.5f, 0.0f), 255.0f)); }
+
+// Quantize.cuh:75-131 (type 0 deadzone, 1 uniform; the uniform product
+// contracted into one fma as the device code is compiled)
+static inline int quantO(float v, float inv, int type) {
+    if (type == 0) return int(v * inv);
+    const float s = v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f);
+    return int(std::fmaf(v, inv, s * 0.5f));
+}
+// the dequantized value before its multiplication by the step
+static inline float unquantBaseO(int q, int type) {
+    if (type == 0) return float(q) + (q > 0 ? 1.0f : (q < 0 ? -1.0f : 0.0f)) * 0.5f;
+    return float(q);
+}
+static inline float unquantO(int q, float step, int type) { return unquantBaseO(q, type) * step; }
+// dequantized value plus a reference (QuantizeKernels.cui:261-262, 279-280):
+// the device code contracts the step multiply and the add into one fma
+static inline float unquantPlusO(int q, float step, float ref, int type) {
+    return std::fmaf(unquantBaseO(q, type), step, ref);
+}
+
+// 5/3 lowpass of the even sample c with neighbours a b | d e
+// (DWTInt2DLowpassKernels.cui:58-88, rounding DWTCommon.cuh:133-142)
+static inline i16 lowpass53O(i16 a, i16 b, i16 c, i16 d, i16 e) {
+    const i16 d1 = i16(b - div2(i16(a + c)));
+    const i16 d3 = i16(d - div2(i16(c + e)));
+    return i16(c + div4(i16(d1 + d3)));
+}
+
+// removeLSB / appendLSB of one element (Bits.cu:62-174)
+static inline i16 removeLsbO(i16 v, i16 shift, u32* bit) {
+    const i16 t = i16(v + shift);
+    *bit = u32(t & 1);
+    return i16((int(t) + (t < 0 ? -1 : 0)) / 2);
+}
+static inline i16 appendLsbO(i16 v, u32 bit, i16 shift) {
+    const i16 t = i16((int(v) * 2) | int(bit));
+    return i16(t + shift);
+}
+
+extern "C" {
+
+// dwtFloat{2D,3D}ForwardFromByte (DWTFloat.cu:653-670): src addresses the
+// channel, element stride `channels`, rows of nx * channels bytes.
+void orc_dwt_float_fwd_from_byte(const u8* src, long channels, float* dst, long nx, long ny, long nz) {
+    std::vector<float> f(nx * ny * nz);
+    for (long i = 0; i < nx * ny * nz; ++i) f[i] = byteToFloatO(src[i * channels]);
+    dwtFloat(f.data(), dst, nx, ny, nz, false);
+}
+
+// dwtFloat{2D,3D}InverseToByte (DWTFloat.cu:673-690): dst addresses the channel.
+void orc_dwt_float_inv_to_byte(const float* src, u8* dst, long channels, long nx, long ny, long nz) {
+    std::vector<float> f(nx * ny * nz);
+    dwtFloat(src, f.data(), nx, ny, nz, true);
+    for (long i = 0; i < nx * ny * nz; ++i) dst[i * channels] = floatToByteO(f[i]);
+}
+
+// dwtFloat{2D,3D}InverseFromSymbolsToByte (DWTFloat.cu:693-712): the dense
+// lowpass (nx/2 x ny/2 x nz/2) and 3 or 7 dense u16 bands (index x+2y+4z-1)
+// dequantized as Quantize.cuh:104-110, then the inverse into bytes.
+void orc_dwt_float_inv_from_symbols_to_byte(const float* lowpass, const u16* const* bands, float step, u8* dst,
+                                            long channels, long nx, long ny, long nz) {
+    const long hx = nx / 2, hy = ny / 2, hz = nz > 1 ? nz / 2 : 1;
+    std::vector<float> coef(nx * ny * nz);
+    for (long z = 0; z < hz; ++z)
+        for (long y = 0; y < hy; ++y)
+            for (long x = 0; x < hx; ++x) coef[(z * ny + y) * nx + x] = lowpass[(z * hy + y) * hx + x];
+    const int nb = nz > 1 ? 8 : 4;
+    for (int b = 1; b < nb; ++b) unquantizeBand(coef.data(), nx, ny, nz, b % 2, (b / 2) % 2, b / 4, step, bands[b - 1]);
+    orc_dwt_float_inv_to_byte(coef.data(), dst, channels, nx, ny, nz);
+}
+
+// dwtFloat2DForwardLowpassOnlyFromByte (DWTFloat.cu:17-83, kernels
+// DWTFloat2DLowpassKernels.cui): the LL band alone, the even outputs of the
+// X pass then of the Y pass - the same numbers as the LL band of the full
+// transform, which is how it is restated here.
+void orc_dwt_float2d_lowpass_from_byte(const u8* src, long channels, float* dst, long nx, long ny) {
+    std::vector<float> full(nx * ny);
+    orc_dwt_float_fwd_from_byte(src, channels, full.data(), nx, ny, 1);
+    for (long y = 0; y < ny / 2; ++y)
+        for (long x = 0; x < nx / 2; ++x) dst[y * (nx / 2) + x] = full[y * nx + x];
+}
+
+// dwtIntForwardLowpassOnly (DWTInt.cu:14-77): predict + update per row, then
+// per column of the row results, keeping only the even samples.
+void orc_dwt_int_lowpass(const i16* src, i16* dst, long nx, long ny) {
+    const long hx = nx / 2, hy = ny / 2;
+    std::vector<i16> xl(ny * hx);
+    for (long y = 0; y < ny; ++y)
+        for (long L = 0; L < hx; ++L) {
+            const i16* r = src + y * nx;
+            xl[y * hx + L] = lowpass53O(r[mirror(2 * L - 2, nx)], r[mirror(2 * L - 1, nx)], r[2 * L],
+                                        r[mirror(2 * L + 1, nx)], r[mirror(2 * L + 2, nx)]);
+        }
+    for (long M = 0; M < hy; ++M)
+        for (long x = 0; x < hx; ++x)
+            dst[M * hx + x] = lowpass53O(xl[mirror(2 * M - 2, ny) * hx + x], xl[mirror(2 * M - 1, ny) * hx + x],
+                                         xl[2 * M * hx + x], xl[mirror(2 * M + 1, ny) * hx + x],
+                                         xl[mirror(2 * M + 2, ny) * hx + x]);
+}
+
+// floatToByte2D / byteToFloat2D (Quantize.cu:19-43, QuantizeKernels.cui:11-34)
+void orc_float_to_byte_2d(u8* out, long channels, long channel, const float* in, long nx, long ny, long rowPitch) {
+    for (long y = 0; y < ny; ++y)
+        for (long x = 0; x < nx; ++x) out[(y * nx + x) * channels + channel] = floatToByteO(in[y * rowPitch + x]);
+}
+void orc_byte_to_float_2d(float* out, const u8* in, long channels, long channel, long nx, long ny, long rowPitch) {
+    for (long y = 0; y < ny; ++y)
+        for (long x = 0; x < nx; ++x) out[y * rowPitch + x] = byteToFloatO(in[(y * nx + x) * channels + channel]);
+}
+
+// quantizeDifferenceToSymbols(Roundtrip)2D (Quantize.cu:276-326,
+// QuantizeKernels.cui:227-263): symbol of (v - (ref - 128)) as 16 bits; the
+// round trip writes back the stored symbol's value plus the reference.
+void orc_quantize_difference_2d(u16* sym, float* data, float step, const u8* ref, long channels, long channel, long nx,
+                                long ny, long rowPitch, int type, int roundtrip) {
+    const float inv = 1.0f / step;
+    for (long y = 0; y < ny; ++y)
+        for (long x = 0; x < nx; ++x) {
+            const float r = byteToFloatO(ref[(y * nx + x) * channels + channel]);
+            float& v = data[y * rowPitch + x];
+            const u16 q = u16(symbolize(quantO(v - r, inv, type)));
+            sym[y * nx + x] = q;
+            if (roundtrip) v = unquantPlusO(unsymbolize(q), step, r, type);
+        }
+}
+// unquantizeDifferenceFromSymbols2D (Quantize.cu:328-352, QuantizeKernels.cui:265-281)
+void orc_unquantize_difference_2d(float* data, const u16* sym, float step, const u8* ref, long channels, long channel,
+                                  long nx, long ny, long rowPitch, int type) {
+    for (long y = 0; y < ny; ++y)
+        for (long x = 0; x < nx; ++x)
+            data[y * rowPitch + x] = unquantPlusO(unsymbolize(sym[y * nx + x]), step,
+                                                  byteToFloatO(ref[(y * nx + x) * channels + channel]), type);
+}
+
+// convertRGBtoYCoCg / convertYCoCgtoRGB (YCoCg.cu:21-88): integer arithmetic
+// with C division; `channels` 3 or 4 (the 4th byte is copied).
+void orc_ycocg(u8* dst, const u8* src, long n, int channels, int toYCoCg) {
+    for (long i = 0; i < n; ++i) {
+        const int a = src[i * channels], b = src[i * channels + 1], c = src[i * channels + 2];
+        const int w = channels == 4 ? src[i * channels + 3] : 0;
+        int o[3];
+        if (toYCoCg) {
+            o[0] = (a + b * 2 + c + 2) / 4;
+            o[1] = (a - c + 1) / 2 + 127;
+            o[2] = (-a + b * 2 - c + 2) / 4 + 127;
+        } else {
+            o[0] = std::min(std::max(a + b - c, 0), 255);
+            o[1] = std::min(std::max(a + c - 127, 0), 255);
+            o[2] = std::min(std::max(a - b - c + 254, 0), 255);
+        }
+        for (int k = 0; k < 3; ++k) dst[i * channels + k] = u8(o[k]);
+        if (channels == 4) dst[i * channels + 3] = u8(w);
+    }
+}
+
+// getLSB / removeLSB / appendLSB (Bits.cu:20-174): mode 0 get, 1 remove
+// (bits may be null), 2 append; bit j of word w is element 32 w + j.
+void orc_lsb(int mode, i16* data, u32* bits, u32 n, i16 shift) {
+    const u32 words = (n + 31) / 32;
+    if (mode != 2 && bits) std::fill(bits, bits + words, 0u);
+    for (u32 e = 0; e < n; ++e) {
+        u32 b = 0;
+        if (mode == 0) {
+            bits[e / 32] |= u32(data[e] & 1) << (e % 32);
+        } else if (mode == 1) {
+            data[e] = removeLsbO(data[e], shift, &b);
+            if (bits) bits[e / 32] |= b << (e % 32);
+        } else {
+            data[e] = appendLsbO(data[e], (bits[e / 32] >> (e % 32)) & 1u, shift);
+        }
+    }
+}
+// shiftElems (Bits.cu:143-151)
+void orc_shift_elems(i16* data, u32 n, i16 shift) {
+    for (u32 e = 0; e < n; ++e) data[e] = i16(data[e] + shift);
+}
+
+// getLowpassImage (CompressImage.cpp:342-365)
+void orc_get_lowpass_image(const u8* image, long nx, long ny, long chTotal, long chProc, u8* out) {
+    std::vector<float> ll((nx / 2) * (ny / 2));
+    for (long c = 0; c < chProc; ++c) {
+        orc_dwt_float2d_lowpass_from_byte(image + c, chTotal, ll.data(), nx, ny);
+        orc_float_to_byte_2d(out, chTotal, c, ll.data(), nx / 2, ny / 2, nx / 2);
+    }
+}
+
+// getLowpassHeightfield (CompressHeightfield.cpp:218-235)
+void orc_get_lowpass_heightfield(const i16* image, long nx, long ny, i16* out, i16 shift) {
+    orc_dwt_int_lowpass(image, out, nx, ny);
+    orc_lsb(1, out, nullptr, u32((nx / 2) * (ny / 2)), shift);
+}
+
+// compressImageOneLevel (CompressImage.cpp:71-128): image (interleaved,
+// chTotal channels) is overwritten with its reconstruction.
+int orc_compress_image_one_level(u8* image, long nx, long ny, long chTotal, long chProc, const u8* lpRef, float step,
+                                 u32 cb, u32 log2Max, u32* words, u32 cap, u32* bitSize) {
+    const long hx = nx / 2, hy = ny / 2, n = hx * hy;
+    std::vector<u16> syms(4 * chProc * n);
+    std::vector<float> coef(nx * ny);
+    const float inv = 1.0f / step;
+    for (long c = 0; c < chProc; ++c) {
+        orc_dwt_float_fwd_from_byte(image + c, chTotal, coef.data(), nx, ny, 1);
+        orc_quantize_difference_2d(syms.data() + c * n, coef.data(), step, lpRef, chTotal, c, hx, hy, nx, 0, 1);
+        for (int b = 1; b < 4; ++b) {
+            u16* out = syms.data() + (chProc + 3 * c + b - 1) * n;
+            // quantizeToSymbolsRoundtrip (QuantizeKernels.cui:95-113): back from the full quantized value
+            for (long y = 0; y < hy; ++y)
+                for (long x = 0; x < hx; ++x) {
+                    float& v = coef[(y + (b / 2) * hy) * nx + x + (b % 2) * hx];
+                    const int q = quantO(v, inv, 0);
+                    out[y * hx + x] = u16(symbolize(q));
+                    v = unquantO(q, step, 0);
+                }
+        }
+        orc_dwt_float_inv_to_byte(coef.data(), image + c, chTotal, nx, ny, 1);
+    }
+    std::vector<const u16*> s(4 * chProc);
+    for (long k = 0; k < 4 * chProc; ++k) s[k] = syms.data() + k * n;
+    BitStream bs;
+    int r = encodeRLHuff(bs, s, u32(n), cb, log2Max);
+    if (r) return r;
+    u32 pos;
+    return finishBits(bs, words, cap, bitSize, &pos);
+}
+
+// decompressImageOneLevel (CompressImage.cpp:135-186)
+int orc_decompress_image_one_level(const u32* words, u32 bitSize, u8* image, long nx, long ny, long chTotal,
+                                   long chProc, const u8* lpRef, float step, u32 cb, u32 log2Max) {
+    const long hx = nx / 2, hy = ny / 2, n = hx * hy;
+    std::vector<u16> syms(4 * chProc * n);
+    std::vector<u16*> o(4 * chProc);
+    for (long k = 0; k < 4 * chProc; ++k) o[k] = syms.data() + k * n;
+    BitReader br{words, bitSize, 0};
+    decodeRLHuff(br, o, u32(n), cb, log2Max);
+    std::vector<float> lp(n);
+    for (long c = 0; c < chProc; ++c) {
+        orc_unquantize_difference_2d(lp.data(), o[c], step, lpRef, chTotal, c, hx, hy, hx, 0);
+        const u16* bands[3] = {o[chProc + 3 * c], o[chProc + 3 * c + 1], o[chProc + 3 * c + 2]};
+        orc_dwt_float_inv_from_symbols_to_byte(lp.data(), bands, step, image + c, chTotal, nx, ny, 1);
+    }
+    return 0;
+}
+
+// compressHeightfieldOneLevel (CompressHeightfield.cpp:82-141)
+int orc_compress_heightfield_one_level(const i16* image, long nx, long ny, i16* lowpass, i16 shift, u32 cb,
+                                       u32 log2Max, u32* words, u32 cap, u32* bitSize) {
+    const long hx = nx / 2, hy = ny / 2, n = hx * hy;
+    std::vector<i16> c(nx * ny);
+    dwtInt(image, c.data(), nx, ny, 1, false);
+    for (long y = 0; y < hy; ++y)
+        for (long x = 0; x < hx; ++x) lowpass[y * hx + x] = c[y * nx + x];
+    std::vector<u32> bits((n + 31) / 32);
+    orc_lsb(1, lowpass, bits.data(), u32(n), shift);
+    std::vector<u16> bands(3 * n);
+    std::vector<const u16*> s(3);
+    for (int b = 1; b < 4; ++b) {
+        for (long y = 0; y < hy; ++y)
+            for (long x = 0; x < hx; ++x)
+                bands[(b - 1) * n + y * hx + x] = u16(symbolize(c[(y + (b / 2) * hy) * nx + x + (b % 2) * hx]));
+        s[b - 1] = bands.data() + (b - 1) * n;
+    }
+    BitStream bs;
+    bs.writeAligned(bits.data(), 4, u32(bits.size()));
+    int r = encodeRLHuff(bs, s, u32(n), cb, log2Max);
+    if (r) return r;
+    u32 pos;
+    return finishBits(bs, words, cap, bitSize, &pos);
+}
+
+// decompressHeightfieldOneLevel (CompressHeightfield.cpp:148-216): lowpass is
+// restored in place, then the image rebuilt.
+int orc_decompress_heightfield_one_level(const u32* words, u32 bitSize, i16* image, long nx, long ny, i16* lowpass,
+                                         i16 shift, u32 cb, u32 log2Max) {
+    const long hx = nx / 2, hy = ny / 2, n = hx * hy;
+    const u32 bitWords = u32((n + 31) / 32);
+    if (bitSize < bitWords * 32) return -1;
+    std::vector<u32> bits(words, words + bitWords);
+    orc_lsb(2, lowpass, bits.data(), u32(n), shift);
+    BitReader br{words, bitSize, bitWords * 32};
+    std::vector<u16> bands(3 * n);
+    std::vector<u16*> ob(3);
+    for (int b = 0; b < 3; ++b) ob[b] = bands.data() + b * n;
+    decodeRLHuff(br, ob, u32(n), cb, log2Max);
+    std::vector<i16> c(nx * ny);
+    for (long y = 0; y < hy; ++y)
+        for (long x = 0; x < hx; ++x) c[y * nx + x] = lowpass[y * hx + x];
+    for (int b = 1; b < 4; ++b)
+        for (long y = 0; y < hy; ++y)
+            for (long x = 0; x < hx; ++x)
+                c[(y + (b / 2) * hy) * nx + x + (b % 2) * hx] = i16(unsymbolize(ob[b - 1][y * hx + x]));
+    dwtInt(c.data(), image, nx, ny, 1, true);
     return 0;
 }
 

@@ -19,8 +19,10 @@
 #include <cudaCompress/InstanceImpl.h>
 #include <cudaCompress/HuffmanTable.h>
 #include <cudaCompress/Encode.h>
+#include <cudaCompress/util/Bits.h>
 #include <cudaCompress/util/DWT.h>
 #include <cudaCompress/util/Quantize.h>
+#include <cudaCompress/util/YCoCg.h>
 #undef private
 
 using namespace cudaCompress;
@@ -136,4 +138,77 @@ void ref_quantize_to_symbols(uint16_t* out, const float* src, uint32_t nx, uint3
     cudaDeviceSynchronize();
 }
 
+// ---- the 2D image side of util (DWT byte / lowpass-only variants, byte
+// quantizers, YCoCg, Bits); all on the default stream as the reference runs
+// them, synchronized before returning.
+void ref_dwt_float_fwd_from_byte(float* dst, float* buf2, float* buf1, const uint8_t* src, int nx, int ny, int nz,
+                                 int ch) {
+    if (nz > 1) util::dwtFloat3DForwardFromByte(dst, buf2, buf1, src, nx, ny, nz, ch);
+    else util::dwtFloat2DForwardFromByte(dst, buf1, src, nx, ny, ch);
+    cudaDeviceSynchronize();
 }
+void ref_dwt_float_inv_to_byte(uint8_t* dst, float* buf2, float* buf1, const float* src, int nx, int ny, int nz,
+                               int ch) {
+    if (nz > 1) util::dwtFloat3DInverseToByte(dst, buf2, buf1, src, nx, ny, nz, ch);
+    else util::dwtFloat2DInverseToByte(dst, buf1, src, nx, ny, ch);
+    cudaDeviceSynchronize();
+}
+void ref_dwt_float_inv_from_symbols_to_byte(uint8_t* dst, float* buf2, float* buf1, const float* lowpass,
+                                            const uint16_t* const* dHighpass, float step, int nx, int ny, int nz,
+                                            int ch) {
+    const ushort* const* hp = reinterpret_cast<const ushort* const*>(dHighpass);
+    if (nz > 1) util::dwtFloat3DInverseFromSymbolsToByte(dst, buf2, buf1, lowpass, hp, step, nx, ny, nz, ch);
+    else util::dwtFloat2DInverseFromSymbolsToByte(dst, buf1, lowpass, hp, step, nx, ny, ch);
+    cudaDeviceSynchronize();
+}
+void ref_dwt_float2d_lowpass_from_byte(float* dst, float* buf, const uint8_t* src, int nx, int ny, int ch) {
+    util::dwtFloat2DForwardLowpassOnlyFromByte(dst, buf, src, nx, ny, ch);
+    cudaDeviceSynchronize();
+}
+void ref_dwt_int_lowpass(short* dst, short* buf, const short* src, int nx, int ny) {
+    util::dwtIntForwardLowpassOnly(dst, buf, src, nx, ny);
+    cudaDeviceSynchronize();
+}
+void ref_float_to_byte_2d(uint8_t* out, uint32_t chCount, uint32_t ch, const float* in, uint32_t nx, uint32_t ny,
+                          uint32_t rowPitch) {
+    util::floatToByte2D(out, chCount, ch, in, nx, ny, rowPitch);
+    cudaDeviceSynchronize();
+}
+void ref_byte_to_float_2d(float* out, const uint8_t* in, uint32_t chCount, uint32_t ch, uint32_t nx, uint32_t ny,
+                          uint32_t rowPitch) {
+    util::byteToFloat2D(out, in, chCount, ch, nx, ny, rowPitch);
+    cudaDeviceSynchronize();
+}
+void ref_quantize_difference_2d(uint16_t* sym, float* data, float step, const uint8_t* ref, uint32_t chCount,
+                                uint32_t ch, uint32_t nx, uint32_t ny, uint32_t rowPitch, int type, int roundtrip) {
+    const util::EQuantizeType t = type ? util::QUANTIZE_UNIFORM : util::QUANTIZE_DEADZONE;
+    if (roundtrip) util::quantizeDifferenceToSymbolsRoundtrip2D(sym, data, step, ref, chCount, ch, nx, ny, rowPitch, t);
+    else util::quantizeDifferenceToSymbols2D(sym, data, step, ref, chCount, ch, nx, ny, rowPitch, t);
+    cudaDeviceSynchronize();
+}
+void ref_unquantize_difference_2d(float* data, const uint16_t* sym, float step, const uint8_t* ref, uint32_t chCount,
+                                  uint32_t ch, uint32_t nx, uint32_t ny, uint32_t rowPitch, int type) {
+    const util::EQuantizeType t = type ? util::QUANTIZE_UNIFORM : util::QUANTIZE_DEADZONE;
+    util::unquantizeDifferenceFromSymbols2D(data, sym, step, ref, chCount, ch, nx, ny, rowPitch, t);
+    cudaDeviceSynchronize();
+}
+void ref_ycocg(uint8_t* dst, const uint8_t* src, int n, int channels, int toYCoCg) {
+    if (channels == 3) {
+        if (toYCoCg) util::convertRGBtoYCoCg(reinterpret_cast<uchar3*>(dst), reinterpret_cast<const uchar3*>(src), n);
+        else util::convertYCoCgtoRGB(reinterpret_cast<uchar3*>(dst), reinterpret_cast<const uchar3*>(src), n);
+    } else {
+        if (toYCoCg) util::convertRGBtoYCoCg(reinterpret_cast<uchar4*>(dst), reinterpret_cast<const uchar4*>(src), n);
+        else util::convertYCoCgtoRGB(reinterpret_cast<uchar4*>(dst), reinterpret_cast<const uchar4*>(src), n);
+    }
+    cudaDeviceSynchronize();
+}
+// mode 0 getLSB, 1 removeLSB (bits may be null), 2 appendLSB, 3 shiftElems
+void ref_lsb(int mode, short* data, uint32_t* bits, uint32_t n, short shift) {
+    if (mode == 0) util::getLSB(data, bits, n);
+    else if (mode == 1) util::removeLSB(data, bits, n, shift);
+    else if (mode == 2) util::appendLSB(data, bits, n, shift);
+    else util::shiftElems(data, n, shift);
+    cudaDeviceSynchronize();
+}
+
+}  // extern "C"

@@ -18,6 +18,11 @@ ref_volume.npz   the reference's example volume codec (examples/CompressVolume.c
                  decoders' outputs (python tests/golden/make_golden.py --gpu --only volume).
                  Inputs are seeded fields (cudacompress_b200.fields), stored as seed +
                  SHA-256 of the generated array.
+ref_image.npz    the 2D image side: util byte-DWT, lowpass-only, byte-image quantizer,
+                 YCoCg and Bits outputs, and the examples' one-level image and
+                 heightfield codecs (CompressImage.cpp, CompressHeightfield.cpp):
+                 streams, reconstructions and lowpass bands, with their inputs
+                 (python tests/golden/make_golden.py --gpu --only image).
 """
 import argparse
 import hashlib
@@ -281,10 +286,226 @@ def make_volume(ref, out_dir):
     print("ref_volume.npz written")
 
 
+def test_image(shape, seed):
+    """Seeded smooth 8-bit test image (y, x, channels): two plane waves per
+    channel plus uniform noise, clipped to [0, 255]."""
+    ny, nx, ch = shape
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    out = np.empty(shape, np.uint8)
+    for c in range(ch):
+        k = rng.uniform(0.02, 0.2, 4)
+        v = 128 + 70 * np.sin(k[0] * x + k[1] * y) + 40 * np.cos(k[2] * x - k[3] * y) + rng.uniform(-12, 12, (ny, nx))
+        out[..., c] = np.clip(np.rint(v), 0, 255).astype(np.uint8)
+    return out
+
+
+def test_heightfield(shape, seed):
+    """Seeded int16 terrain-like field: cumulative sums of small steps."""
+    rng = np.random.default_rng(seed)
+    v = np.cumsum(np.cumsum(rng.integers(-6, 7, shape), axis=0), axis=1)
+    return np.clip(v, -30000, 30000).astype(np.int16)
+
+
+IMAGE_CODEC_CASES = [
+    # name, (ny, nx, channels), channels coded, steps per image
+    ("c3", (48, 64, 3), 3, (4.0,)),
+    ("c4", (64, 96, 4), 3, (2.0,)),
+    ("m3", (64, 64, 4), 3, (2.0, 4.0, 8.0)),
+]
+HEIGHTFIELD_CASES = [("h0", (128, 512), 0), ("h3", (64, 1024), 3)]
+
+
+def make_image(ref, out_dir):
+    import torch
+    i32, u32, f32 = c.c_int, c.c_uint32, c.c_float
+    vp = c.c_void_p
+    u32p = c.POINTER(c.c_uint32)
+    ref.ref_dwt_float_fwd_from_byte.argtypes = [vp] * 4 + [i32] * 4
+    ref.ref_dwt_float_inv_to_byte.argtypes = [vp] * 4 + [i32] * 4
+    ref.ref_dwt_float_inv_from_symbols_to_byte.argtypes = [vp] * 5 + [f32] + [i32] * 4
+    ref.ref_dwt_float2d_lowpass_from_byte.argtypes = [vp] * 3 + [i32] * 3
+    ref.ref_dwt_int_lowpass.argtypes = [vp] * 3 + [i32] * 2
+    ref.ref_float_to_byte_2d.argtypes = [vp, u32, u32, vp, u32, u32, u32]
+    ref.ref_byte_to_float_2d.argtypes = [vp, vp, u32, u32, u32, u32, u32]
+    ref.ref_quantize_difference_2d.argtypes = [vp, vp, f32, vp, u32, u32, u32, u32, u32, i32, i32]
+    ref.ref_unquantize_difference_2d.argtypes = [vp, vp, f32, vp, u32, u32, u32, u32, u32, i32]
+    ref.ref_ycocg.argtypes = [vp, vp, i32, i32, i32]
+    ref.ref_lsb.argtypes = [i32, vp, vp, u32, c.c_int16]
+    ref.ref_images_compress.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, u32p, u32, u32p]
+    ref.ref_images_decompress.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, u32p, u32p]
+    ref.ref_get_lowpass_image.argtypes = [vp, u32, u32, u32, u32, vp]
+    ref.ref_heightfield_compress_one_level.argtypes = [vp, u32, u32, vp, c.c_int16, u32p, u32, u32p]
+    ref.ref_heightfield_decompress_one_level.argtypes = [vp, u32, u32, vp, c.c_int16, u32p, u32]
+    ref.ref_get_lowpass_heightfield.argtypes = [vp, u32, u32, vp, c.c_int16]
+    P = lambda t: c.c_void_p(t.data_ptr())  # noqa: E731
+    cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    out = {}
+
+    # byte DWT forward / inverse, 2D (3 channels) and 3D (2 channels)
+    for name, shape, ch in [("b2", (48, 64), 3), ("b3", (16, 16, 32), 2)]:
+        dims = shape if len(shape) == 3 else (1,) + shape
+        nz, ny, nx = dims
+        img = test_image((nz * ny, nx, ch), 700 + len(shape)).reshape(dims + (ch,))
+        src = cu(img)
+        out[f"{name}_in"] = img
+        for cc in range(ch):
+            dst, b1, b2 = (torch.empty(dims, dtype=torch.float32, device="cuda") for _ in range(3))
+            ref.ref_dwt_float_fwd_from_byte(P(dst), P(b2), P(b1), c.c_void_p(src.data_ptr() + cc), nx, ny, nz, ch)
+            out[f"{name}_fwd{cc}"] = dst.cpu().numpy()
+        # inverse of channel 0's coefficients, scaled to reach the clamp, into channel 1 of a patterned image
+        coef = torch.from_numpy(out[f"{name}_fwd0"] * 1.7).cuda()
+        tgt = cu(np.full(dims + (ch,), 77, np.uint8))
+        b1, b2 = (torch.empty(dims, dtype=torch.float32, device="cuda") for _ in range(2))
+        ref.ref_dwt_float_inv_to_byte(c.c_void_p(tgt.data_ptr() + 1), P(b2), P(b1), P(coef), nx, ny, nz, ch)
+        out[f"{name}_invcoef"] = out[f"{name}_fwd0"] * np.float32(1.7)
+        out[f"{name}_inv"] = tgt.cpu().numpy()
+        # inverse from symbols to bytes: lowpass in a full-size array (default pitches), random bands
+        rng = np.random.default_rng(710 + len(shape))
+        nb = 7 if nz > 1 else 3
+        hz = max(nz // 2, 1)
+        bands = rng.integers(0, 40, (nb, hz, ny // 2, nx // 2)).astype(np.uint16)
+        lpfull = (out[f"{name}_fwd0"]).copy()
+        dband = [cu(bands[k]) for k in range(nb)]
+        ptrs = torch.tensor([t.data_ptr() for t in dband], dtype=torch.int64, device="cuda")
+        tgt = cu(np.full(dims + (ch,), 55, np.uint8))
+        dlp = cu(lpfull)
+        ref.ref_dwt_float_inv_from_symbols_to_byte(c.c_void_p(tgt.data_ptr() + ch - 1), P(b2), P(b1), P(dlp),
+                                                   P(ptrs), 0.75, nx, ny, nz, ch)
+        out[f"{name}_symbands"], out[f"{name}_symlp"], out[f"{name}_symout"] = bands, lpfull, tgt.cpu().numpy()
+
+    # lowpass-only transforms
+    for name, (ny, nx, ch, cc) in [("lf", (48, 64, 3, 1)), ("lfr", (72, 200, 1, 0))]:
+        img = test_image((ny, nx, ch), 720 + nx)
+        dst = torch.full((ny // 2, nx // 2), float("nan"), dtype=torch.float32, device="cuda")
+        buf = torch.empty((ny, nx), dtype=torch.float32, device="cuda")
+        src = cu(img)
+        ref.ref_dwt_float2d_lowpass_from_byte(P(dst), P(buf), c.c_void_p(src.data_ptr() + cc), nx, ny, ch)
+        out[f"{name}_in"], out[f"{name}_meta"], out[f"{name}_out"] = img, np.array([cc], np.int32), dst.cpu().numpy()
+    for name, (ny, nx) in [("li", (128, 512)), ("li2", (64, 1024))]:
+        hf = test_heightfield((ny, nx), 730 + nx)
+        dst = torch.zeros((ny // 2, nx // 2), dtype=torch.int16, device="cuda")
+        buf = torch.empty((ny, nx), dtype=torch.int16, device="cuda")
+        dhf = cu(hf)
+        ref.ref_dwt_int_lowpass(P(dst), P(buf), P(dhf), nx, ny)
+        out[f"{name}_in"], out[f"{name}_out"] = hf, dst.cpu().numpy()
+
+    # byte-image quantizers (40 x 24 region, row pitch 48, 3 channels, channel 1)
+    nx, ny, pitch, chc, ch = 40, 24, 48, 3, 1
+    rng = np.random.default_rng(740)
+    data = rng.normal(0, 40, (ny, pitch)).astype(np.float32)
+    refimg = rng.integers(0, 256, (ny, nx, chc)).astype(np.uint8)
+    qb = torch.zeros((ny, nx, chc), dtype=torch.uint8, device="cuda")
+    d3, dref = cu(data * 3), cu(refimg)
+    ref.ref_float_to_byte_2d(P(qb), chc, ch, P(d3), nx, ny, pitch)
+    fb = torch.zeros((ny, pitch), dtype=torch.float32, device="cuda")
+    ref.ref_byte_to_float_2d(P(fb), P(dref), chc, ch, nx, ny, pitch)
+    out["q_data"], out["q_ref"], out["q_f2b"], out["q_b2f"] = data, refimg, qb.cpu().numpy(), fb.cpu().numpy()
+    for t in (0, 1):
+        for rt in (0, 1):
+            d = cu(data)
+            sym = torch.zeros((ny, nx), dtype=torch.int16, device="cuda")
+            ref.ref_quantize_difference_2d(P(sym), P(d), 3.0, P(dref), chc, ch, nx, ny, pitch, t, rt)
+            out[f"q_sym{t}{rt}"] = sym.cpu().numpy().view(np.uint16)
+            out[f"q_data{t}{rt}"] = d.cpu().numpy()
+        back = cu(np.full((ny, pitch), -1.0, np.float32))
+        dsym = cu(out[f"q_sym{t}0"].view(np.int16))
+        ref.ref_unquantize_difference_2d(P(back), P(dsym), 3.0, P(dref), chc, ch, nx, ny, pitch, t)
+        out[f"q_unq{t}"] = back.cpu().numpy()
+
+    # YCoCg, every byte value, both pixel sizes and directions
+    rng = np.random.default_rng(750)
+    for chn in (3, 4):
+        px = rng.integers(0, 256, (1000, chn)).astype(np.uint8)
+        dpx = cu(px)
+        for d in (1, 0):
+            dst = torch.zeros_like(dpx)
+            ref.ref_ycocg(P(dst), P(dpx), 1000, chn, d)
+            out[f"y{chn}_{d}"] = dst.cpu().numpy()
+        out[f"y{chn}_in"] = px
+
+    # Bits on 8192 elements (whole blocks of 4096, as the reference requires)
+    n = 8192
+    vals = rng.integers(-3000, 3000, n).astype(np.int16)
+    bits0 = rng.integers(0, 2 ** 32, n // 32, dtype=np.uint64).astype(np.uint32)
+    out["l_in"], out["l_bits_in"] = vals, bits0
+    for mode, shift in [(0, 0), (1, 0), (1, 3), (2, 0), (2, -5), (3, 7)]:
+        d = cu(vals)
+        b = cu(bits0.view(np.int32)) if mode == 2 else torch.zeros(n // 32, dtype=torch.int32, device="cuda")
+        ref.ref_lsb(mode, P(d), P(b), n, shift)
+        out[f"l{mode}_{shift}_data"] = d.cpu().numpy()
+        out[f"l{mode}_{shift}_bits"] = b.cpu().numpy().view(np.uint32)
+    d = cu(vals)
+    ref.ref_lsb(1, P(d), None, n, 2)
+    out["l1n_2_data"] = d.cpu().numpy()
+
+    # one image level: single images and a batch of three
+    for name, shape, proc, steps in IMAGE_CODEC_CASES:
+        ny, nx, ch = shape
+        count = len(steps)
+        imgs = [test_image(shape, 760 + 10 * IMAGE_CODEC_CASES.index((name, shape, proc, steps)) + k)
+                for k in range(count)]
+        dimg = [cu(im) for im in imgs]
+        drefs = []
+        for k in range(count):
+            lp = torch.zeros((ny // 2, nx // 2, ch), dtype=torch.uint8, device="cuda")
+            r = ref.ref_get_lowpass_image(P(dimg[k]), nx, ny, ch, proc, P(lp))
+            assert r == 0, r
+            drefs.append(lp)
+        cap = nx * ny * ch * 4 * count + 65536
+        words = np.zeros(cap, np.uint32)
+        offs = np.zeros(count + 1, np.uint32)
+        ip = (c.c_void_p * count)(*[t.data_ptr() for t in dimg])
+        rp = (c.c_void_p * count)(*[t.data_ptr() for t in drefs])
+        qs = (c.c_float * count)(*steps)
+        r = ref.ref_images_compress(ip, rp, qs, count, nx, ny, ch, proc, words.ctypes.data_as(u32p), cap,
+                                    offs.ctypes.data_as(u32p))
+        assert r == 0, r
+        recon = [t.cpu().numpy() for t in dimg]
+        outs = [cu(np.full(shape, 201, np.uint8)) for _ in range(count)]
+        op = (c.c_void_p * count)(*[t.data_ptr() for t in outs])
+        r = ref.ref_images_decompress(op, rp, qs, count, nx, ny, ch, proc, words.ctypes.data_as(u32p),
+                                      offs.ctypes.data_as(u32p))
+        assert r == 0, r
+        out[f"{name}_meta"] = np.array([proc, count], np.int32)
+        out[f"{name}_steps"] = np.array(steps, np.float32)
+        out[f"{name}_offsets"] = offs
+        out[f"{name}_words"] = words[: offs[-1]].copy()
+        for k in range(count):
+            out[f"{name}_in{k}"], out[f"{name}_lp{k}"] = imgs[k], drefs[k].cpu().numpy()
+            out[f"{name}_rec{k}"], out[f"{name}_dec{k}"] = recon[k], outs[k].cpu().numpy()
+
+    # one heightfield level and its lowpass
+    for name, (ny, nx), shift in HEIGHTFIELD_CASES:
+        hf = test_heightfield((ny, nx), 780 + shift)
+        dimg = cu(hf)
+        lp = torch.zeros((ny // 2, nx // 2), dtype=torch.int16, device="cuda")
+        cap = nx * ny + 65536
+        words = np.zeros(cap, np.uint32)
+        nw = c.c_uint32()
+        r = ref.ref_heightfield_compress_one_level(P(dimg), nx, ny, P(lp), shift, words.ctypes.data_as(u32p), cap,
+                                                   c.byref(nw))
+        assert r == 0, r
+        out[f"{name}_in"], out[f"{name}_lp"] = hf, lp.cpu().numpy()
+        out[f"{name}_words"] = words[: nw.value].copy()
+        rec = torch.zeros_like(dimg)
+        r = ref.ref_heightfield_decompress_one_level(P(rec), nx, ny, P(lp), shift, words.ctypes.data_as(u32p),
+                                                     nw.value)
+        assert r == 0, r
+        out[f"{name}_dec"], out[f"{name}_lpdec"] = rec.cpu().numpy(), lp.cpu().numpy()
+        lp2 = torch.zeros_like(lp)
+        r = ref.ref_get_lowpass_heightfield(P(dimg), nx, ny, P(lp2), shift + 2)
+        assert r == 0, r
+        out[f"{name}_getlp"] = lp2.cpu().numpy()
+        out[f"{name}_shift"] = np.array([shift], np.int32)
+    np.savez_compressed(os.path.join(out_dir, "ref_image.npz"), **out)
+    print("ref_image.npz written")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpu", action="store_true", help="also run the reference's GPU code")
-    ap.add_argument("--only", choices=["volume"], help="only the whole-volume fixtures (GPU)")
+    ap.add_argument("--only", choices=["volume", "image"], help="only the whole-volume or image fixtures (GPU)")
     ap.add_argument("--out", default=HERE, help="output directory")
     args = ap.parse_args()
     ref = load_ref_gpu_lib()
@@ -293,11 +514,15 @@ def main():
     if args.only == "volume":
         make_volume(ref, args.out)
         return
+    if args.only == "image":
+        make_image(ref, args.out)
+        return
     make_tables(ref)
     if args.gpu:
         make_streams(ref)
         make_dwt(ref)
         make_volume(ref, args.out)
+        make_image(ref, args.out)
 
 
 if __name__ == "__main__":

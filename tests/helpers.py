@@ -227,6 +227,183 @@ class Oracle:
         return out
 
 
+class ImageOracle:
+    """The oracle's 2D image side (oracle/oracle.cpp): byte DWTs, lowpass-only
+    transforms, byte-image quantizers, YCoCg, Bits and the one-level image and
+    heightfield codecs, on numpy arrays."""
+
+    def __init__(self):
+        self.lib = L = load_oracle()
+        c = ctypes
+        vp, lg, u32, f32, i32 = c.c_void_p, c.c_long, c.c_uint32, c.c_float, c.c_int
+        L.orc_dwt_float_fwd_from_byte.argtypes = [vp, lg, vp, lg, lg, lg]
+        L.orc_dwt_float_inv_to_byte.argtypes = [vp, vp, lg, lg, lg, lg]
+        L.orc_dwt_float_inv_from_symbols_to_byte.argtypes = [vp, vp, f32, vp, lg, lg, lg, lg]
+        L.orc_dwt_float2d_lowpass_from_byte.argtypes = [vp, lg, vp, lg, lg]
+        L.orc_dwt_int_lowpass.argtypes = [vp, vp, lg, lg]
+        L.orc_float_to_byte_2d.argtypes = [vp, lg, lg, vp, lg, lg, lg]
+        L.orc_byte_to_float_2d.argtypes = [vp, vp, lg, lg, lg, lg, lg]
+        L.orc_quantize_difference_2d.argtypes = [vp, vp, f32, vp, lg, lg, lg, lg, lg, i32, i32]
+        L.orc_unquantize_difference_2d.argtypes = [vp, vp, f32, vp, lg, lg, lg, lg, lg, i32]
+        L.orc_ycocg.argtypes = [vp, vp, lg, i32, i32]
+        L.orc_lsb.argtypes = [i32, vp, vp, u32, c.c_int16]
+        L.orc_shift_elems.argtypes = [vp, u32, c.c_int16]
+        L.orc_get_lowpass_image.argtypes = [vp, lg, lg, lg, lg, vp]
+        L.orc_get_lowpass_heightfield.argtypes = [vp, lg, lg, vp, c.c_int16]
+        L.orc_compress_image_one_level.argtypes = [vp, lg, lg, lg, lg, vp, f32, u32, u32, vp, u32, c.POINTER(u32)]
+        L.orc_decompress_image_one_level.argtypes = [vp, u32, vp, lg, lg, lg, lg, vp, f32, u32, u32]
+        L.orc_compress_heightfield_one_level.argtypes = [vp, lg, lg, vp, c.c_int16, u32, u32, vp, u32, c.POINTER(u32)]
+        L.orc_decompress_heightfield_one_level.argtypes = [vp, u32, vp, lg, lg, vp, c.c_int16, u32, u32]
+        for n in ["orc_compress_image_one_level", "orc_decompress_image_one_level",
+                  "orc_compress_heightfield_one_level", "orc_decompress_heightfield_one_level"]:
+            getattr(L, n).restype = c.c_int
+
+    @staticmethod
+    def _p(a, offset=0):
+        return ctypes.c_void_p(a.ctypes.data + offset)
+
+    def dwt_fwd_from_byte(self, img, channel):
+        """img (..., channels) uint8, dims (z, y, x) or (y, x)."""
+        img = np.ascontiguousarray(img)
+        ch = img.shape[-1]
+        dims = img.shape[:-1]
+        nz, ny, nx = (1,) + dims if len(dims) == 2 else dims
+        out = np.zeros(dims, np.float32)
+        self.lib.orc_dwt_float_fwd_from_byte(self._p(img, channel), ch, self._p(out), nx, ny, nz)
+        return out
+
+    def dwt_inv_to_byte(self, coef, target, channel):
+        """Writes channel `channel` of target (..., channels) in place."""
+        coef = np.ascontiguousarray(coef, np.float32)
+        ch = target.shape[-1]
+        dims = coef.shape
+        nz, ny, nx = (1,) + dims if len(dims) == 2 else dims
+        self.lib.orc_dwt_float_inv_to_byte(self._p(coef), self._p(target, channel), ch, nx, ny, nz)
+
+    def dwt_inv_from_symbols_to_byte(self, lowpass, bands, step, target, channel):
+        """lowpass: dense (z/2, y/2, x/2) or (y/2, x/2) float; bands: u16 array of 3 or 7 bands."""
+        lowpass = np.ascontiguousarray(lowpass, np.float32)
+        bands = [np.ascontiguousarray(b, np.uint16) for b in bands]
+        ptrs = (ctypes.c_void_p * len(bands))(*[b.ctypes.data for b in bands])
+        ch = target.shape[-1]
+        dims = target.shape[:-1]
+        nz, ny, nx = (1,) + dims if len(dims) == 2 else dims
+        self.lib.orc_dwt_float_inv_from_symbols_to_byte(self._p(lowpass), ctypes.cast(ptrs, ctypes.c_void_p), step,
+                                                        self._p(target, channel), ch, nx, ny, nz)
+
+    def lowpass_from_byte(self, img, channel):
+        img = np.ascontiguousarray(img)
+        ny, nx, ch = img.shape
+        out = np.zeros((ny // 2, nx // 2), np.float32)
+        self.lib.orc_dwt_float2d_lowpass_from_byte(self._p(img, channel), ch, self._p(out), nx, ny)
+        return out
+
+    def int_lowpass(self, img):
+        img = np.ascontiguousarray(img, np.int16)
+        ny, nx = img.shape
+        out = np.zeros((ny // 2, nx // 2), np.int16)
+        self.lib.orc_dwt_int_lowpass(self._p(img), self._p(out), nx, ny)
+        return out
+
+    def float_to_byte_2d(self, out, channel, data, nx, ny, pitch):
+        self.lib.orc_float_to_byte_2d(self._p(out), out.shape[-1], channel, self._p(data), nx, ny, pitch)
+
+    def byte_to_float_2d(self, out, img, channel, nx, ny, pitch):
+        self.lib.orc_byte_to_float_2d(self._p(out), self._p(img), img.shape[-1], channel, nx, ny, pitch)
+
+    def quantize_difference(self, data, step, ref, channel, nx, ny, pitch, quant_type=0, roundtrip=False):
+        """Returns the symbols; data (float32, row pitch `pitch`) is updated by the round trip."""
+        sym = np.zeros((ny, nx), np.uint16)
+        self.lib.orc_quantize_difference_2d(self._p(sym), self._p(data), step, self._p(ref), ref.shape[-1], channel,
+                                            nx, ny, pitch, quant_type, int(roundtrip))
+        return sym
+
+    def unquantize_difference(self, out, sym, step, ref, channel, nx, ny, pitch, quant_type=0):
+        sym = np.ascontiguousarray(sym, np.uint16)
+        self.lib.orc_unquantize_difference_2d(self._p(out), self._p(sym), step, self._p(ref), ref.shape[-1], channel,
+                                              nx, ny, pitch, quant_type)
+
+    def ycocg(self, px, to_ycocg=True):
+        px = np.ascontiguousarray(px, np.uint8)
+        out = np.zeros_like(px)
+        self.lib.orc_ycocg(self._p(out), self._p(px), px.shape[0], px.shape[1], int(to_ycocg))
+        return out
+
+    def lsb(self, mode, data, bits=None, shift=0):
+        """mode 0 get, 1 remove, 2 append; returns (data, bits) copies."""
+        data = np.array(data, np.int16)
+        n = data.size
+        if bits is None and mode == 0:
+            bits = np.zeros((n + 31) // 32, np.uint32)
+        bits = None if bits is None else np.array(bits, np.uint32)
+        self.lib.orc_lsb(mode, self._p(data), None if bits is None else self._p(bits), n, shift)
+        return data, bits
+
+    def shift_elems(self, data, shift):
+        data = np.array(data, np.int16)
+        self.lib.orc_shift_elems(self._p(data), data.size, shift)
+        return data
+
+    def lowpass_image(self, img, channels_to_process):
+        img = np.ascontiguousarray(img)
+        ny, nx, ch = img.shape
+        out = np.zeros((ny // 2, nx // 2, ch), np.uint8)
+        self.lib.orc_get_lowpass_image(self._p(img), nx, ny, ch, channels_to_process, self._p(out))
+        return out
+
+    def lowpass_heightfield(self, img, shift):
+        img = np.ascontiguousarray(img, np.int16)
+        ny, nx = img.shape
+        out = np.zeros((ny // 2, nx // 2), np.int16)
+        self.lib.orc_get_lowpass_heightfield(self._p(img), nx, ny, self._p(out), shift)
+        return out
+
+    def compress_image(self, img, channels_to_process, lowpass_ref, step, cb=128, log2max=14):
+        """Returns (words, bit size, reconstruction)."""
+        rec = np.array(img, np.uint8)
+        ny, nx, ch = rec.shape
+        lowpass_ref = np.ascontiguousarray(lowpass_ref, np.uint8)
+        cap = rec.size * 4 + 65536
+        words = np.zeros(cap, np.uint32)
+        bits = ctypes.c_uint32()
+        r = self.lib.orc_compress_image_one_level(self._p(rec), nx, ny, ch, channels_to_process, self._p(lowpass_ref),
+                                                  step, cb, log2max, self._p(words), cap, ctypes.byref(bits))
+        assert r == 0, r
+        return words[: (bits.value + 31) // 32].copy(), bits.value, rec
+
+    def decompress_image(self, words, bit_size, out, channels_to_process, lowpass_ref, step, cb=128, log2max=14):
+        ny, nx, ch = out.shape
+        words = np.ascontiguousarray(words, np.uint32)
+        lowpass_ref = np.ascontiguousarray(lowpass_ref, np.uint8)
+        r = self.lib.orc_decompress_image_one_level(self._p(words), bit_size, self._p(out), nx, ny, ch,
+                                                    channels_to_process, self._p(lowpass_ref), step, cb, log2max)
+        assert r == 0, r
+
+    def compress_heightfield_one_level(self, img, shift, cb=128, log2max=14):
+        """Returns (words, bit size, lowpass)."""
+        img = np.ascontiguousarray(img, np.int16)
+        ny, nx = img.shape
+        lp = np.zeros((ny // 2, nx // 2), np.int16)
+        cap = img.size + 65536
+        words = np.zeros(cap, np.uint32)
+        bits = ctypes.c_uint32()
+        r = self.lib.orc_compress_heightfield_one_level(self._p(img), nx, ny, self._p(lp), shift, cb, log2max,
+                                                        self._p(words), cap, ctypes.byref(bits))
+        assert r == 0, r
+        return words[: (bits.value + 31) // 32].copy(), bits.value, lp
+
+    def decompress_heightfield_one_level(self, words, bit_size, shape, lowpass, shift, cb=128, log2max=14):
+        """Returns (image, restored lowpass)."""
+        ny, nx = shape
+        out = np.zeros(shape, np.int16)
+        lp = np.array(lowpass, np.int16)
+        words = np.ascontiguousarray(words, np.uint32)
+        r = self.lib.orc_decompress_heightfield_one_level(self._p(words), bit_size, self._p(out), nx, ny, self._p(lp),
+                                                          shift, cb, log2max)
+        assert r == 0, r
+        return out, lp
+
+
 def symbol_streams(kind, S, n, seed, dtype=np.uint16, max_symbol=200):
     """Seeded symbol streams of the shapes the codec meets."""
     rng = np.random.default_rng(seed)
