@@ -310,7 +310,9 @@ int cc_decompress_heightfield(cc_instance* inst, int16_t* d_image, uint32_t size
  * holds the ceil(n/32) words of the least significant bits of (LL + shift),
  * n = size_x/2 * size_y/2, then one encodeRLHuff call over the 3 symbolized
  * highpass bands.  d_lowpass (n shorts) receives (LL + shift) without that
- * bit; decompress restores it in place (appendLSB) and rebuilds the image.
+ * bit; decompress appends the bit to it in place and adds its own shift
+ * (appendLSB), then rebuilds the image - so, as in the reference, shift 0 on
+ * both sides (or the negated shift to decompress) reproduces the image.
  * getLowpassHeightfield (:218-235): the same d_lowpass, without coding. */
 int cc_compress_heightfield_one_level(cc_instance* inst, const int16_t* d_image, uint32_t size_x, uint32_t size_y,
                                       int16_t* d_lowpass, int16_t lowpass_shift, uint32_t* d_words,
