@@ -20,6 +20,7 @@ LIB = os.path.join(HERE, "_lib")
 OBJ = os.path.join(HERE, "_build")
 
 CUDA_SOURCES = ["instance.cu", "encode.cu", "decode.cu", "dwt.cu", "quantize.cu", "image.cu", "pipeline.cu", "batch.cu",
+                "cuda_timer.cu",
                 "container.cu", "cxx_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", 
