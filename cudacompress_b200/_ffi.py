@@ -119,6 +119,8 @@ _SIGS = {
                                        ctypes.POINTER(c_u64)]),
     "cc_volume_batch_read_stream": (c_int, [c_vp, c_u32, c_vp, c_u64, ctypes.POINTER(c_u64)]),
     "cc_volume_batch_load_streams": (c_int, [c_vp, c_vpp, ctypes.POINTER(c_u64)]),
+    "cc_volume_batch_download_streams": (c_int, [c_vp, c_vp, c_u64, c_vp]),
+    "cc_volume_batch_upload_streams": (c_int, [c_vp, c_vp, c_vp]),
     "cc_volume_batch_status": (c_int, [c_vp]),
     "cc_volume_batch_collect_timings": (None, [c_vp]),
 }

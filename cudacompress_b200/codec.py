@@ -504,5 +504,18 @@ class VolumeBatch:
         bits = (ctypes.c_uint64 * len(ptrs))(*[int(b) for b in bit_sizes])
         check(lib().cc_volume_batch_load_streams(self.handle, arr, bits), "cc_volume_batch_load_streams")
 
+    def download_streams(self, host_words: torch.Tensor, host_extents: torch.Tensor) -> None:
+        """Enqueues the copy of the active volumes' streams into page-locked
+        host tensors (int32 words, int64 extents: offsets then bit sizes);
+        complete once the batch's stream reaches it."""
+        check(lib().cc_volume_batch_download_streams(self.handle, host_words.data_ptr(), host_words.numel(),
+                                                     host_extents.data_ptr()), "cc_volume_batch_download_streams")
+
+    def upload_streams(self, host_words: torch.Tensor, host_extents: torch.Tensor) -> None:
+        """Enqueues the copy of streams laid out as download_streams writes
+        them back into the batch, for decompress()."""
+        check(lib().cc_volume_batch_upload_streams(self.handle, host_words.data_ptr(), host_extents.data_ptr()),
+              "cc_volume_batch_upload_streams")
+
     def collect_timings(self) -> None:
         lib().cc_volume_batch_collect_timings(self.handle)

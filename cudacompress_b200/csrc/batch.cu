@@ -206,6 +206,59 @@ __global__ void __launch_bounds__(256) k_brickConcat(const u32* lpOut, const u32
     for (u64 w = w0 + threadIdx.x; w < w1; w += blockDim.x) out[w] = w < lpW ? lpOut[lpS + w] : hpOut[hpS + (w - lpW)];
 }
 
+// Streams of the first n volumes between the batch's word buffer (HBM) and
+// page-locked host memory, moved by kernels so that nothing waits on the
+// host: the used extent (the streams lie back to back, the last one ending at
+// wordOff[n-1] + its words) is known on the device only.  hExt holds the n
+// word offsets, then the n bit sizes.  16-byte copies when both sides allow.
+template <bool kVec>
+__global__ void __launch_bounds__(256) k_streamsToHost(const u32* __restrict__ words, const u64* __restrict__ wordOff,
+                                                       const u64* __restrict__ bitSize, u32 n, u32* hWords, u64 cap,
+                                                       u64* hExt, u32* err) {
+    const u64 total = wordOff[n - 1] + (bitSize[n - 1] + 31) / 32;
+    const u64 tid = u64(blockIdx.x) * blockDim.x + threadIdx.x, nth = u64(gridDim.x) * blockDim.x;
+    if (tid < n) {
+        hExt[tid] = wordOff[tid];
+        hExt[n + tid] = bitSize[tid];
+    }
+    if (total > cap) {
+        if (tid == 0) atomicOr(err, u32(DEV_ERR_OUTPUT_CAPACITY));
+        return;
+    }
+    u64 done = 0;
+    if (kVec) {
+        const u64 q = total / 4;
+        for (u64 i = tid; i < q; i += nth) reinterpret_cast<uint4*>(hWords)[i] = reinterpret_cast<const uint4*>(words)[i];
+        done = q * 4;
+    }
+    for (u64 i = done + tid; i < total; i += nth) hWords[i] = words[i];
+}
+
+template <bool kVec>
+__global__ void __launch_bounds__(256) k_streamsFromHost(const u32* hWords, const u64* hExt, u32 n, u32* words,
+                                                         u64* wordOff, u64* bitSize, u64 cap, u32* err) {
+    __shared__ u64 sTotal;
+    if (threadIdx.x == 0) sTotal = hExt[n - 1] + (hExt[2 * n - 1] + 31) / 32;   // one host read per CTA
+    __syncthreads();
+    const u64 total = sTotal;
+    const u64 tid = u64(blockIdx.x) * blockDim.x + threadIdx.x, nth = u64(gridDim.x) * blockDim.x;
+    if (total > cap) {
+        if (tid == 0) atomicOr(err, u32(DEV_ERR_CORRUPT));
+        return;
+    }
+    if (tid < n) {
+        wordOff[tid] = hExt[tid];
+        bitSize[tid] = hExt[n + tid];
+    }
+    u64 done = 0;
+    if (kVec) {
+        const u64 q = total / 4;
+        for (u64 i = tid; i < q; i += nth) reinterpret_cast<uint4*>(words)[i] = reinterpret_cast<const uint4*>(hWords)[i];
+        done = q * 4;
+    }
+    for (u64 i = done + tid; i < total; i += nth) words[i] = hWords[i];
+}
+
 template <class List>
 static void prefixOf(const List& li, u32 k, u32& nd, u32& ctas) {
     nd = li.descEnd[k - 1];
@@ -851,6 +904,57 @@ int cc_volume_batch_read_stream(cc_volume_batch* b, uint32_t v, uint32_t* dst, u
     if (!dst) return CC_OK;
     if (words > capacityWords) { setError("cc_volume_batch_read_stream: need %llu words", (unsigned long long)words); return CC_ERR_CAPACITY; }
     CC_TRY_CUDA(cudaMemcpy(dst, b->words + ext[0], words * 4, cudaMemcpyDefault), "copy stream");
+    return CC_OK;
+}
+
+// Device address of page-locked host memory (CC_ERR_INVALID_ARGUMENT if the
+// memory is not page-locked).
+static int hostDevicePointer(const void* h, void** d, const char* what) {
+    cudaPointerAttributes a{};
+    if (!h || cudaPointerGetAttributes(&a, h) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        setError("%s: host buffers must be page-locked (cudaHostAlloc / cudaHostRegister)", what);
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    *d = a.devicePointer ? a.devicePointer : const_cast<void*>(h);
+    return CC_OK;
+}
+
+int cc_volume_batch_download_streams(cc_volume_batch* b, uint32_t* hWords, uint64_t capacityWords, uint64_t* hExt) {
+    const char* what = "cc_volume_batch_download_streams";
+    if (!b || !b->active) { setError("%s: bad argument", what); return CC_ERR_INVALID_ARGUMENT; }
+    cudaSetDevice(b->I->device);
+    void *dW = nullptr, *dE = nullptr;
+    int rc = hostDevicePointer(hWords, &dW, what);
+    if (!rc) rc = hostDevicePointer(hExt, &dE, what);
+    if (rc) return rc;
+    cudaStream_t st = b->hasOwnStream ? b->ownStream : b->user->stream;
+    b->I->stream = st;
+    const bool vec = (reinterpret_cast<uintptr_t>(dW) & 15) == 0;
+    const unsigned g = 148 * 4;
+    if (vec) k_streamsToHost<true><<<g, 256, 0, st>>>(b->words, b->wordOff, b->bitSize, b->active, static_cast<u32*>(dW), capacityWords, static_cast<u64*>(dE), b->I->errors);
+    else k_streamsToHost<false><<<g, 256, 0, st>>>(b->words, b->wordOff, b->bitSize, b->active, static_cast<u32*>(dW), capacityWords, static_cast<u64*>(dE), b->I->errors);
+    countLaunch();
+    CC_TRY_CUDA(cudaGetLastError(), what);
+    return CC_OK;
+}
+
+int cc_volume_batch_upload_streams(cc_volume_batch* b, const uint32_t* hWords, const uint64_t* hExt) {
+    const char* what = "cc_volume_batch_upload_streams";
+    if (!b || !b->active) { setError("%s: bad argument", what); return CC_ERR_INVALID_ARGUMENT; }
+    cudaSetDevice(b->I->device);
+    void *dW = nullptr, *dE = nullptr;
+    int rc = hostDevicePointer(hWords, &dW, what);
+    if (!rc) rc = hostDevicePointer(hExt, &dE, what);
+    if (rc) return rc;
+    cudaStream_t st = b->hasOwnStream ? b->ownStream : b->user->stream;
+    b->I->stream = st;
+    const bool vec = (reinterpret_cast<uintptr_t>(dW) & 15) == 0;
+    const unsigned g = 148 * 4;
+    if (vec) k_streamsFromHost<true><<<g, 256, 0, st>>>(static_cast<const u32*>(dW), static_cast<const u64*>(dE), b->active, b->words, b->wordOff, b->bitSize, b->wordsCap, b->I->errors + 4);
+    else k_streamsFromHost<false><<<g, 256, 0, st>>>(static_cast<const u32*>(dW), static_cast<const u64*>(dE), b->active, b->words, b->wordOff, b->bitSize, b->wordsCap, b->I->errors + 4);
+    countLaunch();
+    CC_TRY_CUDA(cudaGetLastError(), what);
     return CC_OK;
 }
 

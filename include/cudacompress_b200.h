@@ -426,6 +426,17 @@ int cc_volume_batch_read_stream(cc_volume_batch* batch, uint32_t volume, uint32_
  * the batch's buffer for cc_volume_batch_decompress (e.g. streams of
  * cc_compress_volume_float or of another batch with the same shapes). */
 int cc_volume_batch_load_streams(cc_volume_batch* batch, const uint32_t* const* words, const uint64_t* bit_sizes);
+/* The streams of the active volumes between the batch and page-locked host
+ * memory (cudaHostAlloc / cudaHostRegister), fully asynchronous on the
+ * batch's stream: kernels move exactly the used words, whose extent only the
+ * device knows, so the host never waits.  h_extents: 2 x active u64, the word
+ * offset of each stream in h_words, then each bit size.  download after a
+ * compress; upload (the same layout) before a decompress.  A download larger
+ * than capacity_words, or an upload larger than the batch's buffer, is
+ * reported by cc_volume_batch_status. */
+int cc_volume_batch_download_streams(cc_volume_batch* batch, uint32_t* h_words, uint64_t capacity_words,
+                                     uint64_t* h_extents);
+int cc_volume_batch_upload_streams(cc_volume_batch* batch, const uint32_t* h_words, const uint64_t* h_extents);
 /* Synchronizes the instance stream; reports device errors of the last calls. */
 int cc_volume_batch_status(cc_volume_batch* batch);
 /* Adds the batch's timing sections to the instance's (cc_timing_*). */

@@ -131,3 +131,50 @@ def test_batch_decodes_streams_of_the_plain_codec(oracle):
             ref = oracle.decompress_volume(words[i], bits[i], v.shape, 2, q)
             assert np.array_equal(outs[i].cpu().numpy().view(np.uint32), ref.view(np.uint32)), i
     inst.close()
+
+
+def test_batch_stream_download_upload(oracle):
+    """Streams through page-locked host memory without a host wait: the
+    download holds each volume's words at its offset (byte-identical to the
+    oracle's stream), the upload restores them for a decode, and an
+    undersized host buffer is reported."""
+    vols, steps = bricks(9, 2, 77)
+    inst = cc.Instance(0, 7, 1 << 12, 128, 14)
+    s = torch.cuda.Stream()
+    with cc.VolumeBatch(inst, [v.shape for v in vols], 2, steps, graph=True) as b:
+        b.set_stream(s)
+        dv = [torch.from_numpy(v).cuda() for v in vols]
+        torch.cuda.synchronize()
+        cap = sum(cc.volume_stream_capacity_words(*v.shape[::-1]) for v in vols)
+        hw = torch.zeros(cap, dtype=torch.int32).pin_memory()
+        he = torch.zeros(2 * len(vols), dtype=torch.int64).pin_memory()
+        b.compress(dv)
+        b.download_streams(hw, he)
+        s.synchronize()
+        b.status()
+        ext = he.numpy()
+        words = hw.numpy().view(np.uint32)
+        for i, (v, q) in enumerate(zip(vols, steps)):
+            w, bits = oracle.compress_volume(v, 2, q)
+            off, nb = int(ext[i]), int(ext[len(vols) + i])
+            assert nb == bits
+            assert np.array_equal(words[off: off + (nb + 31) // 32], w), i
+        # scramble the device streams, then restore them from the host copy
+        b.compress([torch.zeros_like(v) for v in dv])
+        b.upload_streams(hw, he)
+        outs = [torch.full_like(v, float("nan")) for v in dv]
+        b.decompress(outs)
+        s.synchronize()
+        b.status()
+        for o, v, q in zip(outs, vols, steps):
+            w, bits = oracle.compress_volume(v, 2, q)
+            assert np.array_equal(o.cpu().numpy(), oracle.decompress_volume(w, bits, v.shape, 2, q))
+        small = torch.zeros(16, dtype=torch.int32).pin_memory()
+        b.compress(dv)
+        b.download_streams(small, he)
+        s.synchronize()
+        with pytest.raises(cc.CudaCompressError):
+            b.status()
+        with pytest.raises(cc.CudaCompressError):       # pageable host memory is refused
+            b.download_streams(torch.zeros(cap, dtype=torch.int32), he)
+    inst.close()
