@@ -10,7 +10,10 @@ through the batched codec (one batch of 3 volumes, each stream byte-identical
 to the plain single-volume codec's, replayed as CUDA graphs).
 
   value   raw field bytes / step time, inputs and outputs resident in HBM
-          (GB/s raw, encode+decode); encode_gbs / decode_gbs split it;
+          (GB/s raw, encode+decode), with consecutive steps in flight on 1-3
+          batches (each on its own stream; the count chosen by a short
+          untimed trial, `in_flight_batches`); latency_ms_per_step is one step
+          at a time, and encode_gbs / decode_gbs split that sequential step;
           plain_path_ms_per_step times the per-component plain codec
   e2e     the same through the public API with host buffers: H2D of the
           fields, D2H of the streams (to page-locked host memory), H2D of the
@@ -36,7 +39,8 @@ to the plain single-volume codec's, replayed as CUDA graphs).
 
 Other workloads: --workload bricks-4096 (the full batched-bricks config; under
 torchrun the brick set is partitioned across ranks by byte size, "scaling":
-"strong"), --workload serving (1k / 10k / 50k req/s), --workload volume-128.
+"strong"), --workload serving (1k / 10k / 50k req/s), --workload volume-128,
+--workload heightfield-2048 (the lossless 2D codec, 2048^2 int16, 4 levels).
 `--impl reference` times the CPU path as the reference arm.  Multi-GPU runs
 (torchrun) are weak-scaling replicas: every rank codes its own field, no
 collective on the data path; the time is the max over ranks.
@@ -71,6 +75,9 @@ WORKLOADS["serving"] = dict(rates=(1000.0, 10000.0, 50000.0), requests=3000, edg
                            q0=0.01, levels=3, slots={32: 64, 64: 16, 128: 4}, bricks_per_edge=16, seed=1006,
                            desc="open-loop Poisson brick requests, 90% decode / 10% encode, cubic edge {32,64,128}, "
                                 "q0=0.01*std, 3-level CDF 9/7, 4 GB HBM admission budget")
+WORKLOADS["heightfield-2048"] = dict(n=2048, levels=4, seed=1001,
+                                     desc="2048^2 int16 fBm terrain (10 octaves, H=0.8, [-2000, 8000]), 4-level "
+                                          "CDF 5/3 integer DWT, lossless, RLE+Huffman cb=128")
 FALLBACK_HBM_GBS = 6650.0
 L2_BYTES = 126 * 1024 * 1024
 
@@ -303,6 +310,19 @@ def run_reference(args, wl):
         return run_reference_bricks(args, wl, threads)
     if args.workload == "serving":
         return run_reference_serving(args, wl, threads)
+    if args.workload.startswith("heightfield"):
+        from cudacompress_b200 import fields
+        img = fields.fbm_heightfield(wl["n"], wl["seed"])
+        for _ in range(args.warmup):
+            cpu_reference_heightfield(img, wl["levels"])
+        times = [sum(cpu_reference_heightfield(img, wl["levels"])) for _ in range(args.steps)]
+        step = sum(times) / len(times)
+        value = wl["n"] ** 2 * 2 / step / 1e9
+        line = reference_line(args, wl, value, "GB/s", step, "port", 1,
+                              f"the whole {wl['n']}^2 field per step, oracle port (one thread)")
+        line["dtype"] = "int16"
+        print(json.dumps(line), flush=True)
+        return
     vol = make_fields(wl)[0]
     for _ in range(args.warmup):
         cpu_reference_step(vol, wl, threads)
@@ -661,6 +681,149 @@ def pipelined_e2e(torch, batches, vols_h, vols, dev, C, cc, steps=None):
     return {"ms": ms, "stream_bytes": stream_bytes, "identical": identical}
 
 
+def cpu_reference_heightfield(img, L):
+    """The oracle's port of the heightfield codec (the reference's CPU coder
+    has no 2D integer DWT); one thread.  Returns (encode_s, decode_s)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import Oracle
+    if not _ORACLE:
+        _ORACLE.append(Oracle())
+    orc = _ORACLE[0]
+    t0 = time.perf_counter()
+    words, bits = orc.compress_heightfield(img, L)
+    t1 = time.perf_counter()
+    rec = orc.decompress_heightfield(words, bits, img.shape, L)
+    t2 = time.perf_counter()
+    assert np.array_equal(rec, img), "oracle heightfield round trip mismatch"
+    return t1 - t0, t2 - t1
+
+
+def run_heightfield(args, wl):
+    """The lossless 2D heightfield codec (C1): one step = compress + decompress
+    of one 2048^2 int16 terrain per rank (weak-scaling replicas), through
+    cc_compress_heightfield / cc_decompress_heightfield; the decode is checked
+    bit-exact every run."""
+    import torch
+    import cudacompress_b200 as cc
+    from cudacompress_b200 import fields, replicas
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    n, L = wl["n"], wl["levels"]
+    img_h = fields.fbm_heightfield(n, wl["seed"] + 100 * rank)
+    img = torch.from_numpy(img_h).to(dev)
+    # 5 streams of a level-0 band: room for every level's streams in one
+    # decode call (the codec falls back to one call per level otherwise)
+    inst = cc.Instance(local, 5, (n // 2) ** 2, 128, 14)
+    words = torch.empty(n * n + 64 * 1024, dtype=torch.int32, device=dev)
+    out = torch.empty_like(img)
+    bits = [0]
+
+    def step():
+        _, b = cc.compress_heightfield(inst, img, L, words)
+        cc.decompress_heightfield(inst, out, L, words, b)
+        bits[0] = b
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    if not torch.equal(out, img):
+        raise RuntimeError("heightfield round trip is not lossless")
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = cc.lib().cc_kernel_launches()
+    sampler = ClockSampler(local)
+    start.record()
+    for _ in range(args.steps):
+        step()
+    end.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = cc.lib().cc_kernel_launches() - launches0
+    ms = replicas.max_over_ranks([start.elapsed_time(end) / args.steps], dist, dev)[0]
+    raw = n * n * 2
+    coded = (bits[0] + 7) // 8
+    value = replicas.job_gbs(world, raw, ms)
+    # end to end: image in from pinned host memory, stream out and back, image out
+    pin_in = torch.from_numpy(img_h).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    pin_words = torch.empty(words.numel(), dtype=torch.int32).pin_memory()
+    dimg, dwords = torch.empty_like(img), torch.empty_like(words)
+
+    def e2e_step():
+        dimg.copy_(pin_in, non_blocking=True)
+        _, b = cc.compress_heightfield(inst, dimg, L, words)
+        nw = (b + 31) // 32
+        pin_words[:nw].copy_(words[:nw], non_blocking=True)
+        dwords[:nw].copy_(pin_words[:nw], non_blocking=True)
+        cc.decompress_heightfield(inst, out, L, dwords, b)
+        pin_out.copy_(out, non_blocking=True)
+        return nw * 4
+
+    e2e_step()
+    torch.cuda.synchronize()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record()
+    for _ in range(args.steps):
+        nbytes = e2e_step()
+    e2.record()
+    torch.cuda.synchronize()
+    if not torch.equal(pin_out, pin_in):
+        raise RuntimeError("heightfield end-to-end round trip is not lossless")
+    e2e_ms = replicas.max_over_ranks([s2.elapsed_time(e2) / args.steps], dist, dev)[0]
+    # per-kernel sections of one extra step (event timing on)
+    lib = cc.lib()
+    lib.cc_reset_timings(inst.handle)
+    lib.cc_set_timing(inst.handle, 1)
+    step()
+    torch.cuda.synchronize()
+    sections = {}
+    for i in range(lib.cc_timing_count(inst.handle)):
+        name, t_ms, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_uint32()
+        lib.cc_timing_entry(inst.handle, i, ctypes.byref(name), ctypes.byref(t_ms), ctypes.byref(cnt))
+        sections[name.value.decode()] = round(t_ms.value, 4)
+    lib.cc_set_timing(inst.handle, 0)
+    peak, peak_kind = load_peak()
+    alg = 2 * (raw + coded)
+    achieved = alg / (ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        e, d = cpu_reference_heightfield(img_h, L)
+        cpu = {"value": raw / (e + d) / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": f"the whole {n}^2 field, compress + decompress, oracle port (one thread)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded fBm terrain)",
+            "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": f"replicas{world}",
+                       "l2": f"input {raw >> 20} MiB per step fits L2 (latency-bound config)"},
+            "compression_ratio": raw / max(coded, 1), "lossless": True,
+            "e2e": {"value": replicas.job_gbs(world, raw, e2e_ms), "unit": "GB/s", "h2d_bytes_per_step": raw + nbytes,
+                    "d2h_bytes_per_step": raw + nbytes},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "whole codec (raw + compressed bytes, both directions)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "traffic": None},
+            "sections_ms": dict(sorted(sections.items(), key=lambda kv: -kv[1])),
+            "clocks": clocks, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    inst.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def run_ours(args, wl):
     import torch
     import cudacompress_b200 as cc
@@ -707,30 +870,77 @@ def run_ours(args, wl):
     torch.cuda.synchronize()
     same_as_plain = pbits == streams[0][1] and np.array_equal(
         plain_words[: (pbits + 31) // 32].cpu().numpy().view(np.uint32), streams[0][0])
-    # timed device-resident region
+    # latency: one step at a time (encode / decode split by events)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for k in range(args.steps):
+        step(evs[k])
+    end.record()
+    torch.cuda.synchronize()
+    batch.status()
+    lat_ms = start.elapsed_time(end) / args.steps
+    enc_ms = sum(evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)) / args.steps
+    dec_ms = sum(evs[k][1].elapsed_time(evs[k][2]) for k in range(args.steps)) / args.steps
+    lat_ms, enc_ms, dec_ms = replicas.max_over_ranks([lat_ms, enc_ms, dec_ms], dist, dev)
+
+    # throughput (value): consecutive steps in flight on `nb` batches, each on
+    # its own stream, so one step's latency-bound phases (table builds, the
+    # decoder's walk) overlap another's bandwidth-bound passes; every step
+    # still encodes and decodes all components.  nb in {1, 2, 3} is chosen by
+    # a short untimed trial (more batches in flight contend for HBM and L2).
+    pool = [batch] + [cc.VolumeBatch(inst, [v.shape for v in vols], L, [q0] * C, graph=True) for _ in range(2)]
+    pstreams = [torch.cuda.Stream(dev) for _ in pool]
+    inst_stream = cc.lib().cc_get_instance_stream(inst.handle)
+    prec = [[torch.empty_like(v) for v in vols] for _ in pool]
+
+    def inflight(nb, steps):
+        for b, st in zip(pool[:nb], pstreams):
+            b.set_stream(st)
+        for st in pstreams[:nb]:
+            st.wait_stream(torch.cuda.current_stream())
+        for k in range(steps):
+            i = k % nb
+            pool[i].compress(vols)
+            pool[i].decompress(prec[i])
+        for st in pstreams[:nb]:
+            torch.cuda.current_stream().wait_stream(st)
+
+    trial = {}
+    for nb in (1, 2, 3):
+        inflight(nb, 2 * nb)
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        inflight(nb, 6)
+        e.record()
+        torch.cuda.synchronize()
+        trial[nb] = a.elapsed_time(e) / 6
+    nb = min(trial, key=trial.get)
+    nb = int(replicas.max_over_ranks([nb], dist, dev)[0])      # every rank runs the same count
+    inflight(nb, max(args.warmup, 2 * nb))
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = cc.lib().cc_kernel_launches()
     sampler = ClockSampler(local)
     start.record()
-    for k in range(args.steps):
-        step(evs[k])
+    inflight(nb, args.steps)
     end.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = cc.lib().cc_kernel_launches() - launches0
-    batch.status()
+    for b in pool:
+        b.status()
+    for b in pool:
+        b.set_stream(inst_stream)
     if dist:
         dist.barrier()
-    ms = start.elapsed_time(end) / args.steps
-    enc_ms = sum(evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)) / args.steps
-    dec_ms = sum(evs[k][1].elapsed_time(evs[k][2]) for k in range(args.steps)) / args.steps
-    ms, enc_ms, dec_ms = replicas.max_over_ranks([ms, enc_ms, dec_ms], dist, dev)
+    ms = replicas.max_over_ranks([start.elapsed_time(end) / args.steps], dist, dev)[0]
     raw_step = C * n ** 3 * 4
     value = replicas.job_gbs(world, raw_step, ms)
+    same_inflight = all(torch.equal(prec[(args.steps - 1) % nb][c], recon[c]) for c in range(C))
 
     # the plain per-component path (cc_compress_volume_float / decompress), for comparison
     plain_out = torch.empty_like(vols[0])
@@ -757,8 +967,7 @@ def run_ours(args, wl):
     # decompress, which alternate between two batches on their own streams.
     # Every step moves its own fields in, its streams out and back in, and its
     # reconstruction out.
-    with cc.VolumeBatch(inst, [v.shape for v in vols], L, [q0] * C, graph=True) as batch2:
-        e2e = pipelined_e2e(torch, [batch, batch2], vols_h, vols, dev, C, cc, steps=args.steps)
+    e2e = pipelined_e2e(torch, pool[:2], vols_h, vols, dev, C, cc, steps=args.steps)
     e2e_ms = replicas.max_over_ranks([e2e["ms"]], dist, dev)[0]
     e2e_value = replicas.job_gbs(world, raw_step, e2e_ms)
     h2d = raw_step + e2e["stream_bytes"]
@@ -833,6 +1042,8 @@ def run_ours(args, wl):
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded k^-5/3 random-phase fields)",
+            "in_flight_batches": nb, "in_flight_trial_ms": {str(k): round(v, 4) for k, v in trial.items()},
+            "latency_ms_per_step": lat_ms, "reconstruction_identical_in_flight": bool(same_inflight),
             "config": {"workload": args.workload, "desc": wl["desc"], "parallelism": f"replicas{world}",
                        "l2": f"inputs {C * n ** 3 * 4 >> 20} MiB per step > L2 126 MiB"},
             "encode_gbs": replicas.job_gbs(world, raw_step, enc_ms),
@@ -847,7 +1058,8 @@ def run_ours(args, wl):
             "clocks": clocks, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    batch.close()
+    for b in pool:
+        b.close()
     inst.close()
     if dist:
         dist.destroy_process_group()
@@ -870,6 +1082,8 @@ def main():
         run_bricks(args, wl)
     elif args.workload == "serving":
         run_serving(args, wl)
+    elif args.workload.startswith("heightfield"):
+        run_heightfield(args, wl)
     else:
         run_ours(args, wl)
 

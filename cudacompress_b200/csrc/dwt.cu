@@ -787,18 +787,52 @@ __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ desc
     // all of a thread's column loads are issued before any is used
     constexpr int kLoads = (kBColTileA + 8) / 8;
     float2 vals[kLoads];
+    if (kSymbols && !(D.hx & 1)) {
+        // axis Z (a = z, c = y), even half width: every load is either one
+        // float2 of the lowpass or one 4-byte symbol pair, issued as
+        // predicated loads of raw bits; the dequantization follows once all
+        // of them are in flight
+        const int bx = x >= D.hx, by = c >= D.hy;
+        const int lx = x - bx * D.hx, ly = c - by * D.hy;
+        uint2 raw[kLoads];
+        bool lp[kLoads];
 #pragma unroll
-    for (int i = 0; i < kLoads; ++i) {
-        const int j = a0 - 4 + ty + 8 * i;
-        vals[i] = make_float2(0.0f, 0.0f);
-        if (x < nx && j < na + 4) {
+        for (int i = 0; i < kLoads; ++i) {
+            const int j = a0 - 4 + ty + 8 * i;
+            raw[i] = make_uint2(0u, 0u);
             const int m = mirrorIdx(j, na);
-            const int a = kInverse ? splitPos(m, na) : m;
-            if (kSymbols) {
-                // axis Z: a = z, c = y
-                vals[i] = bandPair(D, x, c, a);
+            const int z = splitPos(m, na), bz = z >= D.hz, lz = z - bz * D.hz;
+            const int b = bx + 2 * by + 4 * bz;
+            lp[i] = b == 0;
+            if (x < nx && j < na + 4) {
+                if (lp[i]) raw[i] = *reinterpret_cast<const uint2*>(D.src + size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx);
+                else raw[i].x = *reinterpret_cast<const u32*>(D.bands + u64(b - 1) * D.bandStride +
+                                                              (u64(lz) * D.hy + ly) * D.hx + lx);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            if (lp[i]) {
+                vals[i] = make_float2(__uint_as_float(raw[i].x), __uint_as_float(raw[i].y));
             } else {
-                vals[i] = *reinterpret_cast<const float2*>(D.src + size_t(x) + size_t(a) * D.sa + size_t(c) * D.sc);
+                const int q0 = unsymbolizeI(raw[i].x & 0xFFFFu), q1 = unsymbolizeI(raw[i].x >> 16);
+                vals[i] = make_float2((float(q0) + signI(q0) * 0.5f) * D.step, (float(q1) + signI(q1) * 0.5f) * D.step);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            const int j = a0 - 4 + ty + 8 * i;
+            vals[i] = make_float2(0.0f, 0.0f);
+            if (x < nx && j < na + 4) {
+                const int m = mirrorIdx(j, na);
+                const int a = kInverse ? splitPos(m, na) : m;
+                if (kSymbols) {
+                    // axis Z: a = z, c = y
+                    vals[i] = bandPair(D, x, c, a);
+                } else {
+                    vals[i] = *reinterpret_cast<const float2*>(D.src + size_t(x) + size_t(a) * D.sa + size_t(c) * D.sc);
+                }
             }
         }
     }

@@ -584,8 +584,10 @@ int cc_compress_heightfield(cc_instance* I, const int16_t* img, uint32_t nx, uin
     return CC_OK;
 }
 
-int cc_decompress_heightfield(cc_instance* I, int16_t* out, uint32_t nx, uint32_t ny, uint32_t levels,
-                              const uint32_t* dWords, uint32_t bitSize) {
+// The heightfield decode one level at a time with a host walk of the stream:
+// for instances too small to decode every level in one call.
+static int decompressHeightfieldPerLevel(cc_instance* I, int16_t* out, uint32_t nx, uint32_t ny, uint32_t levels,
+                                         const uint32_t* dWords, uint32_t bitSize) {
     if (!I || !out || !dWords || levels == 0) { setError("decompressHeightfield: bad argument"); return CC_ERR_INVALID_ARGUMENT; }
     if (I->symBytes != 2) { setError("decompressHeightfield: needs a 16-bit-symbol instance"); return CC_ERR_INVALID_ARGUMENT; }
     cudaSetDevice(I->device);
@@ -630,6 +632,76 @@ int cc_decompress_heightfield(cc_instance* I, int16_t* out, uint32_t nx, uint32_
         for (u32 bi = 1; bi < 4; ++bi) {
             const u32 x = bi % 2, y = bi / 2;
             rc = cc_unsymbolize(coef + u64(y) * hy * sx + u64(x) * hx, static_cast<u16*>(outs[bi - 1]), hx, hy, 1, sx, 0, st);
+            if (rc) return rc;
+        }
+        rc = cc_dwt_int_inverse(l == 0 ? out : cur, tmp, coef, int(sx), int(sy), 1, 0, 0, 0, 0, st);
+        if (rc) return rc;
+    }
+    CC_TRY_CUDA(cudaStreamSynchronize(st), "decompressHeightfield");
+    return cc_decode_status(I);
+}
+
+int cc_decompress_heightfield(cc_instance* I, int16_t* out, uint32_t nx, uint32_t ny, uint32_t levels,
+                              const uint32_t* dWords, uint32_t bitSize) {
+    if (!I || !out || !dWords || levels == 0) { setError("decompressHeightfield: bad argument"); return CC_ERR_INVALID_ARGUMENT; }
+    if (I->symBytes != 2) { setError("decompressHeightfield: needs a 16-bit-symbol instance"); return CC_ERR_INVALID_ARGUMENT; }
+    const u32 f = 1u << levels;
+    if (nx % f || ny % f || (nx >> (levels - 1)) < 8 || (ny >> (levels - 1)) < 8) {
+        setError("decompressHeightfield: sizes must be divisible by 2^levels with coarsest level >= 8");
+        return CC_ERR_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(I->device);
+    cudaStream_t st = I->stream;
+    const u64 N0 = u64(nx) * ny;
+    Bump b{nullptr};
+    b.take<i16>(N0);
+    b.take<i16>(N0);
+    b.take<i16>(N0);
+    b.take<u16>(N0 + 1024);
+    int rc = ensurePipelineWork(I, b.off + 1024);
+    if (rc) return rc;
+    Bump w{I->pipeWork};
+    i16* cur = w.take<i16>(N0);
+    i16* coef = w.take<i16>(N0);
+    i16* tmp = w.take<i16>(N0);
+    u16* syms = w.take<u16>(N0 + 1024);
+    // every stream of every level in one device-walked decode: the LP stream
+    // (Huff), then per level coarse -> fine its 3 bands (RLHuff); the symbols
+    // in the layout LP | level L-1 bands | ... | level 0 bands
+    const u32 L = levels;
+    const u32 lx = nx >> L, ly = ny >> L;
+    std::vector<DecStreamSpec> ds;
+    std::vector<u16*> bandAt(L);
+    u64 at = u64(lx) * ly;
+    ds.push_back(DecStreamSpec{KIND_HUFF, lx * ly, syms, 0});
+    for (int l = int(L) - 1; l >= 0; --l) {
+        const u64 bandN = u64(nx >> (l + 1)) * (ny >> (l + 1));
+        bandAt[l] = syms + at;
+        for (u32 i = 0; i < 3; ++i) ds.push_back(DecStreamSpec{KIND_RLHUFF, u32(bandN), syms + at + i * bandN, 0});
+        at += 3 * bandN;
+    }
+    const DecSourceSpec src{dWords, bitSize, 0};
+    char* slot = I->takeRingSlot();
+    DecPlan dp;
+    rc = decodePrepare(I, ds.data(), u32(ds.size()), &src, 1, slot, I->hostRingBytes, dp);
+    if (rc == CC_ERR_CAPACITY) return decompressHeightfieldPerLevel(I, out, nx, ny, levels, dWords, bitSize);
+    if (rc) return rc;
+    dp.dev = I->dPlan;
+    CC_TRY_CUDA(cudaMemcpyAsync(I->dPlan, slot, dp.bytes, cudaMemcpyHostToDevice, st), "upload plan");
+    cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
+    CC_TRY_CUDA(cudaMemsetAsync(syms + u64(lx) * ly, 0, (at - u64(lx) * ly) * sizeof(u16), st), "zero bands");
+    if ((rc = decodeLaunch(I, dp))) return rc;
+    rc = cc_unsymbolize(cur, syms, lx, ly, 1, 0, 0, st);
+    if (rc) return rc;
+    for (int l = int(L) - 1; l >= 0; --l) {
+        const u32 sx = nx >> l, sy = ny >> l, hx = sx / 2, hy = sy / 2;
+        const u64 bandN = u64(hx) * hy;
+        // assemble [LL | HL ; LH | HH] of this level then invert
+        CC_TRY_CUDA(cudaMemcpy2DAsync(coef, sx * sizeof(i16), cur, hx * sizeof(i16), hx * sizeof(i16), hy,
+                                      cudaMemcpyDeviceToDevice, st), "place lowpass");
+        for (u32 bi = 1; bi < 4; ++bi) {
+            const u32 x = bi % 2, y = bi / 2;
+            rc = cc_unsymbolize(coef + u64(y) * hy * sx + u64(x) * hx, bandAt[l] + (bi - 1) * bandN, hx, hy, 1, sx, 0, st);
             if (rc) return rc;
         }
         rc = cc_dwt_int_inverse(l == 0 ? out : cur, tmp, coef, int(sx), int(sy), 1, 0, 0, 0, 0, st);

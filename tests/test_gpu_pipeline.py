@@ -55,10 +55,12 @@ def test_volume_codec_c0_full_size(oracle):
         assert fields.psnr(vol, rec) > 40
 
 
-@pytest.mark.parametrize("n,levels", [(64, 2), (256, 4)])
-def test_heightfield_codec_matches_oracle_and_is_lossless(oracle, n, levels):
+@pytest.mark.parametrize("n,levels,streams", [(64, 2, 3), (256, 4, 3), (256, 4, 5), (512, 3, 5)])
+def test_heightfield_codec_matches_oracle_and_is_lossless(oracle, n, levels, streams):
+    """3 streams: the decoder walks the stream one level at a time; 5: every
+    level's streams in one device-walked decode."""
     img = fields.fbm_heightfield(n, seed=3000 + n)
-    with cc.Instance(0, 3, (n // 2) ** 2, 128, 14) as inst:
+    with cc.Instance(0, streams, (n // 2) ** 2, 128, 14) as inst:
         words, bits = cc.compress_heightfield(inst, torch.from_numpy(img).cuda(), levels)
         ref_words, ref_bits = oracle.compress_heightfield(img, levels)
         assert bits == ref_bits
