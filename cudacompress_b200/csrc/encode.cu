@@ -623,7 +623,40 @@ static size_t tableBuildSoloSmem(int device) {
 // ---------------------------------------------------------------------------
 constexpr u32 kPackWarps = 8;
 
-template <class Sym>
+// kPer = coding block / 32 consecutive symbols of one lane, from j0: one
+// vector load when the run lies inside the stream and is aligned, else
+// element loads.  Positions at or past count are not read.
+template <class Sym, int kPer>
+__device__ __forceinline__ void laneSyms(const Sym* in, u32 j0, u32 count, u32 (&s)[kPer]) {
+    constexpr int kBytes = kPer * int(sizeof(Sym));
+    constexpr int kAlign = kBytes < 16 ? kBytes : 16;
+    const Sym* q = in + j0;
+    if (kBytes >= 4 && j0 + kPer <= count && (reinterpret_cast<uintptr_t>(q) & uintptr_t(kAlign - 1)) == 0) {
+        constexpr int kWords = kBytes >= 4 ? kBytes / 4 : 1;
+        u32 w[kWords];
+        if (kWords >= 4) {
+#pragma unroll
+            for (int c = 0; c < kWords / 4; ++c) {
+                const uint4 v = reinterpret_cast<const uint4*>(q)[c];
+                w[4 * c] = v.x; w[4 * c + 1] = v.y; w[4 * c + 2] = v.z; w[4 * c + 3] = v.w;
+            }
+        } else if (kWords == 2) {
+            const uint2 v = *reinterpret_cast<const uint2*>(q);
+            w[0] = v.x; w[1] = v.y;
+        } else {
+            w[0] = *reinterpret_cast<const unsigned int*>(q);
+        }
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) s[k] = sizeof(Sym) == 2 ? (w[k >> 1] >> (16 * (k & 1))) & 0xFFFFu : w[k];
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) s[k] = j0 + u32(k) < count ? u32(q[k]) : 0u;
+}
+
+// Bits of every coding block: one warp per block, each lane kPer symbols
+// loaded at once and their code lengths gathered together.
+template <class Sym, int kPer>
 __global__ void __launch_bounds__(kPackWarps * 32) k_blockBits(EncParams p) {
     const u32 gb = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
     const u32 lane = threadIdx.x & 31;
@@ -637,9 +670,13 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_blockBits(EncParams p) {
     if (b >= m.blocks) return;
     const uint2* enc = p.enc + m.histOff;
     const u32 hs = m.histSize;
-    const u32 i0 = b * p.cb, i1 = min(count, i0 + p.cb);
+    const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
+    u32 sv[kPer];
+    laneSyms<Sym, kPer>(in, j0, count, sv);
     u32 bits = 0;
-    for (u32 i = i0 + lane; i < i1; i += 32) bits += enc[min(u32(in[i]), hs - 1u)].y;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+        if (j0 + u32(k) < count) bits += enc[min(sv[k], hs - 1u)].y;
     bits = warpSum(bits);
     if (lane == 0) p.blockBits[gb] = bits;
 }
@@ -738,7 +775,7 @@ __device__ __forceinline__ void orCodeword(u32* win, u32 wLo, u32 wHi, u32 pos, 
 // (gather ownership: no atomics on global memory, no pre-zeroing); the bits
 // of the last owned word that belong to the next block are recomputed from
 // that block's first symbols.
-template <class Sym>
+template <class Sym, int kPer>
 __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
     extern __shared__ u32 winAll[];
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -761,18 +798,19 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
     __syncwarp();
     const uint2* enc = p.enc + m.histOff;
     const u32 hs = m.histSize;
-    const u32 i0 = b * p.cb;
-    const u32 per = p.cb / 32;
-    const u32 j0 = i0 + lane * per;
-    uint2 cw[8];
+    const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
+    u32 sv[kPer];
+    laneSyms<Sym, kPer>(in, j0, count, sv);
+    uint2 cw[kPer];
     u32 lsum = 0;
-    for (u32 k = 0; k < per; ++k) {
-        const u32 j = j0 + k;
-        cw[k] = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        cw[k] = j0 + u32(k) < count ? enc[min(sv[k], hs - 1u)] : make_uint2(0, 0);
         lsum += cw[k].y;
     }
     u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
-    for (u32 k = 0; k < per; ++k) {
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
         orCodeword(win, wLo, wHi, pos, cw[k].x, cw[k].y);
         pos += cw[k].y;
     }
@@ -922,7 +960,16 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
     if (p.totalBlocks) {
         const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
-        { SectionTimer t(I, "enc.block_bits", st); k_blockBits<Sym><<<g, kPackWarps * 32, 0, st>>>(p); countLaunch(); }
+        {
+            SectionTimer t(I, "enc.block_bits", st);
+            switch (p.cb) {
+                case 32: k_blockBits<Sym, 1><<<g, kPackWarps * 32, 0, st>>>(p); break;
+                case 64: k_blockBits<Sym, 2><<<g, kPackWarps * 32, 0, st>>>(p); break;
+                case 128: k_blockBits<Sym, 4><<<g, kPackWarps * 32, 0, st>>>(p); break;
+                default: k_blockBits<Sym, 8><<<g, kPackWarps * 32, 0, st>>>(p); break;
+            }
+            countLaunch();
+        }
         { SectionTimer t(I, "enc.block_scan", st); k_blockScan<<<p.T, 1024, 0, st>>>(p); countLaunch(); }
     }
     { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
@@ -930,7 +977,12 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
         const size_t packSmem = size_t(kPackWarps) * (p.cb + 2) * sizeof(u32);
         SectionTimer t(I, "enc.pack", st);
-        k_pack<Sym><<<g, kPackWarps * 32, packSmem, st>>>(p);
+        switch (p.cb) {
+            case 32: k_pack<Sym, 1><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
+            case 64: k_pack<Sym, 2><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
+            case 128: k_pack<Sym, 4><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
+            default: k_pack<Sym, 8><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
+        }
         countLaunch();
     }
     { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 128, 0, st>>>(p); countLaunch(); }

@@ -231,6 +231,10 @@ __device__ void blockIntrosort(u32* a, int n, u16* lList, u16* rList, u8* mark, 
     Seg* nxt = qB;
     int nCur = counters[0];
     while (nCur > 0) {
+        // counters[1] counts the next round's segments.  Its reset comes
+        // after the barrier that ends the previous round's reads of it (the
+        // third barrier below), and the barrier after the reset orders it
+        // before this round's additions.
         if (threadIdx.x == 0) counters[1] = 0;
         __syncthreads();
         for (int s = warp; s < nCur; s += kWarps) {
@@ -258,6 +262,7 @@ __device__ void blockIntrosort(u32* a, int n, u16* lList, u16* rList, u8* mark, 
         }
         __syncthreads();
         nCur = counters[1];
+        __syncthreads();   // every thread has read the count before thread 0 resets it
         Seg* t = cur;
         cur = nxt;
         nxt = t;

@@ -178,3 +178,29 @@ def test_batch_stream_download_upload(oracle):
         with pytest.raises(cc.CudaCompressError):       # pageable host memory is refused
             b.download_streams(torch.zeros(cap, dtype=torch.int32), he)
     inst.close()
+
+
+def test_batch_back_to_back_encodes_are_deterministic():
+    """Many encodes enqueued back to back (no host wait; the lowpass tables
+    build beside the highpass encode and the previous call's tail) give the
+    same bytes every time.  Guards the table builder's block-cooperative sort,
+    whose round counter once could be reset before a slower warp read it."""
+    bricks_, q = fields.brick_set(512, 1005)
+    dv = [torch.from_numpy(b).cuda() for b in bricks_]
+    inst = cc.Instance(0, 7, 32 ** 3, 128, 14)
+    with cc.VolumeBatch(inst, [b.shape for b in bricks_], 2, [float(v) for v in q], graph=True) as b:
+        cap = sum(cc.volume_stream_capacity_words(*v.shape[::-1]) for v in bricks_)
+        n = 20
+        hw = [torch.zeros(cap, dtype=torch.int32).pin_memory() for _ in range(n)]
+        he = [torch.zeros(2 * len(bricks_), dtype=torch.int64).pin_memory() for _ in range(n)]
+        for i in range(n):
+            b.compress(dv)
+            b.download_streams(hw[i], he[i])
+        torch.cuda.synchronize()
+        b.status()
+        ext = he[0].numpy()
+        total = int(ext[len(bricks_) - 1] + (ext[-1] + 31) // 32)
+        for i in range(1, n):
+            assert np.array_equal(he[i].numpy(), ext), i
+            assert np.array_equal(hw[i].numpy()[:total], hw[0].numpy()[:total]), i
+    inst.close()
