@@ -747,20 +747,31 @@ __device__ __forceinline__ void quantStorePair(const BColDesc& D, int x, int y, 
     *reinterpret_cast<u32*>(base + (u64(lz) * D.hy + ly) * D.hx + lx) = s0 | (s1 << 16);
 }
 
-template <bool kInverse, int kParity, bool kQuantize = false>
-__device__ __forceinline__ void colOutputs(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x, int c,
-                                           int a0) {
-    for (int k = ty; k < kBColTileA; k += 8) {
-        const int a = a0 + k;
+// Eight consecutive outputs of a column pair per thread: the 16 staged
+// samples they use are read from shared memory once into registers (a
+// sliding window) instead of nine reads per output.  The tile's first row
+// is even, so output j has parity j & 1 and its taps are immediates.
+template <bool kInverse, bool kQuantize = false>
+__device__ __forceinline__ void colOutputs8(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x, int c,
+                                            int a0) {
+    static_assert(kBColTileA == 64, "eight outputs per thread row of an 8-row block");
+    const int k0 = 8 * ty;
+    if (a0 + k0 >= D.na) return;
+    float2 w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = s[k0 + i][tx];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int a = a0 + k0 + j;
         if (a >= D.na) break;
         float v0[9], v1[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
-            const float2 t = s[k + i][tx];
-            v0[i] = t.x;
-            v1[i] = t.y;
+            v0[i] = w[j + i].x;
+            v1[i] = w[j + i].y;
         }
-        const float2 r = make_float2(fir9c<kInverse, kParity>(v0), fir9c<kInverse, kParity>(v1));
+        const float2 r = (j & 1) ? make_float2(fir9c<kInverse, 1>(v0), fir9c<kInverse, 1>(v1))
+                                 : make_float2(fir9c<kInverse, 0>(v0), fir9c<kInverse, 0>(v1));
         const int o = kInverse ? a : splitPos(a, D.na);
         if (kQuantize) quantStorePair(D, x, c, o, r);   // axis Z: a = z, c = y
         else *reinterpret_cast<float2*>(D.dst + size_t(x) + size_t(o) * D.da + size_t(c) * D.dc) = r;
@@ -840,8 +851,7 @@ __global__ void __launch_bounds__(256) k_bCols(const BColDesc* __restrict__ desc
     for (int i = 0; i < kLoads; ++i) s[ty + 8 * i][tx] = vals[i];
     __syncthreads();
     if (x >= nx) return;
-    if ((a0 + ty) & 1) colOutputs<kInverse, 1, kQuantize>(D, s, tx, ty, x, c, a0);
-    else colOutputs<kInverse, 0, kQuantize>(D, s, tx, ty, x, c, a0);
+    colOutputs8<kInverse, kQuantize>(D, s, tx, ty, x, c, a0);
 }
 
 // Quantization of one band to u16 symbols (deadzone, Quantize.cuh:55-59), or
