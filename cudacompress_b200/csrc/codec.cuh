@@ -217,6 +217,8 @@ struct cc_instance {
     ccb::u32* headers = nullptr;       // [capHdr]
     ccb::u32* blockBits = nullptr;     // [capBlocks]
     ccb::u32* blockOff = nullptr;      // [capBlocks]
+    ccb::u32* blockTable = nullptr;    // [capBlocks]: table of each coding block of a call
+    ccb::u32* tileStream = nullptr;    // [capTiles]: stream of each run-length tile of a call
     ccb::SegmentLayout* layout = nullptr;  // [capStreams]
     ccb::u32* out = nullptr;           // [outWordsMax]
     ccb::u32* counts = nullptr;        // [capStreams]

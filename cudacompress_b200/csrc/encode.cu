@@ -38,6 +38,8 @@ struct EncParams {
     u32* headers;
     u32* blockBits;
     u32* blockOff;
+    u32* blockTable;  // [totalBlocks] table of each coding block (k_lookupMaps)
+    u32* tileStream;  // [totalTiles] stream of each run-length tile (k_lookupMaps)
     SegmentLayout* layout;
     u32* out;
     u64 outWordsMax;
@@ -65,24 +67,10 @@ __device__ __forceinline__ bool warpFailed(const EncParams& p) {
     return __any_sync(0xffffffffu, *reinterpret_cast<volatile const u32*>(p.errors) != 0);
 }
 
-// Stream owning flattened tile `tile` (largest s with tileOff <= tile).
-__device__ __forceinline__ u32 streamOfTile(const EncParams& p, u32 tile) {
-    u32 lo = 0, hi = p.S;
-    while (hi - lo > 1) {
-        const u32 mid = (lo + hi) >> 1;
-        if (p.streams[mid].tileOff <= tile) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-// Table owning flattened coding block `gb`.
-__device__ __forceinline__ u32 tableOfBlock(const EncParams& p, u32 gb) {
-    u32 lo = 0, hi = p.T;
-    while (hi - lo > 1) {
-        const u32 mid = (lo + hi) >> 1;
-        if (p.tables[mid].blockOff <= gb) lo = mid; else hi = mid;
-    }
-    return lo;
-}
+// Stream owning run-length tile `tile`, and table owning coding block `gb`:
+// one load each from the maps k_lookupMaps writes at the start of a call.
+__device__ __forceinline__ u32 streamOfTile(const EncParams& p, u32 tile) { return p.tileStream[tile]; }
+__device__ __forceinline__ u32 tableOfBlock(const EncParams& p, u32 gb) { return p.blockTable[gb]; }
 
 // Input symbols of table t and their count.
 template <class Sym>
@@ -174,6 +162,22 @@ __device__ __forceinline__ RunSum threadRun(const u32 (&v)[kRlePerThread], u32 b
         }
     }
     return r;
+}
+
+// The call's lookup maps: CTA i < S writes the stream index over its tiles,
+// CTA i < T the table index over its coding blocks (both ranges are the
+// prefix layout of the call's descriptors).
+__global__ void __launch_bounds__(256) k_lookupMaps(EncParams p) {
+    const u32 i = blockIdx.x;
+    if (i < p.S) {
+        const EncStreamDev& sd = p.streams[i];
+        const u32 tiles = u32(ceilDiv(sd.n, kRleTile));
+        for (u32 k = threadIdx.x; k < tiles; k += 256) p.tileStream[sd.tileOff + k] = i;
+    }
+    if (i < p.T) {
+        const EncTableDev& td = p.tables[i];
+        for (u32 k = threadIdx.x; k < td.blocksMax; k += 256) p.blockTable[td.blockOff + k] = i;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -808,11 +812,30 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
         cw[k] = j0 + u32(k) < count ? enc[min(sv[k], hs - 1u)] : make_uint2(0, 0);
         lsum += cw[k].y;
     }
-    u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
+    // the lane's codewords are consecutive: concatenate them in a 64-bit
+    // accumulator (bits left-aligned from the lane's start bit in its first
+    // word) and OR whole words into the window - one shared atomic per word
+    // touched instead of one or two per codeword
+    const u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
+    {
+        u32 w = pos >> 5;
+        u32 n = pos & 31u;
+        unsigned long long acc = 0;
 #pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-        orCodeword(win, wLo, wHi, pos, cw[k].x, cw[k].y);
-        pos += cw[k].y;
+        for (int k = 0; k < kPer; ++k) {
+            const u32 len = cw[k].y;
+            if (len) {
+                acc |= (unsigned long long)cw[k].x << (64u - n - len);
+                n += len;
+            }
+            if (n >= 32u) {
+                if (w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
+                acc <<= 32;
+                n -= 32u;
+                ++w;
+            }
+        }
+        if (n && w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
     }
     // bits of the next block inside the last owned word
     if (b + 1 < m.blocks && (wHi << 5) > off1) {
@@ -945,6 +968,8 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     cudaStream_t st = I->stream;
     CC_TRY_CUDA(cudaMemsetAsync(I->errors, 0, 4 * sizeof(u32), st), "memset errors");
     CC_TRY_CUDA(cudaMemsetAsync(I->streamMax, 0, sizeof(u32) * p.S, st), "memset stream max");
+    k_lookupMaps<<<std::max(p.S, p.T), 256, 0, st>>>(p);
+    countLaunch();
     if (p.totalTiles) { SectionTimer t(I, "enc.summary", st); k_summary<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.rle_scan", st); k_scan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
@@ -1034,6 +1059,8 @@ int encodeLaunch(cc_instance* I, const EncPlan& hp, u32* out, u64 outCap) {
     p.headers = I->headers;
     p.blockBits = I->blockBits;
     p.blockOff = I->blockOff;
+    p.blockTable = I->blockTable;
+    p.tileStream = I->tileStream;
     p.layout = I->layout;
     p.out = out;
     p.outWordsMax = outCap;

@@ -121,6 +121,8 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->headers = c.take<u32>(I->capHdr);
     I->blockBits = c.take<u32>(I->capBlocks + 1);
     I->blockOff = c.take<u32>(I->capBlocks + 1);
+    I->blockTable = c.take<u32>(I->capBlocks + 1);
+    I->tileStream = c.take<u32>(I->capTiles + 1);
     I->layout = c.take<SegmentLayout>(I->capStreams);
     I->out = c.take<u32>(I->outWordsMax);
     I->counts = c.take<u32>(I->capStreams);
