@@ -105,6 +105,8 @@ struct TableMeta {
     u32 codeBits;     // total codeword bits
     u32 blocks;       // coding blocks
     u32 histSize;     // histogram bins of this table
+    u32 actOff;       // first of its coding blocks in the call's list of used blocks
+    u32 pad;
     u64 histOff;      // offset of its histogram and code table
     u64 leafOff;      // offset of its table-builder arrays (by leaf)
     u64 hdrOff;       // offset of its serialized header (words)

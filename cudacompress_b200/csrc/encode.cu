@@ -38,7 +38,7 @@ struct EncParams {
     u32* headers;
     u32* blockBits;
     u32* blockOff;
-    u32* blockTable;  // [totalBlocks] table of each coding block (k_lookupMaps)
+    u32* blockTable;  // [used blocks] table of each coding block in use (k_usedBlocks)
     u32* tileStream;  // [totalTiles] stream of each run-length tile (k_lookupMaps)
     SegmentLayout* layout;
     u32* out;
@@ -67,10 +67,9 @@ __device__ __forceinline__ bool warpFailed(const EncParams& p) {
     return __any_sync(0xffffffffu, *reinterpret_cast<volatile const u32*>(p.errors) != 0);
 }
 
-// Stream owning run-length tile `tile`, and table owning coding block `gb`:
-// one load each from the maps k_lookupMaps writes at the start of a call.
+// Stream owning run-length tile `tile`: one load from the map k_lookupMaps
+// writes at the start of a call.
 __device__ __forceinline__ u32 streamOfTile(const EncParams& p, u32 tile) { return p.tileStream[tile]; }
-__device__ __forceinline__ u32 tableOfBlock(const EncParams& p, u32 gb) { return p.blockTable[gb]; }
 
 // Input symbols of table t and their count.
 template <class Sym>
@@ -164,20 +163,24 @@ __device__ __forceinline__ RunSum threadRun(const u32 (&v)[kRlePerThread], u32 b
     return r;
 }
 
-// The call's lookup maps: CTA i < S writes the stream index over its tiles,
-// CTA i < T the table index over its coding blocks (both ranges are the
+// The call's tile map: CTA s writes the stream index over its tiles (the
 // prefix layout of the call's descriptors).
 __global__ void __launch_bounds__(256) k_lookupMaps(EncParams p) {
     const u32 i = blockIdx.x;
-    if (i < p.S) {
-        const EncStreamDev& sd = p.streams[i];
-        const u32 tiles = u32(ceilDiv(sd.n, kRleTile));
-        for (u32 k = threadIdx.x; k < tiles; k += 256) p.tileStream[sd.tileOff + k] = i;
-    }
-    if (i < p.T) {
-        const EncTableDev& td = p.tables[i];
-        for (u32 k = threadIdx.x; k < td.blocksMax; k += 256) p.blockTable[td.blockOff + k] = i;
-    }
+    const EncStreamDev& sd = p.streams[i];
+    const u32 tiles = u32(ceilDiv(sd.n, kRleTile));
+    for (u32 k = threadIdx.x; k < tiles; k += 256) p.tileStream[sd.tileOff + k] = i;
+}
+
+// The coding blocks in use (those holding symbols after the run-length
+// step), listed table by table: CTA t writes t over its meta.blocks entries
+// from meta.actOff (k_histPlan).  The block-level kernels walk this list
+// instead of every block a table could have.
+__global__ void __launch_bounds__(256) k_usedBlocks(EncParams p) {
+    if (blockFailed(p)) return;
+    const u32 t = blockIdx.x;
+    const TableMeta& m = p.meta[t];
+    for (u32 k = threadIdx.x; k < m.blocks; k += 256) p.blockTable[m.actOff + k] = t;
 }
 
 // ---------------------------------------------------------------------------
@@ -268,8 +271,8 @@ __global__ void __launch_bounds__(1024) k_scan(EncParams p) {
 // instance's 2^log2Max range fails the call (HuffmanTable.cu:411-419).
 __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
     __shared__ u32 scratch[40];
-    __shared__ unsigned long long cH, cL, cW;
-    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; }
+    __shared__ unsigned long long cH, cL, cW, cA;
+    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; cA = 0; }
     __syncthreads();
     for (u32 base = 0; base < p.T; base += 1024) {
         const u32 t = base + threadIdx.x;
@@ -287,21 +290,24 @@ __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
             m.histSize = hs;
             m.blocks = u32(ceilDiv(count, p.cb));
         }
-        u32 tH, tL, tW;
+        u32 tH, tL, tW, tA;
         const u32 eH = blockExclusiveSum<1024>(hs, scratch, &tH);
         const u32 eL = blockExclusiveSum<1024>(ls, scratch, &tL);
         const u32 eW = blockExclusiveSum<1024>(ws, scratch, &tW);
+        const u32 eA = blockExclusiveSum<1024>(m.blocks, scratch, &tA);
         if (t < p.T) {
             m.histOff = cH + eH;
             m.leafOff = cL + eL;
             m.hdrOff = cW + eW;
+            m.actOff = u32(cA + eA);
             p.meta[t] = m;
         }
         __syncthreads();
-        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; }
+        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; cA += tA; }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
+        p.totals[2] = cA;
         p.totals[1] = cH;
         if (cH > p.capHist || cL > p.capLeaves || cW > p.capHdr) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
     }
@@ -658,31 +664,34 @@ __device__ __forceinline__ void laneSyms(const Sym* in, u32 j0, u32 count, u32 (
     for (int k = 0; k < kPer; ++k) s[k] = j0 + u32(k) < count ? u32(q[k]) : 0u;
 }
 
-// Bits of every coding block: one warp per block, each lane kPer symbols
-// loaded at once and their code lengths gathered together.
+// Bits of every coding block in use: warps walk the list of used blocks
+// (k_usedBlocks); each lane loads its kPer symbols at once and gathers their
+// code lengths together.
 template <class Sym, int kPer>
 __global__ void __launch_bounds__(kPackWarps * 32) k_blockBits(EncParams p) {
-    const u32 gb = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
     const u32 lane = threadIdx.x & 31;
-    if (gb >= p.totalBlocks || warpFailed(p)) return;
-    const u32 t = tableOfBlock(p, gb);
-    const EncTableDev td = p.tables[t];
-    const u32 b = gb - td.blockOff;
-    u32 count;
-    const Sym* in = tableInput<Sym>(p, td, count);
-    const TableMeta& m = p.meta[t];
-    if (b >= m.blocks) return;
-    const uint2* enc = p.enc + m.histOff;
-    const u32 hs = m.histSize;
-    const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
-    u32 sv[kPer];
-    laneSyms<Sym, kPer>(in, j0, count, sv);
-    u32 bits = 0;
+    if (warpFailed(p)) return;
+    const u32 used = u32(p.totals[2]);
+    const u32 stride = gridDim.x * kPackWarps;
+    for (u32 i = blockIdx.x * kPackWarps + (threadIdx.x >> 5); i < used; i += stride) {
+        const u32 t = p.blockTable[i];
+        const TableMeta& m = p.meta[t];
+        const EncTableDev td = p.tables[t];
+        const u32 b = i - m.actOff;
+        u32 count;
+        const Sym* in = tableInput<Sym>(p, td, count);
+        const uint2* enc = p.enc + m.histOff;
+        const u32 hs = m.histSize;
+        const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
+        u32 sv[kPer];
+        laneSyms<Sym, kPer>(in, j0, count, sv);
+        u32 bits = 0;
 #pragma unroll
-    for (int k = 0; k < kPer; ++k)
-        if (j0 + u32(k) < count) bits += enc[min(sv[k], hs - 1u)].y;
-    bits = warpSum(bits);
-    if (lane == 0) p.blockBits[gb] = bits;
+        for (int k = 0; k < kPer; ++k)
+            if (j0 + u32(k) < count) bits += enc[min(sv[k], hs - 1u)].y;
+        bits = warpSum(bits);
+        if (lane == 0) p.blockBits[td.blockOff + b] = bits;
+    }
 }
 
 // Exclusive scan of one table's block bits (one block per table).
@@ -783,72 +792,75 @@ template <class Sym, int kPer>
 __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
     extern __shared__ u32 winAll[];
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const u32 gb = blockIdx.x * kPackWarps + warp;
-    if (gb >= p.totalBlocks || warpFailed(p)) return;
-    const u32 t = tableOfBlock(p, gb);
-    const EncTableDev td = p.tables[t];
-    const u32 b = gb - td.blockOff;
+    if (warpFailed(p)) return;
     u32* win = winAll + warp * (p.cb + 2);
-    u32 count;
-    const Sym* in = tableInput<Sym>(p, td, count);
-    const TableMeta m = p.meta[t];
-    if (b >= m.blocks) return;
-    const u32* bo = p.blockOff + td.blockOff;
-    const u32 off0 = bo[b];
-    const u32 off1 = (b + 1 < m.blocks) ? bo[b + 1] : m.codeBits;
-    const u32 wLo = (off0 + 31) >> 5, wHi = (off1 + 31) >> 5;
-    if (wLo >= wHi) return;
-    for (u32 w = lane; w < wHi - wLo; w += 32) win[w] = 0;
-    __syncwarp();
-    const uint2* enc = p.enc + m.histOff;
-    const u32 hs = m.histSize;
-    const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
-    u32 sv[kPer];
-    laneSyms<Sym, kPer>(in, j0, count, sv);
-    uint2 cw[kPer];
-    u32 lsum = 0;
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-        cw[k] = j0 + u32(k) < count ? enc[min(sv[k], hs - 1u)] : make_uint2(0, 0);
-        lsum += cw[k].y;
-    }
-    // the lane's codewords are consecutive: concatenate them in a 64-bit
-    // accumulator (bits left-aligned from the lane's start bit in its first
-    // word) and OR whole words into the window - one shared atomic per word
-    // touched instead of one or two per codeword
-    const u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
-    {
-        u32 w = pos >> 5;
-        u32 n = pos & 31u;
-        unsigned long long acc = 0;
+    const u32 used = u32(p.totals[2]);
+    const u32 stride = gridDim.x * kPackWarps;
+    for (u32 i = blockIdx.x * kPackWarps + warp; i < used; i += stride) {
+        const u32 t = p.blockTable[i];
+        const TableMeta m = p.meta[t];
+        const EncTableDev td = p.tables[t];
+        const u32 b = i - m.actOff;
+        u32 count;
+        const Sym* in = tableInput<Sym>(p, td, count);
+        const u32* bo = p.blockOff + td.blockOff;
+        const u32 off0 = bo[b];
+        const u32 off1 = (b + 1 < m.blocks) ? bo[b + 1] : m.codeBits;
+        const u32 wLo = (off0 + 31) >> 5, wHi = (off1 + 31) >> 5;
+        if (wLo >= wHi) continue;
+        for (u32 w = lane; w < wHi - wLo; w += 32) win[w] = 0;
+        __syncwarp();
+        const uint2* enc = p.enc + m.histOff;
+        const u32 hs = m.histSize;
+        const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
+        u32 sv[kPer];
+        laneSyms<Sym, kPer>(in, j0, count, sv);
+        uint2 cw[kPer];
+        u32 lsum = 0;
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-            const u32 len = cw[k].y;
-            if (len) {
-                acc |= (unsigned long long)cw[k].x << (64u - n - len);
-                n += len;
-            }
-            if (n >= 32u) {
-                if (w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
-                acc <<= 32;
-                n -= 32u;
-                ++w;
-            }
+            cw[k] = j0 + u32(k) < count ? enc[min(sv[k], hs - 1u)] : make_uint2(0, 0);
+            lsum += cw[k].y;
         }
-        if (n && w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
+        // the lane's codewords are consecutive: concatenate them in a 64-bit
+        // accumulator (bits left-aligned from the lane's start bit in its
+        // first word) and OR whole words into the window - one shared atomic
+        // per word touched instead of one or two per codeword
+        const u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
+        {
+            u32 w = pos >> 5;
+            u32 n = pos & 31u;
+            unsigned long long acc = 0;
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                const u32 len = cw[k].y;
+                if (len) {
+                    acc |= (unsigned long long)cw[k].x << (64u - n - len);
+                    n += len;
+                }
+                if (n >= 32u) {
+                    if (w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
+                    acc <<= 32;
+                    n -= 32u;
+                    ++w;
+                }
+            }
+            if (n && w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
+        }
+        // bits of the next block inside the last owned word
+        if (b + 1 < m.blocks && (wHi << 5) > off1) {
+            const u32 j = (b + 1) * p.cb + lane;
+            uint2 c = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
+            u32 q = off1 + warpInclusiveSum(c.y) - c.y;
+            if (q < (wHi << 5)) orCodeword(win, wLo, wHi, q, c.x, c.y);
+        }
+        __syncwarp();
+        const u32 which = (p.streams[td.stream].kind == KIND_RLHUFF && td.which) ? 1u : 0u;
+        const SegmentLayout& L = p.layout[td.stream];
+        u32* dst = p.out + L.startWord + L.cwWord[which];
+        for (u32 w = lane; w < wHi - wLo; w += 32) dst[wLo + w] = win[w];
+        __syncwarp();   // the window is cleared for the next block only after these reads
     }
-    // bits of the next block inside the last owned word
-    if (b + 1 < m.blocks && (wHi << 5) > off1) {
-        const u32 j = (b + 1) * p.cb + lane;
-        uint2 c = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
-        u32 q = off1 + warpInclusiveSum(c.y) - c.y;
-        if (q < (wHi << 5)) orCodeword(win, wLo, wHi, q, c.x, c.y);
-    }
-    __syncwarp();
-    const u32 which = (p.streams[td.stream].kind == KIND_RLHUFF && td.which) ? 1u : 0u;
-    const SegmentLayout& L = p.layout[td.stream];
-    u32* dst = p.out + L.startWord + L.cwWord[which];
-    for (u32 w = lane; w < wHi - wLo; w += 32) dst[wLo + w] = win[w];
 }
 
 // Count words, table headers, codeword bit counts and offset increments.
@@ -968,8 +980,7 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     cudaStream_t st = I->stream;
     CC_TRY_CUDA(cudaMemsetAsync(I->errors, 0, 4 * sizeof(u32), st), "memset errors");
     CC_TRY_CUDA(cudaMemsetAsync(I->streamMax, 0, sizeof(u32) * p.S, st), "memset stream max");
-    k_lookupMaps<<<std::max(p.S, p.T), 256, 0, st>>>(p);
-    countLaunch();
+    if (p.S) { k_lookupMaps<<<p.S, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) { SectionTimer t(I, "enc.summary", st); k_summary<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.rle_scan", st); k_scan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
@@ -983,8 +994,12 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
     { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
+    // used-block list (after the plan, k_histPlan); the block kernels walk it
+    // with a grid of a few CTAs per SM
+    if (p.totalBlocks && p.T) { k_usedBlocks<<<p.T, 256, 0, st>>>(p); countLaunch(); }
+    const u32 blockGrid = u32(std::max(1, I->smCount > 0 ? I->smCount : 148)) * 8u;
     if (p.totalBlocks) {
-        const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
+        const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(p.totalBlocks, kPackWarps)));
         {
             SectionTimer t(I, "enc.block_bits", st);
             switch (p.cb) {
@@ -999,7 +1014,7 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     }
     { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
     if (p.totalBlocks) {
-        const u32 g = u32(ceilDiv(p.totalBlocks, kPackWarps));
+        const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(p.totalBlocks, kPackWarps)));
         const size_t packSmem = size_t(kPackWarps) * (p.cb + 2) * sizeof(u32);
         SectionTimer t(I, "enc.pack", st);
         switch (p.cb) {
