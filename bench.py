@@ -93,14 +93,39 @@ def load_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """SM clock and throttle-reason samples taken during the timed region.
+    The timed regions last tens of milliseconds, so NVML is polled from a
+    thread every millisecond (read-only queries; the GPU is found by its PCI
+    bus id, which CUDA_VISIBLE_DEVICES does not renumber); nvidia-smi at 200
+    ms is the fallback."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    BITS = (0x8, 0x40, 0x20, 0x4)   # NVML clocks event reason bits, in NAMES order
 
-    def __init__(self, gpu_index: int):
-        self.lines = []
-        self.proc = None
+    def __init__(self, gpu_index: int, period_s: float = 0.001):
+        self.lines, self.samples = [], []
+        self.proc, self.nvml = None, None
+        self.period = period_s
+        self._halt = threading.Event()
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                pr = torch.cuda.get_device_properties(gpu_index)
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(
+                    f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self.nvml, self.h = pynvml, h
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(gpu_index)], stdout=subprocess.PIPE,
@@ -110,11 +135,29 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml, self.h
+        while not self._halt.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((sm, rs))
+            except Exception:
+                return
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self._halt.set()
+            self.thread.join(timeout=2)
+            sm = [a for a, _ in self.samples]
+            reasons = {nm for _, rs in self.samples for nm, b in zip(self.NAMES, self.BITS) if rs & b}
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 1 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -124,7 +167,6 @@ class ClockSampler:
             self.proc.kill()
         self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -134,11 +176,11 @@ class ClockSampler:
                 smax.append(float(parts[2]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(self.NAMES, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ------------------------------------------------------------------ fields

@@ -522,6 +522,13 @@ static int dwtScratchFor(int device, float** out) {
 // k_quantize, over all volumes of a batch in one launch.  A CTA reads its
 // descriptor index from the launch's CTA map (one load) and the descriptor.
 // ---------------------------------------------------------------------------
+// floor(k / d) for 0 <= k < 2^22 and 1 <= d < 2^13 from r = 1/d rounded to
+// nearest: (k + 1/2) / d lies at least 1/(2d) from an integer, and the two
+// roundings move it by at most (k/d) 2^-23 < 1/(2d).
+__device__ __forceinline__ int quotient(int k, float r) {
+    return int(__float2uint_rz((float(k) + 0.5f) * r));
+}
+
 template <bool kInverse>
 __device__ __forceinline__ void rowPairs4(const float* w, float4& a, float4& b) {
     // four (even, odd) output pairs from the 16-sample window w[0..15]
@@ -557,12 +564,22 @@ __global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ desc
     const int nx = D.nx, hn = nx >> 1;
     const int x0 = xt * D.W, Wt = min(D.W, nx - x0), Wp = Wt + 8;
     const int rows = D.ny * D.nz, r0 = rg * D.R, R = min(D.R, rows - r0);
+    // row j of the tile: (y0 + j, z0) carried over slices (R <= 128 rows, so
+    // at most one carry when ny >= 128)
+    const int z0 = r0 / D.ny, y0 = r0 - z0 * D.ny;
+    auto rowYZ = [&](int j, int& y, int& z) {
+        y = y0 + j;
+        z = z0;
+        while (y >= D.ny) { y -= D.ny; ++z; }
+    };
     auto srcRow = [&](int j) {
-        const int r = r0 + j, z = r / D.ny, y = r - z * D.ny;
+        int y, z;
+        rowYZ(j, y, z);
         return src + size_t(z) * D.srcSlice + size_t(y) * D.srcRow;
     };
     auto dstRow = [&](int j) {
-        const int r = r0 + j, z = r / D.ny, y = r - z * D.ny;
+        int y, z;
+        rowYZ(j, y, z);
         return dst + size_t(z) * D.dstSlice + size_t(y) * D.dstRow;
     };
     const int tid = threadIdx.x;
@@ -573,12 +590,13 @@ __global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ desc
         float4 body[kBody];
         float halo[kBody];
         const int U = kInverse ? Wt >> 3 : Wt >> 2;
+        const float rU = __frcp_rn(float(U));
 #pragma unroll
         for (int i = 0; i < kBody; ++i) {
             const int k = tid + 256 * (kInverse ? (i >> 1) : i);
             body[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (k < R * U) {
-                const int j = k / U, q = k - j * U;
+                const int j = quotient(k, rU), q = k - j * U;
                 const float* row = srcRow(j);
                 if (kInverse) body[i] = *reinterpret_cast<const float4*>(row + (i & 1) * hn + (x0 >> 1) + 4 * q);
                 else body[i] = *reinterpret_cast<const float4*>(row + x0 + 4 * q);
@@ -598,7 +616,7 @@ __global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ desc
         for (int i = 0; i < kBody; ++i) {
             const int k = tid + 256 * (kInverse ? (i >> 1) : i);
             if (k < R * U) {
-                const int j = k / U, q = k - j * U;
+                const int j = quotient(k, rU), q = k - j * U;
                 if (kInverse) {
                     if (i & 1) {
                         const float4 l = body[i - 1], h = body[i];
@@ -618,11 +636,12 @@ __global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ desc
         __syncthreads();
         // outputs: four pairs per thread-step
         const int Q = Wt >> 3;
+        const float rQ = __frcp_rn(float(Q));
 #pragma unroll
         for (int i = 0; i < kBRowOutputs / 2048; ++i) {
             const int k = tid + 256 * i;
             if (k < R * Q) {
-                const int j = k / Q, q = k - j * Q;
+                const int j = quotient(k, rQ), q = k - j * Q;
                 const float* w4 = s + j * Wp + 8 * q;
                 float w[16];
 #pragma unroll
