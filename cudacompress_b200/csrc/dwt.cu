@@ -797,6 +797,52 @@ __device__ __forceinline__ void colOutputs8(const BColDesc& D, const float2 (*s)
     }
 }
 
+// The same outputs with the quantizer fused into the store (axis Z, a = z,
+// c = y), for an even half width hx and hz = na / 2: the thread's x and y fix
+// its octant up to bz, and output a lands in octant bz = a & 1 at lz = a >> 1
+// (a's split position is a / 2 or hz + a / 2), so every store goes to one of
+// two per-thread bases.  Symbols as quantStorePair computes them.
+__device__ __forceinline__ void colOutputs8Quantize(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x,
+                                                    int c, int a0) {
+    const int k0 = 8 * ty;
+    if (a0 + k0 >= D.na) return;
+    float2 w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = s[k0 + i][tx];
+    const int bx = x >= D.hx, by = c >= D.hy;
+    const int lx = x - bx * D.hx, ly = c - by * D.hy, be = bx + 2 * by;
+    const u64 slice = u64(D.hy) * D.hx, inPlane = u64(ly) * D.hx + lx;
+    u16* const oddBase = D.symOut + u64(be + 3) * D.bandStride + inPlane;        // octant be + 4
+    u16* const evenSym = be ? D.symOut + u64(be - 1) * D.bandStride + inPlane     // octant be
+                            : D.lpSymOut + inPlane;                               // LLL, coarsest level
+    const bool evenFloat = be == 0 && !D.lastLevel;                              // LLL kept as floats
+    float* const evenF = D.dst + size_t(x) + size_t(c) * D.dc;
+    const float invEven = be ? D.inv : D.invLP;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int a = a0 + k0 + j;
+        if (a >= D.na) break;
+        float v0[9], v1[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            v0[i] = w[j + i].x;
+            v1[i] = w[j + i].y;
+        }
+        const float2 r = (j & 1) ? make_float2(fir9c<false, 1>(v0), fir9c<false, 1>(v1))
+                                 : make_float2(fir9c<false, 0>(v0), fir9c<false, 0>(v1));
+        const u64 lz = u64(a >> 1);
+        if (j & 1) {
+            const u32 s0 = symbolizeI(int(r.x * D.inv)) & 0xFFFFu, s1 = symbolizeI(int(r.y * D.inv)) & 0xFFFFu;
+            *reinterpret_cast<u32*>(oddBase + lz * slice) = s0 | (s1 << 16);
+        } else if (evenFloat) {
+            *reinterpret_cast<float2*>(evenF + size_t(a >> 1) * D.da) = r;
+        } else {
+            const u32 s0 = symbolizeI(int(r.x * invEven)) & 0xFFFFu, s1 = symbolizeI(int(r.y * invEven)) & 0xFFFFu;
+            *reinterpret_cast<u32*>(evenSym + lz * slice) = s0 | (s1 << 16);
+        }
+    }
+}
+
 // Y or Z pass: 64 x-columns (a column pair per thread, float2 accesses; all
 // level extents are even and x is the unit-stride axis) by kBColTileA axis
 // positions per CTA.  The output parity of a thread is fixed (kBColTileA and
@@ -817,32 +863,34 @@ __global__ void __launch_bounds__(256, 4) k_bCols(const BColDesc* __restrict__ d
     // all of a thread's column loads are issued before any is used
     constexpr int kLoads = (kBColTileA + 8) / 8;
     float2 vals[kLoads];
-    if (kSymbols && !(D.hx & 1)) {
-        // axis Z (a = z, c = y), even half width: every load is either one
-        // float2 of the lowpass or one 4-byte symbol pair, issued as
-        // predicated loads of raw bits; the dequantization follows once all
-        // of them are in flight
+    if (kSymbols && !(D.hx & 1) && 2 * D.hz == na) {
+        // axis Z (a = z, c = y), even half width, hz = na / 2: the thread's
+        // rows j = a0 - 4 + ty + 8i all have the parity of ty, and so have
+        // their mirrored indices m, so all lie in octant bx + 2by + 4 (ty
+        // odd) or bx + 2by (ty even), at lz = m >> 1.  Each load is one
+        // float2 of the lowpass (octant 0) or one 4-byte symbol pair, issued
+        // as predicated loads of raw bits; the dequantization follows once
+        // all of them are in flight.
         const int bx = x >= D.hx, by = c >= D.hy;
         const int lx = x - bx * D.hx, ly = c - by * D.hy;
+        const int b = bx + 2 * by + ((ty & 1) ? 4 : 0);
+        const u64 slice = u64(D.hy) * D.hx;
+        const u16* const band = D.bands + u64(b ? b - 1 : 0) * D.bandStride + u64(ly) * D.hx + lx;
+        const float* const lpBase = D.src + size_t(ly) * D.lpRow + lx;
         uint2 raw[kLoads];
-        bool lp[kLoads];
 #pragma unroll
         for (int i = 0; i < kLoads; ++i) {
             const int j = a0 - 4 + ty + 8 * i;
             raw[i] = make_uint2(0u, 0u);
-            const int m = mirrorIdx(j, na);
-            const int z = splitPos(m, na), bz = z >= D.hz, lz = z - bz * D.hz;
-            const int b = bx + 2 * by + 4 * bz;
-            lp[i] = b == 0;
             if (x < nx && j < na + 4) {
-                if (lp[i]) raw[i] = *reinterpret_cast<const uint2*>(D.src + size_t(lz) * D.lpSlice + size_t(ly) * D.lpRow + lx);
-                else raw[i].x = *reinterpret_cast<const u32*>(D.bands + u64(b - 1) * D.bandStride +
-                                                              (u64(lz) * D.hy + ly) * D.hx + lx);
+                const int lz = mirrorIdx(j, na) >> 1;
+                if (b == 0) raw[i] = *reinterpret_cast<const uint2*>(lpBase + size_t(lz) * D.lpSlice);
+                else raw[i].x = *reinterpret_cast<const u32*>(band + u64(lz) * slice);
             }
         }
 #pragma unroll
         for (int i = 0; i < kLoads; ++i) {
-            if (lp[i]) {
+            if (b == 0) {
                 vals[i] = make_float2(__uint_as_float(raw[i].x), __uint_as_float(raw[i].y));
             } else {
                 const int q0 = unsymbolizeI(raw[i].x & 0xFFFFu), q1 = unsymbolizeI(raw[i].x >> 16);
@@ -870,7 +918,8 @@ __global__ void __launch_bounds__(256, 4) k_bCols(const BColDesc* __restrict__ d
     for (int i = 0; i < kLoads; ++i) s[ty + 8 * i][tx] = vals[i];
     __syncthreads();
     if (x >= nx) return;
-    colOutputs8<kInverse, kQuantize>(D, s, tx, ty, x, c, a0);
+    if (kQuantize && !(D.hx & 1) && 2 * D.hz == na) colOutputs8Quantize(D, s, tx, ty, x, c, a0);
+    else colOutputs8<kInverse, kQuantize>(D, s, tx, ty, x, c, a0);
 }
 
 // Quantization of one band to u16 symbols (deadzone, Quantize.cuh:55-59), or
