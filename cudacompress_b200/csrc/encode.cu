@@ -51,6 +51,7 @@ struct EncParams {
     u32* orderWork;
     u32* leafSymWork;
     u32 heapCap;      // leaves that fit the shared-memory builder of tableBuild
+    u32 buildLo, buildHi;   // k_tableBuild builds the tables with buildLo <= leaves <= buildHi
 };
 
 constexpr u32 kSmemSymBins = 4096;
@@ -419,6 +420,7 @@ __global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
 // global memory (huffman_build.cuh).
 // ---------------------------------------------------------------------------
 constexpr u32 kBuildThreads = 256;
+constexpr u32 kBuildSplitLeaves = 2048;   // tables built with a 41 KB shared-memory heap
 
 __device__ __forceinline__ void putBits(u32* words, u32 pos, u32 value, u32 count) {
     // MSB-first, count <= 32, words pre-zeroed; atomics because neighbouring
@@ -478,6 +480,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     u32 L;
     if (quirkLeaf) {
         L = 1;
+        if (L < p.buildLo || L > p.buildHi) return;   // uniform: the other build launch has it
         if (threadIdx.x == 0) {
             leafSym[0] = 0;
             const u64 key = (u64(1) << 32) | 0u;
@@ -485,6 +488,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         }
     } else if (count == 0) {
         L = 0;
+        if (L < p.buildLo || L > p.buildHi) return;
     } else {
         const u32 nb = symbolMax + 1;
         const u32 per = (nb + kBuildThreads - 1) / kBuildThreads;
@@ -494,6 +498,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         u32 tot;
         u32 off = blockExclusiveSum<kBuildThreads>(c, sScan, &tot);
         L = tot;
+        if (L < p.buildLo || L > p.buildHi) return;
         const bool toSmem = L <= p.heapCap;
         const bool quirk65535 = p.symBytes == 2 && p.bins == 65536u && symbolMax == 65535u;
         for (u32 b = b0; b < b1; ++b) {
@@ -993,7 +998,29 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     if (I->tableBuildSoloSM && p.T <= u32(I->smCount)) buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
     CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
-    { SectionTimer t(I, "enc.table_build", st); k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(p); countLaunch(); }
+    {
+        SectionTimer t(I, "enc.table_build", st);
+        EncParams q = p;
+        q.buildLo = 0;
+        q.buildHi = ~0u;
+        if (!I->tableBuildSoloSM && p.T > 1 && p.heapCap > kBuildSplitLeaves) {
+            // tables of up to kBuildSplitLeaves leaves first, with the shared
+            // memory they need (41 KB instead of 164 KB per CTA, so kernels of
+            // other calls in flight keep running beside the sequential merges);
+            // the larger ones in a second launch whose other CTAs return after
+            // counting their leaves
+            q.heapCap = kBuildSplitLeaves;
+            q.buildHi = kBuildSplitLeaves;
+            const size_t small = sizeof(u64) * (q.heapCap + 2) + 3 * sizeof(u32) * size_t(q.heapCap);
+            k_tableBuild<<<p.T, kBuildThreads, small, st>>>(q);
+            countLaunch();
+            q.heapCap = p.heapCap;
+            q.buildLo = kBuildSplitLeaves + 1;
+            q.buildHi = ~0u;
+        }
+        k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(q);
+        countLaunch();
+    }
     // used-block list (after the plan, k_histPlan); the block kernels walk it
     // with a grid of a few CTAs per SM
     if (p.totalBlocks && p.T) { k_usedBlocks<<<p.T, 256, 0, st>>>(p); countLaunch(); }
