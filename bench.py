@@ -930,9 +930,9 @@ def run_ours(args, wl):
     # throughput (value): consecutive steps in flight on `nb` batches, each on
     # its own stream, so one step's latency-bound phases (table builds, the
     # decoder's walk) overlap another's bandwidth-bound passes; every step
-    # still encodes and decodes all components.  nb in {1, 2, 3} is chosen by
-    # a short untimed trial (more batches in flight contend for HBM and L2).
-    pool = [batch] + [cc.VolumeBatch(inst, [v.shape for v in vols], L, [q0] * C, graph=True) for _ in range(2)]
+    # still encodes and decodes all components.  nb in {1, 2, 3, 4} is chosen
+    # by a short untimed trial (more batches in flight contend for HBM and L2).
+    pool = [batch] + [cc.VolumeBatch(inst, [v.shape for v in vols], L, [q0] * C, graph=True) for _ in range(3)]
     pstreams = [torch.cuda.Stream(dev) for _ in pool]
     inst_stream = cc.lib().cc_get_instance_stream(inst.handle)
     prec = [[torch.empty_like(v) for v in vols] for _ in pool]
@@ -950,7 +950,7 @@ def run_ours(args, wl):
             torch.cuda.current_stream().wait_stream(st)
 
     trial = {}
-    for nb in (1, 2, 3):
+    for nb in (1, 2, 3, 4):
         inflight(nb, 2 * nb)
         torch.cuda.synchronize()
         a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
