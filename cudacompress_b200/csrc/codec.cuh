@@ -185,6 +185,10 @@ struct cc_instance {
     unsigned codingBlockSize = 0;
     unsigned log2Max = 0;
     cudaStream_t stream = nullptr;
+    // the table build's large-table launch runs on this side stream beside
+    // the small-table launch on `stream` (fork / join by the two events)
+    cudaStream_t buildSide = nullptr;
+    cudaEvent_t buildFork = nullptr, buildJoin = nullptr;
 
     // derived sizes
     ccb::u32 bins = 0;          // 1 << log2Max

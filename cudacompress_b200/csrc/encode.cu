@@ -1004,22 +1004,28 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         q.buildLo = 0;
         q.buildHi = ~0u;
         if (!I->tableBuildSoloSM && p.T > 1 && p.heapCap > kBuildSplitLeaves) {
-            // tables of up to kBuildSplitLeaves leaves first, with the shared
-            // memory they need (41 KB instead of 164 KB per CTA, so kernels of
-            // other calls in flight keep running beside the sequential merges);
-            // the larger ones in a second launch whose other CTAs return after
-            // counting their leaves
+            // tables of up to kBuildSplitLeaves leaves with the shared memory
+            // they need (41 KB instead of 164 KB per CTA, so kernels of other
+            // calls in flight keep running beside the sequential merges); the
+            // larger ones at the same time in a launch on the side stream whose
+            // other CTAs return after counting their leaves
+            EncParams big = q;
+            big.buildLo = kBuildSplitLeaves + 1;
             q.heapCap = kBuildSplitLeaves;
             q.buildHi = kBuildSplitLeaves;
             const size_t small = sizeof(u64) * (q.heapCap + 2) + 3 * sizeof(u32) * size_t(q.heapCap);
+            CC_TRY_CUDA(cudaEventRecord(I->buildFork, st), "table build fork");
+            CC_TRY_CUDA(cudaStreamWaitEvent(I->buildSide, I->buildFork, 0), "table build fork");
+            k_tableBuild<<<p.T, kBuildThreads, buildSmem, I->buildSide>>>(big);
+            countLaunch();
+            CC_TRY_CUDA(cudaEventRecord(I->buildJoin, I->buildSide), "table build join");
             k_tableBuild<<<p.T, kBuildThreads, small, st>>>(q);
             countLaunch();
-            q.heapCap = p.heapCap;
-            q.buildLo = kBuildSplitLeaves + 1;
-            q.buildHi = ~0u;
+            CC_TRY_CUDA(cudaStreamWaitEvent(st, I->buildJoin, 0), "table build join");
+        } else {
+            k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(q);
+            countLaunch();
         }
-        k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(q);
-        countLaunch();
     }
     // used-block list (after the plan, k_histPlan); the block kernels walk it
     // with a grid of a few CTAs per SM

@@ -255,6 +255,12 @@ int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 el
         cc_destroy_instance(I);
         return cudaFail(e, "cudaHostAlloc(words)");
     }
+    if ((e = cudaStreamCreateWithFlags(&I->buildSide, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&I->buildFork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&I->buildJoin, cudaEventDisableTiming)) != cudaSuccess) {
+        cc_destroy_instance(I);
+        return cudaFail(e, "table build stream");
+    }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) { cc_destroy_instance(I); return cudaFail(e, "instance init"); }
     *out = I;
     return CC_OK;
@@ -276,6 +282,9 @@ void cc_destroy_instance(cc_instance* I) {
     }
     if (I->hostDown) cudaFreeHost(I->hostDown);
     if (I->hostWords) cudaFreeHost(I->hostWords);
+    if (I->buildFork) cudaEventDestroy(I->buildFork);
+    if (I->buildJoin) cudaEventDestroy(I->buildJoin);
+    if (I->buildSide) cudaStreamDestroy(I->buildSide);
     I->resolveTimings();
     for (cudaEvent_t e : I->freeEvents) cudaEventDestroy(e);
     if (I->arena) cudaFree(I->arena);
