@@ -715,6 +715,15 @@ __device__ __forceinline__ float bandSample(const BColDesc& D, int x, int y, int
     return (float(q) + signI(q) * 0.5f) * D.step;   // Quantize.cuh:104-110
 }
 
+// (float(q) + sign(q) * 0.5f) * step for q = unsymbolize(s), the dequantizer
+// of Quantize.cuh:104-110, without the sign selects: float(q) +- 1/2 is
+// exactly float(m) / 2 with m = 0, s + 1 or -(s + 2) for s zero, even or
+// odd (|m| < 2^24), so the one rounding, the product with step, is the same.
+__device__ __forceinline__ float dequantSym(u32 s, float step) {
+    const int m = s == 0u ? 0 : ((s & 1u) ? -int(s + 2u) : int(s + 1u));
+    return (float(m) * 0.5f) * step;
+}
+
 // The samples (x, x + 1), x even, of that pass.  With an even half width hx
 // both lie in one band at an even offset: one 4-byte symbol pair, or one
 // float2 of the lowpass (all pitches even, bases 16-byte aligned).
@@ -878,24 +887,25 @@ __global__ void __launch_bounds__(256, 4) k_bCols(const BColDesc* __restrict__ d
         const u16* const band = D.bands + u64(b ? b - 1 : 0) * D.bandStride + u64(ly) * D.hx + lx;
         const float* const lpBase = D.src + size_t(ly) * D.lpRow + lx;
         uint2 raw[kLoads];
+        auto loadRows = [&](auto position) {
+#pragma unroll
+            for (int i = 0; i < kLoads; ++i) {
+                const int j = a0 - 4 + ty + 8 * i;
+                raw[i] = make_uint2(0u, 0u);
+                if (x < nx && j < na + 4) {
+                    const int lz = position(j) >> 1;
+                    if (b == 0) raw[i] = *reinterpret_cast<const uint2*>(lpBase + size_t(lz) * D.lpSlice);
+                    else raw[i].x = *reinterpret_cast<const u32*>(band + u64(lz) * slice);
+                }
+            }
+        };
+        // tiles whose rows a0 - 4 .. a0 + kBColTileA + 3 all lie inside need no mirroring
+        if (a0 >= 4 && a0 + kBColTileA + 4 <= na) loadRows([](int j) { return j; });
+        else loadRows([na](int j) { return mirrorIdx(j, na); });
 #pragma unroll
         for (int i = 0; i < kLoads; ++i) {
-            const int j = a0 - 4 + ty + 8 * i;
-            raw[i] = make_uint2(0u, 0u);
-            if (x < nx && j < na + 4) {
-                const int lz = mirrorIdx(j, na) >> 1;
-                if (b == 0) raw[i] = *reinterpret_cast<const uint2*>(lpBase + size_t(lz) * D.lpSlice);
-                else raw[i].x = *reinterpret_cast<const u32*>(band + u64(lz) * slice);
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < kLoads; ++i) {
-            if (b == 0) {
-                vals[i] = make_float2(__uint_as_float(raw[i].x), __uint_as_float(raw[i].y));
-            } else {
-                const int q0 = unsymbolizeI(raw[i].x & 0xFFFFu), q1 = unsymbolizeI(raw[i].x >> 16);
-                vals[i] = make_float2((float(q0) + signI(q0) * 0.5f) * D.step, (float(q1) + signI(q1) * 0.5f) * D.step);
-            }
+            if (b == 0) vals[i] = make_float2(__uint_as_float(raw[i].x), __uint_as_float(raw[i].y));
+            else vals[i] = make_float2(dequantSym(raw[i].x & 0xFFFFu, D.step), dequantSym(raw[i].x >> 16, D.step));
         }
     } else {
 #pragma unroll
