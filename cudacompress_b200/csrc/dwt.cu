@@ -908,21 +908,25 @@ __global__ void __launch_bounds__(256, 4) k_bCols(const BColDesc* __restrict__ d
             else vals[i] = make_float2(dequantSym(raw[i].x & 0xFFFFu, D.step), dequantSym(raw[i].x >> 16, D.step));
         }
     } else {
+        auto loadRows = [&](auto position) {
 #pragma unroll
-        for (int i = 0; i < kLoads; ++i) {
-            const int j = a0 - 4 + ty + 8 * i;
-            vals[i] = make_float2(0.0f, 0.0f);
-            if (x < nx && j < na + 4) {
-                const int m = mirrorIdx(j, na);
-                const int a = kInverse ? splitPos(m, na) : m;
-                if (kSymbols) {
-                    // axis Z: a = z, c = y
-                    vals[i] = bandPair(D, x, c, a);
-                } else {
-                    vals[i] = *reinterpret_cast<const float2*>(D.src + size_t(x) + size_t(a) * D.sa + size_t(c) * D.sc);
+            for (int i = 0; i < kLoads; ++i) {
+                const int j = a0 - 4 + ty + 8 * i;
+                vals[i] = make_float2(0.0f, 0.0f);
+                if (x < nx && j < na + 4) {
+                    const int m = position(j);
+                    const int a = kInverse ? splitPos(m, na) : m;
+                    if (kSymbols) {
+                        // axis Z: a = z, c = y
+                        vals[i] = bandPair(D, x, c, a);
+                    } else {
+                        vals[i] = *reinterpret_cast<const float2*>(D.src + size_t(x) + size_t(a) * D.sa + size_t(c) * D.sc);
+                    }
                 }
             }
-        }
+        };
+        if (a0 >= 4 && a0 + kBColTileA + 4 <= na) loadRows([](int j) { return j; });
+        else loadRows([na](int j) { return mirrorIdx(j, na); });
     }
 #pragma unroll
     for (int i = 0; i < kLoads; ++i) s[ty + 8 * i][tx] = vals[i];
