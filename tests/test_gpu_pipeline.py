@@ -55,7 +55,36 @@ def test_volume_codec_c0_full_size(oracle):
         assert fields.psnr(vol, rec) > 40
 
 
-@pytest.mark.parametrize("n,levels,streams", [(64, 2, 3), (256, 4, 3), (256, 4, 5), (512, 3, 5)])
+def test_vector_field_256_full_size(oracle):
+    """The bench workload at full size: 3 x 256^3 fields (the bench's seeds),
+    3 levels, q0 = 0.01, one batch replayed as CUDA graphs.  Component 0's
+    stream is word-identical to the oracle's and its reconstruction
+    bit-identical; the other components' streams equal the plain codec's."""
+    n, levels, q0 = 256, 3, 0.01
+    vols = [fields.turbulence_field(n, 1024, 64, seed) for seed in (1002, 1003, 1004)]
+    dev = [torch.from_numpy(v).cuda() for v in vols]
+    outs = [torch.empty_like(d) for d in dev]
+    with cc.Instance(0, 7, (n // 2) ** 3, 128, 14) as inst:
+        with cc.VolumeBatch(inst, [v.shape for v in vols], levels, [q0] * 3, graph=True) as batch:
+            for _ in range(2):   # the second pass replays the captured graphs
+                batch.compress(dev)
+                batch.decompress(outs)
+            torch.cuda.synchronize()
+            batch.status()
+            streams = [batch.read_stream(c) for c in range(3)]
+        ref_words, ref_bits = oracle.compress_volume(vols[0], levels, q0)
+        assert streams[0][1] == ref_bits and np.array_equal(streams[0][0], ref_words)
+        want = oracle.decompress_volume(ref_words, ref_bits, vols[0].shape, levels, q0)
+        assert np.array_equal(outs[0].cpu().numpy().view(np.uint32), want.view(np.uint32))
+        cap = cc.volume_stream_capacity_words(n, n, n)
+        plain = torch.empty(cap, dtype=torch.int32, device="cuda")
+        for c in (1, 2):
+            _, bits = cc.compress_volume_float(inst, dev[c], levels, q0, plain)
+            assert bits == streams[c][1] and np.array_equal(stream_of(plain, bits), streams[c][0])
+            assert fields.psnr(vols[c], outs[c].cpu().numpy()) > 50
+
+
+@pytest.mark.parametrize("n,levels,streams", [(64, 2, 3), (256, 4, 3), (256, 4, 5), (512, 3, 5), (2048, 4, 5)])
 def test_heightfield_codec_matches_oracle_and_is_lossless(oracle, n, levels, streams):
     """3 streams: the decoder walks the stream one level at a time; 5: every
     level's streams in one device-walked decode."""
