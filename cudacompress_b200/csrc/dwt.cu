@@ -854,8 +854,11 @@ __device__ __forceinline__ void colOutputs8Quantize(const BColDesc& D, const flo
 
 // Y or Z pass: 64 x-columns (a column pair per thread, float2 accesses; all
 // level extents are even and x is the unit-stride axis) by kBColTileA axis
-// positions per CTA.  The output parity of a thread is fixed (kBColTileA and
-// the row step 8 are even), so its taps are compile-time immediates.
+// positions per CTA.  The CTA stages the tile's kBColTileA + 8 input rows in
+// shared memory (nine loads in flight per thread; tiles away from both ends
+// skip the mirroring), then every thread computes eight consecutive outputs
+// (colOutputs8).  The descriptor is a register copy, and up to 64 registers
+// per thread (four CTAs per SM) keep the 16-sample window in registers.
 static_assert(kBColTileX == 64, "a column-pass CTA has 32 threads of column pairs per row");
 
 template <bool kInverse, bool kSymbols, bool kQuantize = false>
