@@ -49,6 +49,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import gc
 import json
 import os
 import statistics
@@ -532,9 +533,19 @@ def measure_serving(wl, local, requests=None, rates=None):
     offline = serving.poisson_requests(n, 1e12, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"], wl["seed"] + 2)
     out["offline"] = serving.latency_stats(srv.run(offline))
     for rate in (rates or wl["rates"]):
+        # a short run at the same rate first: fill levels met only at this
+        # rate get their graphs captured outside the measured run
+        srv.run(serving.poisson_requests(max(200, n // 5), rate, wl["edges"], wl["decode_frac"],
+                                         wl["bricks_per_edge"], wl["seed"] + int(rate) + 7))
         reqs = serving.poisson_requests(n, rate, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"],
                                         wl["seed"] + int(rate))
-        st = serving.latency_stats(srv.run(reqs))
+        gc.collect()
+        gc.disable()   # no collector pause inside the measured run
+        try:
+            done = srv.run(reqs)
+        finally:
+            gc.enable()
+        st = serving.latency_stats(done)
         dec = [r for r in reqs if r.op == serving.DECODE and r.edge == min(wl["edges"])]
         if dec:
             lat = np.array([r.done - r.arrival for r in dec]) * 1e3
