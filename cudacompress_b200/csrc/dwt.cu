@@ -553,7 +553,7 @@ __device__ __forceinline__ void rowPairs4(const float* w, float4& a, float4& b) 
 // interleaves them on the way into shared memory - and float4 stores of four
 // pairs per thread.  Otherwise scalar loads and stores.
 template <bool kInverse>
-__global__ void __launch_bounds__(256) k_bRows(const BRowDesc* __restrict__ descs, const u32* __restrict__ map,
+__global__ void __launch_bounds__(256, 6) k_bRows(const BRowDesc* __restrict__ descs, const u32* __restrict__ map,
                                                const float* const* inTab, float* const* outTab) {
     __shared__ __align__(16) float s[kBRowSmem];
     const BRowDesc D = descs[map[blockIdx.x]];
