@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(256) k_zeroHist(EncParams p) {
 // plain histogram of a Huff stream.  Bins below kSmemSymBins are counted in
 // shared memory with warp-aggregated increments.
 template <class Sym>
-__global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
+__global__ void __launch_bounds__(kRleThreads, 6) k_write(EncParams p) {
     __shared__ RunSum smem[9];
     __shared__ u32 hSym[kSmemSymBins];
     __shared__ u32 hZc[256];
