@@ -862,7 +862,7 @@ __device__ __forceinline__ void colOutputs8Quantize(const BColDesc& D, const flo
 static_assert(kBColTileX == 64, "a column-pass CTA has 32 threads of column pairs per row");
 
 template <bool kInverse, bool kSymbols, bool kQuantize = false>
-__global__ void __launch_bounds__(256, kSymbols ? 4 : (kQuantize ? 4 : 6)) k_bCols(const BColDesc* __restrict__ descs, const u32* __restrict__ map) {
+__global__ void __launch_bounds__(256, kSymbols ? 5 : (kQuantize ? 4 : 6)) k_bCols(const BColDesc* __restrict__ descs, const u32* __restrict__ map) {
     __shared__ float2 s[kBColTileA + 8][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const BColDesc D = descs[map[blockIdx.x]];   // a copy: the output stores cannot alias it
