@@ -857,8 +857,10 @@ __device__ __forceinline__ void colOutputs8Quantize(const BColDesc& D, const flo
 // positions per CTA.  The CTA stages the tile's kBColTileA + 8 input rows in
 // shared memory (nine loads in flight per thread; tiles away from both ends
 // skip the mirroring), then every thread computes eight consecutive outputs
-// (colOutputs8).  The descriptor is a register copy, and up to 64 registers
-// per thread (four CTAs per SM) keep the 16-sample window in registers.
+// (colOutputs8).  The descriptor is a register copy; the register bounds
+// (six CTAs per SM for the plain passes, five with the dequantizer, four with
+// the quantizer) are the tightest that keep the 16-sample window in
+// registers without spills.
 static_assert(kBColTileX == 64, "a column-pass CTA has 32 threads of column pairs per row");
 
 template <bool kInverse, bool kSymbols, bool kQuantize = false>
