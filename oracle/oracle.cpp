@@ -723,6 +723,15 @@ void orc_dwt_double_inv(const double* src, double* dst, long nx, long ny, long n
 void orc_dwt_int_fwd(const i16* src, i16* dst, long nx, long ny, long nz) { dwtInt(src, dst, nx, ny, nz, false); }
 void orc_dwt_int_inv(const i16* src, i16* dst, long nx, long ny, long nz) { dwtInt(src, dst, nx, ny, nz, true); }
 
+// getMaxAbs (util/Quantize.cu:355-361): reduceArray with OperatorMax over
+// FunctorAbs (reduce/reduce_app.cui:122-142, tools/Operator.h:31-52,
+// tools/Functor.h:25-29), whose identity is -FLT_MAX.
+float orc_max_abs(const float* src, long n) {
+    float m = -3.40282347e38f;
+    for (long i = 0; i < n; ++i) m = std::max(m, std::fabs(src[i]));
+    return m;
+}
+
 // Quantize.cu:78-100 on a dense (nx,ny,nz) block with the reference's pitches.
 void orc_quantize_to_symbols16(u16* out, const float* src, long nx, long ny, long nz, float step, long rowPitch, long slicePitch) {
     float inv = 1.0f / step;

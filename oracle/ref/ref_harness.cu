@@ -202,6 +202,68 @@ void ref_ycocg(uint8_t* dst, const uint8_t* src, int n, int channels, int toYCoC
     }
     cudaDeviceSynchronize();
 }
+// The lossless 2D heightfield codec of the scope, composed from the
+// reference library's own calls: per level util::dwtIntForward (2D, sizeZ 1),
+// the three detail bands symbolized in x + 2y order (util::symbolize with the
+// level's pitch, CompressHeightfield.cpp:119-126) and coded with one
+// encodeRLHuff; the last lowpass band symbolized and coded with encodeHuff.
+// Stream order as compressVolumeLossless (CompressVolume.cpp:234-272): the
+// lowpass segment first, then the levels coarse to fine, each appended at a
+// word boundary.  dImg is the device image (nx * ny shorts, dense).
+int ref_heightfield_compress(const short* dImg, uint32_t nx, uint32_t ny, uint32_t levels, uint32_t* words,
+                             uint32_t cap, uint32_t* nWords) {
+    Instance* inst = createInstance(0, 3, (nx / 2) * (ny / 2), 128, 14);
+    if (!inst) return -1;
+    const size_t n = size_t(nx) * ny;
+    short *cur = nullptr, *coef = nullptr, *buf = nullptr;
+    Symbol16* sym = nullptr;
+    const size_t bandCap = n / 4 + 64;          // encode pads each stream by up to 8 symbols
+    cudaMalloc(&cur, n * sizeof(short));
+    cudaMalloc(&coef, n * sizeof(short));
+    cudaMalloc(&buf, n * sizeof(short));
+    cudaMalloc(&sym, 3 * bandCap * sizeof(Symbol16));
+    cudaMemcpy(cur, dImg, n * sizeof(short), cudaMemcpyDeviceToDevice);
+    std::vector<std::vector<uint>> levelBits(levels);
+    bool ok = true;
+    uint32_t sx = nx, sy = ny;
+    for (uint32_t l = 0; l < levels && ok; ++l) {
+        util::dwtIntForward(coef, buf, cur, int(sx), int(sy), 1);
+        const uint32_t hx = sx / 2, hy = sy / 2;
+        std::vector<Symbol16*> s(3);
+        for (uint32_t b = 1; b < 4; ++b) {
+            s[b - 1] = sym + (b - 1) * bandCap;
+            const short* src = coef + (b % 2) * hx + (b / 2) * size_t(hy) * sx;
+            util::symbolize(s[b - 1], src, hx, hy, 1, sx, sx * sy);
+        }
+        BitStream bs(&levelBits[l]);
+        ok = encodeRLHuff(inst, bs, s.data(), 3, hx * hy);
+        cudaMemcpy2D(cur, hx * sizeof(short), coef, sx * sizeof(short), hx * sizeof(short), hy,
+                     cudaMemcpyDeviceToDevice);
+        sx = hx;
+        sy = hy;
+    }
+    std::vector<uint> bits;
+    if (ok) {
+        util::symbolize(sym, cur, sx, sy, 1, sx, sx * sy);
+        BitStream bs(&bits);
+        ok = encodeHuff(inst, bs, &sym, 1, sx * sy);
+    }
+    cudaDeviceSynchronize();
+    if (ok) {
+        for (int l = int(levels) - 1; l >= 0; --l) bits.insert(bits.end(), levelBits[l].begin(), levelBits[l].end());
+    }
+    cudaFree(cur);
+    cudaFree(coef);
+    cudaFree(buf);
+    cudaFree(sym);
+    destroyInstance(inst);
+    if (!ok) return -2;
+    if (bits.size() > cap) return -3;
+    std::memcpy(words, bits.data(), bits.size() * 4);
+    *nWords = uint32_t(bits.size());
+    return 0;
+}
+
 // mode 0 getLSB, 1 removeLSB (bits may be null), 2 appendLSB, 3 shiftElems
 void ref_lsb(int mode, short* data, uint32_t* bits, uint32_t n, short shift) {
     if (mode == 0) util::getLSB(data, bits, n);

@@ -22,8 +22,8 @@ struct Session {
         // leaves out; small volumes need the slack
         cfg.bufferSize += size_t(64) << 20;
         // runLengthDecode (RunLength.cu:261) asks for per-stream capacity of
-        // the padded stride, 32 coding blocks of 128 symbols
-        if (cfg.elemCountPerBlockMax < 32u * 128u) cfg.elemCountPerBlockMax = 32u * 128u;
+        // the stride padded to whole groups of 32 coding blocks of 128 symbols
+        cfg.elemCountPerBlockMax = (cfg.elemCountPerBlockMax + 32u * 128u - 1) / (32u * 128u) * (32u * 128u);
         ok = shared.create(cfg) && res.create(shared.getConfig());
     }
     ~Session() {

@@ -18,6 +18,13 @@ ref_volume.npz   the reference's example volume codec (examples/CompressVolume.c
                  decoders' outputs (python tests/golden/make_golden.py --gpu --only volume).
                  Inputs are seeded fields (cudacompress_b200.fields), stored as seed +
                  SHA-256 of the generated array.
+ref_digests.json SHA-256 digests and word counts of the reference's streams (and
+                 reconstructions) at the scope's full sizes: the 128^3 volume, the
+                 3 x 256^3 vector field at q0 in {0.002, 0.01, 0.05}, a sample of the
+                 uneven bricks and the 2048^2 lossless heightfield
+                 (python tests/golden/make_golden.py --gpu --only digests).  The
+                 streams themselves are megabytes, so only their digests are kept;
+                 inputs are regenerated from the recorded generator parameters.
 ref_image.npz    the 2D image side: util byte-DWT, lowpass-only, byte-image quantizer,
                  YCoCg and Bits outputs, and the examples' one-level image and
                  heightfield codecs (CompressImage.cpp, CompressHeightfield.cpp):
@@ -286,6 +293,64 @@ def make_volume(ref, out_dir):
     print("ref_volume.npz written")
 
 
+def make_digests(ref, out_dir):
+    """Digests of the reference's streams and reconstructions at the full
+    sizes of the scope (cases in digest_cases.py)."""
+    import json
+    import torch
+    import digest_cases as dc
+    u32p = c.POINTER(c.c_uint32)
+    ref.ref_volume_compress.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float,
+                                        c.c_int, c.c_int, u32p, c.c_uint32, u32p]
+    ref.ref_volume_decompress.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float,
+                                          c.c_int, c.c_int, u32p, c.c_uint32]
+    ref.ref_heightfield_compress.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32, c.c_uint32, u32p, c.c_uint32, u32p]
+    P = lambda t: c.c_void_p(t.data_ptr())  # noqa: E731
+
+    def volume(v, levels, q):
+        nz, ny, nx = v.shape
+        cap = v.size * 2 + 65536
+        words = np.zeros(cap, np.uint32)
+        nw = c.c_uint32()
+        d = torch.from_numpy(v).cuda()
+        r = ref.ref_volume_compress(P(d), nx, ny, nz, levels, q, 0, 0, words.ctypes.data_as(u32p), cap, c.byref(nw))
+        assert r == 0, r
+        w = words[: nw.value].copy()
+        rec = torch.full(v.shape, float("nan"), dtype=torch.float32, device="cuda")
+        r = ref.ref_volume_decompress(P(rec), nx, ny, nz, levels, q, 0, 0, w.ctypes.data_as(u32p), len(w))
+        assert r == 0, r
+        return w, rec.cpu().numpy()
+
+    out = {"volumes": [], "bricks": None, "heightfield": None}
+    for case in dc.volume_cases():
+        v = dc.volume_input(case)
+        w, rec = volume(v, case["levels"], case["q0"])
+        out["volumes"].append(dict(case, input_sha256=dc.sha256(v), words=int(len(w)), stream_sha256=dc.sha256(w),
+                                   recon_sha256=dc.sha256(rec)))
+        print(case["name"], len(w), "words")
+    bricks, qs = dc.brick_inputs()
+    items = []
+    for i, (b, q) in enumerate(zip(bricks, qs)):
+        w, rec = volume(b, dc.BRICK_LEVELS, q)
+        items.append(dict(index=i, shape=list(b.shape), q0=q, input_sha256=dc.sha256(b), words=int(len(w)),
+                          stream_sha256=dc.sha256(w), recon_sha256=dc.sha256(rec)))
+    out["bricks"] = dict(count=dc.BRICK_COUNT, seed=dc.BRICK_SEED, levels=dc.BRICK_LEVELS, items=items)
+    img = dc.heightfield_input()
+    n = dc.HEIGHTFIELD["n"]
+    cap = img.size + 65536
+    words = np.zeros(cap, np.uint32)
+    nw = c.c_uint32()
+    r = ref.ref_heightfield_compress(P(torch.from_numpy(img).cuda()), n, n, dc.HEIGHTFIELD["levels"],
+                                     words.ctypes.data_as(u32p), cap, c.byref(nw))
+    assert r == 0, r
+    w = words[: nw.value]
+    out["heightfield"] = dict(dc.HEIGHTFIELD, input_sha256=dc.sha256(img), words=int(len(w)),
+                              stream_sha256=dc.sha256(w))
+    with open(os.path.join(out_dir, "ref_digests.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("ref_digests.json written")
+
+
 def test_image(shape, seed):
     """Seeded smooth 8-bit test image (y, x, channels): two plane waves per
     channel plus uniform noise, clipped to [0, 255]."""
@@ -505,7 +570,7 @@ def make_image(ref, out_dir):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpu", action="store_true", help="also run the reference's GPU code")
-    ap.add_argument("--only", choices=["volume", "image"], help="only the whole-volume or image fixtures (GPU)")
+    ap.add_argument("--only", choices=["volume", "image", "digests"], help="only the whole-volume or image fixtures (GPU)")
     ap.add_argument("--out", default=HERE, help="output directory")
     args = ap.parse_args()
     ref = load_ref_gpu_lib()
@@ -517,12 +582,16 @@ def main():
     if args.only == "image":
         make_image(ref, args.out)
         return
+    if args.only == "digests":
+        make_digests(ref, args.out)
+        return
     make_tables(ref)
     if args.gpu:
         make_streams(ref)
         make_dwt(ref)
         make_volume(ref, args.out)
         make_image(ref, args.out)
+        make_digests(ref, args.out)
 
 
 if __name__ == "__main__":

@@ -105,6 +105,8 @@ class Oracle:
         L.orc_dwt_int_inv.argtypes = [I16P, I16P, c.c_long, c.c_long, c.c_long]
         L.orc_quantize_to_symbols16.argtypes = [U16P, F32P, c.c_long, c.c_long, c.c_long, c.c_float, c.c_long, c.c_long]
         L.orc_unquantize_from_symbols16.argtypes = [F32P, U16P, c.c_long, c.c_long, c.c_long, c.c_float, c.c_long, c.c_long]
+        L.orc_max_abs.argtypes = [F32P, c.c_long]
+        L.orc_max_abs.restype = c.c_float
         L.orc_rle_encode16.argtypes = [U16P, c.c_uint32, U16P, U16P]
         L.orc_rle_encode16.restype = c.c_uint32
         L.orc_encode.argtypes = [c.c_int, c.c_int, c.c_void_p, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, U32P,
@@ -152,6 +154,10 @@ class Oracle:
         nz, ny, nx = a.shape if a.ndim == 3 else (1,) + a.shape
         (self.lib.orc_dwt_int_inv if inverse else self.lib.orc_dwt_int_fwd)(a, out, nx, ny, nz)
         return out
+
+    def max_abs(self, a):
+        a = np.ascontiguousarray(a, np.float32).ravel()
+        return np.float32(self.lib.orc_max_abs(a, a.size))
 
     def quantize(self, a, step):
         a = np.ascontiguousarray(a, np.float32)

@@ -60,6 +60,24 @@ def test_quantize_matches_oracle(oracle, step):
     assert bits_equal(host(back), oracle.unquantize(got, step))
 
 
+@pytest.mark.parametrize("n", [1, 7, 1000, 1 << 20, (1 << 24) + 3])
+def test_get_max_abs_matches_oracle(oracle, inst, n):
+    """getMaxAbs (util/Quantize.cu:355-361): the largest magnitude, exact."""
+    rng = np.random.default_rng(n)
+    a = (rng.standard_normal(n) * 3).astype(np.float32)
+    if n > 8:
+        a[:4] = [np.float32(1e-40), -0.0, 0.0, -np.float32(1e-39)]
+        a[n // 3] = -50.0          # the largest magnitude is negative
+        a[n - 1] = 49.5
+    out = torch.full((1,), -1.0, dtype=torch.float32, device="cuda")
+    cc.get_max_abs(inst, dev(a), n, out)
+    assert bits_equal(host(out), np.array([oracle.max_abs(a)], np.float32))
+    # a second call on other data overwrites the result
+    b = np.full(n, -0.25, np.float32)
+    cc.get_max_abs(inst, dev(b), n, out)
+    assert host(out)[0] == np.float32(0.25)
+
+
 def test_symbolize_roundtrip():
     rng = np.random.default_rng(4)
     a = rng.integers(-3000, 3000, (4, 16, 32)).astype(np.int16)
