@@ -20,18 +20,24 @@ to the plain single-volume codec's, replayed as CUDA graphs).
           streams, D2H of the reconstructions, every step, inside the timed
           region; steps are software-pipelined (copy engines overlap the
           codec; consecutive steps alternate between two batches)
-  batched_vs_per_brick  1024 uneven bricks (edges {16..64} per axis, q0
-          log-uniform [0.002, 0.05]) in one batch vs one plain call per brick
+  q0_sweep  the vector field at q0 in {0.002, 0.01, 0.05} std: per q0 the
+          compression ratio, PSNR per component, encode / decode GB/s raw of
+          one step at a time, and the FP32-vs-FP64 error of component 0
+          (coefficients against the FP64 transform with the same taps,
+          reconstruction against the FP64 inverse of the same symbols)
+  batched_vs_per_brick  the 4096 uneven bricks (edges {16..64} per axis, q0
+          log-uniform [0.002, 0.05]) in one batch vs one plain call per brick,
+          coding block chosen by the autotuner
   serving the continuous-batching brick service at 10k req/s (Poisson, 90%
           decode, edges {32, 64, 128}): p50 / p99 latency, bricks/s
-  roofline  the dominant bandwidth-bound kernel section (CUDA-event timed
-          inside the library; the batched transform's passes, each counted
-          with its own input read once and output written once) against the
-          measured HBM copy bandwidth; its `traffic` is the section's DRAM
-          bytes from an ncu capture (profiles/traffic.json)
-  pipeline_roofline  the whole codec with algorithmic bytes = raw +
-          compressed (intermediate passes not counted), step, encode and
-          decode fractions of the same peak
+  roofline  the whole codec step against the measured HBM copy bandwidth:
+          algorithmic bytes = raw + compressed bytes each way (intermediate
+          passes do not count) over the in-flight step time; `traffic` is the
+          step's DRAM bytes from ncu (profiles/traffic.json); beside it the
+          step's dominant kernel section and every bandwidth section (CUDA
+          events inside the library) with its own algorithmic bytes
+  pipeline_roofline  the same fraction, plus encode and decode of one step
+          at a time
   cpu_baseline  the reference's own CPU coder (src/CPU RunLengthCPU /
           HuffmanTableCPU / HuffmanCPU, built from the reference sources into
           oracle/_ref) plus the oracle's CPU DWT/quantize port (the reference
@@ -72,7 +78,8 @@ WORKLOADS = {
 WORKLOADS["bricks-4096"] = dict(count=4096, levels=2, seed=1005, plain_sample=256,
                                 desc="4096 float32 bricks, edges {16,24,32,48,64} per axis, q0 log-uniform "
                                      "[0.002,0.05]*std, 2-level CDF 9/7, RLE+Huffman cb=128, per-brick tables")
-WORKLOADS["serving"] = dict(rates=(1000.0, 10000.0, 50000.0), requests=3000, edges=(32, 64, 128), decode_frac=0.9,
+WORKLOADS["serving"] = dict(rates=(1000.0, 10000.0, 50000.0), requests=100000, max_seconds=20.0,
+                           edges=(32, 64, 128), decode_frac=0.9,
                            q0=0.01, levels=3, slots={32: 64, 64: 16, 128: 4}, bricks_per_edge=16, seed=1006,
                            desc="open-loop Poisson brick requests, 90% decode / 10% encode, cubic edge {32,64,128}, "
                                 "q0=0.01*std, 3-level CDF 9/7, 4 GB HBM admission budget")
@@ -80,6 +87,14 @@ WORKLOADS["heightfield-2048"] = dict(n=2048, levels=4, seed=1001,
                                      desc="2048^2 int16 fBm terrain (10 octaves, H=0.8, [-2000, 8000]), 4-level "
                                           "CDF 5/3 integer DWT, lossless, RLE+Huffman cb=128")
 FALLBACK_HBM_GBS = 6650.0
+Q0_SWEEP = (0.002, 0.01, 0.05)
+# sections that time a group of other sections (not one kernel)
+COMPOSITE_SECTIONS = ("batch.lowpass_encode",)
+SECTION_NOTES = {
+    "lp.enc.table_build": "k_tableBuild: latency-bound, one CTA per Huffman table replaying libstdc++'s heap and "
+                          "introsort exactly (sequential merge of ~1670 leaves per lowpass table)",
+    "enc.table_build": "k_tableBuild: latency-bound (sequential libstdc++-order heap merge per table)",
+}
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -210,6 +225,7 @@ def cpu_reference_volume(vol, L, q0, threads):
     if not _ORACLE:
         _ORACLE.append(Oracle())
     orc = _ORACLE[0]
+    orc.lib.orc_set_threads(threads)
     vol = np.ascontiguousarray(vol, np.float32)
     nz, ny, nx = vol.shape
     total = vol.size
@@ -366,24 +382,29 @@ def run_reference(args, wl):
         line["dtype"] = "int16"
         print(json.dumps(line), flush=True)
         return
-    vol = make_fields(wl)[0]
+    vols = make_fields(wl)
+    # every step codes every component of the workload (encode + decode); the
+    # warm-up steps code component 0 only
     for _ in range(args.warmup):
-        cpu_reference_step(vol, wl, threads)
+        cpu_reference_step(vols[0], wl, threads)
     times = []
     kind = "port"
     for _ in range(args.steps):
-        e, d, kind = cpu_reference_step(vol, wl, threads)
-        times.append(e + d)
-    raw = wl["n"] ** 3 * 4
+        t = 0.0
+        for v in vols:
+            e, d, kind = cpu_reference_step(v, wl, threads)
+            t += e + d
+        times.append(t)
+    raw = wl["n"] ** 3 * 4 * len(vols)
     step = sum(times) / len(times)
     value = raw / step / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": wl["desc"], "sample": "one component per step"},
+        "config": {"workload": args.workload, "desc": wl["desc"], "sample": "all components per step"},
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
-                         "sample": f"1 of {wl['comps']} components ({wl['n']}^3 f32) encode+decode per step"},
+                         "sample": f"all {wl['comps']} components ({wl['n']}^3 f32) encode+decode per step"},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -419,11 +440,15 @@ def section_bytes(name, wl, coded_bytes, counts):
         "pipe.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
         "pipe.quantize": (hp + lp) * 6 * C,
         "enc.rle_summary": hp * 2 * C,
-        "enc.summary": (hp + lp) * 2 * C,
+        "enc.summary": hp * 2 * C,
         "enc.rle_write_hist": hp * 2 * C + counts.get("compact", 0) * 4,
         "enc.histogram": lp * 2 * C,
-        "enc.block_bits": (lp * C + 2 * counts.get("compact", 0)) * 2,
-        "enc.pack": (lp * C + 2 * counts.get("compact", 0)) * 2 + coded_bytes,
+        "enc.block_bits": 2 * counts.get("compact", 0) * 2,
+        "enc.pack": 2 * counts.get("compact", 0) * 2 + coded_bytes,
+        "lp.enc.summary": lp * 2 * C,
+        "lp.enc.rle_write_hist": lp * 2 * C,
+        "lp.enc.block_bits": lp * 2 * C,
+        "lp.enc.pack": lp * 2 * C + lp * C,
         "dec.huffman": lp * 2 * C,
         "dec.zero_counts": counts.get("compact", 0) * 2,
         "dec.symbols_scatter": counts.get("compact", 0) * 4 + hp * 2 * C,
@@ -527,17 +552,21 @@ def measure_serving(wl, local, requests=None, rates=None):
         sources[e] = bl
     srv = serving.BrickServer(local, sources, wl["slots"], wl["levels"], wl["q0"], budget_bytes=4 << 30)
     n = requests or wl["requests"]
-    out = {"requests_per_rate": n, "store_bytes": srv.store_bytes}
+    out = {"requests_per_rate": {}, "store_bytes": srv.store_bytes, "budget_bytes": srv.budget}
     warm = serving.poisson_requests(200, 1e9, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"], wl["seed"] + 1)
     srv.run(warm)                     # captures the graphs of the common fill levels
-    offline = serving.poisson_requests(n, 1e12, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"], wl["seed"] + 2)
+    offline = serving.poisson_requests(min(n, 20000), 1e12, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"],
+                                       wl["seed"] + 2)
     out["offline"] = serving.latency_stats(srv.run(offline))
     for rate in (rates or wl["rates"]):
+        # at most max_seconds of arrivals per rate (10^5 requests at 10k req/s)
+        nr = min(n, int(rate * wl.get("max_seconds", 20.0)))
+        out["requests_per_rate"][str(int(rate))] = nr
         # a short run at the same rate first: fill levels met only at this
         # rate get their graphs captured outside the measured run
-        srv.run(serving.poisson_requests(max(200, n // 5), rate, wl["edges"], wl["decode_frac"],
+        srv.run(serving.poisson_requests(max(200, nr // 10), rate, wl["edges"], wl["decode_frac"],
                                          wl["bricks_per_edge"], wl["seed"] + int(rate) + 7))
-        reqs = serving.poisson_requests(n, rate, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"],
+        reqs = serving.poisson_requests(nr, rate, wl["edges"], wl["decode_frac"], wl["bricks_per_edge"],
                                         wl["seed"] + int(rate))
         gc.collect()
         gc.disable()   # no collector pause inside the measured run
@@ -877,6 +906,97 @@ def run_heightfield(args, wl):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """A small self-contained case for profilers (ncu): one batch of
+    `--comps` seeded n^3 float32 fields (the vector field's generator and
+    seeds), `--warmup` encode + decode passes, then `--steps` more; no timing,
+    no other legs.  Launch order per step: the forward transform (per level
+    the row pass, the Y pass and the Z pass with the quantizer fused), the
+    encoders, then the decoder and the inverse transform."""
+    import torch
+    import cudacompress_b200 as cc
+    from cudacompress_b200 import fields
+    n, C = args.n, args.comps
+    vols = [torch.from_numpy(fields.turbulence_field(n, 1024, min(64, n // 4), seed)).cuda()
+            for seed in fields.SEED_C2[:C]]
+    outs = [torch.empty_like(v) for v in vols]
+    with cc.Instance(0, 7, (n // 2) ** 3, 128, 14) as inst:
+        with cc.VolumeBatch(inst, [v.shape for v in vols], 3, [args.q0] * C, graph=True) as batch:
+            for _ in range(args.warmup + args.steps):
+                batch.compress(vols)
+                batch.decompress(outs)
+            torch.cuda.synchronize()
+            batch.status()
+    print(json.dumps({"profile_case": {"n": n, "comps": C, "q0": args.q0, "passes": args.warmup + args.steps}}))
+
+
+def compact_count(cc, torch, vol, levels, q0):
+    """Run-length output entries (nonzero symbols plus one (0, 255) entry per
+    whole 256 zeros before them; RunLengthKernels.cui:5-45) of every highpass
+    band of one volume: the compact-symbol count of its encoder.  Symbols
+    from the library's own transform and quantizer."""
+    from cudacompress_b200 import accuracy
+    coef = accuracy.multilevel_fp32(vol, levels)
+    nz, ny, nx = vol.shape
+    total = 0
+    for lvl in range(levels):
+        step = float(np.float32(q0) / np.float32(1 << lvl))
+        hz, hy, hx = nz >> (lvl + 1), ny >> (lvl + 1), nx >> (lvl + 1)
+        sym = torch.empty((hz, hy, hx), dtype=torch.int16, device=vol.device)
+        for b in range(1, 8):
+            x0, y0, z0 = (b & 1) * hx, ((b >> 1) & 1) * hy, (b >> 2) * hz
+            cc.quantize_to_symbols(sym, coef[z0:z0 + hz, y0:y0 + hy, x0:x0 + hx], hx, hy, hz, step, nx, nx * ny)
+            idx = torch.nonzero(sym.reshape(-1)).reshape(-1)
+            if idx.numel():
+                prev = torch.cat([torch.tensor([-1], device=idx.device), idx[:-1]])
+                total += int(idx.numel() + ((idx - prev - 1) // 256).sum())
+    return total
+
+
+def measure_q0_sweep(inst, vols, vols_h, levels, q0s, steps, warmup):
+    """The vector field's quantization sweep: per q0 one batch of all
+    components (CUDA graphs), sequential steps with encode and decode split by
+    events; compression ratio, PSNR per component, GB/s raw, and the FP32 vs
+    FP64 error of component 0 (cudacompress_b200.accuracy: coefficients
+    against the FP64 transform, reconstruction against the FP64 inverse of the
+    same symbols)."""
+    import torch
+    import cudacompress_b200 as cc
+    from cudacompress_b200 import accuracy, fields
+    C = len(vols)
+    raw = sum(v.numel() for v in vols) * 4
+    recon = [torch.empty_like(v) for v in vols]
+    err = accuracy.error_report(inst, vols[0], levels, q0s)
+    out = {"fp64_coefficients_component0": err["coefficients"]}
+    for q0 in q0s:
+        b = cc.VolumeBatch(inst, [v.shape for v in vols], levels, [q0] * C, graph=True)
+        for _ in range(max(warmup, 1)):
+            b.compress(vols)
+            b.decompress(recon)
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        torch.cuda.synchronize()
+        for k in range(steps):
+            evs[k][0].record()
+            b.compress(vols)
+            evs[k][1].record()
+            b.decompress(recon)
+            evs[k][2].record()
+        torch.cuda.synchronize()
+        b.status()
+        enc_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / steps
+        dec_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / steps
+        coded = sum(b.read_stream(c)[1] for c in range(C)) / 8
+        b.close()
+        out[str(q0)] = {
+            "compression_ratio": raw / coded, "bits_per_voxel": 8 * coded / (raw / 4),
+            "psnr_db": [fields.psnr(vols_h[c], recon[c].cpu().numpy()) for c in range(C)],
+            "encode_ms": enc_ms, "decode_ms": dec_ms, "gbs_raw": 2 * raw / ((enc_ms + dec_ms) / 1e3) / 1e9,
+            "encode_gbs": raw / (enc_ms / 1e3) / 1e9, "decode_gbs": raw / (dec_ms / 1e3) / 1e9,
+            "fp64_reconstruction_component0": err["reconstruction"][str(q0)],
+        }
+    return out
+
+
 def run_ours(args, wl):
     import torch
     import cudacompress_b200 as cc
@@ -1050,49 +1170,67 @@ def run_ours(args, wl):
         sections[name.value.decode()] = (t_ms.value, cnt.value)
     lib.cc_set_timing(inst.handle, 0)
     peak, peak_kind = load_peak()
-    total_sec = sum(v[0] for v in sections.values()) or 1.0
-    counts = {"compact": 0}
-    # the dominant bandwidth-bound section (sections with algorithmic bytes);
-    # the overall dominant section is reported beside it
-    top = max(sections.items(), key=lambda kv: kv[1][0]) if sections else ("none", (0.0, 0))
-    bw = [kv for kv in sections.items() if section_bytes(kv[0], wl, coded_bytes, counts)]
-    dom = max(bw, key=lambda kv: kv[1][0]) if bw else top
-    dom_bytes = section_bytes(dom[0], wl, coded_bytes, counts)
-    achieved = (dom_bytes / (dom[1][0] / 1e3) / 1e9) if dom_bytes and dom[1][0] > 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            traffic = json.load(f).get(dom[0])
-    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": traffic, "launches": dom[1][1], "share": dom[1][0] / total_sec,
-                "algorithmic_bytes_per_step": dom_bytes, "per_unit": SECTION_UNITS.get(dom[0]),
-                "dominant_section": {"name": top[0], "ms": top[1][0], "share": top[1][0] / total_sec,
-                                     "note": "enc.table_build is latency-bound (sequential libstdc++-order heap merge)"
-                                     if top[0] == "enc.table_build" else None}}
+    # compact symbols of all highpass streams (algorithmic bytes of the
+    # entropy sections)
+    counts = {"compact": sum(compact_count(cc, torch, vols[c], L, q0) for c in range(C))}
+    kernel_secs = {k: v for k, v in sections.items() if k not in COMPOSITE_SECTIONS}
+    total_sec = sum(v[0] for v in kernel_secs.values()) or 1.0
+    bw = {}
+    for k, (t, cnt) in kernel_secs.items():
+        b = section_bytes(k, wl, coded_bytes, counts)
+        if b and t > 0:
+            bw[k] = {"ms": t, "algorithmic_bytes": b, "gbs": b / (t / 1e3) / 1e9, "frac": b / (t / 1e3) / 1e9 / peak,
+                     "launches": cnt, "share": t / total_sec}
+    top = max(kernel_secs.items(), key=lambda kv: kv[1][0]) if kernel_secs else ("none", (0.0, 0))
+    top_bytes = section_bytes(top[0], wl, coded_bytes, counts) or 0
     # whole codec (algorithmic: raw + compressed bytes; intermediate passes do not count)
     step_alg = 2 * (raw_step + coded_bytes)
     enc_gbs_alg = (raw_step + coded_bytes) / (enc_ms / 1e3) / 1e9
     dec_gbs_alg = (raw_step + coded_bytes) / (dec_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("step_total")
     pipeline = {"achieved": step_alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": step_alg / (ms / 1e3) / 1e9 / peak,
                 "algorithmic_bytes_per_step": step_alg,
                 "encode_frac": enc_gbs_alg / peak, "decode_frac": dec_gbs_alg / peak}
+    # the headline roofline is the whole codec step (every kernel of encode +
+    # decode; algorithmic bytes = raw + compressed each way), with the step's
+    # dominant kernel section and every bandwidth section beside it
+    roofline = {"bound": "hbm", "kernel": "whole codec step (encode + decode, all kernels)",
+                "achieved": pipeline["achieved"], "peak": peak, "unit": "GB/s", "frac": pipeline["frac"],
+                "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes_per_step": step_alg,
+                "per_unit": "raw field bytes in + compressed bytes out (encode), compressed in + raw out (decode)",
+                "dominant_section": {"name": top[0], "ms": top[1][0], "share": top[1][0] / total_sec,
+                                     "algorithmic_bytes": top_bytes,
+                                     "frac": (top_bytes / (top[1][0] / 1e3) / 1e9 / peak) if top[1][0] else None,
+                                     "note": SECTION_NOTES.get(top[0])},
+                "sections": bw}
 
     bricks = None
     if rank == 0 and world == 1 and not args.no_bricks:
-        bricks = measure_bricks(1024, 2, 1005, max(2, args.steps // 2), 2, 128, local)
+        bw3 = WORKLOADS["bricks-4096"]
+        bricks = measure_bricks(bw3["count"], bw3["levels"], bw3["seed"], max(2, args.steps // 2), 2, 128, local,
+                                autotune=True)
+    sweep = None
+    if rank == 0 and world == 1 and not args.no_sweep:
+        sweep = measure_q0_sweep(inst, vols, vols_h, L, Q0_SWEEP, max(3, args.steps // 2), 2)
     serve = None
     if rank == 0 and world == 1 and not args.no_bricks:
-        serve = measure_serving(WORKLOADS["serving"], local, requests=1500, rates=(10000.0,))
+        serve = measure_serving(WORKLOADS["serving"], local, requests=20000, rates=(10000.0,))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         e, d, kind = cpu_reference_step(vols_h[0], wl, threads)
+        e1, d1, _ = cpu_reference_step(vols_h[0], wl, 1)
         cpu = {"value": n ** 3 * 4 / (e + d) / 1e9, "unit": "GB/s", "cores": threads, "kind": kind,
-               "sample": f"1 of {C} components ({n}^3 f32) encode+decode; DWT/quantize stages are the oracle port"}
+               "sample": f"1 of {C} components ({n}^3 f32) encode+decode; DWT/quantize stages are the oracle port",
+               "single_core": {"value": n ** 3 * 4 / (e1 + d1) / 1e9, "unit": "GB/s", "cores": 1,
+                               "encode_s": e1, "decode_s": d1},
+               "all_cores": {"encode_s": e, "decode_s": d, "cores": threads}}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -1106,6 +1244,7 @@ def run_ours(args, wl):
             "decode_gbs": replicas.job_gbs(world, raw_step, dec_ms),
             "compression_ratio": raw_step / max(coded_bytes, 1), "psnr_db": psnr,
             "plain_path_ms_per_step": plain_ms, "streams_identical_to_plain_codec": bool(same_as_plain),
+            "q0_sweep": sweep, "compact_symbols_per_step": counts["compact"],
             "batched_vs_per_brick": bricks, "serving": serve,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
@@ -1131,9 +1270,17 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="vector-field-256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bricks", action="store_true", help="skip the batched-vs-per-brick measurement")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the q0 sweep of the vector field")
+    ap.add_argument("--profile", action="store_true",
+                    help="a small case for profilers only: one batch of --comps n^3 fields, --warmup + --steps passes")
+    ap.add_argument("--n", type=int, default=256, help="--profile: field edge")
+    ap.add_argument("--comps", type=int, default=3, help="--profile: components")
+    ap.add_argument("--q0", type=float, default=0.01, help="--profile: quantization step (times std)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args, wl)
     elif args.workload.startswith("bricks"):
         run_bricks(args, wl)

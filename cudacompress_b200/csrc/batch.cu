@@ -324,7 +324,7 @@ static int batchEnqueueDecompress(cc_volume_batch* b) {
     cudaStream_t st = I->stream;
     const u32 k = b->active;
     u32 nd, ctas;
-    CC_TRY_CUDA(cudaMemsetAsync(b->syms, 0, b->symEnd[k - 1] * sizeof(u16), st), "zero symbols");
+    // no zeroing of the symbols: the decoder writes every element of every band
     DecPlan dp = b->dec;
     dp.S = b->decS[k - 1];
     dp.T = b->decT[k - 1];
@@ -446,7 +446,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     // histogram bins: every table at most 2^log2Max; budget 2^26 bins (the
     // device plan fails a call that needs more)
     histBins = std::min<u64>(u64(2 * S) * user->bins, u64(1) << 26);
-    cudaSetDevice(user->device);
+    DeviceGuard deviceGuard(user->device);
     cc_volume_batch* b = new cc_volume_batch();
     b->user = user;
     b->count = count;
@@ -823,7 +823,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
 
 void cc_volume_batch_destroy(cc_volume_batch* b) {
     if (!b) return;
-    if (b->I) cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I ? b->I->device : -1);
     cudaDeviceSynchronize();
     for (auto& kv : b->gCompress) cudaGraphExecDestroy(kv.second);
     for (auto& kv : b->gDecompress) cudaGraphExecDestroy(kv.second);
@@ -862,7 +862,7 @@ int cc_volume_batch_use_graph(cc_volume_batch* b, int enable) {
 
 int cc_volume_batch_compress(cc_volume_batch* b, const float* const* dVolumes) {
     if (!b || !dVolumes) { setError("cc_volume_batch_compress: null argument"); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I->device);
     b->I->stream = b->hasOwnStream ? b->ownStream : b->user->stream;
     b->I->timing = b->user->timing;
     b->ILP->timing = b->user->timing;
@@ -873,7 +873,7 @@ int cc_volume_batch_compress(cc_volume_batch* b, const float* const* dVolumes) {
 
 int cc_volume_batch_decompress(cc_volume_batch* b, float* const* dVolumes) {
     if (!b || !dVolumes) { setError("cc_volume_batch_decompress: null argument"); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I->device);
     b->I->stream = b->hasOwnStream ? b->ownStream : b->user->stream;
     b->I->timing = b->user->timing;
     int rc = uploadTable(b, reinterpret_cast<const void* const*>(dVolumes), b->outTab);
@@ -894,7 +894,7 @@ int cc_volume_batch_stream(const cc_volume_batch* b, const uint32_t** dWords, co
 int cc_volume_batch_read_stream(cc_volume_batch* b, uint32_t v, uint32_t* dst, uint64_t capacityWords,
                                 uint64_t* bitSize) {
     if (!b || !bitSize || v >= b->count) { setError("cc_volume_batch_read_stream: bad argument"); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I->device);
     u64 ext[2] = {0, 0};
     CC_TRY_CUDA(cudaMemcpyAsync(&ext[0], b->wordOff + v, sizeof(u64), cudaMemcpyDeviceToHost, b->I->stream), "read offset");
     CC_TRY_CUDA(cudaMemcpyAsync(&ext[1], b->bitSize + v, sizeof(u64), cudaMemcpyDeviceToHost, b->I->stream), "read size");
@@ -923,7 +923,7 @@ static int hostDevicePointer(const void* h, void** d, const char* what) {
 int cc_volume_batch_download_streams(cc_volume_batch* b, uint32_t* hWords, uint64_t capacityWords, uint64_t* hExt) {
     const char* what = "cc_volume_batch_download_streams";
     if (!b || !b->active) { setError("%s: bad argument", what); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I->device);
     void *dW = nullptr, *dE = nullptr;
     int rc = hostDevicePointer(hWords, &dW, what);
     if (!rc) rc = hostDevicePointer(hExt, &dE, what);
@@ -942,7 +942,7 @@ int cc_volume_batch_download_streams(cc_volume_batch* b, uint32_t* hWords, uint6
 int cc_volume_batch_upload_streams(cc_volume_batch* b, const uint32_t* hWords, const uint64_t* hExt) {
     const char* what = "cc_volume_batch_upload_streams";
     if (!b || !b->active) { setError("%s: bad argument", what); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I->device);
     void *dW = nullptr, *dE = nullptr;
     int rc = hostDevicePointer(hWords, &dW, what);
     if (!rc) rc = hostDevicePointer(hExt, &dE, what);
@@ -960,7 +960,7 @@ int cc_volume_batch_upload_streams(cc_volume_batch* b, const uint32_t* hWords, c
 
 int cc_volume_batch_load_streams(cc_volume_batch* b, const uint32_t* const* words, const uint64_t* bitSizes) {
     if (!b || !words || !bitSizes) { setError("cc_volume_batch_load_streams: null argument"); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(b->I->device);
+    DeviceGuard deviceGuard(b->I->device);
     cudaStream_t st = b->hasOwnStream ? b->ownStream : b->user->stream;
     b->I->stream = st;
     cudaEventSynchronize(b->extEvent);   // the previous load has read the pinned offsets

@@ -17,6 +17,22 @@ void countLaunch(unsigned n = 1);
 void setError(const char* fmt, ...);
 int cudaFail(cudaError_t e, const char* what);
 
+// Makes `device` current for the scope of an entry point and restores the
+// caller's current device on exit (the reference's calls leave it alone).
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (device >= 0 && device != prev) cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 // Capacities of an instance made for a batch of volumes (instead of the
 // reference's streamCountMax x elemCountPerStreamMax contract).
 struct InstanceCaps {
@@ -104,6 +120,7 @@ struct DecSourceSpec {
 };
 struct DecPlan {
     u32 S = 0, T = 0, B = 0, nRl = 0, nH = 0, rlBlocks = 0, hBlocks = 0;
+    u32 rlMaxN = 0;   // largest output of an RLHuff stream (symbols)
     size_t bytes = 0;
     size_t offStreams = 0, offTables = 0, offSources = 0, offRl = 0, offH = 0;   // within dev
     void* dev = nullptr;

@@ -24,8 +24,11 @@ enum CodecKind : int { KIND_RLHUFF = 0, KIND_HUFF = 1 };
 
 // Tile of the run-length passes: 256 threads x 8 symbols.
 constexpr u32 kRleThreads = 256;
-constexpr u32 kRlePerThread = 8;
+constexpr u32 kRlePerThread = 32;
 constexpr u32 kRleTile = kRleThreads * kRlePerThread;
+// The Huffman block kernels take coding blocks in runs of kRunSymbols symbols
+// of one table (32 per lane of a warp): 1024 / codingBlockSize blocks.
+constexpr u32 kRunSymbols = 1024;
 
 // Leaves of a table whose Huffman build runs in shared memory (20 bytes per
 // leaf: heap key, sort key, two parent links); larger tables use global memory.
@@ -106,7 +109,7 @@ struct TableMeta {
     u32 blocks;       // coding blocks
     u32 histSize;     // histogram bins of this table
     u32 actOff;       // first of its coding blocks in the call's list of used blocks
-    u32 pad;
+    u32 runOff;       // first of its runs (kRunSymbols symbols of coding blocks) in the call's run list
     u64 histOff;      // offset of its histogram and code table
     u64 leafOff;      // offset of its table-builder arrays (by leaf)
     u64 hdrOff;       // offset of its serialized header (words)
@@ -224,6 +227,7 @@ struct cc_instance {
     ccb::u32* blockBits = nullptr;     // [capBlocks]
     ccb::u32* blockOff = nullptr;      // [capBlocks]
     ccb::u32* blockTable = nullptr;    // [capBlocks]: table of each coding block of a call
+    ccb::u32* runTable = nullptr;      // [capBlocks]: table of each run of coding blocks of a call
     ccb::u32* tileStream = nullptr;    // [capTiles]: stream of each run-length tile of a call
     ccb::SegmentLayout* layout = nullptr;  // [capStreams]
     ccb::u32* out = nullptr;           // [outWordsMax]

@@ -27,6 +27,7 @@ namespace ccb {
 struct DecParams {
     u32 S, T, nSrc, nRl, nH;
     u32 rlBlocks, hBlocks;     // coding blocks (upper bounds) of the RLHuff / Huff streams
+    u32 rlMaxN;                // largest output of an RLHuff stream
     u32 cb, log2Max, symBytes, leavesMax;
     u32 stageWords;            // run-length decode: staged code words per warp
     u64 capLeaves;
@@ -513,6 +514,29 @@ __global__ void __launch_bounds__(1024) k_decRlTasks(DecParams p) {
     if (threadIdx.x == 0) reinterpret_cast<u32*>(p.rlTasks + p.rlTaskCap)[0] = min(carry, p.rlTaskCap);
 }
 
+// The RLHuff streams' outputs, zeroed before the symbol pass writes the
+// nonzero symbols (so callers need not zero them): CTA (k, c) zeroes chunk c
+// of kZeroChunk symbols of RLHuff stream k, 16-byte stores.
+constexpr u32 kZeroChunk = 16384;
+
+template <class Sym>
+__global__ void __launch_bounds__(256) k_decZero(DecParams p) {
+    const DecStreamDesc& sd = p.streams[p.rlList[blockIdx.x]];
+    const u64 lo = u64(blockIdx.y) * kZeroChunk;
+    if (lo >= sd.n) return;
+    const u64 hi = min(u64(sd.n), lo + kZeroChunk);
+    Sym* o = reinterpret_cast<Sym*>(sd.out);
+    constexpr u64 kPer = 16 / sizeof(Sym);
+    const u64 mis = (reinterpret_cast<uintptr_t>(o + lo) & 15u) / sizeof(Sym);
+    const u64 head = min(hi - lo, mis ? kPer - mis : 0);
+    if (threadIdx.x < head) o[lo + threadIdx.x] = Sym(0);
+    const u64 a = lo + head;
+    const u64 nv = (hi - a) / kPer;
+    uint4* v = reinterpret_cast<uint4*>(o + a);
+    for (u64 k = threadIdx.x; k < nv; k += 256) v[k] = make_uint4(0u, 0u, 0u, 0u);
+    for (u64 k = a + nv * kPer + threadIdx.x; k < hi; k += 256) o[k] = Sym(0);
+}
+
 // decodeRLHuff (RunLengthKernels.cui:56-66 for the scatter): one lane per
 // coding block, 32 consecutive blocks of one stream per warp (k_decRlTasks).
 // Zero counts (kSymbols false): decode, store, and sum (zc + 1) per block.
@@ -742,6 +766,7 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
             d.blockFirst = u32(rlBlocks);
             rlBlocks += nb;
             rl[dc.nRl++] = s;
+            dc.rlMaxN = std::max<u32>(dc.rlMaxN, ns[s]);
         } else {
             d.blockFirst = u32(hBlocks);
             hBlocks += nb;
@@ -804,6 +829,11 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
                                         sizeof(Sym) == 2 ? kAttrDecSc16 : kAttrDecSc32, I->device, smem),
                     "decRl smem");
         { SectionTimer t(I, "dec.rl_tasks", st); k_decRlTasks<<<1, 1024, 0, st>>>(p); countLaunch(); }
+        {
+            SectionTimer t(I, "dec.zero_fill", st);
+            k_decZero<Sym><<<dim3(p.nRl, u32(ceilDiv(p.rlMaxN, kZeroChunk))), 256, 0, st>>>(p);
+            countLaunch();
+        }
         { SectionTimer t(I, "dec.zero_counts", st); k_decRl<Sym, false><<<g, 128, smem, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.nRl, 1024, 0, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.symbols_scatter", st); k_decRl<Sym, true><<<g, 128, smem, st>>>(p); countLaunch(); }
@@ -837,6 +867,7 @@ static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
     p.nRl = dc.nRl;
     p.nH = dc.nH;
     p.rlBlocks = dc.rlBlocks;
+    p.rlMaxN = dc.rlMaxN;
     p.hBlocks = dc.hBlocks;
     p.cb = I->codingBlockSize;
     p.stageWords = decRlStageWords(I->codingBlockSize, I->symBytes);
@@ -1001,7 +1032,7 @@ int cc_decode(cc_instance* I, int kind, int symbolBytes, const uint32_t* const* 
                  symbolBytes, symbolBytes == 2 ? "<=" : ">");
         return CC_ERR_INVALID_ARGUMENT;
     }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     return decodeDevice(I, kind, words, bitSizes, bitPositions, bsCount, bsIndex, dOut, S, n);
 }
 

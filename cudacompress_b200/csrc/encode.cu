@@ -39,6 +39,7 @@ struct EncParams {
     u32* blockBits;
     u32* blockOff;
     u32* blockTable;  // [used blocks] table of each coding block in use (k_usedBlocks)
+    u32* runTable;    // [runs] table of each run of coding blocks (k_usedBlocks)
     u32* tileStream;  // [totalTiles] stream of each run-length tile (k_lookupMaps)
     SegmentLayout* layout;
     u32* out;
@@ -84,25 +85,74 @@ __device__ __forceinline__ const Sym* tableInput(const EncParams& p, const EncTa
     return reinterpret_cast<const Sym*>(sd.in);
 }
 
-// Loads kRlePerThread symbols starting at `base` (zero beyond n).
+// Run-length tiles: kRleWarps warps x 32 groups x 32 symbols.  Warp w
+// covers symbols [w * 1024, (w + 1) * 1024) of the tile; group k of it is 32
+// consecutive symbols, symbol k * 32 + i held by lane i.  A ballot gives a
+// group's nonzero mask, kept by lane k, so a warp describes its 1024
+// symbols with one mask per lane and the run-length bookkeeping is warp
+// scans over the groups.  Positions are kept +1 so that 0 means "no
+// nonzero".
+constexpr u32 kRleWarps = kRleThreads / 32;
+static_assert(kRleTile == kRleWarps * 1024, "a tile is 32 groups of 32 symbols per warp");
+
 template <class Sym>
-__device__ __forceinline__ void loadSyms(const Sym* in, u32 base, u32 n, u32 (&v)[kRlePerThread]) {
-    const bool vec = ((reinterpret_cast<uintptr_t>(in) & 15u) == 0) && base + kRlePerThread <= n;
-    if (vec) {
-        if (sizeof(Sym) == 2) {
-            uint4 q = *reinterpret_cast<const uint4*>(in + base);
-            u32 w[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i) { v[2 * i] = w[i] & 0xFFFFu; v[2 * i + 1] = w[i] >> 16; }
-        } else {
-            uint4 a = *reinterpret_cast<const uint4*>(in + base);
-            uint4 b = *reinterpret_cast<const uint4*>(in + base + 4);
-            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-        }
-    } else {
-#pragma unroll
-        for (u32 i = 0; i < kRlePerThread; ++i) v[i] = (base + i < n) ? u32(in[base + i]) : 0u;
+struct WarpSyms {
+    u32 x[16];      // this lane's symbol of groups 2j (low half) and 2j + 1 (high half); u16 symbols
+    u32 y[32];      // 32-bit symbols (Sym = u32)
+    __device__ __forceinline__ u32 at(u32 k) const {   // k a compile-time constant after unrolling
+        return sizeof(Sym) == 2 ? (x[k >> 1] >> (16 * (k & 1))) & 0xFFFFu : y[k];
     }
+};
+
+// Group data of lane k of the calling warp (its group k).
+struct GroupRuns {
+    u32 mask, cnt, firstP1, lastP1;
+};
+
+// Loads the warp's 1024 symbols from stream position wbase (zero beyond n)
+// and returns lane k's group k mask data; maxSym receives the warp's largest
+// symbol.
+template <class Sym>
+__device__ __forceinline__ GroupRuns loadGroups(const Sym* in, u32 wbase, u32 n, WarpSyms<Sym>& v, u32& maxSym) {
+    const u32 lane = threadIdx.x & 31u;
+#pragma unroll
+    for (u32 k = 0; k < 32; ++k) {
+        const u32 pos = wbase + 32u * k + lane;
+        const u32 x = pos < n ? u32(in[pos]) : 0u;
+        if (sizeof(Sym) == 2) {
+            if (k & 1) v.x[k >> 1] |= x << 16;
+            else v.x[k >> 1] = x;
+        } else {
+            v.y[k] = x;
+        }
+    }
+    GroupRuns g{0u, 0u, 0u, 0u};
+    u32 m = 0;
+#pragma unroll
+    for (u32 k = 0; k < 32; ++k) {
+        const u32 x = v.at(k);
+        m = max(m, x);
+        const u32 b = __ballot_sync(0xffffffffu, x != 0u);
+        if (lane == k) g.mask = b;
+    }
+    maxSym = __reduce_max_sync(0xffffffffu, m);
+    const u32 gb = wbase + 32u * lane;
+    g.cnt = __popc(g.mask);
+    g.firstP1 = g.mask ? gb + u32(__ffs(g.mask)) : 0u;
+    g.lastP1 = g.mask ? gb + 32u - u32(__clz(g.mask)) : 0u;
+    return g;
+}
+
+// Exclusive max-scan of lastP1 over the warp's lanes (0 for lane 0).
+__device__ __forceinline__ u32 warpExclusiveMax(u32 v) {
+    const u32 lane = threadIdx.x & 31u;
+#pragma unroll
+    for (u32 d = 1; d < 32; d <<= 1) {
+        const u32 t = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v = max(v, t);
+    }
+    const u32 e = __shfl_up_sync(0xffffffffu, v, 1);
+    return lane ? e : 0u;
 }
 
 __device__ __forceinline__ RunSum shflUpRun(RunSum r, int delta) {
@@ -120,46 +170,6 @@ __device__ __forceinline__ RunSum warpInclusiveRun(RunSum r) {
     for (int o = 1; o < 32; o <<= 1) {
         RunSum t = shflUpRun(r, o);
         if (lane >= o) r = runCombine(t, r);
-    }
-    return r;
-}
-
-// Order-preserving block scan of RunSum (kRleThreads threads): exclusive
-// prefix of the calling thread; *total receives the block aggregate.
-__device__ RunSum blockScanRun(RunSum r, RunSum* smem /*[9]*/, RunSum* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    RunSum inc = warpInclusiveRun(r);
-    if (lane == 31) smem[warp] = inc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        RunSum acc{0, 0, 0, 0};
-        for (int w = 0; w < int(kRleThreads / 32); ++w) {
-            RunSum x = smem[w];
-            smem[w] = acc;
-            acc = runCombine(acc, x);
-        }
-        smem[8] = acc;
-    }
-    __syncthreads();
-    RunSum exclLane = shflUpRun(inc, 1);
-    if (lane == 0) exclLane = RunSum{0, 0, 0, 0};
-    RunSum res = runCombine(smem[warp], exclLane);
-    if (total) *total = smem[8];
-    __syncthreads();
-    return res;
-}
-
-__device__ __forceinline__ RunSum threadRun(const u32 (&v)[kRlePerThread], u32 base, u32 n) {
-    RunSum r{0, 0, 0, 0};
-#pragma unroll
-    for (u32 i = 0; i < kRlePerThread; ++i) {
-        if (base + i < n && v[i] != 0) {
-            u32 q = base + i + 1;
-            if (r.cnt == 0) r.firstP1 = q;
-            else r.ext += (q - r.lastP1 - 1) / 256u;
-            r.lastP1 = q;
-            r.cnt++;
-        }
     }
     return r;
 }
@@ -182,37 +192,53 @@ __global__ void __launch_bounds__(256) k_usedBlocks(EncParams p) {
     const u32 t = blockIdx.x;
     const TableMeta& m = p.meta[t];
     for (u32 k = threadIdx.x; k < m.blocks; k += 256) p.blockTable[m.actOff + k] = t;
+    const u32 runs = u32(ceilDiv(m.blocks, kRunSymbols / p.cb));
+    for (u32 k = threadIdx.x; k < runs; k += 256) p.runTable[m.runOff + k] = t;
 }
 
 // ---------------------------------------------------------------------------
 // Run-length encode (RunLength.cu:82-188 semantics: each nonzero symbol with
 // the count of zeros before it; runs of 256+ zeros emit (0, 255) entries;
 // trailing zeros dropped).
-// Pass 1: per tile, the run summary (RLHuff) and the largest symbol.
+// Pass 1: per tile, the run summary (RLHuff) and the largest symbol, from
+// the warps' group masks.
 // ---------------------------------------------------------------------------
 template <class Sym>
 __global__ void __launch_bounds__(kRleThreads) k_summary(EncParams p) {
-    __shared__ RunSum smem[9];
+    __shared__ RunSum sRun[kRleWarps];
     __shared__ u32 sStream, sMaxSym;
     const u32 tile = blockIdx.x;
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) { sStream = streamOfTile(p, tile); sMaxSym = 0; }
     __syncthreads();
     const u32 s = sStream;
     const EncStreamDev sd = p.streams[s];
     const u32 n = sd.n;
     const Sym* in = reinterpret_cast<const Sym*>(sd.in);
-    const u32 base = (tile - sd.tileOff) * kRleTile + threadIdx.x * kRlePerThread;
-    u32 v[kRlePerThread];
-    loadSyms(in, base, n, v);
-    u32 m = 0;
-#pragma unroll
-    for (u32 i = 0; i < kRlePerThread; ++i) m = max(m, v[i]);
-    m = warpMax(m);
-    if ((threadIdx.x & 31) == 0 && m) atomicMax(&sMaxSym, m);
+    const u32 wbase = (tile - sd.tileOff) * kRleTile + warp * 1024u;
+    WarpSyms<Sym> v;
+    u32 m;
+    const GroupRuns g = loadGroups(in, wbase, n, v, m);
+    if (lane == 0 && m) atomicMax(&sMaxSym, m);
     if (sd.kind == KIND_RLHUFF) {
-        RunSum total;
-        blockScanRun(threadRun(v, base, n), smem, &total);   // synchronizes the block
-        if (threadIdx.x == 0) p.tiles[tile] = total;
+        // the warp's summary: (0, 255) entries of the gaps whose previous
+        // nonzero lies in the warp
+        const u32 prevW = warpExclusiveMax(g.lastP1);
+        const u32 e = (g.mask && prevW) ? (g.firstP1 - prevW - 1u) / 256u : 0u;
+        RunSum w;
+        w.cnt = __reduce_add_sync(0xffffffffu, g.cnt);
+        w.ext = __reduce_add_sync(0xffffffffu, e);
+        w.firstP1 = __reduce_min_sync(0xffffffffu, g.mask ? g.firstP1 : 0xFFFFFFFFu);
+        w.lastP1 = __reduce_max_sync(0xffffffffu, g.lastP1);
+        if (!w.cnt) w.firstP1 = 0;
+        if (lane == 0) sRun[warp] = w;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            RunSum acc{0, 0, 0, 0};
+#pragma unroll
+            for (u32 k = 0; k < kRleWarps; ++k) acc = runCombine(acc, sRun[k]);
+            p.tiles[tile] = acc;
+        }
     } else {
         __syncthreads();
     }
@@ -272,8 +298,8 @@ __global__ void __launch_bounds__(1024) k_scan(EncParams p) {
 // instance's 2^log2Max range fails the call (HuffmanTable.cu:411-419).
 __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
     __shared__ u32 scratch[40];
-    __shared__ unsigned long long cH, cL, cW, cA;
-    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; cA = 0; }
+    __shared__ unsigned long long cH, cL, cW, cA, cR;
+    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; cA = 0; cR = 0; }
     __syncthreads();
     for (u32 base = 0; base < p.T; base += 1024) {
         const u32 t = base + threadIdx.x;
@@ -291,24 +317,27 @@ __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
             m.histSize = hs;
             m.blocks = u32(ceilDiv(count, p.cb));
         }
-        u32 tH, tL, tW, tA;
+        u32 tH, tL, tW, tA, tR;
         const u32 eH = blockExclusiveSum<1024>(hs, scratch, &tH);
         const u32 eL = blockExclusiveSum<1024>(ls, scratch, &tL);
         const u32 eW = blockExclusiveSum<1024>(ws, scratch, &tW);
         const u32 eA = blockExclusiveSum<1024>(m.blocks, scratch, &tA);
+        const u32 eR = blockExclusiveSum<1024>(u32(ceilDiv(m.blocks, kRunSymbols / p.cb)), scratch, &tR);
         if (t < p.T) {
             m.histOff = cH + eH;
             m.leafOff = cL + eL;
             m.hdrOff = cW + eW;
             m.actOff = u32(cA + eA);
+            m.runOff = u32(cR + eR);
             p.meta[t] = m;
         }
         __syncthreads();
-        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; cA += tA; }
+        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; cA += tA; cR += tR; }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         p.totals[2] = cA;
+        p.totals[3] = cR;
         p.totals[1] = cH;
         if (cH > p.capHist || cL > p.capLeaves || cW > p.capHdr) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
     }
@@ -321,14 +350,33 @@ __global__ void __launch_bounds__(256) k_zeroHist(EncParams p) {
 }
 
 // Pass 4: compact symbols + zero counts (RLHuff) and both histograms, or the
-// plain histogram of a Huff stream.  Bins below kSmemSymBins are counted in
-// shared memory with warp-aggregated increments.
+// plain histogram of a Huff stream.  Symbol bins below kWriteSymBins are
+// counted in shared memory.
+//
+// RLHuff: a tile's run-length entries form one contiguous range of the
+// stream's compact arrays.  Group k of a warp starts its entries after the
+// entries of the tile's groups before it (a warp scan of the groups' counts
+// plus their (0, 255) entries, and a block combine over the warps); inside a
+// group a nonzero's rank is the popcount of the mask below its lane, and its
+// zero count the distance to the set bit below it (or to the nonzero before
+// the group).  Entries are staged in shared memory at their positions within
+// the tile, then copied out with consecutive threads on consecutive entries.
+// Both histograms are counted over the staged entries: the eight most
+// frequent keys of each (zero counts 0..7, symbols 1..8) with warp ballots,
+// the others with shared-memory atomics.  A tile whose entries exceed the
+// stage (a zero run of millions ends in it) writes them directly.
+constexpr u32 kWriteSymBins = 4096;   // symbol bins counted in shared memory by k_write
+
 template <class Sym>
-__global__ void __launch_bounds__(kRleThreads, 6) k_write(EncParams p) {
-    __shared__ RunSum smem[9];
-    __shared__ u32 hSym[kSmemSymBins];
+__global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
+    constexpr u32 kStage = sizeof(Sym) == 2 ? 4096u : 2048u;
+    __shared__ u32 sLast[kRleWarps], sEnt[kRleWarps];
+    __shared__ u32 hSym[kWriteSymBins];
     __shared__ u32 hZc[256];
-    __shared__ u32 extraTotal, sStream;
+    __shared__ __align__(16) Sym sComp[kStage];
+    __shared__ __align__(16) Sym sZcs[kStage];
+    __shared__ u32 sStream;
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) sStream = streamOfTile(p, blockIdx.x);
     if (blockFailed(p)) return;   // synchronizes (sStream visible)
     const u32 tile = blockIdx.x;
@@ -336,23 +384,24 @@ __global__ void __launch_bounds__(kRleThreads, 6) k_write(EncParams p) {
     const EncStreamDev sd = p.streams[s];
     const u32 n = sd.n;
     const TableMeta mS = p.meta[sd.tableFirst];
-    const u32 smemBins = min(mS.histSize, kSmemSymBins);
+    const u32 smemBins = min(mS.histSize, kWriteSymBins);
     for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads) hSym[i] = 0;
     hZc[threadIdx.x] = 0;
-    if (threadIdx.x == 0) extraTotal = 0;
     const Sym* in = reinterpret_cast<const Sym*>(sd.in);
-    const u32 base = (tile - sd.tileOff) * kRleTile + threadIdx.x * kRlePerThread;
-    u32 v[kRlePerThread];
-    loadSyms(in, base, n, v);
+    const u32 wbase = (tile - sd.tileOff) * kRleTile + warp * 1024u;
+    WarpSyms<Sym> v;
+    u32 mUnused;
+    const GroupRuns g = loadGroups(in, wbase, n, v, mUnused);
     u32* gSym = p.hist + mS.histOff;
     if (sd.kind != KIND_RLHUFF) {
         __syncthreads();
 #pragma unroll
-        for (u32 i = 0; i < kRlePerThread; ++i) {
-            const bool valid = base + i < n;
-            const bool toSmem = valid && v[i] < smemBins;
-            aggregatedIncrement(hSym, toSmem ? v[i] : 0u, toSmem);
-            if (valid && !toSmem && v[i] < mS.histSize) atomicAdd(gSym + v[i], 1u);
+        for (u32 k = 0; k < 32; ++k) {
+            const u32 x = v.at(k);
+            const bool valid = wbase + 32u * k + lane < n;
+            const bool toSmem = valid && x < smemBins;
+            aggregatedIncrement(hSym, toSmem ? x : 0u, toSmem);
+            if (valid && !toSmem && x < mS.histSize) atomicAdd(gSym + x, 1u);
         }
         __syncthreads();
         for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads)
@@ -361,50 +410,123 @@ __global__ void __launch_bounds__(kRleThreads, 6) k_write(EncParams p) {
     }
     const TableMeta mZ = p.meta[sd.tableFirst + 1];
     u32* gZc = p.hist + mZ.histOff;
-    const RunSum E = blockScanRun(threadRun(v, base, n), smem, nullptr);   // synchronizes (histograms zeroed)
-    const TileStart ts = p.tileStart[tile];
-    u32 prevP1 = E.cnt ? E.lastP1 : ts.prevP1;
-    u32 outPos = ts.out + (E.cnt ? E.cnt + E.ext + (E.firstP1 - ts.prevP1 - 1u) / 256u : 0u);
-    Sym* comp = reinterpret_cast<Sym*>(p.compact) + sd.compactOff;
-    Sym* zcs = reinterpret_cast<Sym*>(p.zc) + sd.compactOff;
-    u32 extras = 0;
-    bool rangeErr = false;
+    // the nonzero before each group: in the warp, in the warps before, or
+    // before the tile
+    const u32 lastW = __reduce_max_sync(0xffffffffu, g.lastP1);
+    if (lane == 0) sLast[warp] = lastW;
+    __syncthreads();   // also orders the histogram zeroing
+    u32 lastBefore = 0;
 #pragma unroll
-    for (u32 i = 0; i < kRlePerThread; ++i) {
-        const bool nz = base + i < n && v[i] != 0;
-        u32 z = 0;
-        if (nz) {
-            const u32 q = base + i + 1;
-            z = q - prevP1 - 1;
-            const u32 e = z / 256u;
-            for (u32 k = 0; k < e; ++k) {
-                comp[outPos] = Sym(0);
-                zcs[outPos] = Sym(255);
-                ++outPos;
+    for (u32 w = 0; w < kRleWarps; ++w)
+        if (w < warp) lastBefore = max(lastBefore, sLast[w]);
+    const TileStart ts = p.tileStart[tile];
+    u32 prev = max(warpExclusiveMax(g.lastP1), lastBefore);
+    if (!prev) prev = ts.prevP1;
+    const u32 e = g.mask ? (g.firstP1 - prev - 1u) / 256u : 0u;   // (0, 255) entries before the group
+    const u32 ent = g.cnt + e;
+    const u32 entIncl = warpInclusiveSum(ent);
+    if (lane == 31) sEnt[warp] = entIncl;
+    __syncthreads();
+    u32 warpOut = 0, entries = 0;
+#pragma unroll
+    for (u32 w = 0; w < kRleWarps; ++w) {
+        const u32 x = sEnt[w];
+        if (w < warp) warpOut += x;
+        entries += x;
+    }
+    const u32 groupOut = warpOut + entIncl - ent;
+    Sym* comp = reinterpret_cast<Sym*>(p.compact) + sd.compactOff + ts.out;
+    Sym* zcs = reinterpret_cast<Sym*>(p.zc) + sd.compactOff + ts.out;
+    const bool staged = entries <= kStage;                // block-uniform
+    Sym* oc = staged ? sComp : comp;
+    Sym* oz = staged ? sZcs : zcs;
+    {
+#pragma unroll
+        for (u32 k = 0; k < 32; ++k) {
+            const u32 mk = __shfl_sync(0xffffffffu, g.mask, k);
+            if (mk == 0u) continue;                           // warp-uniform
+            const u32 ok = __shfl_sync(0xffffffffu, groupOut, k);
+            const u32 ek = __shfl_sync(0xffffffffu, e, k);
+            const u32 pk = __shfl_sync(0xffffffffu, prev, k);
+            for (u32 t = lane; t < ek; t += 32) {
+                oc[ok + t] = Sym(0);
+                oz[ok + t] = Sym(255);
             }
-            extras += e;
-            comp[outPos] = Sym(v[i]);
-            zcs[outPos] = Sym(z & 255u);
-            ++outPos;
-            prevP1 = q;
+            if ((mk >> lane) & 1u) {
+                const u32 below = mk & ((1u << lane) - 1u);
+                const u32 gb = wbase + 32u * k;
+                const u32 q = gb + lane + 1u;
+                const u32 pp = below ? gb + 32u - u32(__clz(below)) : pk;
+                const u32 o = ok + ek + u32(__popc(below));
+                oc[o] = Sym(v.at(k));
+                oz[o] = Sym((q - pp - 1u) & 255u);
+            }
         }
-        const u32 sym = v[i];
-        const bool toSmem = nz && sym < smemBins;
-        aggregatedIncrement(hSym, toSmem ? sym : 0u, toSmem);
-        if (nz && !toSmem && sym < mS.histSize) atomicAdd(gSym + sym, 1u);
-        const bool zcOk = (z & 255u) < mZ.histSize;
-        rangeErr |= nz && !zcOk;
-        aggregatedIncrement(hZc, z & 255u, nz && zcOk);
+    }
+    __syncthreads();
+    // histograms (and the copy-out of a staged tile)
+    const Sym* hc = staged ? sComp : comp;
+    const Sym* hz = staged ? sZcs : zcs;
+    const bool fast = staged && mZ.histSize == 256u && smemBins > 8u;   // block-uniform
+    // the eight most frequent keys of each histogram (zero counts 0..7,
+    // symbols 1..8) in per-lane 8-bit counters, four keys per register (at
+    // most kStage / kRleThreads = 16 entries per lane), added once per warp
+    // at the end; integer ALU work only
+    u32 z03 = 0, z47 = 0, s03 = 0, s47 = 0;
+    bool rangeErr = false;
+    for (u32 j0 = 0; j0 < entries; j0 += kRleThreads) {
+        const u32 j = j0 + threadIdx.x;
+        const bool act = j < entries;
+        const u32 sym = act ? u32(hc[j]) : 0u;
+        const u32 zc = act ? u32(hz[j]) : 0u;
+        if (act && staged) {
+            comp[j] = Sym(sym);
+            zcs[j] = Sym(zc);
+        }
+        if (fast) {
+            if (act) {
+                const u32 zi = 1u << ((zc & 3u) << 3);
+                if (zc < 4u) z03 += zi;
+                else if (zc < 8u) z47 += zi;
+                else atomicAdd(hZc + zc, 1u);
+                const u32 k = sym - 1u;            // keys 1..8 -> 0..7
+                const u32 si = 1u << ((k & 3u) << 3);
+                if (k < 4u) s03 += si;
+                else if (k < 8u) s47 += si;
+                else if (sym < smemBins) atomicAdd(hSym + sym, 1u);
+                else if (sym < mS.histSize) atomicAdd(gSym + sym, 1u);
+            }
+        } else {
+            const bool toSmem = act && sym < smemBins;
+            aggregatedIncrement(hSym, toSmem ? sym : 0u, toSmem);
+            if (act && !toSmem && sym < mS.histSize) atomicAdd(gSym + sym, 1u);
+            const bool zcOk = zc < mZ.histSize;
+            rangeErr |= act && !zcOk;
+            aggregatedIncrement(hZc, zc, act && zcOk);
+        }
+    }
+    if (fast) {
+        // widen to 16-bit fields (keys k, k + 2 per register) and sum over the warp
+        u32 a[8] = {z03 & 0x00FF00FFu, (z03 >> 8) & 0x00FF00FFu, z47 & 0x00FF00FFu, (z47 >> 8) & 0x00FF00FFu,
+                    s03 & 0x00FF00FFu, (s03 >> 8) & 0x00FF00FFu, s47 & 0x00FF00FFu, (s47 >> 8) & 0x00FF00FFu};
+#pragma unroll
+        for (u32 o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (u32 i = 0; i < 8; ++i) a[i] += __shfl_xor_sync(0xffffffffu, a[i], o);
+        if (lane == 0) {
+            // a[0]: keys 0, 2; a[1]: 1, 3; a[2]: 4, 6; a[3]: 5, 7 (zero counts); a[4..7] the same for symbols - 1
+            const u32 key[4] = {0u, 1u, 4u, 5u};
+#pragma unroll
+            for (u32 i = 0; i < 4; ++i) {
+                const u32 zl = a[i] & 0xFFFFu, zh = a[i] >> 16, sl = a[4 + i] & 0xFFFFu, sh = a[4 + i] >> 16;
+                if (zl) atomicAdd(hZc + key[i], zl);
+                if (zh) atomicAdd(hZc + key[i] + 2u, zh);
+                if (sl) atomicAdd(hSym + key[i] + 1u, sl);
+                if (sh) atomicAdd(hSym + key[i] + 3u, sh);
+            }
+        }
     }
     if (rangeErr) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
-    const u32 e = warpSum(extras);
-    if ((threadIdx.x & 31) == 0 && e) atomicAdd(&extraTotal, e);
-    __syncthreads();
-    if (threadIdx.x == 0 && extraTotal) {
-        hSym[0] += extraTotal;
-        if (mZ.histSize > 255u) hZc[255] += extraTotal;
-        else atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
-    }
     __syncthreads();
     for (u32 i = threadIdx.x; i < smemBins; i += kRleThreads)
         if (hSym[i]) atomicAdd(gSym + i, hSym[i]);
@@ -638,64 +760,70 @@ static size_t tableBuildSoloSmem(int device) {
 // ---------------------------------------------------------------------------
 constexpr u32 kPackWarps = 8;
 
-// kPer = coding block / 32 consecutive symbols of one lane, from j0: one
-// vector load when the run lies inside the stream and is aligned, else
-// element loads.  Positions at or past count are not read.
-template <class Sym, int kPer>
-__device__ __forceinline__ void laneSyms(const Sym* in, u32 j0, u32 count, u32 (&s)[kPer]) {
-    constexpr int kBytes = kPer * int(sizeof(Sym));
-    constexpr int kAlign = kBytes < 16 ? kBytes : 16;
-    const Sym* q = in + j0;
-    if (kBytes >= 4 && j0 + kPer <= count && (reinterpret_cast<uintptr_t>(q) & uintptr_t(kAlign - 1)) == 0) {
-        constexpr int kWords = kBytes >= 4 ? kBytes / 4 : 1;
-        u32 w[kWords];
-        if (kWords >= 4) {
+// A lane's 32 symbols of a run, packed as they lie in memory (two 16-bit
+// symbols or one 32-bit symbol per word): one 16-byte vector per 8 or 4
+// symbols when the run lies inside the stream and is aligned, else element
+// loads.  Positions at or past count read 0.
+template <class Sym>
+struct LaneRun {
+    static constexpr u32 kWords = 32 * sizeof(Sym) / 4;
+    u32 w[kWords];
+    __device__ __forceinline__ u32 at(u32 k) const {   // k a compile-time constant after unrolling
+        return sizeof(Sym) == 2 ? (w[k >> 1] >> (16 * (k & 1))) & 0xFFFFu : w[k];
+    }
+    __device__ __forceinline__ void load(const Sym* in, u32 j0, u32 count) {
+        const Sym* q = in + j0;
+        if (j0 + 32u <= count && (reinterpret_cast<uintptr_t>(q) & 15u) == 0) {
 #pragma unroll
-            for (int c = 0; c < kWords / 4; ++c) {
+            for (u32 c = 0; c < kWords / 4; ++c) {
                 const uint4 v = reinterpret_cast<const uint4*>(q)[c];
                 w[4 * c] = v.x; w[4 * c + 1] = v.y; w[4 * c + 2] = v.z; w[4 * c + 3] = v.w;
             }
-        } else if (kWords == 2) {
-            const uint2 v = *reinterpret_cast<const uint2*>(q);
-            w[0] = v.x; w[1] = v.y;
-        } else {
-            w[0] = *reinterpret_cast<const unsigned int*>(q);
+            return;
         }
 #pragma unroll
-        for (int k = 0; k < kPer; ++k) s[k] = sizeof(Sym) == 2 ? (w[k >> 1] >> (16 * (k & 1))) & 0xFFFFu : w[k];
-        return;
+        for (u32 c = 0; c < kWords; ++c) {
+            if (sizeof(Sym) == 2) {
+                const u32 lo = j0 + 2 * c < count ? u32(q[2 * c]) : 0u;
+                const u32 hi = j0 + 2 * c + 1 < count ? u32(q[2 * c + 1]) : 0u;
+                w[c] = lo | (hi << 16);
+            } else {
+                w[c] = j0 + c < count ? u32(q[c]) : 0u;
+            }
+        }
     }
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) s[k] = j0 + u32(k) < count ? u32(q[k]) : 0u;
-}
+};
 
-// Bits of every coding block in use: warps walk the list of used blocks
-// (k_usedBlocks); each lane loads its kPer symbols at once and gathers their
-// code lengths together.
-template <class Sym, int kPer>
+// Bits of every coding block in use.  Warps walk the call's run list
+// (k_usedBlocks): a run is kRunSymbols consecutive symbols of one table, 32
+// per lane, so cb / 32 lanes share a coding block; each lane sums the code
+// lengths of its symbols and the block's lanes add theirs.
+template <class Sym>
 __global__ void __launch_bounds__(kPackWarps * 32) k_blockBits(EncParams p) {
     const u32 lane = threadIdx.x & 31;
     if (warpFailed(p)) return;
-    const u32 used = u32(p.totals[2]);
+    const u32 runs = u32(p.totals[3]);
+    const u32 lpb = p.cb / 32u, bpr = kRunSymbols / p.cb;
     const u32 stride = gridDim.x * kPackWarps;
-    for (u32 i = blockIdx.x * kPackWarps + (threadIdx.x >> 5); i < used; i += stride) {
-        const u32 t = p.blockTable[i];
+    for (u32 r = blockIdx.x * kPackWarps + (threadIdx.x >> 5); r < runs; r += stride) {
+        const u32 t = p.runTable[r];
         const TableMeta& m = p.meta[t];
         const EncTableDev td = p.tables[t];
-        const u32 b = i - m.actOff;
+        const u32 rb = r - m.runOff;
         u32 count;
         const Sym* in = tableInput<Sym>(p, td, count);
         const uint2* enc = p.enc + m.histOff;
         const u32 hs = m.histSize;
-        const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
-        u32 sv[kPer];
-        laneSyms<Sym, kPer>(in, j0, count, sv);
+        const u32 j0 = rb * kRunSymbols + lane * 32u;
+        LaneRun<Sym> sv;
+        sv.load(in, j0, count);
         u32 bits = 0;
 #pragma unroll
-        for (int k = 0; k < kPer; ++k)
-            if (j0 + u32(k) < count) bits += enc[min(sv[k], hs - 1u)].y;
-        bits = warpSum(bits);
-        if (lane == 0) p.blockBits[td.blockOff + b] = bits;
+        for (u32 k = 0; k < 32; ++k)
+            if (j0 + k < count) bits += enc[min(sv.at(k), hs - 1u)].y;
+        for (u32 o = 1; o < lpb; o <<= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
+        const u32 b = rb * bpr + lane / lpb;
+        if (lane % lpb == 0 && b < m.blocks) p.blockBits[td.blockOff + b] = bits;
     }
 }
 
@@ -789,59 +917,65 @@ __device__ __forceinline__ void orCodeword(u32* win, u32 wLo, u32 wHi, u32 pos, 
     }
 }
 
-// Each warp writes the output words whose first bit lies in its coding block
-// (gather ownership: no atomics on global memory, no pre-zeroing); the bits
-// of the last owned word that belong to the next block are recomputed from
-// that block's first symbols.
-template <class Sym, int kPer>
+// Packing, by runs of coding blocks (as k_blockBits): the run's codewords
+// are contiguous in the table's bit stream from its first block's offset, so
+// a lane's start bit is that offset plus the code lengths of the lanes
+// before it.  Each warp writes the output words whose first bit lies in its
+// run (gather ownership: no atomics on global memory, no pre-zeroing),
+// assembling them in a shared-memory window; the bits of the last owned word
+// that belong to the next run are recomputed from that run's first symbols.
+// A lane looks its codes up twice (lengths, then codes), keeping registers
+// for the symbols only.
+constexpr u32 kPackWindowWords = kRunSymbols * 31u / 32u + 2u;
+
+template <class Sym>
 __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
-    extern __shared__ u32 winAll[];
+    __shared__ u32 winAll[kPackWarps * kPackWindowWords];
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warpFailed(p)) return;
-    u32* win = winAll + warp * (p.cb + 2);
-    const u32 used = u32(p.totals[2]);
+    u32* win = winAll + warp * kPackWindowWords;
+    const u32 runs = u32(p.totals[3]);
+    const u32 bpr = kRunSymbols / p.cb;
     const u32 stride = gridDim.x * kPackWarps;
-    for (u32 i = blockIdx.x * kPackWarps + warp; i < used; i += stride) {
-        const u32 t = p.blockTable[i];
+    for (u32 r = blockIdx.x * kPackWarps + warp; r < runs; r += stride) {
+        const u32 t = p.runTable[r];
         const TableMeta m = p.meta[t];
         const EncTableDev td = p.tables[t];
-        const u32 b = i - m.actOff;
+        const u32 rb = r - m.runOff;
+        const u32 bFirst = rb * bpr, bEnd = min(bFirst + bpr, m.blocks);
         u32 count;
         const Sym* in = tableInput<Sym>(p, td, count);
         const u32* bo = p.blockOff + td.blockOff;
-        const u32 off0 = bo[b];
-        const u32 off1 = (b + 1 < m.blocks) ? bo[b + 1] : m.codeBits;
+        const u32 off0 = bo[bFirst];
+        const u32 off1 = bEnd < m.blocks ? bo[bEnd] : m.codeBits;
         const u32 wLo = (off0 + 31) >> 5, wHi = (off1 + 31) >> 5;
         if (wLo >= wHi) continue;
         for (u32 w = lane; w < wHi - wLo; w += 32) win[w] = 0;
-        __syncwarp();
         const uint2* enc = p.enc + m.histOff;
         const u32 hs = m.histSize;
-        const u32 j0 = b * u32(kPer * 32) + lane * u32(kPer);
-        u32 sv[kPer];
-        laneSyms<Sym, kPer>(in, j0, count, sv);
-        uint2 cw[kPer];
+        const u32 j0 = rb * kRunSymbols + lane * 32u;
+        LaneRun<Sym> sv;
+        sv.load(in, j0, count);
         u32 lsum = 0;
 #pragma unroll
-        for (int k = 0; k < kPer; ++k) {
-            cw[k] = j0 + u32(k) < count ? enc[min(sv[k], hs - 1u)] : make_uint2(0, 0);
-            lsum += cw[k].y;
-        }
+        for (u32 k = 0; k < 32; ++k)
+            if (j0 + k < count) lsum += enc[min(sv.at(k), hs - 1u)].y;
+        __syncwarp();
         // the lane's codewords are consecutive: concatenate them in a 64-bit
         // accumulator (bits left-aligned from the lane's start bit in its
         // first word) and OR whole words into the window - one shared atomic
-        // per word touched instead of one or two per codeword
+        // per word touched
         const u32 pos = off0 + warpInclusiveSum(lsum) - lsum;
         {
             u32 w = pos >> 5;
             u32 n = pos & 31u;
             unsigned long long acc = 0;
 #pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                const u32 len = cw[k].y;
-                if (len) {
-                    acc |= (unsigned long long)cw[k].x << (64u - n - len);
-                    n += len;
+            for (u32 k = 0; k < 32; ++k) {
+                const uint2 c = j0 + k < count ? enc[min(sv.at(k), hs - 1u)] : make_uint2(0u, 0u);
+                if (c.y) {
+                    acc |= (unsigned long long)c.x << (64u - n - c.y);
+                    n += c.y;
                 }
                 if (n >= 32u) {
                     if (w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
@@ -852,11 +986,11 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
             }
             if (n && w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
         }
-        // bits of the next block inside the last owned word
-        if (b + 1 < m.blocks && (wHi << 5) > off1) {
-            const u32 j = (b + 1) * p.cb + lane;
-            uint2 c = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
-            u32 q = off1 + warpInclusiveSum(c.y) - c.y;
+        // bits of the next run inside the last owned word
+        if (bEnd < m.blocks && (wHi << 5) > off1) {
+            const u32 j = bEnd * p.cb + lane;
+            const uint2 c = j < count ? enc[min(u32(in[j]), hs - 1u)] : make_uint2(0, 0);
+            const u32 q = off1 + warpInclusiveSum(c.y) - c.y;
             if (q < (wHi << 5)) orCodeword(win, wLo, wHi, q, c.x, c.y);
         }
         __syncwarp();
@@ -864,7 +998,7 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
         const SegmentLayout& L = p.layout[td.stream];
         u32* dst = p.out + L.startWord + L.cwWord[which];
         for (u32 w = lane; w < wHi - wLo; w += 32) dst[wLo + w] = win[w];
-        __syncwarp();   // the window is cleared for the next block only after these reads
+        __syncwarp();   // the window is cleared for the next run only after these reads
     }
 }
 
@@ -1031,31 +1165,18 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     // with a grid of a few CTAs per SM
     if (p.totalBlocks && p.T) { k_usedBlocks<<<p.T, 256, 0, st>>>(p); countLaunch(); }
     const u32 blockGrid = u32(std::max(1, I->smCount > 0 ? I->smCount : 148)) * 8u;
+    // runs of the call: at most the used blocks / blocks per run, plus one per table
+    const u32 runBound = u32(ceilDiv(p.totalBlocks, kRunSymbols / p.cb)) + p.T;
     if (p.totalBlocks) {
-        const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(p.totalBlocks, kPackWarps)));
-        {
-            SectionTimer t(I, "enc.block_bits", st);
-            switch (p.cb) {
-                case 32: k_blockBits<Sym, 1><<<g, kPackWarps * 32, 0, st>>>(p); break;
-                case 64: k_blockBits<Sym, 2><<<g, kPackWarps * 32, 0, st>>>(p); break;
-                case 128: k_blockBits<Sym, 4><<<g, kPackWarps * 32, 0, st>>>(p); break;
-                default: k_blockBits<Sym, 8><<<g, kPackWarps * 32, 0, st>>>(p); break;
-            }
-            countLaunch();
-        }
+        const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(runBound, kPackWarps)));
+        { SectionTimer t(I, "enc.block_bits", st); k_blockBits<Sym><<<g, kPackWarps * 32, 0, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "enc.block_scan", st); k_blockScan<<<p.T, 1024, 0, st>>>(p); countLaunch(); }
     }
     { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
     if (p.totalBlocks) {
-        const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(p.totalBlocks, kPackWarps)));
-        const size_t packSmem = size_t(kPackWarps) * (p.cb + 2) * sizeof(u32);
+        const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(runBound, kPackWarps)));
         SectionTimer t(I, "enc.pack", st);
-        switch (p.cb) {
-            case 32: k_pack<Sym, 1><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
-            case 64: k_pack<Sym, 2><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
-            case 128: k_pack<Sym, 4><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
-            default: k_pack<Sym, 8><<<g, kPackWarps * 32, packSmem, st>>>(p); break;
-        }
+        k_pack<Sym><<<g, kPackWarps * 32, 0, st>>>(p);
         countLaunch();
     }
     { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 128, 0, st>>>(p); countLaunch(); }
@@ -1108,6 +1229,7 @@ int encodeLaunch(cc_instance* I, const EncPlan& hp, u32* out, u64 outCap) {
     p.blockBits = I->blockBits;
     p.blockOff = I->blockOff;
     p.blockTable = I->blockTable;
+    p.runTable = I->runTable;
     p.tileStream = I->tileStream;
     p.layout = I->layout;
     p.out = out;
@@ -1177,7 +1299,7 @@ int cc_encode(cc_instance* I, int kind, int symbolBytes, const void* const* dStr
     }
     if (S > I->streamCountMax) { setError("stream count %u exceeds instance limit %u", S, I->streamCountMax); return CC_ERR_CAPACITY; }
     if (n > I->elemCountPerStreamMax) { setError("symbol count %u exceeds instance limit %u", n, I->elemCountPerStreamMax); return CC_ERR_CAPACITY; }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     std::vector<EncStream> st(S);
     for (u32 i = 0; i < S; ++i) {
         st[i].in = dStreams[i];

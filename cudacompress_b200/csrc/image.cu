@@ -207,7 +207,7 @@ int compressImages(cc_instance* I, cc_image* imgs, u32 count, u32 sx, u32 sy, u3
             return CC_ERR_INVALID_ARGUMENT;
         }
     if (!count) return CC_OK;
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 pixels = u64(sx) * sy, streams = u64(perImage) * count;
     // scratch words of all images when they are copied out one by one
@@ -292,7 +292,7 @@ int decompressImages(cc_instance* I, const cc_image* imgs, u32 count, u32 sx, u3
             return CC_ERR_INVALID_ARGUMENT;
         }
     if (!count) return CC_OK;
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 pixels = u64(sx) * sy, streams = u64(perImage) * count;
     Bump b{nullptr};
@@ -324,7 +324,6 @@ int decompressImages(cc_instance* I, const cc_image* imgs, u32 count, u32 sx, u3
         for (u32 c = 0; c < chProc; ++c)
             for (u32 k = 0; k < 3; ++k) hostPtrs[(u64(i) * chProc + c) * 3 + k] = s0 + (chProc + 3 * u64(c) + k) * n;
     }
-    CC_TRY_CUDA(cudaMemsetAsync(syms, 0, streams * n * sizeof(u16), st), "zero symbols");
     CC_TRY_CUDA(cudaMemcpyAsync(dPtrs, hostPtrs.data(), hostPtrs.size() * sizeof(void*), cudaMemcpyHostToDevice, st),
                 "upload band pointers");
     if ((rc = decodeDevice(I, KIND_RLHUFF, hw.data(), bits.data(), pos.data(), count, bsIndex.data(), outs.data(),
@@ -508,7 +507,7 @@ int cc_compress_heightfield_one_level(cc_instance* I, const int16_t* image, uint
         return CC_ERR_CAPACITY;
     }
     if (capacity < bitsWords) { setError("%s: needs more than %llu words", what, (unsigned long long)capacity); return CC_ERR_CAPACITY; }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 pixels = u64(sx) * sy;
     Bump b{nullptr};
@@ -552,7 +551,7 @@ int cc_decompress_heightfield_one_level(cc_instance* I, int16_t* image, uint32_t
         return CC_ERR_CAPACITY;
     }
     if (u64(bitSize) < bitsWords * 32) { setError("%s: stream shorter than the lowpass bits", what); return CC_ERR_CORRUPT_STREAM; }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 pixels = u64(sx) * sy;
     Bump b{nullptr};
@@ -570,7 +569,6 @@ int cc_decompress_heightfield_one_level(cc_instance* I, int16_t* image, uint32_t
     if ((rc = cc_append_lsb(lowpass, words, u32(n), shift, st))) return rc;
     CC_TRY_CUDA(cudaMemcpy2DAsync(dwt1, sx * sizeof(i16), lowpass, hx * sizeof(i16), hx * sizeof(i16), hy,
                                   cudaMemcpyDeviceToDevice, st), "place lowpass");
-    CC_TRY_CUDA(cudaMemsetAsync(syms, 0, 3 * n * sizeof(u16), st), "zero bands");
     const u32* hw = host.data();
     u32 pos = u32(bitsWords * 32);
     void* outs[3] = {syms, syms + n, syms + 2 * n};

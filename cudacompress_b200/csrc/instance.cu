@@ -122,6 +122,7 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->blockBits = c.take<u32>(I->capBlocks + 1);
     I->blockOff = c.take<u32>(I->capBlocks + 1);
     I->blockTable = c.take<u32>(I->capBlocks + 1);
+    I->runTable = c.take<u32>(I->capBlocks + 1);
     I->tileStream = c.take<u32>(I->capTiles + 1);
     I->layout = c.take<SegmentLayout>(I->capStreams);
     I->out = c.take<u32>(I->outWordsMax);

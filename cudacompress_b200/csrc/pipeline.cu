@@ -203,7 +203,6 @@ int decodeVolumeSymbols(cc_instance* I, const u32* const* dWords, const u32* bit
         const bool huff = rleOnly && l > 0;
         for (u32 c = 0; c < count; ++c) {
             u16* first = syms + c * vs.total + vs.level[l];
-            if (!huff) CC_TRY_CUDA(cudaMemsetAsync(first, 0, 7 * vs.band[l] * sizeof(u16), st), "zero bands");
             for (u32 i = 0; i < 7; ++i) {
                 outs[c * 7 + i] = first + i * vs.band[l];
                 bsIndex[c * 7 + i] = c;
@@ -229,7 +228,7 @@ int compressVolumeFloat(cc_instance* I, const float* vol, u32 nx, u32 ny, u32 nz
         setError("%s: instance needs >= 7 streams of >= %llu symbols", what, (unsigned long long)band0);
         return CC_ERR_CAPACITY;
     }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 N0 = cube(nx, ny, nz);
     const VolumeSymbols vs = volumeSymbols(nx, ny, nz, L);
@@ -282,7 +281,7 @@ int decompressVolumeFloat(cc_instance* I, const cc_volume_channel* ch, u32 count
         if (!ch[c].d_volume || !ch[c].d_words) { setError("%s: channel %u: null pointer", what, c); return CC_ERR_INVALID_ARGUMENT; }
     if (!volumeSizesOk(nx, ny, nz, L, what)) return CC_ERR_INVALID_ARGUMENT;
     if (I->symBytes != 2) { setError("%s: needs a 16-bit-symbol instance", what); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 N0 = cube(nx, ny, nz);
     const VolumeSymbols vs = volumeSymbols(nx, ny, nz, L);
@@ -341,7 +340,7 @@ int compressVolumeQuantFirst(cc_instance* I, const float* vol, u32 nx, u32 ny, u
         setError("%s: instance needs >= 7 streams of >= %llu symbols", what, (unsigned long long)band0);
         return CC_ERR_CAPACITY;
     }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 N0 = cube(nx, ny, nz);
     const VolumeSymbols vs = volumeSymbols(nx, ny, nz, L);
@@ -395,7 +394,7 @@ int decompressVolumeQuantFirst(cc_instance* I, const cc_volume_channel* ch, u32 
         if (!ch[c].d_volume || !ch[c].d_words) { setError("%s: channel %u: null pointer", what, c); return CC_ERR_INVALID_ARGUMENT; }
     if (!volumeSizesOk(nx, ny, nz, L, what)) return CC_ERR_INVALID_ARGUMENT;
     if (I->symBytes != 2) { setError("%s: needs a 16-bit-symbol instance", what); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 N0 = cube(nx, ny, nz);
     const VolumeSymbols vs = volumeSymbols(nx, ny, nz, L);
@@ -525,7 +524,7 @@ int cc_compress_heightfield(cc_instance* I, const int16_t* img, uint32_t nx, uin
         setError("compressHeightfield: instance needs >= 3 streams of >= %llu symbols", (unsigned long long)band0);
         return CC_ERR_CAPACITY;
     }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 N0 = u64(nx) * ny;
     Bump b{nullptr};
@@ -590,7 +589,7 @@ static int decompressHeightfieldPerLevel(cc_instance* I, int16_t* out, uint32_t 
                                          const uint32_t* dWords, uint32_t bitSize) {
     if (!I || !out || !dWords || levels == 0) { setError("decompressHeightfield: bad argument"); return CC_ERR_INVALID_ARGUMENT; }
     if (I->symBytes != 2) { setError("decompressHeightfield: needs a 16-bit-symbol instance"); return CC_ERR_INVALID_ARGUMENT; }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 words = ceilDiv(bitSize, 32);
     if (words > I->hostWordsMax) { setError("decompressHeightfield: stream larger than instance staging"); return CC_ERR_CAPACITY; }
@@ -623,7 +622,6 @@ static int decompressHeightfieldPerLevel(cc_instance* I, int16_t* out, uint32_t 
         const u32 sx = nx >> l, sy = ny >> l, hx = sx / 2, hy = sy / 2;
         const u64 bandN = u64(hx) * hy;
         for (u32 i = 0; i < 3; ++i) outs[i] = syms + i * bandN;
-        CC_TRY_CUDA(cudaMemsetAsync(syms, 0, 3 * bandN * sizeof(u16), st), "zero bands");
         if ((rc = decodeDevice(I, KIND_RLHUFF, &hw, &bitSize, &pos, 1, nullptr, outs, 3, u32(bandN)))) return rc;
         pos = u32(alignUp(pos, 32));
         // assemble [LL | HL ; LH | HH] of this level then invert
@@ -650,7 +648,7 @@ int cc_decompress_heightfield(cc_instance* I, int16_t* out, uint32_t nx, uint32_
         setError("decompressHeightfield: sizes must be divisible by 2^levels with coarsest level >= 8");
         return CC_ERR_INVALID_ARGUMENT;
     }
-    cudaSetDevice(I->device);
+    DeviceGuard deviceGuard(I->device);
     cudaStream_t st = I->stream;
     const u64 N0 = u64(nx) * ny;
     Bump b{nullptr};
@@ -689,7 +687,6 @@ int cc_decompress_heightfield(cc_instance* I, int16_t* out, uint32_t nx, uint32_
     dp.dev = I->dPlan;
     CC_TRY_CUDA(cudaMemcpyAsync(I->dPlan, slot, dp.bytes, cudaMemcpyHostToDevice, st), "upload plan");
     cudaEventRecord(I->ringEvent[(I->ringNext + cc_instance::kRing - 1) % cc_instance::kRing], st);
-    CC_TRY_CUDA(cudaMemsetAsync(syms + u64(lx) * ly, 0, (at - u64(lx) * ly) * sizeof(u16), st), "zero bands");
     if ((rc = decodeLaunch(I, dp))) return rc;
     rc = cc_unsymbolize(cur, syms, lx, ly, 1, 0, 0, st);
     if (rc) return rc;

@@ -1,15 +1,23 @@
 """Continuous-batching brick service over the batched volume codec.
 
 Requests ask to encode a brick (a device float32 volume) or to decode one of
-the compressed bricks kept resident on the device.  The server keeps one
-batched codec (cc_volume_batch) per (brick edge, operation) with a fixed
-number of slots, each on its own CUDA stream, so that work for different
-sizes and operations overlaps on the GPU.  Every time a batch is idle the
-loop fills it with the oldest waiting requests of its kind - as many as
-slots and the HBM admission budget allow - and launches it (replayed as a
-CUDA graph per fill level); requests that arrive meanwhile wait for the next
-launch of their batch, not for the whole queue to drain.  Latency is
-arrival -> result ready (the host sees the batch's completion event).
+the compressed bricks kept resident on the device.  The server keeps, per
+(brick edge, operation), a lane of two batched codecs (cc_volume_batch) with
+a fixed number of slots each, every codec on its own CUDA stream.  While one
+codec of a lane is on the GPU the other admits the requests that arrived
+meanwhile - as many as its slots and the HBM admission budget allow - and
+launches at once (replayed as a CUDA graph per fill level), so a request waits
+for a free slot group, not for the lane's running batch to drain.  Decode
+lanes run on high-priority streams and are filled first, so small decodes are
+not held behind large encodes.  Latency is arrival -> result ready (the host
+sees the batch's completion event).
+
+Admission: a request holds its output (decode) or input (encode) volume,
+edge^3 * 4 bytes, from launch to completion; the resident compressed store
+plus everything admitted stays within `budget_bytes`.  A budget that cannot
+hold the store plus one request of the largest edge is rejected at
+construction, so every request fits once the GPU drains and the loop always
+makes progress.
 
 Results do not depend on the mix: every brick has its own Huffman tables and
 its own stream, so a brick decoded alone and in a full batch is bit-identical.
@@ -17,8 +25,9 @@ its own stream, so a brick decoded alone and in a full batch is bit-identical.
 from __future__ import annotations
 
 import time
+from collections import deque
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Tuple
+from typing import Deque, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -37,30 +46,63 @@ class Request:
     brick: int = 0             # DECODE: index of the resident brick; ENCODE: index of the source brick
     done: float = -1.0
     result: Optional[object] = None
+    launched: float = -1.0     # when its batch was launched (seconds after the start of the run)
 
 
 @dataclass
-class _Lane:
-    """One batched codec with its slots, stream and in-flight state."""
-    edge: int
-    op: int
+class _Group:
+    """One batched codec of a lane: its slots, stream and in-flight state."""
     batch: VolumeBatch
     stream: torch.cuda.Stream
     outs: List[torch.Tensor]
-    queue: List[Request] = field(default_factory=list)
     inflight: List[Request] = field(default_factory=list)
     event: Optional[torch.cuda.Event] = None
     bytes_inflight: int = 0
 
 
+@dataclass
+class _Lane:
+    edge: int
+    op: int
+    groups: List[_Group]
+    queue: Deque[Request] = field(default_factory=deque)
+
+
+def request_bytes(edge: int) -> int:
+    """Device bytes a request of this edge holds while admitted."""
+    return edge ** 3 * 4
+
+
+def validate_budget(store_bytes: int, edges: Sequence[int], budget_bytes: int) -> None:
+    """Raises ValueError unless the budget holds the resident store plus one
+    request of the largest edge (otherwise such a request could never run)."""
+    need = store_bytes + request_bytes(max(edges))
+    if need > budget_bytes:
+        raise ValueError(f"HBM admission budget {budget_bytes} B cannot hold the resident store ({store_bytes} B) "
+                         f"plus one {max(edges)}^3 request ({request_bytes(max(edges))} B)")
+
+
+def admit(queue_bytes: Sequence[int], slots: int, budget_left: int) -> int:
+    """How many requests from the head of a queue (their bytes, in arrival
+    order) one launch takes: at most `slots`, in order, while they fit."""
+    take = 0
+    for b in queue_bytes:
+        if take == slots or b > budget_left:
+            break
+        budget_left -= b
+        take += 1
+    return take
+
+
 class BrickServer:
-    """edges: brick edge lengths served; slots: slots per edge; sources: per
-    edge a list of device float32 bricks (encode inputs, and what the resident
-    compressed store holds); budget: HBM bytes admitted requests may hold
-    (outputs of decodes, inputs of encodes) on top of the resident store."""
+    """sources: per edge a list of device float32 bricks (encode inputs, and
+    what the resident compressed store holds); slots: slots per codec of each
+    edge's lanes; groups: codecs per lane; budget_bytes: HBM bytes the store
+    plus admitted requests may hold."""
 
     def __init__(self, device: int, sources: Dict[int, List[torch.Tensor]], slots: Dict[int, int], levels: int,
-                 q0: float, budget_bytes: int = 4 << 30, graph: bool = True, keep_results: bool = False):
+                 q0: float, budget_bytes: int = 4 << 30, graph: bool = True, keep_results: bool = False,
+                 groups: int = 2):
         self.inst = Instance(device, 7, 1 << 12, 128, 14)
         self.levels = levels
         self.q0 = q0
@@ -70,81 +112,85 @@ class BrickServer:
         self.lanes: Dict[Tuple[int, int], _Lane] = {}
         for edge, k in slots.items():
             for op in (ENCODE, DECODE):
-                b = VolumeBatch(self.inst, [(edge, edge, edge)] * k, levels, [q0] * k, graph=graph)
-                st = torch.cuda.Stream(device=device)
-                b.set_stream(st)
-                outs = [torch.empty((edge,) * 3, dtype=torch.float32, device=f"cuda:{device}") for _ in range(k)] \
-                    if op == DECODE else []
-                self.lanes[(edge, op)] = _Lane(edge, op, b, st, outs)
+                gs = []
+                for _ in range(groups):
+                    b = VolumeBatch(self.inst, [(edge, edge, edge)] * k, levels, [q0] * k, graph=graph)
+                    st = torch.cuda.Stream(device=device, priority=-1 if op == DECODE else 0)
+                    b.set_stream(st)
+                    outs = [torch.empty((edge,) * 3, dtype=torch.float32, device=f"cuda:{device}")
+                            for _ in range(k)] if op == DECODE else []
+                    gs.append(_Group(b, st, outs))
+                self.lanes[(edge, op)] = _Lane(edge, op, gs)
+        # filling order: decodes before encodes, small edges first
+        self.order = sorted(self.lanes.values(), key=lambda ln: (ln.op != DECODE, ln.edge))
         # resident compressed store: every source brick, compressed once
         self.store: Dict[int, List[Tuple[torch.Tensor, int]]] = {}
         self.store_bytes = 0
         for edge, bricks in sources.items():
-            lane = self.lanes[(edge, ENCODE)]
+            g = self.lanes[(edge, ENCODE)].groups[0]
+            k = len(g.batch.shapes)
             entries = []
-            for i in range(0, len(bricks), len(lane.batch.shapes)):
-                chunk = bricks[i:i + len(lane.batch.shapes)]
-                lane.batch.set_active(len(chunk))
-                lane.batch.compress(chunk)
+            for i in range(0, len(bricks), k):
+                chunk = bricks[i:i + k]
+                g.batch.set_active(len(chunk))
+                g.batch.compress(chunk)
                 for j in range(len(chunk)):
-                    words, bits = lane.batch.read_stream(j)
+                    words, bits = g.batch.read_stream(j)
                     t = torch.from_numpy(words.view(np.int32)).to(f"cuda:{device}")
                     entries.append((t, bits))
                     self.store_bytes += t.numel() * 4
             self.store[edge] = entries
         torch.cuda.synchronize()
+        validate_budget(self.store_bytes, list(slots), budget_bytes)
+        self.peak_admitted = 0
 
     def close(self):
         for lane in self.lanes.values():
-            lane.batch.close()
+            for g in lane.groups:
+                g.batch.close()
         self.inst.close()
 
     # ------------------------------------------------------------------ loop
-    @staticmethod
-    def _request_bytes(r: Request) -> int:
-        return r.edge ** 3 * 4
-
-    def _launch(self, lane: _Lane, used: int) -> int:
-        """Fills an idle lane from its queue within the budget; returns bytes admitted."""
-        k = len(lane.batch.shapes)
-        take = []
-        budget_left = self.budget - self.store_bytes - used
-        while lane.queue and len(take) < k and self._request_bytes(lane.queue[0]) <= budget_left:
-            r = lane.queue.pop(0)
-            budget_left -= self._request_bytes(r)
-            take.append(r)
-        if not take:
+    def _launch(self, lane: _Lane, g: _Group, used: int, now: float) -> int:
+        """Fills an idle codec from its lane's queue within the budget;
+        returns the bytes admitted."""
+        k = len(g.batch.shapes)
+        n = admit([request_bytes(r.edge) for r in list(lane.queue)[:k]], k, self.budget - self.store_bytes - used)
+        if n == 0:
             return 0
-        b = lane.batch
-        b.set_active(len(take))
+        take = [lane.queue.popleft() for _ in range(n)]
+        b = g.batch
+        b.set_active(n)
         if lane.op == ENCODE:
             b.compress([self.sources[lane.edge][r.brick] for r in take])
         else:
             entries = [self.store[lane.edge][r.brick] for r in take]
             b.load_streams([w for w, _ in entries], [bits for _, bits in entries])
-            b.decompress(lane.outs[:len(take)])
+            b.decompress(g.outs[:n])
         ev = torch.cuda.Event()
-        ev.record(lane.stream)
-        lane.event = ev
-        lane.inflight = take
-        lane.bytes_inflight = sum(self._request_bytes(r) for r in take)
-        return lane.bytes_inflight
+        ev.record(g.stream)
+        g.event = ev
+        g.inflight = take
+        for r in take:
+            r.launched = now
+        g.bytes_inflight = sum(request_bytes(r.edge) for r in take)
+        return g.bytes_inflight
 
-    def _complete(self, lane: _Lane, now: float) -> int:
-        freed = lane.bytes_inflight
-        for j, r in enumerate(lane.inflight):
+    def _complete(self, lane: _Lane, g: _Group, now: float) -> int:
+        freed = g.bytes_inflight
+        for j, r in enumerate(g.inflight):
             r.done = now
             if self.keep:
                 if lane.op == DECODE:
-                    with torch.cuda.stream(lane.stream):
-                        r.result = lane.outs[j].clone()
+                    with torch.cuda.stream(g.stream):
+                        r.result = g.outs[j].clone()
                 else:
-                    r.result = lane.batch.read_stream(j)
+                    r.result = g.batch.read_stream(j)
         if self.keep:
-            lane.stream.synchronize()
-        lane.inflight = []
-        lane.event = None
-        lane.bytes_inflight = 0
+            g.stream.synchronize()
+        g.inflight = []
+        g.event = None
+        g.bytes_inflight = 0
         return freed
 
     def run(self, requests: List[Request]) -> List[Request]:
@@ -162,18 +208,27 @@ class BrickServer:
                 self.lanes[(r.edge, r.op)].queue.append(r)
                 nxt += 1
             progressed = False
-            for lane in self.lanes.values():
-                if lane.event is not None and lane.event.query():
-                    t = time.perf_counter() - t0
-                    pending -= len(lane.inflight)
-                    used -= self._complete(lane, t)
-                    progressed = True
-                if lane.event is None and lane.queue:
-                    got = self._launch(lane, used)
-                    used += got
-                    progressed = progressed or got > 0
-            if not progressed and nxt < len(reqs) and all(l.event is None for l in self.lanes.values()) \
-                    and not any(l.queue for l in self.lanes.values()):
+            for lane in self.order:
+                for g in lane.groups:
+                    if g.event is not None and g.event.query():
+                        pending -= len(g.inflight)
+                        used -= self._complete(lane, g, time.perf_counter() - t0)
+                        progressed = True
+            busy = False
+            for lane in self.order:
+                for g in lane.groups:
+                    if g.event is None and lane.queue:
+                        got = self._launch(lane, g, used, time.perf_counter() - t0)
+                        used += got
+                        progressed = progressed or got > 0
+                    busy = busy or g.event is not None
+            self.peak_admitted = max(self.peak_admitted, used)
+            queued = any(lane.queue for lane in self.order)
+            if queued and not busy:
+                # nothing on the GPU and still nothing admitted: cannot happen
+                # with a validated budget; fail instead of spinning
+                raise RuntimeError("a queued request does not fit the HBM budget on an idle GPU")
+            if not progressed and not busy and not queued and nxt < len(reqs):
                 # idle until the next arrival
                 wait = reqs[nxt].arrival - (time.perf_counter() - t0)
                 if wait > 0:

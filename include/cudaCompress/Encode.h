@@ -23,7 +23,8 @@ bool encodeShutdown(Instance* pInstance);
 // - encode* appends to the bit stream(s) and returns once it is complete.
 // - decode* reads from the current position, advances it, and returns once
 //   the work is queued on the instance stream.
-// - decodeRLHuff outputs must be zeroed by the caller.
+// - decodeRLHuff outputs must be zeroed by the caller in the reference;
+//   here every output symbol is written, so zeroing is not needed.
 // - Symbol16 calls need log2HuffmanDistinctSymbolCountMax <= 16, Symbol32
 //   calls need > 16 (the reference silently misreads the buffers otherwise;
 //   here the call returns false).

@@ -106,9 +106,10 @@ int cc_encode_to_buffer(cc_instance* inst, int kind, int symbol_bytes, const voi
 
 /* Decode (decodeRLHuff / decodeHuff, Encode.h:29-52).  Stream i is read from
  * bit stream bs_index[i] (NULL = all from bit stream 0) of `bitstream_count`
- * host word buffers; positions advance in stream order.  Outputs of
- * decodeRLHuff must be zeroed by the caller (Encode.h:22); no output padding
- * is required.  Asynchronous on the instance stream: returns once the work is
+ * host word buffers; positions advance in stream order.  Every output
+ * symbol is written (the reference asks the caller to zero decodeRLHuff's
+ * outputs first, Encode.h:22; here that is not needed, and harmless); no
+ * output padding is required.  Asynchronous on the instance stream: returns once the work is
  * queued; host memory may be reused on return. */
 int cc_decode(cc_instance* inst, int kind, int symbol_bytes, const uint32_t* const* words,
               const uint32_t* bit_sizes, uint32_t* bit_positions, uint32_t bitstream_count,
@@ -168,7 +169,9 @@ int cc_dwt_float2d_forward_lowpass_only_from_byte(float* d_dst, float* d_buf, co
  * <= 2^20 floats (e.g. 128 x 128 x 64, or 1024 x 1024 in 2D); larger volumes
  * are rejected with CC_ERR_CAPACITY.  Runs on the current device; its first
  * call there resolves the array's device address (make it before any stream
- * capture).  Calls share the array: calls that overlap on the GPU race. */
+ * capture); that address is kept for the life of the process, so after a
+ * cudaDeviceReset on that device this entry point must not be called again.
+ * Calls share the array: calls that overlap on the GPU race. */
 int cc_dwt_float_forward_static(float* d_dst, const float* d_src, int size_x, int size_y, int size_z,
                                 int src_channel_count, int dst_row_pitch, int dst_slice_pitch, int src_row_pitch,
                                 int src_slice_pitch, void* stream);

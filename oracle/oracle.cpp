@@ -22,6 +22,8 @@
 #include <queue>
 #include <vector>
 
+#include <omp.h>
+
 typedef uint32_t u32;
 typedef uint16_t u16;
 typedef int16_t i16;
@@ -722,6 +724,9 @@ void orc_dwt_double_fwd(const double* src, double* dst, long nx, long ny, long n
 void orc_dwt_double_inv(const double* src, double* dst, long nx, long ny, long nz) { dwtFloat(src, dst, nx, ny, nz, true); }
 void orc_dwt_int_fwd(const i16* src, i16* dst, long nx, long ny, long nz) { dwtInt(src, dst, nx, ny, nz, false); }
 void orc_dwt_int_inv(const i16* src, i16* dst, long nx, long ny, long nz) { dwtInt(src, dst, nx, ny, nz, true); }
+
+// Threads of the OpenMP loops (the CPU baseline's single- and all-core runs).
+void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 
 // getMaxAbs (util/Quantize.cu:355-361): reduceArray with OperatorMax over
 // FunctorAbs (reduce/reduce_app.cui:122-142, tools/Operator.h:31-52,

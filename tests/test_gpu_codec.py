@@ -215,12 +215,30 @@ def test_decode_rlhuff_roundtrip(oracle, inst, kind):
     streams = symbol_streams(kind, 4, n, seed=77)
     ref_words, ref_bits, _ = oracle.encode(0, streams)
     bs = cc.BitStream(ref_words, ref_bits)
-    outs = [torch.zeros(n, dtype=torch.int16, device="cuda") for _ in range(4)]
+    # outputs hold garbage: the decoder writes every symbol (zeros included)
+    outs = [torch.full((n,), -1, dtype=torch.int16, device="cuda") for _ in range(4)]
     assert cc.decode_rlhuff(inst, bs, outs, n), cc.last_error()
     assert cc.decode_status(inst) == 0, cc.last_error()
     for i in range(4):
         assert np.array_equal(host(outs[i]).view(np.uint16), streams[i])
     assert bs.pos == ref_bits
+
+
+def test_decode_rlhuff_long_runs_into_garbage(oracle, inst):
+    """Zero runs far longer than a coding block's shared-memory stage (the
+    in-place fill path), an all-zero stream and trailing zeros, decoded into
+    outputs full of garbage."""
+    n = 1 << 18
+    streams = np.zeros((3, n), np.uint16)
+    streams[0, [5, 70000, 70001, 200000]] = [3, 9, 1, 4]      # runs of ~70k and ~130k zeros
+    streams[2, ::4099] = 7                                      # runs of 4098 zeros
+    ref_words, ref_bits, _ = oracle.encode(0, streams)
+    bs = cc.BitStream(ref_words, ref_bits)
+    outs = [torch.full((n,), -1, dtype=torch.int16, device="cuda") for _ in range(3)]
+    assert cc.decode_rlhuff(inst, bs, outs, n), cc.last_error()
+    assert cc.decode_status(inst) == 0, cc.last_error()
+    for i in range(3):
+        assert np.array_equal(host(outs[i]).view(np.uint16), streams[i]), i
 
 
 @pytest.mark.parametrize("kind", ["dense", "laplace", "single"])

@@ -66,3 +66,29 @@ def test_latency_stats(server):
     done = server.run(reqs)
     st = serving.latency_stats(done)
     assert st["requests"] == 40 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_budget_defers_requests_and_results_stay_equal():
+    """A budget that holds the resident store plus eight 32^3 requests: forty
+    32^3 decodes arriving at once run in launches the budget cuts short,
+    never more than the budget admitted, each result equal to the brick
+    decoded alone."""
+    src = fields.turbulence_field(64, 128, 16, seed=1007)
+    sources = {32: [torch.from_numpy(np.ascontiguousarray(src[i * 8:i * 8 + 32, :32, :32])).cuda() for i in range(4)],
+               64: [torch.from_numpy(src.copy()).cuda()]}
+    probe = serving.BrickServer(0, sources, {32: 6, 64: 1}, levels=3, q0=0.02)
+    store = probe.store_bytes
+    probe.close()
+    budget = store + serving.request_bytes(64)          # = eight 32^3 requests
+    with pytest.raises(ValueError):
+        serving.BrickServer(0, sources, {32: 6, 64: 1}, levels=3, q0=0.02, budget_bytes=budget - 1)
+    s = serving.BrickServer(0, sources, {32: 6, 64: 1}, levels=3, q0=0.02, budget_bytes=budget, keep_results=True)
+    try:
+        reqs = [serving.Request(i, serving.DECODE, 32, 0.0, i % 4) for i in range(40)]
+        done = s.run(reqs)
+        assert all(r.done > 0 for r in done)
+        assert 0 < s.peak_admitted <= budget - s.store_bytes
+        assert s.peak_admitted == 8 * serving.request_bytes(32)  # the budget, not the 12 slots, bound the run
+        check(s, done)
+    finally:
+        s.close()
