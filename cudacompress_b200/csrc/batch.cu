@@ -62,6 +62,8 @@ struct cc_volume_batch {
     struct Rows { const ccb::BRowDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
     struct Cols { const ccb::BColDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
     struct Quant { const ccb::BQuantDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    struct Levels { const ccb::BLevelDesc* d; const ccb::u32* map; ccb::u32 n, ctas; std::vector<ccb::u32> descEnd, ctaEnd; };
+    std::vector<Levels> fwdLevel;              // per level: the fused forward pass
     std::vector<Rows> fwdRows, invRows;        // per level
     std::vector<Cols> fwdY, fwdZ, invZ, invY;  // per level
     Quant quant{}, dequantLP{};
@@ -114,6 +116,15 @@ void addCols(std::vector<BColDesc>& v, u32& ctas, BColDesc d) {
     d.tilesA = u32(ceilDiv(d.na, kBColTileA));
     d.ctaOff = ctas;
     ctas += d.tilesX * d.tilesA * u32(d.nc);
+    v.push_back(d);
+}
+
+void addLevel(std::vector<BLevelDesc>& v, u32& ctas, BLevelDesc d) {
+    d.tilesX = int(ceilDiv(d.nx, kLvTX));
+    d.tilesY = int(ceilDiv(d.ny, kLvTY));
+    d.chunksZ = int(ceilDiv(d.nz, kLvZC));
+    d.ctaOff = ctas;
+    ctas += u32(d.tilesX) * u32(d.tilesY) * u32(d.chunksZ);
     v.push_back(d);
 }
 
@@ -271,13 +282,10 @@ static int batchEnqueueCompress(cc_volume_batch* b) {
     const u32 k = b->active;
     u32 nd, ctas;
     for (u32 l = 0; l < b->levels; ++l) {
+        // one fused pass per level: X, Y, Z filters and the deadzone quantization
         SectionTimer t(I, "batch.dwt_forward", st);
-        prefixOf(b->fwdRows[l], k, nd, ctas);
-        launchBatchRows(b->fwdRows[l].d, b->fwdRows[l].map, ctas, false, b->inTab, b->outTab, st);
-        prefixOf(b->fwdY[l], k, nd, ctas);
-        launchBatchCols(b->fwdY[l].d, b->fwdY[l].map, ctas, false, false, st);
-        prefixOf(b->fwdZ[l], k, nd, ctas);
-        launchBatchCols(b->fwdZ[l].d, b->fwdZ[l].map, ctas, false, false, st, true);   // + deadzone quantization
+        prefixOf(b->fwdLevel[l], k, nd, ctas);
+        launchBatchLevelFwd(b->fwdLevel[l].d, b->fwdLevel[l].map, ctas, b->inTab, st);
     }
     // fork: the lowpass streams on the side stream
     cc_instance* ILP = b->ILP;
@@ -519,6 +527,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     auto t1 = [&](u32 v) { return reinterpret_cast<float*>(t1At) + tOff[v]; };
     auto t2 = [&](u32 v) { return reinterpret_cast<float*>(t2At) + tOff[v]; };
     auto sy = [&](u32 v) { return reinterpret_cast<u16*>(symAt) + symOff[v]; };
+    std::vector<std::vector<BLevelDesc>> fl(L);
+    std::vector<u32> flC(L, 0);
     std::vector<std::vector<BRowDesc>> fr(L), ir(L);
     std::vector<std::vector<BColDesc>> fy(L), fz(L), iz(L), iy(L);
     std::vector<u32> frC(L, 0), irC(L, 0), fyC(L, 0), fzC(L, 0), izC(L, 0), iyC(L, 0);
@@ -532,6 +542,24 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
         const u32 X = b->nx[v], Y = b->ny[v], Z = b->nz[v];
         for (u32 l = 0; l < L; ++l) {
             const int sx = int(X >> l), syz = int(Y >> l), sz = int(Z >> l);
+            // the fused forward level: input (level 0: the caller's volume;
+            // else the LLL octant of level l-1, tight in lev(l-1)) -> the
+            // highpass symbols and the LLL octant, tight in lev(l) (or the
+            // lowpass band's symbols at the coarsest level)
+            BLevelDesc fd{};
+            fd.vol = int(v);
+            fd.src = l == 0 ? nullptr : lev(l - 1, v);
+            fd.nx = sx; fd.ny = syz; fd.nz = sz;
+            fd.srcRow = sx;
+            fd.srcSlice = sx * syz;
+            fd.lpOut = lev(l, v);
+            fd.symOut = sy(v) + sl[v].level[l];
+            fd.lpSymOut = sy(v) + sl[v].lp;
+            fd.bandStride = sl[v].bandStride[l];
+            fd.inv = 1.0f / (b->q0[v] / float(1u << l));              // Quantize.cu:90: reciprocal on the host
+            fd.invLP = 1.0f / (b->q0[v] / float(1u << (L - 1)));
+            fd.lastLevel = l + 1 == L ? 1 : 0;
+            addLevel(fl[l], flC[l], fd);
             // X: input (level 0: the caller's volume, tight; else the LLL octant of level l-1) -> t1
             BRowDesc r{};
             r.vol = int(v);
@@ -633,9 +661,10 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
 
     // ---- device plan ----
     auto bytesOf = [](size_t n, size_t e) { return n * e; };
-    std::vector<size_t> frAt(L), irAt(L), fyAt(L), fzAt(L), izAt(L), iyAt(L);
+    std::vector<size_t> flAt(L), frAt(L), irAt(L), fyAt(L), fzAt(L), izAt(L), iyAt(L);
     A.off = alignUp(A.off, 256);
     for (u32 l = 0; l < L; ++l) {
+        flAt[l] = A.take(bytesOf(fl[l].size(), sizeof(BLevelDesc)), 64);
         frAt[l] = A.take(bytesOf(fr[l].size(), sizeof(BRowDesc)), 64);
         irAt[l] = A.take(bytesOf(ir[l].size(), sizeof(BRowDesc)), 64);
         fyAt[l] = A.take(bytesOf(fy[l].size(), sizeof(BColDesc)), 64);
@@ -653,8 +682,9 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
         maps.push_back(std::move(m));
         return maps.size() - 1;
     };
-    std::vector<size_t> frMap(L), irMap(L), fyMap(L), fzMap(L), izMap(L), iyMap(L);
+    std::vector<size_t> flMap(L), frMap(L), irMap(L), fyMap(L), fzMap(L), izMap(L), iyMap(L);
     for (u32 l = 0; l < L; ++l) {
+        flMap[l] = addMap(ctaMapOf(fl[l], flC[l]));
         frMap[l] = addMap(ctaMapOf(fr[l], frC[l]));
         irMap[l] = addMap(ctaMapOf(ir[l], irC[l]));
         fyMap[l] = addMap(ctaMapOf(fy[l], fyC[l]));
@@ -691,6 +721,12 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     auto rebaseF = [&](const float* p) -> float* { return p ? reinterpret_cast<float*>(base + reinterpret_cast<uintptr_t>(p)) : nullptr; };
     auto rebaseS = [&](const u16* p) -> u16* { return p ? reinterpret_cast<u16*>(base + reinterpret_cast<uintptr_t>(p)) : nullptr; };
     for (u32 l = 0; l < L; ++l) {
+        for (auto& d : fl[l]) {
+            d.src = rebaseF(d.src);
+            d.lpOut = rebaseF(d.lpOut);
+            d.symOut = rebaseS(d.symOut);
+            d.lpSymOut = rebaseS(d.lpSymOut);
+        }
         for (auto& d : fr[l]) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); }
         for (auto& d : ir[l]) { d.src = rebaseF(d.src); d.dst = rebaseF(d.dst); }
         for (auto* vv : {&fy[l], &fz[l], &iz[l], &iy[l]})
@@ -732,7 +768,8 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     };
     e = cudaMemset(b->mem, 0, b->memBytes);
     for (u32 l = 0; l < L && e == cudaSuccess; ++l) {
-        e = up(frAt[l], fr[l].data(), fr[l].size() * sizeof(BRowDesc));
+        e = up(flAt[l], fl[l].data(), fl[l].size() * sizeof(BLevelDesc));
+        if (e == cudaSuccess) e = up(frAt[l], fr[l].data(), fr[l].size() * sizeof(BRowDesc));
         if (e == cudaSuccess) e = up(irAt[l], ir[l].data(), ir[l].size() * sizeof(BRowDesc));
         if (e == cudaSuccess) e = up(fyAt[l], fy[l].data(), fy[l].size() * sizeof(BColDesc));
         if (e == cudaSuccess) e = up(fzAt[l], fz[l].data(), fz[l].size() * sizeof(BColDesc));
@@ -751,9 +788,11 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->extEvent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { cc_volume_batch_destroy(b); return cudaFail(e, "volume batch set-up"); }
+    b->fwdLevel.resize(L);
     b->fwdRows.resize(L); b->invRows.resize(L); b->fwdY.resize(L); b->fwdZ.resize(L); b->invZ.resize(L); b->invY.resize(L);
     auto mapPtr = [&](size_t m) { return reinterpret_cast<const u32*>(base + mapAt[m]); };
     for (u32 l = 0; l < L; ++l) {
+        b->fwdLevel[l] = {reinterpret_cast<const BLevelDesc*>(base + flAt[l]), mapPtr(flMap[l]), u32(fl[l].size()), flC[l]};
         b->fwdRows[l] = {reinterpret_cast<const BRowDesc*>(base + frAt[l]), mapPtr(frMap[l]), u32(fr[l].size()), frC[l]};
         b->invRows[l] = {reinterpret_cast<const BRowDesc*>(base + irAt[l]), mapPtr(irMap[l]), u32(ir[l].size()), irC[l]};
         b->fwdY[l] = {reinterpret_cast<const BColDesc*>(base + fyAt[l]), mapPtr(fyMap[l]), u32(fy[l].size()), fyC[l]};
@@ -774,6 +813,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
         }
     };
     for (u32 l = 0; l < L; ++l) {
+        prefix(b->fwdLevel[l], fl[l], 1);
         prefix(b->fwdRows[l], fr[l], 1);
         prefix(b->invRows[l], ir[l], 1);
         prefix(b->fwdY[l], fy[l], 1);

@@ -58,6 +58,29 @@ struct BQuantDesc {
     u32 ctaOff;             // kBQuantPerCta elements per CTA
 };
 
+// One forward level in one pass (k_bLevelFwd): a CTA owns kLvTX x kLvTY
+// outputs of the level's XY plane (positions in the filtering domain) and
+// kLvZC output slices; it streams the input slices through X and Y filters
+// in shared memory and a 9-slice Z window in registers, and stores the seven
+// highpass octants as quantized symbols and the LLL octant as float (tight
+// hx x hy x hz, the next level's input) - or, at the coarsest level, as
+// symbols too.
+struct BLevelDesc {
+    const float* src;       // level input; nullptr: the volume's entry of the input pointer table
+    int vol;
+    int nx, ny, nz;         // level extents (even, >= 8)
+    int srcRow, srcSlice;
+    float* lpOut;           // LLL octant, tight (not the coarsest level)
+    u16* symOut;            // highpass octant b at symOut + (b - 1) * bandStride, tight hx x hy x hz
+    u16* lpSymOut;          // coarsest level: the LLL octant's symbols, tight
+    u64 bandStride;
+    float inv, invLP;       // reciprocal quantization steps (highpass, lowpass band)
+    int lastLevel;
+    int tilesX, tilesY, chunksZ;
+    u32 ctaOff;
+};
+constexpr int kLvTX = 64, kLvTY = 16, kLvZC = 32;
+
 constexpr int kBRowOutputs = 4096;    // outputs per row-pass CTA
 constexpr int kBRowMaxWidth = 2048;   // row tile width
 constexpr int kBRowMaxRows = 128;     // rows per row-pass CTA
@@ -72,6 +95,7 @@ void launchBatchRows(const BRowDesc* d, const u32* map, u32 ctas, bool inverse, 
 void launchBatchCols(const BColDesc* d, const u32* map, u32 ctas, bool inverse, bool fromSymbols, cudaStream_t st,
                      bool quantizeStore = false);
 void launchBatchQuant(const BQuantDesc* d, const u32* map, u32 ctas, bool dequantize, cudaStream_t st);
+void launchBatchLevelFwd(const BLevelDesc* d, const u32* map, u32 ctas, const float* const* inTab, cudaStream_t st);
 
 // Row tiling of an X pass over an nx-wide level: tile width, rows per CTA.
 inline void batchRowTiling(int nx, int& W, int& R) {

@@ -50,6 +50,44 @@ __device__ __forceinline__ float fir9c(const float* v) {
     return sum;
 }
 
+// Two outputs of one parity at once, their windows at a and b: Blackwell's
+// packed fma.rn.f32x2 does both lanes' fmaf in one instruction, each lane
+// rounded exactly as fir9c's scalar chain.
+template <bool kInverse, int kParity>
+__device__ __forceinline__ float2 fir9x2(const float* a, const float* b) {
+    constexpr float kF[2][9] = {
+        {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+        {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+    constexpr float kI[2][9] = {
+        {0.0f, 0.0337282f, -0.0575435f, -0.5337281f, 1.1150871f, -0.5337281f, -0.0575435f, 0.0337282f, 0.0f},
+        {0.0534975f, -0.0912718f, -0.1564465f, 0.5912718f, 1.2058980f, 0.5912718f, -0.1564465f, -0.0912718f, 0.0534975f}};
+    float2 sum = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const float c = kInverse ? kI[kParity][i] : kF[kParity][i];
+        sum = __ffma2_rn(make_float2(c, c), make_float2(a[i], b[i]), sum);
+    }
+    return sum;
+}
+
+// The same over a window of value pairs (lane x: one output, lane y: the other).
+template <bool kInverse, int kParity>
+__device__ __forceinline__ float2 fir9p(const float2* w) {
+    constexpr float kF[2][9] = {
+        {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+        {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+    constexpr float kI[2][9] = {
+        {0.0f, 0.0337282f, -0.0575435f, -0.5337281f, 1.1150871f, -0.5337281f, -0.0575435f, 0.0337282f, 0.0f},
+        {0.0534975f, -0.0912718f, -0.1564465f, 0.5912718f, 1.2058980f, 0.5912718f, -0.1564465f, -0.0912718f, 0.0534975f}};
+    float2 sum = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const float c = kInverse ? kI[kParity][i] : kF[kParity][i];
+        sum = __ffma2_rn(make_float2(c, c), w[i], sum);
+    }
+    return sum;
+}
+
 template <bool kInverse>
 __device__ __forceinline__ float fir9(const float* v, int parity) {
     const float* c = kInverse ? c_inv[parity] : c_fwd[parity];
@@ -1008,6 +1046,208 @@ __global__ void __launch_bounds__(256) k_bQuant(const BQuantDesc* __restrict__ d
                 if (eg[g] + u32(i) < total) D.sym[eg[g] + u32(i)] = sv[i];
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// One forward level in one pass (BLevelDesc).  For each input slice of the
+// CTA's Z chunk (with 4 slices of mirrored halo each side) the tile's rows
+// y0-4 .. y0+TY+3 and columns x0-4 .. x0+TX+3 are staged in shared memory,
+// filtered along X (outputs x0 .. x0+TX-1 of every staged row), then along Y
+// (outputs y0 .. y0+TY-1); each thread keeps, for its column and its four
+// rows, the Y outputs of the last nine slices in registers, and once an
+// output slice's nine inputs are in it filters along Z, quantizes and stores.
+// The taps and fmaf chains are those of the separate X, Y and Z passes, in
+// that order, so the coefficients - and symbols - are bit-identical.  The
+// next slice's loads are issued before the current slice is filtered.
+// ---------------------------------------------------------------------------
+constexpr int kLvRows = kLvTY + 8;               // staged rows
+constexpr int kLvCols = kLvTX + 8;               // staged columns
+constexpr int kLvStage = kLvRows * kLvCols;
+constexpr int kLvLoads = (kLvStage + 255) / 256;  // staged elements per thread
+static_assert(kLvTX == 64 && kLvTY == 16, "256 threads: one column and four rows of Y/Z outputs each");
+
+// Z outputs of output slice i - 8 from the ring (slices i-8 .. i-1, taps
+// 0..7) and the newest slice i (tap 8), two outputs per packed fma.
+template <int kParity>
+__device__ __forceinline__ void zRing(const float2 (*ring)[2][256], int i, float2 n02, float2 n13, float2& v02,
+                                      float2& v13) {
+    constexpr float kF[2][9] = {
+        {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+        {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+    const int t = int(threadIdx.x);
+    float2 a = make_float2(0.0f, 0.0f), b = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int slot = (i + q) & 7;   // slice i - 8 + q
+        const float c = kF[kParity][q];
+        a = __ffma2_rn(make_float2(c, c), ring[slot][0][t], a);
+        b = __ffma2_rn(make_float2(c, c), ring[slot][1][t], b);
+    }
+    const float c8 = kF[kParity][8];
+    v02 = __ffma2_rn(make_float2(c8, c8), n02, a);
+    v13 = __ffma2_rn(make_float2(c8, c8), n13, b);
+}
+
+__global__ void __launch_bounds__(256, 4) k_bLevelFwd(const BLevelDesc* __restrict__ descs,
+                                                     const u32* __restrict__ map, const float* const* inTab) {
+    __shared__ __align__(16) float sIn[kLvRows * kLvCols];
+    __shared__ __align__(16) float sX[kLvRows * kLvTX];
+    // each thread's Y outputs of the last eight slices, rows (0, 2) and (1, 3)
+    // as pairs: a ring indexed by slice & 7 (thread-private, no barriers)
+    __shared__ float2 sZ[8][2][256];
+    // the descriptor's fields in registers (the output stores could alias it)
+    const BLevelDesc& Dg = descs[map[blockIdx.x]];
+    const float* const src = Dg.src ? Dg.src : inTab[Dg.vol];
+    float* const lpOut = Dg.lpOut;
+    u16* const symOut = Dg.symOut;
+    u16* const lpSymOut = Dg.lpSymOut;
+    const u64 bandStride = Dg.bandStride;
+    const float inv = Dg.inv, invLP = Dg.invLP;
+    const bool lastLevel = Dg.lastLevel != 0;
+    const int srcRow = Dg.srcRow;
+    const BLevelDesc& D = Dg;
+    const u32 local = blockIdx.x - D.ctaOff;
+    const int tilesX = D.tilesX, tilesY = D.tilesY;
+    const int tX = int(local % u32(tilesX));
+    const u32 rest = local / u32(tilesX);
+    const int tY = int(rest % u32(tilesY)), cZ = int(rest / u32(tilesY));
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    const int x0 = tX * kLvTX, y0 = tY * kLvTY, z0 = cZ * kLvZC;
+    const int TXe = min(kLvTX, nx - x0), TYe = min(kLvTY, ny - y0), ZCe = min(kLvZC, nz - z0);
+    const int colsE = TXe + 8, rowsE = TYe + 8;
+    const int tid = int(threadIdx.x);
+    const size_t srcSlice = size_t(D.srcSlice);
+    // Staging.  Interior tiles (the columns need no mirroring, whole tile
+    // width, 16-byte aligned rows) move 18 float4 per staged row; other
+    // tiles move single floats with mirrored indices.  Per thread: the source
+    // offsets within a slice of its staged elements (-1: not needed).
+    const bool vec = x0 >= 4 && TXe == kLvTX && x0 + kLvTX + 4 <= nx && (srcRow & 3) == 0 &&
+                     (srcSlice & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;   // CTA-uniform
+    constexpr int kVecPerRow = kLvCols / 4;                            // 18
+    constexpr int kVecLoads = (kLvRows * kVecPerRow + 255) / 256;      // 2
+    int soff[kLvLoads];
+#pragma unroll
+    for (int k = 0; k < kLvLoads; ++k) {
+        soff[k] = -1;
+        if (vec) {
+            const int e = tid + 256 * k;
+            const int r = e / kVecPerRow, q = e - r * kVecPerRow;
+            if (k < kVecLoads && e < kLvRows * kVecPerRow && r < rowsE)
+                soff[k] = mirrorIdx(y0 - 4 + r, ny) * srcRow + x0 - 4 + 4 * q;
+        } else {
+            const int e = tid + 256 * k;
+            const int r = e / kLvCols, cc = e - r * kLvCols;
+            if (e < kLvStage && r < rowsE && cc < colsE)
+                soff[k] = mirrorIdx(y0 - 4 + r, ny) * srcRow + mirrorIdx(x0 - 4 + cc, nx);
+        }
+    }
+    float pre[kLvLoads];
+    float4 pre4[kVecLoads];
+    auto fetch = [&](int i) {
+        const float* sl = src + size_t(mirrorIdx(z0 - 4 + i, nz)) * srcSlice;
+        if (vec) {
+#pragma unroll
+            for (int k = 0; k < kVecLoads; ++k)
+                pre4[k] = soff[k] >= 0 ? *reinterpret_cast<const float4*>(sl + soff[k]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kLvLoads; ++k) pre[k] = soff[k] >= 0 ? sl[soff[k]] : 0.0f;
+        }
+    };
+    // the Y and Z outputs of this thread: column c, rows 4 yg .. 4 yg + 3;
+    // the two warps of a row group take the even and the odd columns, so
+    // that a warp's outputs share their octant (no divergent stores)
+    const int c = 2 * (tid & 31) + ((tid >> 5) & 1), yg = tid >> 6;
+    const int hx = nx >> 1, hy = ny >> 1;
+    const bool colOk = c < TXe;
+    // store addressing of the thread's outputs: octant bits of x and y
+    // (rows 4 yg + j: y parity = j & 1) and the in-plane offsets
+    const int x = x0 + c;
+    const int bxy[2] = {x & 1, (x & 1) + 2};
+    u32 xyOff[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) xyOff[j] = u32((y0 + 4 * yg + j) >> 1) * u32(hx) + u32(x >> 1);
+    const u64 plane = u64(hx) * u64(hy);
+
+    const int nSlices = ZCe + 8;
+    fetch(0);
+    for (int i = 0; i < nSlices; ++i) {
+        if (vec) {
+#pragma unroll
+            for (int k = 0; k < kVecLoads; ++k) {
+                const int e = tid + 256 * k;
+                if (e < kLvRows * kVecPerRow) reinterpret_cast<float4*>(sIn)[e] = pre4[k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kLvLoads; ++k) {
+                const int e = tid + 256 * k;
+                if (e < kLvStage) sIn[e] = pre[k];
+            }
+        }
+        __syncthreads();
+        if (i + 1 < nSlices) fetch(i + 1);
+        // X: 8 consecutive outputs of one staged row per task (24 rows x 8 groups)
+        if (tid < kLvRows * (kLvTX / 8)) {
+            const int r = tid >> 3, g = tid & 7;
+            if (r < rowsE && 8 * g < TXe) {
+                float w[16];
+                const float4* s4 = reinterpret_cast<const float4*>(sIn + r * kLvCols + 8 * g);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 v = s4[q];
+                    w[4 * q] = v.x; w[4 * q + 1] = v.y; w[4 * q + 2] = v.z; w[4 * q + 3] = v.w;
+                }
+                float4* o4 = reinterpret_cast<float4*>(sX + r * kLvTX + 8 * g);
+                o4[0] = make_float4(fir9c<false, 0>(w), fir9c<false, 1>(w + 1), fir9c<false, 0>(w + 2),
+                                    fir9c<false, 1>(w + 3));
+                o4[1] = make_float4(fir9c<false, 0>(w + 4), fir9c<false, 1>(w + 5), fir9c<false, 0>(w + 6),
+                                    fir9c<false, 1>(w + 7));
+            }
+        }
+        __syncthreads();
+        // Y: four outputs of column c from twelve X outputs (rows 0, 2 and 1, 3 paired)
+        float2 n02, n13;
+        {
+            float yw[12];
+#pragma unroll
+            for (int q = 0; q < 12; ++q) yw[q] = sX[(4 * yg + q) * kLvTX + c];
+            n02 = make_float2(fir9c<false, 0>(yw), fir9c<false, 0>(yw + 2));
+            n13 = make_float2(fir9c<false, 1>(yw + 1), fir9c<false, 1>(yw + 3));
+        }
+        // Z: output slice z once its nine input slices are in
+        if (i >= 8 && colOk) {
+            const int z = z0 + i - 8;
+            float2 v02, v13;
+            if (z & 1) zRing<1>(sZ, i, n02, n13, v02, v13);
+            else zRing<0>(sZ, i, n02, n13, v02, v13);
+            const float v[4] = {v02.x, v13.x, v02.y, v13.y};
+            const u64 zOff = u64(z >> 1) * plane;
+            const int bz = (z & 1) << 2;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (4 * yg + j < TYe) {
+                    const int b = bxy[j & 1] + bz;
+                    const u64 li = zOff + xyOff[j];
+                    if (b == 0) {
+                        if (lastLevel) lpSymOut[li] = u16(symbolizeI(int(v[j] * invLP)));
+                        else lpOut[li] = v[j];
+                    } else {
+                        symOut[u64(b - 1) * bandStride + li] = u16(symbolizeI(int(v[j] * inv)));
+                    }
+                }
+            }
+        }
+        // the newest slice replaces the oldest, just used
+        sZ[i & 7][0][tid] = n02;
+        sZ[i & 7][1][tid] = n13;
+    }
+}
+
+void launchBatchLevelFwd(const BLevelDesc* d, const u32* map, u32 ctas, const float* const* inTab, cudaStream_t st) {
+    if (!ctas) return;
+    k_bLevelFwd<<<ctas, 256, 0, st>>>(d, map, inTab);
+    countLaunch();
 }
 
 void launchBatchRows(const BRowDesc* d, const u32* map, u32 ctas, bool inverse, const float* const* inTab,
