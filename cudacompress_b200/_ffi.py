@@ -23,6 +23,7 @@ _SIGS = {
     "cc_last_error": (ctypes.c_char_p, []),
     "cc_version": (ctypes.c_char_p, []),
     "cc_kernel_launches": (c_u64, []),
+    "cc_inject_allocation_failures": (c_int, [c_int, c_int]),
     "cc_create_instance": (c_int, [ctypes.POINTER(c_vp), c_int, c_u32, c_u32, c_u32, c_u32]),
     "cc_destroy_instance": (None, [c_vp]),
     "cc_get_instance_cuda_device": (c_int, [c_vp]),

@@ -180,7 +180,7 @@ def encode_huff(inst: Instance, bs: BitStream, streams: Sequence[torch.Tensor], 
 
 
 def decode_rlhuff(inst: Instance, bs: BitStream, outs: Sequence[torch.Tensor], symbol_count_per_block: int) -> bool:
-    """decodeRLHuff (Encode.h:29); outputs must be zeroed."""
+    """decodeRLHuff (Encode.h:29); every output symbol is written (no zeroing needed)."""
     return _decode(inst, RLHUFF, bs, outs, symbol_count_per_block)
 
 

@@ -714,7 +714,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     const size_t encAt = A.take(b->enc.bytes, 256), encLPAt = A.take(b->encLP.bytes, 256);
     const size_t decAt = A.take(b->dec.bytes, 256);
     b->memBytes = alignUp(A.off, 256);
-    cudaError_t e = cudaMalloc(&b->mem, b->memBytes);
+    cudaError_t e = deviceAlloc(reinterpret_cast<void**>(&b->mem), b->memBytes);
     if (e != cudaSuccess) { b->mem = nullptr; cc_volume_batch_destroy(b); return cudaFail(e, "cudaMalloc(volume batch)"); }
     char* base = b->mem;
     // rebase the device pointers written as offsets
@@ -782,9 +782,9 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
     if (e == cudaSuccess) e = up(encAt, encHost.data(), b->enc.bytes);
     if (e == cudaSuccess) e = up(encLPAt, encLPHost.data(), b->encLP.bytes);
     if (e == cudaSuccess) e = up(decAt, decHost.data(), b->dec.bytes);
-    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&b->hostPlan), sizeof(void*) * count, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = pinnedAlloc(reinterpret_cast<void**>(&b->hostPlan), sizeof(void*) * count);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->tabEvent, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&b->hostExt), 2 * sizeof(u64) * count, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = pinnedAlloc(reinterpret_cast<void**>(&b->hostExt), 2 * sizeof(u64) * count);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->extEvent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { cc_volume_batch_destroy(b); return cudaFail(e, "volume batch set-up"); }

@@ -17,6 +17,12 @@ void countLaunch(unsigned n = 1);
 void setError(const char* fmt, ...);
 int cudaFail(cudaError_t e, const char* what);
 
+// Every device (cudaMalloc) and page-locked host (cudaHostAlloc) allocation
+// of the library goes through these, so that a test can make chosen ones
+// fail as an out-of-memory would (cc_inject_allocation_failures).
+cudaError_t deviceAlloc(void** p, size_t bytes);
+cudaError_t pinnedAlloc(void** p, size_t bytes);
+
 // Makes `device` current for the scope of an entry point and restores the
 // caller's current device on exit (the reference's calls leave it alone).
 struct DeviceGuard {

@@ -29,8 +29,40 @@ void setError(const char* fmt, ...) {
     g_lastError = buf;
 }
 
+// Allocation fault injection (cc_inject_allocation_failures): the next
+// `skip` allocations succeed, then `fail` of them report
+// cudaErrorMemoryAllocation without allocating.
+static std::atomic<int> g_allocSkip{0}, g_allocFail{0};
+
+static bool injectedFailure() {
+    if (g_allocFail.load(std::memory_order_relaxed) <= 0) return false;
+    int s = g_allocSkip.load();
+    while (s > 0) {
+        if (g_allocSkip.compare_exchange_weak(s, s - 1)) return false;
+    }
+    int f = g_allocFail.load();
+    while (f > 0) {
+        if (g_allocFail.compare_exchange_weak(f, f - 1)) return true;
+    }
+    return false;
+}
+
+cudaError_t deviceAlloc(void** p, size_t bytes) {
+    if (injectedFailure()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t pinnedAlloc(void** p, size_t bytes) {
+    if (injectedFailure()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+}
+
 int cudaFail(cudaError_t e, const char* what) {
     setError("%s: %s", what, cudaGetErrorString(e));
+    // the error is reported here: clear it from the runtime's per-thread
+    // last error (a failed allocation is not sticky), so that a later call's
+    // launch check does not report it again
+    (void)cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? CC_ERR_OUT_OF_MEMORY : CC_ERR_CUDA;
 }
 
@@ -54,7 +86,7 @@ int ensurePipelineWork(cc_instance* I, size_t bytes) {
     if (I->pipeWork) cudaFree(I->pipeWork);
     I->pipeWork = nullptr;
     I->pipeWorkBytes = 0;
-    cudaError_t e = cudaMalloc(&I->pipeWork, bytes);
+    cudaError_t e = deviceAlloc(reinterpret_cast<void**>(&I->pipeWork), bytes);
     if (e != cudaSuccess) return cudaFail(e, "cudaMalloc(pipeline workspace)");
     I->pipeWorkBytes = bytes;
     return CC_OK;
@@ -234,13 +266,13 @@ int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 el
 
     size_t bytes = 0;
     layoutArena(I, nullptr, &bytes);
-    if ((e = cudaMalloc(&I->arena, bytes)) != cudaSuccess) { delete I; return cudaFail(e, "cudaMalloc(instance arena)"); }
+    if ((e = deviceAlloc(reinterpret_cast<void**>(&I->arena), bytes)) != cudaSuccess) { delete I; return cudaFail(e, "cudaMalloc(instance arena)"); }
     I->arenaBytes = bytes;
     layoutArena(I, I->arena, &bytes);
     cudaMemset(I->arena, 0, bytes);
 
     for (int i = 0; i < cc_instance::kRing; ++i) {
-        if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostRing[i]), I->hostRingBytes, cudaHostAllocDefault)) != cudaSuccess) {
+        if ((e = pinnedAlloc(reinterpret_cast<void**>(&I->hostRing[i]), I->hostRingBytes)) != cudaSuccess) {
             cc_destroy_instance(I);
             return cudaFail(e, "cudaHostAlloc(ring)");
         }
@@ -248,11 +280,11 @@ int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 el
         cudaEventRecord(I->ringEvent[i], 0);
     }
     I->hostDownBytes = alignUp(u64(I->capStreams) * sizeof(SegmentLayout) + 256, 4096);
-    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostDown), I->hostDownBytes, cudaHostAllocDefault)) != cudaSuccess) {
+    if ((e = pinnedAlloc(reinterpret_cast<void**>(&I->hostDown), I->hostDownBytes)) != cudaSuccess) {
         cc_destroy_instance(I);
         return cudaFail(e, "cudaHostAlloc(down)");
     }
-    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&I->hostWords), I->hostWordsMax * 4, cudaHostAllocDefault)) != cudaSuccess) {
+    if ((e = pinnedAlloc(reinterpret_cast<void**>(&I->hostWords), I->hostWordsMax * 4)) != cudaSuccess) {
         cc_destroy_instance(I);
         return cudaFail(e, "cudaHostAlloc(words)");
     }
@@ -270,6 +302,13 @@ int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 el
 }  // namespace ccb
 
 extern "C" {
+
+int cc_inject_allocation_failures(int skip, int fail) {
+    const int prev = g_allocFail.load();
+    g_allocSkip.store(skip > 0 ? skip : 0);
+    g_allocFail.store(fail > 0 ? fail : 0);
+    return prev;
+}
 
 void cc_destroy_instance(cc_instance* I) {
     if (!I) return;

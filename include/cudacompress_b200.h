@@ -42,6 +42,12 @@ const char* cc_last_error(void);
 uint64_t cc_kernel_launches(void);
 /* Library version string. */
 const char* cc_version(void);
+/* Test hook, no counterpart in the reference: the library's next `skip`
+ * device or page-locked host allocations succeed, then the following `fail`
+ * report out-of-memory without allocating (every entry point must then
+ * return a status and release what it holds).  0, 0 turns it off; returns
+ * the previous pending failure count. */
+int cc_inject_allocation_failures(int skip, int fail);
 
 /* ---- Instance (include/cudaCompress/Instance.h:26-45, src/cudaCompress/Instance.cpp:8-67) ---- */
 
