@@ -470,13 +470,13 @@ def measure_bricks(count, levels, seed, steps, warmup, plain_sample, local, auto
     vols = [torch.from_numpy(b).to(dev) for b in bricks]
     raw = sum(b.size for b in bricks) * 4
     tuned = None
-    cb = 128
+    cb, zc = 128, 0
     if autotune:
         from cudacompress_b200 import autotune as at
-        cb, tt = at.tune_coding_block(local, vols, levels, [float(v) for v in q])
-        tuned = {"coding_block": cb, "ms_per_pass": {str(k): v for k, v in tt.items()}}
+        cb, zc, tt = at.tune(local, vols, levels, [float(v) for v in q])
+        tuned = {"coding_block": cb, "z_chunk": zc, "ms_per_pass": tt}
     inst = cc.Instance(local, 7, 32 ** 3, cb, 14)
-    batch = cc.VolumeBatch(inst, [b.shape for b in bricks], levels, [float(v) for v in q], graph=True)
+    batch = cc.VolumeBatch(inst, [b.shape for b in bricks], levels, [float(v) for v in q], graph=True, z_chunk=zc)
     outs = [torch.empty_like(v) for v in vols]
     for _ in range(max(warmup, 1)):
         batch.compress(vols)
@@ -530,7 +530,7 @@ def measure_bricks(count, levels, seed, steps, warmup, plain_sample, local, auto
         "per_brick_sample": P, "speedup": batched_bps / plain_bps,
         "same_reconstruction_on_sample": bool(same), "psnr_db_mean_sample": float(np.mean(ps)),
         "sample_bits_per_voxel": bits / sum(bricks[i].size for i in range(min(count, 64))),
-        "autotune": tuned, "coding_block": cb,
+        "autotune": tuned, "coding_block": cb, "z_chunk": zc or 32,
     }
 
 

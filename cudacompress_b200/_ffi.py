@@ -110,6 +110,8 @@ _SIGS = {
     "cc_container_write": (c_int, [c_vp, c_u64, c_vp, c_vp, c_u32, ctypes.POINTER(c_u64)]),
     "cc_container_read": (c_int, [c_vp, c_u64, c_vp, c_vp, c_u32, c_u32p]),
     "cc_volume_batch_create": (c_int, [c_vp, c_u32, c_u32p, c_u32, ctypes.POINTER(c_float), ctypes.POINTER(c_vp)]),
+    "cc_volume_batch_create_ex": (c_int, [c_vp, c_u32, c_u32p, c_u32, ctypes.POINTER(c_float), c_u32,
+                                          ctypes.POINTER(c_vp)]),
     "cc_volume_batch_destroy": (None, [c_vp]),
     "cc_volume_batch_use_graph": (c_int, [c_vp, c_int]),
     "cc_volume_batch_set_active": (c_int, [c_vp, c_u32]),

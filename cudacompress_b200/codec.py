@@ -429,7 +429,7 @@ class VolumeBatch:
     (z, y, x) shapes, `quant_steps` one step per volume.  Each volume's
     stream equals compress_volume_float's."""
 
-    def __init__(self, inst: Instance, sizes, levels: int, quant_steps, graph: bool = False):
+    def __init__(self, inst: Instance, sizes, levels: int, quant_steps, graph: bool = False, z_chunk: int = 0):
         self.inst = inst
         self.count = len(sizes)
         self.shapes = [tuple(int(v) for v in s) for s in sizes]
@@ -439,8 +439,9 @@ class VolumeBatch:
         arr = (ctypes.c_uint32 * len(flat))(*flat)
         steps = (ctypes.c_float * self.count)(*[float(q) for q in quant_steps])
         h = ctypes.c_void_p()
-        check(lib().cc_volume_batch_create(inst.handle, self.count, arr, levels, steps, ctypes.byref(h)),
+        check(lib().cc_volume_batch_create_ex(inst.handle, self.count, arr, levels, steps, z_chunk, ctypes.byref(h)),
               "cc_volume_batch_create")
+        self.z_chunk = z_chunk
         self.handle = h
         self.levels = levels
         if graph:

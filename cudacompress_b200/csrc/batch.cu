@@ -122,7 +122,7 @@ void addCols(std::vector<BColDesc>& v, u32& ctas, BColDesc d) {
 void addLevel(std::vector<BLevelDesc>& v, u32& ctas, BLevelDesc d) {
     d.tilesX = int(ceilDiv(d.nx, kLvTX));
     d.tilesY = int(ceilDiv(d.ny, kLvTY));
-    d.chunksZ = int(ceilDiv(d.nz, kLvZC));
+    d.chunksZ = int(ceilDiv(d.nz, u64(d.zChunk)));
     d.ctaOff = ctas;
     ctas += u32(d.tilesX) * u32(d.tilesY) * u32(d.chunksZ);
     v.push_back(d);
@@ -423,7 +423,18 @@ extern "C" {
 
 int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* sizes, uint32_t levels,
                            const float* quantSteps, cc_volume_batch** out) {
+    return cc_volume_batch_create_ex(user, count, sizes, levels, quantSteps, 0, out);
+}
+
+int cc_volume_batch_create_ex(cc_instance* user, uint32_t count, const uint32_t* sizes, uint32_t levels,
+                              const float* quantSteps, uint32_t zChunk, cc_volume_batch** out) {
     if (!out) { setError("cc_volume_batch_create: out is NULL"); return CC_ERR_INVALID_ARGUMENT; }
+    if (zChunk == 0) zChunk = kLvZCDefault;
+    if (zChunk < 8 || zChunk > 256) {
+        setError("cc_volume_batch_create_ex: z_chunk must be 0 (default) or 8..256 (got %u)", zChunk);
+        *out = nullptr;
+        return CC_ERR_INVALID_ARGUMENT;
+    }
     *out = nullptr;
     if (!user || !sizes || !quantSteps || count == 0 || levels == 0 || levels > 8) {
         setError("cc_volume_batch_create: bad argument");
@@ -559,6 +570,7 @@ int cc_volume_batch_create(cc_instance* user, uint32_t count, const uint32_t* si
             fd.inv = 1.0f / (b->q0[v] / float(1u << l));              // Quantize.cu:90: reciprocal on the host
             fd.invLP = 1.0f / (b->q0[v] / float(1u << (L - 1)));
             fd.lastLevel = l + 1 == L ? 1 : 0;
+            fd.zChunk = int(zChunk);
             addLevel(fl[l], flC[l], fd);
             // X: input (level 0: the caller's volume, tight; else the LLL octant of level l-1) -> t1
             BRowDesc r{};

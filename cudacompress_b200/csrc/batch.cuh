@@ -60,7 +60,7 @@ struct BQuantDesc {
 
 // One forward level in one pass (k_bLevelFwd): a CTA owns kLvTX x kLvTY
 // outputs of the level's XY plane (positions in the filtering domain) and
-// kLvZC output slices; it streams the input slices through X and Y filters
+// zChunk output slices; it streams the input slices through X and Y filters
 // in shared memory and a 9-slice Z window in registers, and stores the seven
 // highpass octants as quantized symbols and the LLL octant as float (tight
 // hx x hy x hz, the next level's input) - or, at the coarsest level, as
@@ -77,9 +77,11 @@ struct BLevelDesc {
     float inv, invLP;       // reciprocal quantization steps (highpass, lowpass band)
     int lastLevel;
     int tilesX, tilesY, chunksZ;
+    int zChunk;             // output slices per CTA (the Z extent of its tile)
     u32 ctaOff;
 };
-constexpr int kLvTX = 64, kLvTY = 16, kLvZC = 32;
+constexpr int kLvTX = 64, kLvTY = 16;
+constexpr int kLvZCDefault = 32;   // default Z extent of a tile (cc_volume_batch_create_ex: 8..256)
 
 constexpr int kBRowOutputs = 4096;    // outputs per row-pass CTA
 constexpr int kBRowMaxWidth = 2048;   // row tile width

@@ -1112,8 +1112,9 @@ __global__ void __launch_bounds__(256, 4) k_bLevelFwd(const BLevelDesc* __restri
     const u32 rest = local / u32(tilesX);
     const int tY = int(rest % u32(tilesY)), cZ = int(rest / u32(tilesY));
     const int nx = D.nx, ny = D.ny, nz = D.nz;
-    const int x0 = tX * kLvTX, y0 = tY * kLvTY, z0 = cZ * kLvZC;
-    const int TXe = min(kLvTX, nx - x0), TYe = min(kLvTY, ny - y0), ZCe = min(kLvZC, nz - z0);
+    const int zChunk = D.zChunk;
+    const int x0 = tX * kLvTX, y0 = tY * kLvTY, z0 = cZ * zChunk;
+    const int TXe = min(kLvTX, nx - x0), TYe = min(kLvTY, ny - y0), ZCe = min(zChunk, nz - z0);
     const int colsE = TXe + 8, rowsE = TYe + 8;
     const int tid = int(threadIdx.x);
     const size_t srcSlice = size_t(D.srcSlice);

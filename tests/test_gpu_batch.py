@@ -204,3 +204,32 @@ def test_batch_back_to_back_encodes_are_deterministic():
             assert np.array_equal(he[i].numpy(), ext), i
             assert np.array_equal(hw[i].numpy()[:total], hw[0].numpy()[:total]), i
     inst.close()
+
+
+@pytest.mark.parametrize("z_chunk", [8, 16, 64, 256])
+def test_tile_depth_does_not_change_the_streams(oracle, z_chunk):
+    """The forward transform's tile depth (an autotuner knob) changes no
+    coefficient: streams and reconstructions equal the oracle's for every
+    depth, including depths larger than the volumes."""
+    vols, steps = bricks(6, 2, seed=77)
+    dev = [torch.from_numpy(v).cuda() for v in vols]
+    outs = [torch.full_like(d, float("nan")) for d in dev]
+    with cc.Instance(0, 7, 1 << 12, 128, 14) as inst:
+        with cc.VolumeBatch(inst, [v.shape for v in vols], 2, steps, graph=True, z_chunk=z_chunk) as b:
+            b.compress(dev)
+            b.decompress(outs)
+            b.status()
+            for i, (v, q) in enumerate(zip(vols, steps)):
+                words, bits = b.read_stream(i)
+                rw, rb = oracle.compress_volume(v, 2, q)
+                assert bits == rb and np.array_equal(words, rw), i
+                want = oracle.decompress_volume(rw, rb, v.shape, 2, q)
+                assert np.array_equal(outs[i].cpu().numpy().view(np.uint32), want.view(np.uint32)), i
+
+
+def test_tile_depth_out_of_range_is_rejected():
+    vols, steps = bricks(2, 2, seed=78)
+    with cc.Instance(0, 7, 1 << 12, 128, 14) as inst:
+        for bad in (4, 257):
+            with pytest.raises(cc.CudaCompressError):
+                cc.VolumeBatch(inst, [v.shape for v in vols], 2, steps, z_chunk=bad)
