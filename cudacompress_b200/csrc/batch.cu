@@ -430,8 +430,8 @@ int cc_volume_batch_create_ex(cc_instance* user, uint32_t count, const uint32_t*
                               const float* quantSteps, uint32_t zChunk, cc_volume_batch** out) {
     if (!out) { setError("cc_volume_batch_create: out is NULL"); return CC_ERR_INVALID_ARGUMENT; }
     if (zChunk == 0) zChunk = kLvZCDefault;
-    if (zChunk < 8 || zChunk > 256) {
-        setError("cc_volume_batch_create_ex: z_chunk must be 0 (default) or 8..256 (got %u)", zChunk);
+    if (zChunk < 8 || zChunk > 256 || (zChunk & 1)) {
+        setError("cc_volume_batch_create_ex: z_chunk must be 0 (default) or even in 8..256 (got %u)", zChunk);
         *out = nullptr;
         return CC_ERR_INVALID_ARGUMENT;
     }

@@ -1053,59 +1053,61 @@ __global__ void __launch_bounds__(256) k_bQuant(const BQuantDesc* __restrict__ d
 // CTA's Z chunk (with 4 slices of mirrored halo each side) the tile's rows
 // y0-4 .. y0+TY+3 and columns x0-4 .. x0+TX+3 are staged in shared memory,
 // filtered along X (outputs x0 .. x0+TX-1 of every staged row), then along Y
-// (outputs y0 .. y0+TY-1); each thread keeps, for its column and its four
-// rows, the Y outputs of the last nine slices in registers, and once an
-// output slice's nine inputs are in it filters along Z, quantizes and stores.
-// The taps and fmaf chains are those of the separate X, Y and Z passes, in
-// that order, so the coefficients - and symbols - are bit-identical.  The
-// next slice's loads are issued before the current slice is filtered.
+// (outputs y0 .. y0+TY-1); each thread keeps the Y outputs of its column
+// pair and row pair for the last eight slices in a thread-private ring, and
+// once an output slice's nine inputs are in it filters along Z, quantizes
+// and stores.  The taps and fmaf chains are those of the separate X, Y and Z
+// passes, in that order, so the coefficients - and symbols - are
+// bit-identical.  Every filter runs on value pairs with Blackwell's packed
+// fma.rn.f32x2 (each lane rounded as the scalar fmaf):
+//  * the staged rows are stored interleaved in pairs (rows 2p, 2p+1 of a
+//    column side by side), so X filters two rows at once;
+//  * the X outputs are stored row-major, so Y and Z filter two adjacent
+//    columns at once (one coefficient for both);
+//  * warp w owns output rows 2w, 2w+1 and lane l columns 2l, 2l+1: its four
+//    outputs of a slice are one per octant band and share the in-band
+//    offset, and a warp's store to a band is 64 contiguous bytes.
+// The slice loop is unrolled by eight, so ring slots and the z parity are
+// constants.  The next slice's loads are issued before the current slice is
+// filtered.
 // ---------------------------------------------------------------------------
 constexpr int kLvRows = kLvTY + 8;               // staged rows
 constexpr int kLvCols = kLvTX + 8;               // staged columns
-constexpr int kLvStage = kLvRows * kLvCols;
-constexpr int kLvLoads = (kLvStage + 255) / 256;  // staged elements per thread
-static_assert(kLvTX == 64 && kLvTY == 16, "256 threads: one column and four rows of Y/Z outputs each");
+constexpr int kLvPairs = kLvRows / 2;            // staged row pairs
+constexpr int kLvQuads = kLvCols / 4;            // 16-byte column groups of a staged row
+// padded strides: a row pair of the stage is 37 16-byte units (odd, so two
+// row pairs' groups fall in different banks), an X output row 18 units
+constexpr int kLvPairStride = kLvCols + 2;       // float2
+constexpr int kLvXStride = kLvTX + 8;            // float
+static_assert(kLvTX == 64 && kLvTY == 16, "256 threads: a column pair and a row pair of outputs each");
+static_assert(kLvPairs * kLvQuads <= 256, "one vector staging task per thread");
 
-// Z outputs of output slice i - 8 from the ring (slices i-8 .. i-1, taps
-// 0..7) and the newest slice i (tap 8), two outputs per packed fma.
-template <int kParity>
-__device__ __forceinline__ void zRing(const float2 (*ring)[2][256], int i, float2 n02, float2 n13, float2& v02,
-                                      float2& v13) {
-    constexpr float kF[2][9] = {
-        {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
-        {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
-    const int t = int(threadIdx.x);
-    float2 a = make_float2(0.0f, 0.0f), b = make_float2(0.0f, 0.0f);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int slot = (i + q) & 7;   // slice i - 8 + q
-        const float c = kF[kParity][q];
-        a = __ffma2_rn(make_float2(c, c), ring[slot][0][t], a);
-        b = __ffma2_rn(make_float2(c, c), ring[slot][1][t], b);
-    }
-    const float c8 = kF[kParity][8];
-    v02 = __ffma2_rn(make_float2(c8, c8), n02, a);
-    v13 = __ffma2_rn(make_float2(c8, c8), n13, b);
-}
+// Forward taps as a constexpr table (kFwdTap[parity][tap]) for the Z chains.
+__device__ constexpr float kFwdTap[2][9] = {
+    {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+    {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+
+template <int K>
+struct SliceK {
+    static constexpr int value = K;
+};
 
 __global__ void __launch_bounds__(256, 4) k_bLevelFwd(const BLevelDesc* __restrict__ descs,
                                                      const u32* __restrict__ map, const float* const* inTab) {
-    __shared__ __align__(16) float sIn[kLvRows * kLvCols];
-    __shared__ __align__(16) float sX[kLvRows * kLvTX];
-    // each thread's Y outputs of the last eight slices, rows (0, 2) and (1, 3)
-    // as pairs: a ring indexed by slice & 7 (thread-private, no barriers)
-    __shared__ float2 sZ[8][2][256];
+    __shared__ __align__(16) float2 sIn[kLvPairs * kLvPairStride];   // (row 2p, row 2p+1) per staged column
+    __shared__ __align__(16) float sX[kLvRows * kLvXStride];         // X outputs, row-major
+    __shared__ float2 sZ[8][2][256];                           // Y outputs of the last eight slices
     // the descriptor's fields in registers (the output stores could alias it)
-    const BLevelDesc& Dg = descs[map[blockIdx.x]];
-    const float* const src = Dg.src ? Dg.src : inTab[Dg.vol];
-    float* const lpOut = Dg.lpOut;
-    u16* const symOut = Dg.symOut;
-    u16* const lpSymOut = Dg.lpSymOut;
-    const u64 bandStride = Dg.bandStride;
-    const float inv = Dg.inv, invLP = Dg.invLP;
-    const bool lastLevel = Dg.lastLevel != 0;
-    const int srcRow = Dg.srcRow;
-    const BLevelDesc& D = Dg;
+    const BLevelDesc& D = descs[map[blockIdx.x]];
+    const float* const src = D.src ? D.src : inTab[D.vol];
+    // lowpass output: symbols (last level) or floats; offsets below 2^31
+    const bool lastLevel = D.lastLevel != 0;
+    char* const lpBase = lastLevel ? reinterpret_cast<char*>(D.lpSymOut) : reinterpret_cast<char*>(D.lpOut);
+    u16* const symOut = D.symOut;
+    const u32 bandStride = u32(D.bandStride);
+    const float inv = D.inv, invLP = D.invLP;
+    const int srcRow = D.srcRow;
+    const u32 srcSlice = u32(D.srcSlice);
     const u32 local = blockIdx.x - D.ctaOff;
     const int tilesX = D.tilesX, tilesY = D.tilesY;
     const int tX = int(local % u32(tilesX));
@@ -1117,131 +1119,149 @@ __global__ void __launch_bounds__(256, 4) k_bLevelFwd(const BLevelDesc* __restri
     const int TXe = min(kLvTX, nx - x0), TYe = min(kLvTY, ny - y0), ZCe = min(zChunk, nz - z0);
     const int colsE = TXe + 8, rowsE = TYe + 8;
     const int tid = int(threadIdx.x);
-    const size_t srcSlice = size_t(D.srcSlice);
-    // Staging.  Interior tiles (the columns need no mirroring, whole tile
-    // width, 16-byte aligned rows) move 18 float4 per staged row; other
-    // tiles move single floats with mirrored indices.  Per thread: the source
-    // offsets within a slice of its staged elements (-1: not needed).
-    const bool vec = x0 >= 4 && TXe == kLvTX && x0 + kLvTX + 4 <= nx && (srcRow & 3) == 0 &&
-                     (srcSlice & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;   // CTA-uniform
-    constexpr int kVecPerRow = kLvCols / 4;                            // 18
-    constexpr int kVecLoads = (kLvRows * kVecPerRow + 255) / 256;      // 2
-    int soff[kLvLoads];
+    // Staging: thread t < 216 moves the staged column group vq (four
+    // columns) of the rows 2vp, 2vp+1 and interleaves them.  A group inside
+    // the volume with 16-byte aligned rows is one float4 per row; a group
+    // reaching over an edge (mirrored) or in unaligned rows is four floats.
+    const bool task = tid < kLvPairs * kLvQuads;
+    const int vp = tid / kLvQuads, vq = tid - vp * kLvQuads;
+    const int xs = x0 - 4 + 4 * vq;   // first source column of the group
+    const bool aligned = ((srcRow | int(srcSlice)) & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+    const bool wide = aligned && xs >= 0 && xs + 3 < nx;
+    int rowOff[2];   // source row offsets within a slice (-1: not needed)
 #pragma unroll
-    for (int k = 0; k < kLvLoads; ++k) {
-        soff[k] = -1;
-        if (vec) {
-            const int e = tid + 256 * k;
-            const int r = e / kVecPerRow, q = e - r * kVecPerRow;
-            if (k < kVecLoads && e < kLvRows * kVecPerRow && r < rowsE)
-                soff[k] = mirrorIdx(y0 - 4 + r, ny) * srcRow + x0 - 4 + 4 * q;
-        } else {
-            const int e = tid + 256 * k;
-            const int r = e / kLvCols, cc = e - r * kLvCols;
-            if (e < kLvStage && r < rowsE && cc < colsE)
-                soff[k] = mirrorIdx(y0 - 4 + r, ny) * srcRow + mirrorIdx(x0 - 4 + cc, nx);
-        }
+    for (int k = 0; k < 2; ++k) {
+        const int r = 2 * vp + k;
+        rowOff[k] = task && r < rowsE && 4 * vq < colsE ? mirrorIdx(y0 - 4 + r, ny) * srcRow : -1;
     }
-    float pre[kLvLoads];
-    float4 pre4[kVecLoads];
+    float4 pre4[2];
     auto fetch = [&](int i) {
-        const float* sl = src + size_t(mirrorIdx(z0 - 4 + i, nz)) * srcSlice;
-        if (vec) {
+        const float* sl = src + u64(u32(mirrorIdx(z0 - 4 + i, nz))) * srcSlice;
 #pragma unroll
-            for (int k = 0; k < kVecLoads; ++k)
-                pre4[k] = soff[k] >= 0 ? *reinterpret_cast<const float4*>(sl + soff[k]) : make_float4(0.f, 0.f, 0.f, 0.f);
-        } else {
+        for (int k = 0; k < 2; ++k) {
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (rowOff[k] >= 0) {
+                const float* row = sl + rowOff[k];
+                if (wide) {
+                    v = *reinterpret_cast<const float4*>(row + xs);
+                } else {
+                    float t[4];
 #pragma unroll
-            for (int k = 0; k < kLvLoads; ++k) pre[k] = soff[k] >= 0 ? sl[soff[k]] : 0.0f;
+                    for (int e = 0; e < 4; ++e) t[e] = 4 * vq + e < colsE ? row[mirrorIdx(xs + e, nx)] : 0.0f;
+                    v = make_float4(t[0], t[1], t[2], t[3]);
+                }
+            }
+            pre4[k] = v;
         }
     };
-    // the Y and Z outputs of this thread: column c, rows 4 yg .. 4 yg + 3;
-    // the two warps of a row group take the even and the odd columns, so
-    // that a warp's outputs share their octant (no divergent stores)
-    const int c = 2 * (tid & 31) + ((tid >> 5) & 1), yg = tid >> 6;
+    auto stage = [&]() {
+        if (task) {
+            float4* d = reinterpret_cast<float4*>(sIn + vp * kLvPairStride + 4 * vq);
+            d[0] = make_float4(pre4[0].x, pre4[1].x, pre4[0].y, pre4[1].y);
+            d[1] = make_float4(pre4[0].z, pre4[1].z, pre4[0].w, pre4[1].w);
+        }
+    };
+    // X tasks: row pair xp, output columns 4 xg .. 4 xg + 3 (192 tasks);
+    // warp w takes the row pairs 2w, 2w+1, and each quarter warp four
+    // column groups of both (conflict-free 16-byte loads)
+    const int xp = 2 * (tid >> 5) + ((tid >> 2) & 1), xg = (tid & 3) + 4 * ((tid & 31) >> 3);
+    const bool xTask = tid < kLvPairs * 16 && 2 * xp < rowsE && 4 * xg < TXe;
+    // Y/Z outputs: warp w rows 2w, 2w+1; lane l columns 2l, 2l+1
+    const int w = tid >> 5, l = tid & 31;
+    const bool outOk = 2 * w < TYe && 2 * l < TXe;
     const int hx = nx >> 1, hy = ny >> 1;
-    const bool colOk = c < TXe;
-    // store addressing of the thread's outputs: octant bits of x and y
-    // (rows 4 yg + j: y parity = j & 1) and the in-plane offsets
-    const int x = x0 + c;
-    const int bxy[2] = {x & 1, (x & 1) + 2};
-    u32 xyOff[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) xyOff[j] = u32((y0 + 4 * yg + j) >> 1) * u32(hx) + u32(x >> 1);
-    const u64 plane = u64(hx) * u64(hy);
+    const u32 plane = u32(hx) * u32(hy);
+    const u32 inPlane = u32((y0 >> 1) + w) * u32(hx) + u32((x0 >> 1) + l);
 
     const int nSlices = ZCe + 8;
-    fetch(0);
-    for (int i = 0; i < nSlices; ++i) {
-        if (vec) {
-#pragma unroll
-            for (int k = 0; k < kVecLoads; ++k) {
-                const int e = tid + 256 * k;
-                if (e < kLvRows * kVecPerRow) reinterpret_cast<float4*>(sIn)[e] = pre4[k];
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < kLvLoads; ++k) {
-                const int e = tid + 256 * k;
-                if (e < kLvStage) sIn[e] = pre[k];
-            }
-        }
+    int i0 = 0;
+    // slice i = i0 + k (kc: k as a constant; i0 is a multiple of 8)
+    auto slice = [&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const int i = i0 + k;
+        if (i >= nSlices) return;                           // CTA-uniform
+        stage();
         __syncthreads();
         if (i + 1 < nSlices) fetch(i + 1);
-        // X: 8 consecutive outputs of one staged row per task (24 rows x 8 groups)
-        if (tid < kLvRows * (kLvTX / 8)) {
-            const int r = tid >> 3, g = tid & 7;
-            if (r < rowsE && 8 * g < TXe) {
-                float w[16];
-                const float4* s4 = reinterpret_cast<const float4*>(sIn + r * kLvCols + 8 * g);
+        // X: two rows, four outputs (columns of both parities); window
+        // element m is tap m - o of output o, taken in tap order as it loads
+        if (xTask) {
+            const float4* s4 = reinterpret_cast<const float4*>(sIn + xp * kLvPairStride + 4 * xg);
+            float2 o[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float4 v = s4[q];
-                    w[4 * q] = v.x; w[4 * q + 1] = v.y; w[4 * q + 2] = v.z; w[4 * q + 3] = v.w;
-                }
-                float4* o4 = reinterpret_cast<float4*>(sX + r * kLvTX + 8 * g);
-                o4[0] = make_float4(fir9c<false, 0>(w), fir9c<false, 1>(w + 1), fir9c<false, 0>(w + 2),
-                                    fir9c<false, 1>(w + 3));
-                o4[1] = make_float4(fir9c<false, 0>(w + 4), fir9c<false, 1>(w + 5), fir9c<false, 0>(w + 6),
-                                    fir9c<false, 1>(w + 7));
-            }
-        }
-        __syncthreads();
-        // Y: four outputs of column c from twelve X outputs (rows 0, 2 and 1, 3 paired)
-        float2 n02, n13;
-        {
-            float yw[12];
+            for (int j = 0; j < 4; ++j) o[j] = make_float2(0.0f, 0.0f);
 #pragma unroll
-            for (int q = 0; q < 12; ++q) yw[q] = sX[(4 * yg + q) * kLvTX + c];
-            n02 = make_float2(fir9c<false, 0>(yw), fir9c<false, 0>(yw + 2));
-            n13 = make_float2(fir9c<false, 1>(yw + 1), fir9c<false, 1>(yw + 3));
-        }
-        // Z: output slice z once its nine input slices are in
-        if (i >= 8 && colOk) {
-            const int z = z0 + i - 8;
-            float2 v02, v13;
-            if (z & 1) zRing<1>(sZ, i, n02, n13, v02, v13);
-            else zRing<0>(sZ, i, n02, n13, v02, v13);
-            const float v[4] = {v02.x, v13.x, v02.y, v13.y};
-            const u64 zOff = u64(z >> 1) * plane;
-            const int bz = (z & 1) << 2;
+            for (int q = 0; q < 6; ++q) {
+                const float4 v = s4[q];
+                const float2 wm[2] = {make_float2(v.x, v.y), make_float2(v.z, v.w)};
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (4 * yg + j < TYe) {
-                    const int b = bxy[j & 1] + bz;
-                    const u64 li = zOff + xyOff[j];
-                    if (b == 0) {
-                        if (lastLevel) lpSymOut[li] = u16(symbolizeI(int(v[j] * invLP)));
-                        else lpOut[li] = v[j];
-                    } else {
-                        symOut[u64(b - 1) * bandStride + li] = u16(symbolizeI(int(v[j] * inv)));
+                for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int tap = 2 * q + h - j;
+                        if (tap >= 0 && tap <= 8) {
+                            const float c = kFwdTap[j & 1][tap];
+                            o[j] = __ffma2_rn(make_float2(c, c), wm[h], o[j]);
+                        }
                     }
                 }
             }
+            float4* d = reinterpret_cast<float4*>(sX + (2 * xp) * kLvXStride + 4 * xg);
+            d[0] = make_float4(o[0].x, o[1].x, o[2].x, o[3].x);
+            d[kLvXStride / 4] = make_float4(o[0].y, o[1].y, o[2].y, o[3].y);
+        }
+        __syncthreads();
+        // Y: rows 2w (even taps) and 2w+1 (odd taps) of columns 2l, 2l+1
+        float2 ne, no;
+        {
+            float2 yw[10];
+#pragma unroll
+            for (int q = 0; q < 10; ++q) yw[q] = *reinterpret_cast<const float2*>(sX + (2 * w + q) * kLvXStride + 2 * l);
+            ne = fir9p<false, 0>(yw);
+            no = fir9p<false, 1>(yw + 1);
+        }
+        // Z: output slice z = z0 + i - 8 once its nine input slices are in
+        // (z0 and i0 are even, so z has the parity of k): slices i-8 .. i-1
+        // from the ring (slot (k + q) & 7 holds slice i - 8 + q), slice i
+        // in registers
+        if (i >= 8 && outOk) {
+            float2 ve = make_float2(0.0f, 0.0f), vo = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float c = kFwdTap[k & 1][q];
+                ve = __ffma2_rn(make_float2(c, c), sZ[(k + q) & 7][0][tid], ve);
+                vo = __ffma2_rn(make_float2(c, c), sZ[(k + q) & 7][1][tid], vo);
+            }
+            constexpr float c8 = kFwdTap[k & 1][8];
+            ve = __ffma2_rn(make_float2(c8, c8), ne, ve);
+            vo = __ffma2_rn(make_float2(c8, c8), no, vo);
+            const u64 li = u64(u32((z0 + i - 8) >> 1)) * plane + inPlane;
+            constexpr int bz = (k & 1) << 2;
+            // octants (x even, y even), (x odd, y even), (x even, y odd), (x odd, y odd)
+            if (bz == 0) {
+                if (lastLevel) reinterpret_cast<u16*>(lpBase)[li] = u16(symbolizeI(int(ve.x * invLP)));
+                else reinterpret_cast<float*>(lpBase)[li] = ve.x;
+            } else {
+                symOut[u64(bz - 1) * bandStride + li] = u16(symbolizeI(int(ve.x * inv)));
+            }
+            symOut[u64(bz) * bandStride + li] = u16(symbolizeI(int(ve.y * inv)));
+            symOut[u64(bz + 1) * bandStride + li] = u16(symbolizeI(int(vo.x * inv)));
+            symOut[u64(bz + 2) * bandStride + li] = u16(symbolizeI(int(vo.y * inv)));
         }
         // the newest slice replaces the oldest, just used
-        sZ[i & 7][0][tid] = n02;
-        sZ[i & 7][1][tid] = n13;
+        sZ[k][0][tid] = ne;
+        sZ[k][1][tid] = no;
+    };
+    fetch(0);
+    for (; i0 < nSlices; i0 += 8) {
+        slice(SliceK<0>{});
+        slice(SliceK<1>{});
+        slice(SliceK<2>{});
+        slice(SliceK<3>{});
+        slice(SliceK<4>{});
+        slice(SliceK<5>{});
+        slice(SliceK<6>{});
+        slice(SliceK<7>{});
     }
 }
 

@@ -412,7 +412,8 @@ typedef struct cc_volume_batch cc_volume_batch;
 int cc_volume_batch_create(cc_instance* inst, uint32_t count, const uint32_t* sizes, uint32_t levels,
                            const float* quant_steps, cc_volume_batch** out);
 /* The same with the forward transform's tile depth: each CTA of a level's
- * fused pass codes z_chunk output slices (0 = the default 32; 8..256).  A
+ * fused pass codes z_chunk output slices (0 = the default 32; else even,
+ * 8..256).  A
  * tuning knob only (cudacompress_b200.autotune): the streams do not change. */
 int cc_volume_batch_create_ex(cc_instance* inst, uint32_t count, const uint32_t* sizes, uint32_t levels,
                               const float* quant_steps, uint32_t z_chunk, cc_volume_batch** out);

@@ -230,6 +230,6 @@ def test_tile_depth_does_not_change_the_streams(oracle, z_chunk):
 def test_tile_depth_out_of_range_is_rejected():
     vols, steps = bricks(2, 2, seed=78)
     with cc.Instance(0, 7, 1 << 12, 128, 14) as inst:
-        for bad in (4, 257):
+        for bad in (4, 9, 257):
             with pytest.raises(cc.CudaCompressError):
                 cc.VolumeBatch(inst, [v.shape for v in vols], 2, steps, z_chunk=bad)
