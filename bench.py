@@ -416,11 +416,12 @@ METRIC = "enc/dec GB/s raw (%HBM peak); batched vs per-brick GB/s at fixed PSNR;
 # ---------------------------------------------------------- section bytes
 # per-unit algorithmic bytes of the sections the roofline may pick
 SECTION_UNITS = {
-    "batch.dwt_forward": "per pass (k_bRows / k_bCols, 3 per level): its input read once + its output written "
-                         "once, 8 B/voxel; the Z pass stores the 7 highpass octants as 2-byte symbols (quantization "
-                         "fused) and the LLL octant as float, or as symbols at the coarsest level",
-    "batch.dwt_inverse": "per pass (k_bCols from symbols, k_bCols, k_bRows per level): 2 B/symbol + 4 B/lowpass "
-                         "voxel in and 4 B/voxel out for the first, 8 B/voxel for the others",
+    "batch.dwt_forward": "per level (one fused k_bLevelFwd launch): the level's input read once (4 B/voxel) and "
+                         "its outputs written once: 7 highpass octants as 2-byte symbols, the lowpass octant as "
+                         "float (4 B) or, at the coarsest level, as 2-byte symbols",
+    "batch.dwt_inverse": "per level (three launches: k_bCols from symbols, k_bCols, k_bRows): the level's inputs "
+                         "read once (2 B/highpass symbol, 4 B/lowpass voxel) and its output written once "
+                         "(4 B/voxel); the intermediate passes' traffic is not credited",
 }
 
 
@@ -433,9 +434,9 @@ def section_bytes(name, wl, coded_bytes, counts):
     lp = vols[-1] // 8
     m = {
         "pipe.dwt_forward": sum(8 * v for v in vols) * C,
-        "batch.dwt_forward": sum(2 * 8 * v + 4 * v + 2 * (7 * v // 8) + (2 if i == len(vols) - 1 else 4) * (v // 8)
+        "batch.dwt_forward": sum(4 * v + 2 * (7 * v // 8) + (2 if i == len(vols) - 1 else 4) * (v // 8)
                                  for i, v in enumerate(vols)) * C,
-        "batch.dwt_inverse": sum(4 * (v // 8) + 2 * (7 * v // 8) + 4 * v + 2 * 8 * v for v in vols) * C,
+        "batch.dwt_inverse": sum(4 * (v // 8) + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
         "batch.quantize": (hp + lp) * 6 * C,
         "pipe.dwt_inverse": sum(4 * v // 8 + 2 * (7 * v // 8) + 4 * v for v in vols) * C,
         "pipe.quantize": (hp + lp) * 6 * C,
@@ -1181,6 +1182,8 @@ def run_ours(args, wl):
         if b and t > 0:
             bw[k] = {"ms": t, "algorithmic_bytes": b, "gbs": b / (t / 1e3) / 1e9, "frac": b / (t / 1e3) / 1e9 / peak,
                      "launches": cnt, "share": t / total_sec}
+            if k in SECTION_UNITS:
+                bw[k]["per_unit"] = SECTION_UNITS[k]
     top = max(kernel_secs.items(), key=lambda kv: kv[1][0]) if kernel_secs else ("none", (0.0, 0))
     top_bytes = section_bytes(top[0], wl, coded_bytes, counts) or 0
     # whole codec (algorithmic: raw + compressed bytes; intermediate passes do not count)

@@ -24,3 +24,14 @@ def test_budget_validation():
         serving.validate_budget(100, [32, 64], 99 + serving.request_bytes(64))
     with pytest.raises(ValueError):
         serving.validate_budget(4 << 30, [128], 4 << 30)           # the store alone fills the budget
+
+
+def test_fill_levels_are_powers_of_two_and_the_slot_count():
+    assert serving.fill_levels(64) == [1, 2, 4, 8, 16, 32, 64]
+    assert serving.fill_levels(12) == [1, 2, 4, 8, 12]
+    assert serving.fill_levels(1) == [1]
+    assert serving.fill_level(0, 16) == 0
+    assert serving.fill_level(7, 16) == 4      # the rest waits for the lane's other codec
+    assert serving.fill_level(16, 16) == 16
+    assert serving.fill_level(11, 12) == 8
+    assert serving.fill_level(12, 12) == 12
