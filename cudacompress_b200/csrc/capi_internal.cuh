@@ -145,10 +145,6 @@ enum SmemAttrKernel {
     kAttrTableBuild = 0,
     kAttrDecHuff16,
     kAttrDecHuff32,
-    kAttrDecZc16,
-    kAttrDecZc32,
-    kAttrDecSc16,
-    kAttrDecSc32,
     kAttrCount
 };
 cudaError_t ensureSmemAttribute(const void* kernel, int which, int device, size_t bytes);

@@ -29,7 +29,6 @@ struct DecParams {
     u32 rlBlocks, hBlocks;     // coding blocks (upper bounds) of the RLHuff / Huff streams
     u32 rlMaxN;                // largest output of an RLHuff stream
     u32 cb, log2Max, symBytes, leavesMax;
-    u32 stageWords;            // run-length decode: staged code words per warp
     u64 capLeaves;
     DecStreamDesc* streams;
     DecTableDesc* tables;
@@ -61,18 +60,6 @@ struct WordSrc {
         const u32 b = u32(bit & 31u);
         const u64 window = (u64(at(wi)) << 32) | at(wi + 1);
         return u32((window << b) >> (64 - count));
-    }
-};
-
-// Code words of a warp's coding blocks staged in shared memory; indices
-// outside the staged range read 0 like WordSrc past its end.
-struct StagedWords {
-    const u32* w;
-    u64 base;
-    u32 n;
-    __device__ __forceinline__ u32 at(u64 i) const {
-        const u64 k = i - base;
-        return k < n ? w[k] : 0u;
     }
 };
 
@@ -424,64 +411,6 @@ __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
     for (u64 k = lane; k < total; k += 32) out[base + k] = rows[(k / p.cb) * rowPitch + (k % p.cb)];
 }
 
-// Copies n words from ws (from word lo) to shared memory, eight loads in
-// flight per lane.
-__device__ __forceinline__ void stageWordsIn(u32* dst, const WordSrc& ws, u64 lo, u32 n, u32 lane) {
-    for (u32 base = 0; base < n; base += 256) {
-        u32 v[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const u32 k = base + lane + 32u * i;
-            v[i] = k < n ? ws.at(lo + k) : 0u;
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const u32 k = base + lane + 32u * i;
-            if (k < n) dst[k] = v[i];
-        }
-    }
-}
-
-// Copies n elements of type Sym to shared memory (16-byte vectors when src
-// is 16-byte aligned), eight loads in flight per lane.
-template <class Sym>
-__device__ __forceinline__ void stageSymsIn(Sym* dst, const Sym* src, u32 n, u32 lane) {
-    constexpr u32 kPer = 16 / sizeof(Sym);
-    u32 done = 0;
-    if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
-        const u32 nv = n / kPer;
-        const uint4* s4 = reinterpret_cast<const uint4*>(src);
-        uint4* d4 = reinterpret_cast<uint4*>(dst);
-        for (u32 base = 0; base < nv; base += 256) {
-            uint4 v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const u32 k = base + lane + 32u * i;
-                if (k < nv) v[i] = s4[k];
-            }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const u32 k = base + lane + 32u * i;
-                if (k < nv) d4[k] = v[i];
-            }
-        }
-        done = nv * kPer;
-    }
-    for (u32 base = done; base < n; base += 256) {
-        Sym v[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const u32 k = base + lane + 32u * i;
-            if (k < n) v[i] = src[k];
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const u32 k = base + lane + 32u * i;
-            if (k < n) dst[k] = v[i];
-        }
-    }
-}
-
 // Coding blocks of RLHuff stream s that a decode covers: its run-length
 // symbol count in blocks, within the blocks planned for its length.
 __device__ __forceinline__ u32 rlBlocksOf(const DecParams& p, const DecStreamDesc& sd) {
@@ -539,97 +468,176 @@ __global__ void __launch_bounds__(256) k_decZero(DecParams p) {
 
 // decodeRLHuff (RunLengthKernels.cui:56-66 for the scatter): one lane per
 // coding block, 32 consecutive blocks of one stream per warp (k_decRlTasks).
-// Zero counts (kSymbols false): decode, store, and sum (zc + 1) per block.
-// Symbols: decode and scatter out[scan(zc) + i] = symbol.  The blocks' code
-// words are staged in shared memory with coalesced loads, the decoded values go to
-// shared rows, zero counts are written out row by row, and the scatter runs
-// block by block on the blocks' zero counts (staged over the code words
-// once decoded): every lane takes cb/32 consecutive elements and a warp scan
-// of their (zc + 1) sums gives the positions.
+// Each lane decodes its block in rounds of kRlRound symbols into its row of
+// the warp's shared rows, its bit reader staying in registers between
+// rounds; after a round the warp moves the rows out block by block, lane k
+// taking the block's element k of the round.  Zero counts (kSymbols false)
+// are stored and their (zc + 1) summed per block.  Symbols are scattered to
+// out[block start + sum of (zc + 1) before the element + zc]: the round's
+// zero counts of the warp's blocks are staged with coalesced loads and a
+// warp scan gives the positions.  Lanes read their code words through L1;
+// the CTA stages the lookup table of its first warp's stream in shared
+// memory (a warp decoding another stream reads its table from global
+// memory).  About 13 KB of shared memory per CTA of four warps.
+constexpr u32 kRlRound = 32;
+
+struct BitReader {
+    u64 w;      // next word
+    u32 bpos;   // bit position in hi
+    u32 hi, lo;
+};
+
+// Decodes cnt symbols from r, calling emit(i, symbol) (decodeBlock's steps).
+template <bool kValueLut, class Lut, class Emit>
+__device__ __forceinline__ void decodeRun(const WordSrc& ws, const DecTable& D, u32 nSym, const u32* syms,
+                                          const Lut& lut, BitReader& r, u32 cnt, bool& corrupt, Emit emit) {
+    for (u32 i = 0; i < cnt; ++i) {
+        const u32 v = __funnelshift_l(r.lo, r.hi, r.bpos);
+        const u32 e = lut(v >> (32 - kLutBits));
+        u32 len, val;
+        if (e) {
+            len = e >> 24;
+            val = e & 0xFFFFFFu;
+            if (!kValueLut) {
+                if (val >= nSym) { corrupt = true; return; }
+                val = syms[val];
+            }
+        } else {
+            len = kLutBits + 1;
+            while (len <= 31 && int(v >> (32 - len)) > D.maxCode[len - 1]) ++len;
+            if (len > 31) { corrupt = true; return; }
+            const u32 idx = u32(D.firstIndex[len - 1] + int(v >> (32 - len)) - D.minCode[len - 1]);
+            if (idx >= nSym) { corrupt = true; return; }
+            val = syms[idx];
+        }
+        emit(i, val);
+        r.bpos += len;
+        if (r.bpos >= 32) {
+            r.hi = r.lo;
+            r.lo = ws.at(r.w);
+            ++r.w;
+            r.bpos -= 32;
+        }
+    }
+}
+
 template <class Sym, bool kSymbols>
 __global__ void __launch_bounds__(128) k_decRl(DecParams p) {
-    extern __shared__ __align__(16) unsigned char dyn[];
+    constexpr u32 kPitch = kRlRound + (sizeof(Sym) == 2 ? 2 : 1);
+    __shared__ Sym sRows[4][32 * kPitch];
+    __shared__ Sym sZc[kSymbols ? 4 : 1][32 * kRlRound];
+    __shared__ u32 sLut[1u << kLutBits];
+    __shared__ u32 sLutTable, sFail;
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const u32 rowPitch = p.cb + (sizeof(Sym) == 2 ? 2 : 1);
-    const u32 warpBytes = p.stageWords * 4u + u32(alignUp(u64(32) * rowPitch * sizeof(Sym), 16));
-    u32* words = reinterpret_cast<u32*>(dyn + warp * warpBytes);
-    Sym* rows = reinterpret_cast<Sym*>(dyn + warp * warpBytes + p.stageWords * 4u);
-    if (__any_sync(0xffffffffu, capacityFailed(p))) return;
     const u32 wt = blockIdx.x * 4u + warp;
-    if (wt >= reinterpret_cast<const u32*>(p.rlTasks + p.rlTaskCap)[0]) return;
-    const u64 task = p.rlTasks[wt];
-    const u32 s = u32(task >> 32), bFirst = u32(task);
+    const bool hasTask = wt < reinterpret_cast<const u32*>(p.rlTasks + p.rlTaskCap)[0];
+    u32 s = 0, bFirst = 0, t = 0;
+    if (hasTask) {
+        const u64 task = p.rlTasks[wt];
+        s = u32(task >> 32);
+        bFirst = u32(task);
+        t = p.streams[s].tableFirst + (kSymbols ? 0u : 1u);
+    }
+    if (threadIdx.x == 0) {
+        sFail = capacityFailed(p) ? 1u : 0u;
+        sLutTable = hasTask ? t : 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    if (sFail) return;   // CTA-uniform
+    const u32 lutT = sLutTable;
+    if (lutT != 0xFFFFFFFFu) {
+        const u32* g = p.lut + (u64(lutT) << kLutBits);
+        for (u32 e = threadIdx.x; e < (1u << kLutBits); e += 128) sLut[e] = g[e];
+    }
+    __syncthreads();
+    if (!hasTask) return;
     const DecStreamDesc sd = p.streams[s];
     const u32 b = bFirst + lane;
     const u32 blocks = rlBlocksOf(p, sd);
     const bool mine = b < blocks;
-    const u32 t = sd.tableFirst + (kSymbols ? 0u : 1u);
-    const DecTableDesc& td = p.tables[t];
-    const WordSrc ws = srcOf(p, s);
-    const u32* lut = p.lut + (u64(t) << kLutBits);
-    const u32* symv = p.syms + td.symOff;
-    const u32 cnt = mine ? min(p.cb, sd.m - b * p.cb) : 0u;
-    const u64 bit = mine ? td.cwWord * 32ull + p.blockOff[td.blockOff + b] : 0ull;
-    bool corrupt = false;
-    u32 sum = 0;
     const u32 nMine = __popc(__ballot_sync(0xffffffffu, mine));   // lanes 0 .. nMine-1
     if (nMine == 0) return;
-    const u64 cw0 = td.cwWord * 32ull;
-    const u64 startBit = cw0 + p.blockOff[td.blockOff + bFirst];
-    const u64 endBit = cw0 + (bFirst + nMine < blocks ? p.blockOff[td.blockOff + bFirst + nMine] : td.cwBits);
-    const u64 wLo = startBit >> 5, wHi = ((endBit + 31) >> 5) + 2;
-    const bool staged = endBit >= startBit && wHi - wLo <= p.stageWords;
-    if (staged) stageWordsIn(words, ws, wLo, u32(wHi - wLo), lane);
-    __syncwarp();
-    if (mine) {
-        auto emit = [&](u32 i, u32 v) {
-            rows[lane * rowPitch + i] = Sym(v);
-            if (!kSymbols) sum += v + 1;
-        };
-        if (staged) decodeBlock<sizeof(Sym) == 2>(StagedWords{words, wLo, u32(wHi - wLo)}, p.dec[t], symv, lut, bit, cnt, corrupt, emit);
-        else decodeBlock<sizeof(Sym) == 2>(ws, p.dec[t], symv, lut, bit, cnt, corrupt, emit);
+    const DecTableDesc& td = p.tables[t];
+    const WordSrc ws = srcOf(p, s);
+    const u32* symv = p.syms + td.symOff;
+    const u32* lutG = p.lut + (u64(t) << kLutBits);
+    const bool lutShared = t == lutT;   // warp-uniform
+    const DecTable& D = p.dec[t];
+    const u32 nSym = D.nSym;
+    const bool single = nSym <= 1;
+    const u32 singleVal = D.single;
+    bool corrupt = nSym == 0xFFFFFFFFu;
+    const u32 cnt = mine ? min(p.cb, sd.m - b * p.cb) : 0u;
+    BitReader rd{0ull, 0u, 0u, 0u};
+    if (mine && !corrupt && !single) {
+        const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
+        rd.w = bit >> 5;
+        rd.bpos = u32(bit & 31u);
+        rd.hi = ws.at(rd.w);
+        rd.lo = ws.at(rd.w + 1);
+        rd.w += 2;
     }
-    __syncwarp();
-    if (!kSymbols) {
-        if (mine) p.blockSum[td.blockOff + b] = sum;
-        Sym* zc = reinterpret_cast<Sym*>(p.zc) + sd.zcOff;
-        for (u32 j = 0; j < nMine; ++j) {
-            const u32 c = min(p.cb, sd.m - (bFirst + j) * p.cb);
-            for (u32 k = lane; k < c; k += 32) zc[u64(bFirst + j) * p.cb + k] = rows[j * rowPitch + k];
+    u32 sum = 0;   // zero counts: the block's sum of (zc + 1)
+    // symbols: the block's next output position (its start from the zero-count scan)
+    u32 pos = 0;
+    if (kSymbols && mine) pos = p.blockSum[p.tables[t + 1].blockOff + b];
+    Sym* rows = sRows[warp];
+    const u32 cnt0 = __shfl_sync(0xffffffffu, cnt, 0);   // the first block is the longest
+    for (u32 r0 = 0; r0 < cnt0; r0 += kRlRound) {
+        const u32 n = cnt > r0 ? min(kRlRound, cnt - r0) : 0u;
+        if (!corrupt) {
+            auto emit = [&](u32 i, u32 v) {
+                rows[lane * kPitch + i] = Sym(v);
+                if (!kSymbols) sum += v + 1u;
+            };
+            if (single) {
+                for (u32 i = 0; i < n; ++i) emit(i, singleVal);
+            } else if (lutShared) {
+                decodeRun<sizeof(Sym) == 2>(ws, D, nSym, symv, [&](u32 k) { return sLut[k]; }, rd, n, corrupt, emit);
+            } else {
+                decodeRun<sizeof(Sym) == 2>(ws, D, nSym, symv, [&](u32 k) { return lutG[k]; }, rd, n, corrupt, emit);
+            }
         }
-    } else {
-        // the blocks' zero counts, over the code words
-        Sym* zs = reinterpret_cast<Sym*>(words);
-        const u32 zn = min(nMine * p.cb, sd.m - bFirst * p.cb);
-        stageSymsIn(zs, reinterpret_cast<const Sym*>(p.zc) + sd.zcOff + u64(bFirst) * p.cb, zn, lane);
         __syncwarp();
-        const u32 zcBlockOff = p.tables[t + 1].blockOff;
-        const u32 myStart = mine ? p.blockSum[zcBlockOff + b] : 0u;   // block starts: one load for all 32
-        Sym* out = reinterpret_cast<Sym*>(sd.out);
-        const u32 E = (p.cb + 31) / 32;
-        for (u32 j = 0; j < nMine; ++j) {
-            const u32 start = __shfl_sync(0xffffffffu, myStart, j);
-            const u32 bj = bFirst + j;
-            const u32 c = min(p.cb, sd.m - bj * p.cb);
-            const u32 e0 = min(lane * E, c), e1 = min(e0 + E, c);
-            const Sym* z = zs + j * p.cb;
-            u32 local = 0;
-            for (u32 e = e0; e < e1; ++e) local += u32(z[e]) + 1u;
-            u32 incl = local;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const u32 y = __shfl_up_sync(0xffffffffu, incl, d);
-                if (int(lane) >= d) incl += y;
+        const u32 k = r0 + lane;   // the element of every block this lane moves
+        if (!kSymbols) {
+            Sym* zc = reinterpret_cast<Sym*>(p.zc) + sd.zcOff;
+            for (u32 j = 0; j < nMine; ++j) {
+                const u32 c = min(p.cb, sd.m - (bFirst + j) * p.cb);
+                if (k < c) zc[u64(bFirst + j) * p.cb + k] = rows[j * kPitch + lane];
             }
-            u32 pos = start + incl - local;
-            for (u32 e = e0; e < e1; ++e) {
-                pos += u32(z[e]);
-                if (pos < sd.n) out[pos] = rows[j * rowPitch + e];
-                else corrupt = true;
-                ++pos;
+        } else {
+            Sym* zs = sZc[warp];
+            const Sym* zcG = reinterpret_cast<const Sym*>(p.zc) + sd.zcOff;
+            for (u32 j = 0; j < nMine; ++j) {
+                const u32 c = min(p.cb, sd.m - (bFirst + j) * p.cb);
+                zs[j * kRlRound + lane] = k < c ? zcG[u64(bFirst + j) * p.cb + k] : Sym(0);
+            }
+            __syncwarp();
+            Sym* out = reinterpret_cast<Sym*>(sd.out);
+            for (u32 j = 0; j < nMine; ++j) {
+                const u32 c = min(p.cb, sd.m - (bFirst + j) * p.cb);
+                const bool act = k < c;
+                const u32 z = act ? u32(zs[j * kRlRound + lane]) : 0u;
+                const u32 v = act ? z + 1u : 0u;
+                u32 incl = v;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const u32 y = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (int(lane) >= d) incl += y;
+                }
+                const u32 at = __shfl_sync(0xffffffffu, pos, j) + incl - v + z;
+                if (act) {
+                    if (at < sd.n) out[at] = rows[j * kPitch + lane];
+                    else corrupt = true;
+                }
+                const u32 tot = __shfl_sync(0xffffffffu, incl, 31);
+                if (lane == j) pos += tot;
             }
         }
+        __syncwarp();
     }
+    if (!kSymbols && mine) p.blockSum[td.blockOff + b] = sum;
     if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
 }
 
@@ -793,18 +801,6 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
     return CC_OK;
 }
 
-// Run-length decode staging: code words per warp (12 bits per symbol on
-// average fit; longer blocks decode from global memory) and the dynamic
-// shared memory of a 4-warp block.
-// (the area also holds the 32 blocks' zero counts in the scatter).
-static u32 decRlStageWords(u32 cb, size_t symBytes) {
-    return u32(alignUp(std::max<u64>(u64(12) * cb + 4, u64(32) * cb * symBytes / 4), 4));
-}
-static size_t decRlSmem(u32 cb, u32 stageWords, size_t symBytes) {
-    const u64 rowPitch = cb + (symBytes == 2 ? 2 : 1);
-    return 4 * (size_t(stageWords) * 4 + size_t(alignUp(u64(32) * rowPitch * symBytes, 16)));
-}
-
 template <class Sym>
 static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
     cudaStream_t st = I->stream;
@@ -821,22 +817,15 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
     }
     if (p.rlBlocks) {
         const u32 g = u32(ceilDiv(u64(p.rlBlocks) / 32 + p.nRl, 4));   // warp tasks <= rlBlocks / 32 + nRl
-        const size_t smem = decRlSmem(p.cb, p.stageWords, sizeof(Sym));
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<Sym, false>),
-                                        sizeof(Sym) == 2 ? kAttrDecZc16 : kAttrDecZc32, I->device, smem),
-                    "decRl smem");
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<Sym, true>),
-                                        sizeof(Sym) == 2 ? kAttrDecSc16 : kAttrDecSc32, I->device, smem),
-                    "decRl smem");
         { SectionTimer t(I, "dec.rl_tasks", st); k_decRlTasks<<<1, 1024, 0, st>>>(p); countLaunch(); }
         {
             SectionTimer t(I, "dec.zero_fill", st);
             k_decZero<Sym><<<dim3(p.nRl, u32(ceilDiv(p.rlMaxN, kZeroChunk))), 256, 0, st>>>(p);
             countLaunch();
         }
-        { SectionTimer t(I, "dec.zero_counts", st); k_decRl<Sym, false><<<g, 128, smem, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.zero_counts", st); k_decRl<Sym, false><<<g, 128, 0, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.nRl, 1024, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "dec.symbols_scatter", st); k_decRl<Sym, true><<<g, 128, smem, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.symbols_scatter", st); k_decRl<Sym, true><<<g, 128, 0, st>>>(p); countLaunch(); }
     }
     CC_TRY_CUDA(cudaGetLastError(), "decode launch");
     return CC_OK;
@@ -844,16 +833,11 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
 
 int prepareDecodeAttributes(cc_instance* I) {
     const size_t smem = size_t(32) * (I->codingBlockSize + 2) * I->symBytes;
-    const size_t rl = decRlSmem(I->codingBlockSize, decRlStageWords(I->codingBlockSize, I->symBytes), I->symBytes);
     const int dev = I->device;
     if (I->symBytes == 2) {
         CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u16>), kAttrDecHuff16, dev, smem), "decHuff smem");
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u16, false>), kAttrDecZc16, dev, rl), "decRl smem");
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u16, true>), kAttrDecSc16, dev, rl), "decRl smem");
     } else {
         CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<u32>), kAttrDecHuff32, dev, smem), "decHuff smem");
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u32, false>), kAttrDecZc32, dev, rl), "decRl smem");
-        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decRl<u32, true>), kAttrDecSc32, dev, rl), "decRl smem");
     }
     return CC_OK;
 }
@@ -870,7 +854,6 @@ static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
     p.rlMaxN = dc.rlMaxN;
     p.hBlocks = dc.hBlocks;
     p.cb = I->codingBlockSize;
-    p.stageWords = decRlStageWords(I->codingBlockSize, I->symBytes);
     p.log2Max = I->log2Max;
     p.symBytes = I->symBytes;
     p.leavesMax = I->leavesMax;
