@@ -911,9 +911,9 @@ def run_profile(args):
     """A small self-contained case for profilers (ncu): one batch of
     `--comps` seeded n^3 float32 fields (the vector field's generator and
     seeds), `--warmup` encode + decode passes, then `--steps` more; no timing,
-    no other legs.  Launch order per step: the forward transform (per level
-    the row pass, the Y pass and the Z pass with the quantizer fused), the
-    encoders, then the decoder and the inverse transform."""
+    no other legs.  Launch order per step: the forward transform (one fused
+    launch per level, the quantizer included), the encoders, then the
+    decoder and the inverse transform (three passes per level)."""
     import torch
     import cudacompress_b200 as cc
     from cudacompress_b200 import fields
