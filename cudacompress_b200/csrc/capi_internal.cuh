@@ -145,6 +145,8 @@ enum SmemAttrKernel {
     kAttrTableBuild = 0,
     kAttrDecHuff16,
     kAttrDecHuff32,
+    kAttrWrite16,
+    kAttrWrite32,
     kAttrCount
 };
 cudaError_t ensureSmemAttribute(const void* kernel, int which, int device, size_t bytes);

@@ -55,7 +55,6 @@ struct EncParams {
     u32 buildLo, buildHi;   // k_tableBuild builds the tables with buildLo <= leaves <= buildHi
 };
 
-constexpr u32 kSmemSymBins = 4096;
 
 // Error flag of the call, read once per block and shared so that every
 // thread of the block takes the same branch.
@@ -362,19 +361,28 @@ __global__ void __launch_bounds__(256) k_zeroHist(EncParams p) {
 // the group).  Entries are staged in shared memory at their positions within
 // the tile, then copied out with consecutive threads on consecutive entries.
 // Both histograms are counted over the staged entries: the eight most
-// frequent keys of each (zero counts 0..7, symbols 1..8) with warp ballots,
-// the others with shared-memory atomics.  A tile whose entries exceed the
-// stage (a zero run of millions ends in it) writes them directly.
+// frequent keys of each (zero counts 0..7, symbols 1..8) in per-lane
+// counters, the others with shared-memory atomics.  The stage (dynamic
+// shared memory) holds a whole tile's entries for 16-bit symbols - up to one
+// per symbol, plus the (0, 255) entries of zero runs inside the tile - so
+// only a tile that a zero run of millions of symbols ends in writes its
+// entries directly (and counts them with warp-aggregated atomics).
 constexpr u32 kWriteSymBins = 4096;   // symbol bins counted in shared memory by k_write
 
 template <class Sym>
+constexpr u32 writeStage() { return sizeof(Sym) == 2 ? kRleTile + kRleTile / 256u : kRleTile / 2u; }
+template <class Sym>
+constexpr size_t writeSmem() { return 2 * sizeof(Sym) * size_t(writeStage<Sym>()); }
+
+template <class Sym>
 __global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
-    constexpr u32 kStage = sizeof(Sym) == 2 ? 4096u : 2048u;
+    constexpr u32 kStage = writeStage<Sym>();
+    extern __shared__ __align__(16) unsigned char dynWrite[];
     __shared__ u32 sLast[kRleWarps], sEnt[kRleWarps];
     __shared__ u32 hSym[kWriteSymBins];
     __shared__ u32 hZc[256];
-    __shared__ __align__(16) Sym sComp[kStage];
-    __shared__ __align__(16) Sym sZcs[kStage];
+    Sym* const sComp = reinterpret_cast<Sym*>(dynWrite);
+    Sym* const sZcs = sComp + kStage;
     __shared__ u32 sStream;
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) sStream = streamOfTile(p, blockIdx.x);
@@ -470,8 +478,8 @@ __global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
     const bool fast = staged && mZ.histSize == 256u && smemBins > 8u;   // block-uniform
     // the eight most frequent keys of each histogram (zero counts 0..7,
     // symbols 1..8) in per-lane 8-bit counters, four keys per register (at
-    // most kStage / kRleThreads = 16 entries per lane), added once per warp
-    // at the end; integer ALU work only
+    // most ceil(kStage / kRleThreads) = 33 entries per lane), added once per
+    // warp at the end; integer ALU work only
     u32 z03 = 0, z47 = 0, s03 = 0, s47 = 0;
     bool rangeErr = false;
     for (u32 j0 = 0; j0 < entries; j0 += kRleThreads) {
@@ -1124,7 +1132,14 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     { SectionTimer t(I, "enc.rle_scan", st); k_scan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
-    if (p.totalTiles) { SectionTimer t(I, "enc.rle_write_hist", st); k_write<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
+    if (p.totalTiles) {
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_write<Sym>),
+                                        sizeof(Sym) == 2 ? kAttrWrite16 : kAttrWrite32, I->device, writeSmem<Sym>()),
+                    "write smem");
+        SectionTimer t(I, "enc.rle_write_hist", st);
+        k_write<Sym><<<p.totalTiles, kRleThreads, writeSmem<Sym>(), st>>>(p);
+        countLaunch();
+    }
     size_t buildSmem = sizeof(u64) * (p.heapCap + 2) + 3 * sizeof(u32) * size_t(p.heapCap);
     // an instance whose tables run beside other kernels (the batched codec's
     // lowpass encode) may ask for an SM of its own per table: the sequential
@@ -1192,6 +1207,12 @@ int prepareKernelAttributes(cc_instance* I) {
     if (I->tableBuildSoloSM) buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
     CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
+    if (I->symBytes == 2)
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_write<u16>), kAttrWrite16, I->device,
+                                        writeSmem<u16>()), "write smem");
+    else
+        CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_write<u32>), kAttrWrite32, I->device,
+                                        writeSmem<u32>()), "write smem");
     return prepareDecodeAttributes(I);
 }
 
