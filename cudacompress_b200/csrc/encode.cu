@@ -932,12 +932,12 @@ __device__ __forceinline__ void orCodeword(u32* win, u32 wLo, u32 wHi, u32 pos, 
 // run (gather ownership: no atomics on global memory, no pre-zeroing),
 // assembling them in a shared-memory window; the bits of the last owned word
 // that belong to the next run are recomputed from that run's first symbols.
-// A lane looks its codes up twice (lengths, then codes), keeping registers
-// for the symbols only.
+// A lane looks each code up once and keeps code and length packed in a
+// register until its bit offset is known.
 constexpr u32 kPackWindowWords = kRunSymbols * 31u / 32u + 2u;
 
 template <class Sym>
-__global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
+__global__ void __launch_bounds__(kPackWarps * 32, 3) k_pack(EncParams p) {
     __shared__ u32 winAll[kPackWarps * kPackWindowWords];
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warpFailed(p)) return;
@@ -962,12 +962,24 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
         const uint2* enc = p.enc + m.histOff;
         const u32 hs = m.histSize;
         const u32 j0 = rb * kRunSymbols + lane * 32u;
-        LaneRun<Sym> sv;
-        sv.load(in, j0, count);
+        // one lookup per symbol: code and length kept packed (code << 5 |
+        // length) while the lane's bit offset is scanned; a warp meeting a
+        // code longer than 27 bits looks its codes up again instead
+        u32 pk[32];
         u32 lsum = 0;
+        bool longCode = false;
+        {
+            LaneRun<Sym> sv;
+            sv.load(in, j0, count);
 #pragma unroll
-        for (u32 k = 0; k < 32; ++k)
-            if (j0 + k < count) lsum += enc[min(sv.at(k), hs - 1u)].y;
+            for (u32 k = 0; k < 32; ++k) {
+                const uint2 c = j0 + k < count ? enc[min(sv.at(k), hs - 1u)] : make_uint2(0u, 0u);
+                lsum += c.y;
+                longCode |= c.y > 27u;
+                pk[k] = (c.x << 5) | c.y;
+            }
+        }
+        const bool reload = __any_sync(0xffffffffu, longCode);
         __syncwarp();
         // the lane's codewords are consecutive: concatenate them in a 64-bit
         // accumulator (bits left-aligned from the lane's start bit in its
@@ -978,18 +990,28 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_pack(EncParams p) {
             u32 w = pos >> 5;
             u32 n = pos & 31u;
             unsigned long long acc = 0;
-#pragma unroll
-            for (u32 k = 0; k < 32; ++k) {
-                const uint2 c = j0 + k < count ? enc[min(sv.at(k), hs - 1u)] : make_uint2(0u, 0u);
-                if (c.y) {
-                    acc |= (unsigned long long)c.x << (64u - n - c.y);
-                    n += c.y;
+            auto put = [&](u32 code, u32 len) {
+                if (len) {
+                    acc |= (unsigned long long)code << (64u - n - len);
+                    n += len;
                 }
                 if (n >= 32u) {
                     if (w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
                     acc <<= 32;
                     n -= 32u;
                     ++w;
+                }
+            };
+            if (!reload) {
+#pragma unroll
+                for (u32 k = 0; k < 32; ++k) put(pk[k] >> 5, pk[k] & 31u);
+            } else {
+                LaneRun<Sym> sv;
+                sv.load(in, j0, count);
+#pragma unroll
+                for (u32 k = 0; k < 32; ++k) {
+                    const uint2 c = j0 + k < count ? enc[min(sv.at(k), hs - 1u)] : make_uint2(0u, 0u);
+                    put(c.x, c.y);
                 }
             }
             if (n && w >= wLo && w < wHi) atomicOr(win + (w - wLo), u32(acc >> 32));
