@@ -254,6 +254,38 @@ def test_decode_huff_roundtrip(oracle, inst, kind):
         assert np.array_equal(host(outs[i]).view(np.uint16), streams[i])
 
 
+def fibonacci_stream(count, seed):
+    """Symbols 1..count with Fibonacci counts (code lengths up to count - 1
+    bits), shuffled."""
+    fib = [1, 1]
+    while len(fib) < count:
+        fib.append(fib[-1] + fib[-2])
+    s = np.repeat(np.arange(1, count + 1, dtype=np.uint16), fib)
+    np.random.default_rng(seed).shuffle(s)
+    return s
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_codes_longer_than_27_bits(oracle, kind):
+    """Codewords of 28-29 bits (the packer keeps codes of up to 27 bits
+    packed with their lengths and looks longer ones up again): streams,
+    tables and the decode identical to the oracle's."""
+    s = fibonacci_stream(30, seed=31 + kind)
+    n = len(s)
+    streams = np.stack([s, np.roll(s, 1000)])
+    with cc.Instance(0, 2, n, 128, 14) as big:
+        bs = encode_gpu(big, kind, streams)
+        ref_words, ref_bits, _ = oracle.encode(kind, streams)
+        assert bs.bit_size == ref_bits
+        assert np.array_equal(bs.raw(), ref_words)
+        outs = [torch.full((n,), -1, dtype=torch.int16, device="cuda") for _ in range(2)]
+        dec = cc.decode_rlhuff if kind == 0 else cc.decode_huff
+        assert dec(big, cc.BitStream(ref_words, ref_bits), outs, n), cc.last_error()
+        assert cc.decode_status(big) == 0
+        for i in range(2):
+            assert np.array_equal(host(outs[i]).view(np.uint16), streams[i])
+
+
 @pytest.mark.parametrize("cb", [32, 64, 256])
 def test_coding_block_sizes(oracle, cb):
     with cc.Instance(0, 4, 40000, cb, 14) as inst_cb:
