@@ -223,6 +223,8 @@ struct cc_instance {
     ccb::u32* hist = nullptr;          // [capHist]
     uint2* enc = nullptr;              // [capHist] (code, len) by symbol
     ccb::TableMeta* meta = nullptr;    // [capTables]
+    ccb::u32* bigTables = nullptr;     // [capTables]: tables the big-heap build walks (k_histPlan)
+    ccb::u32* midTables = nullptr;     // [capTables]: tables the medium-heap build walks
     ccb::u32* headers = nullptr;       // [capHdr]
     ccb::u32* blockBits = nullptr;     // [capBlocks]
     ccb::u32* blockOff = nullptr;      // [capBlocks]

@@ -51,8 +51,11 @@ struct EncParams {
     u32* parentWork;
     u32* orderWork;
     u32* leafSymWork;
+    u32* bigTables;   // tables whose leaf bound exceeds kBuildSplitLeaves (k_histPlan); count in totals[4]
+    u32* midTables;   // tables whose leaf bound exceeds kTinyLeaves; count in totals[5]
     u32 heapCap;      // leaves that fit the shared-memory builder of tableBuild
     u32 buildLo, buildHi;   // k_tableBuild builds the tables with buildLo <= leaves <= buildHi
+    u32 buildList;    // k_tableBuild: which tables its CTAs take (BuildList)
 };
 
 
@@ -292,13 +295,20 @@ __global__ void __launch_bounds__(1024) k_scan(EncParams p) {
     }
 }
 
+// Table builders by size (k_tableBuild): a warp per table of up to
+// kTinyLeaves leaves (5 KB of heap, up to 32 tables per SM), 256 threads and
+// a 41 KB heap up to kBuildSplitLeaves, the full heap above.
+constexpr u32 kTinyLeaves = 256;
+constexpr int kTinySegs = int(kTinyLeaves / 17u) + 1;   // sort segments longer than 16 keys
+constexpr u32 kBuildSplitLeaves = 2048;
+
 // Pass 3 (one block): histogram / builder / header offsets of every table,
 // sized from the largest symbol of its stream.  A symbol outside the
 // instance's 2^log2Max range fails the call (HuffmanTable.cu:411-419).
 __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
     __shared__ u32 scratch[40];
-    __shared__ unsigned long long cH, cL, cW, cA, cR;
-    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; cA = 0; cR = 0; }
+    __shared__ unsigned long long cH, cL, cW, cA, cR, cB, cM;
+    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; cA = 0; cR = 0; cB = 0; cM = 0; }
     __syncthreads();
     for (u32 base = 0; base < p.T; base += 1024) {
         const u32 t = base + threadIdx.x;
@@ -316,7 +326,18 @@ __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
             m.histSize = hs;
             m.blocks = u32(ceilDiv(count, p.cb));
         }
-        u32 tH, tL, tW, tA, tR;
+        // a table can have more leaves than a builder holds only if its bins
+        // and its symbols both exceed it: the lists of tables the medium and
+        // the big builders walk (a table on both is built by the one whose
+        // leaf range holds its exact leaf count)
+        const u32 bound = min(hs, m.count);
+        const u32 big = t < p.T && bound > kBuildSplitLeaves ? 1u : 0u;
+        const u32 mid = t < p.T && bound > kTinyLeaves ? 1u : 0u;
+        u32 tH, tL, tW, tA, tR, tB, tM;
+        const u32 eB = blockExclusiveSum<1024>(big, scratch, &tB);
+        const u32 eM = blockExclusiveSum<1024>(mid, scratch, &tM);
+        if (big) p.bigTables[cB + eB] = t;
+        if (mid) p.midTables[cM + eM] = t;
         const u32 eH = blockExclusiveSum<1024>(hs, scratch, &tH);
         const u32 eL = blockExclusiveSum<1024>(ls, scratch, &tL);
         const u32 eW = blockExclusiveSum<1024>(ws, scratch, &tW);
@@ -331,12 +352,14 @@ __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
             p.meta[t] = m;
         }
         __syncthreads();
-        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; cA += tA; cR += tR; }
+        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; cA += tA; cR += tR; cB += tB; cM += tM; }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         p.totals[2] = cA;
         p.totals[3] = cR;
+        p.totals[4] = cB;
+        p.totals[5] = cM;
         p.totals[1] = cH;
         if (cH > p.capHist || cL > p.capLeaves || cW > p.capHdr) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
     }
@@ -550,7 +573,6 @@ __global__ void __launch_bounds__(kRleThreads) k_write(EncParams p) {
 // global memory (huffman_build.cuh).
 // ---------------------------------------------------------------------------
 constexpr u32 kBuildThreads = 256;
-constexpr u32 kBuildSplitLeaves = 2048;   // tables built with a 41 KB shared-memory heap
 
 __device__ __forceinline__ void putBits(u32* words, u32 pos, u32 value, u32 count) {
     // MSB-first, count <= 32, words pre-zeroed; atomics because neighbouring
@@ -567,16 +589,19 @@ __device__ __forceinline__ void putBits(u32* words, u32 pos, u32 value, u32 coun
     }
 }
 
-__global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
+// Builds table t (all kThreads threads of the block; returns uniformly).
+// kSegs: the sort's segment queue (segments longer than 16 keys in a round:
+// at most heapCap / 17).
+template <u32 kThreads, int kSegs>
+__device__ void buildTable(const EncParams& p, u32 t) {
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ u32 sScan[40];
     __shared__ u32 sMax, sMaxLen, sAllEmpty;
     __shared__ u32 lenCount[32], firstIndex[33], firstCode[33];
-    __shared__ tb::Seg sSegA[tb::kMaxSegs], sSegB[tb::kMaxSegs];
+    __shared__ tb::Seg sSegA[kSegs], sSegB[kSegs];
     __shared__ int sSegCount[4];
     if (threadIdx.x == 0) { sMax = 0; sAllEmpty = 1; }
     if (blockFailed(p)) return;
-    const u32 t = blockIdx.x;
     const EncTableDev td = p.tables[t];
     const EncStreamDev es = p.streams[td.stream];
     TableMeta meta = p.meta[t];
@@ -586,11 +611,11 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
 
     // 1. largest present symbol
     if (es.kind == KIND_RLHUFF)
-        for (u32 s = es.groupFirst + threadIdx.x; s < es.groupFirst + es.groupSize; s += kBuildThreads)
+        for (u32 s = es.groupFirst + threadIdx.x; s < es.groupFirst + es.groupSize; s += kThreads)
             if (p.counts[s]) atomicAnd(&sAllEmpty, 0u);
     u32 localMax = 0;
     bool any = false;
-    for (u32 b = threadIdx.x; b < meta.histSize; b += kBuildThreads)
+    for (u32 b = threadIdx.x; b < meta.histSize; b += kThreads)
         if (hist[b]) { localMax = b; any = true; }
     if (any) atomicMax(&sMax, localMax);
     __syncthreads();
@@ -621,12 +646,12 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         if (L < p.buildLo || L > p.buildHi) return;
     } else {
         const u32 nb = symbolMax + 1;
-        const u32 per = (nb + kBuildThreads - 1) / kBuildThreads;
+        const u32 per = (nb + kThreads - 1) / kThreads;
         const u32 b0 = threadIdx.x * per, b1 = min(nb, b0 + per);
         u32 c = 0;
         for (u32 b = b0; b < b1; ++b) c += hist[b] ? 1u : 0u;
         u32 tot;
-        u32 off = blockExclusiveSum<kBuildThreads>(c, sScan, &tot);
+        u32 off = blockExclusiveSum<kThreads>(c, sScan, &tot);
         L = tot;
         if (L < p.buildLo || L > p.buildHi) return;
         const bool toSmem = L <= p.heapCap;
@@ -653,7 +678,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         __syncthreads();
         const u32 root = L >= 2 ? 2 * L - 2 : 0;
         u32 localMax = 0;
-        for (u32 i = threadIdx.x; i < L; i += kBuildThreads) {
+        for (u32 i = threadIdx.x; i < L; i += kThreads) {
             u32 d = 0, node = i;
             while (node != root && d < 32) { node = parentS[node]; ++d; }
             order[i] = (min(d, 31u) << 27) | i;
@@ -665,7 +690,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
             u16* lList = reinterpret_cast<u16*>(dyn);            // reuses the heap area (5 bytes per key)
             u16* rList = lList + p.heapCap;
             u8* mark = reinterpret_cast<u8*>(rList + p.heapCap);
-            tb::blockIntrosort<kBuildThreads>(order, int(L), lList, rList, mark, sSegA, sSegB, sSegCount);
+            tb::blockIntrosort<kThreads>(order, int(L), lList, rList, mark, sSegA, sSegB, sSegCount);
         }
     } else if (threadIdx.x == 0) {
         // tables larger than the shared-memory builder: sequential, global memory
@@ -695,7 +720,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         return;
     }
     // 4. canonical codes (HuffmanTable.cu:551-593)
-    for (u32 k = threadIdx.x; k < L; k += kBuildThreads) {
+    for (u32 k = threadIdx.x; k < L; k += kThreads) {
         u32 len = order[k] >> 27;
         if (len) atomicAdd(&lenCount[len - 1], 1u);
     }
@@ -712,7 +737,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     }
     __syncthreads();
     uint2* enc = p.enc + meta.histOff;
-    for (u32 k = threadIdx.x; k < L; k += kBuildThreads) {
+    for (u32 k = threadIdx.x; k < L; k += kThreads) {
         u32 len = order[k] >> 27;
         u32 sym = leafSym[order[k] & hb::kLeafMask];
         u32 code = len ? firstCode[len] + (k - firstIndex[len]) : 0u;
@@ -725,7 +750,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
     const u32 headerBits = fixedBits + L * symbolBits;
     u32* hdr = p.headers + meta.hdrOff;
     const u32 hdrWords = u32(ceilDiv(headerBits, 32));
-    for (u32 w = threadIdx.x; w < hdrWords; w += kBuildThreads) hdr[w] = 0;
+    for (u32 w = threadIdx.x; w < hdrWords; w += kThreads) hdr[w] = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
         u32 pos = 0;
@@ -734,7 +759,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         putBits(hdr, pos, L, p.log2Max); pos += p.log2Max;
         putBits(hdr, pos, symbolBits, longSym ? 5 : 4);
     }
-    for (u32 k = threadIdx.x; k < L; k += kBuildThreads)
+    for (u32 k = threadIdx.x; k < L; k += kThreads)
         putBits(hdr, fixedBits + k * symbolBits, leafSym[order[k] & hb::kLeafMask], symbolBits);
     if (threadIdx.x == 0) {
         meta.symbolMax = symbolMax;
@@ -743,6 +768,28 @@ __global__ void __launch_bounds__(kBuildThreads) k_tableBuild(EncParams p) {
         meta.headerBits = headerBits;
         meta.codeBits = 0;
         p.meta[t] = meta;
+    }
+}
+
+// Which tables a k_tableBuild launch builds (those of its leaf range among):
+enum BuildList : u32 {
+    kBuildEach = 0,   // table blockIdx.x
+    kBuildBig = 1,    // the big-bound list (bigTables, count totals[4]), grid-stride
+    kBuildMid = 2,    // the medium-bound list (midTables, count totals[5]), grid-stride
+};
+
+template <u32 kThreads, int kSegs>
+__global__ void __launch_bounds__(kThreads) k_tableBuild(EncParams p) {
+    if (p.buildList == kBuildEach) {
+        buildTable<kThreads, kSegs>(p, blockIdx.x);
+        return;
+    }
+    const bool big = p.buildList == kBuildBig;
+    const u32 n = u32(p.totals[big ? 4 : 5]);
+    const u32* list = big ? p.bigTables : p.midTables;
+    for (u32 i = blockIdx.x; i < n; i += gridDim.x) {
+        buildTable<kThreads, kSegs>(p, list[i]);
+        __syncthreads();   // the next table reuses the shared memory
     }
 }
 
@@ -756,7 +803,7 @@ static size_t tableBuildSoloSmem(int device) {
         int optin = 0;
         cudaFuncAttributes fa{};
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-        cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(k_tableBuild));
+        cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(k_tableBuild<kBuildThreads, tb::kMaxSegs>));
         cached[device] = optin > int(fa.sharedSizeBytes) ? size_t(optin) - fa.sharedSizeBytes : 0;
     }
     return cached[device];
@@ -1166,35 +1213,56 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     // an instance whose tables run beside other kernels (the batched codec's
     // lowpass encode) may ask for an SM of its own per table: the sequential
     // heap merge is latency-bound and loses issue slots to co-resident CTAs
-    if (I->tableBuildSoloSM && p.T <= u32(I->smCount)) buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
-    CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
+    if (I->tableBuildSoloSM && p.T <= u32(std::max(1, I->smCount > 0 ? I->smCount : 148)))
+        buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
+    CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild<kBuildThreads, tb::kMaxSegs>),
+                                    kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
     {
         SectionTimer t(I, "enc.table_build", st);
         EncParams q = p;
         q.buildLo = 0;
         q.buildHi = ~0u;
-        if (!I->tableBuildSoloSM && p.T > 1 && p.heapCap > kBuildSplitLeaves) {
-            // tables of up to kBuildSplitLeaves leaves with the shared memory
-            // they need (41 KB instead of 164 KB per CTA, so kernels of other
-            // calls in flight keep running beside the sequential merges); the
-            // larger ones at the same time in a launch on the side stream whose
-            // other CTAs return after counting their leaves
-            EncParams big = q;
-            big.buildLo = kBuildSplitLeaves + 1;
-            q.heapCap = kBuildSplitLeaves;
-            q.buildHi = kBuildSplitLeaves;
-            const size_t small = sizeof(u64) * (q.heapCap + 2) + 3 * sizeof(u32) * size_t(q.heapCap);
+        const u32 sms = u32(std::max(1, I->smCount > 0 ? I->smCount : 148));
+        const bool solo = I->tableBuildSoloSM && p.T <= sms;
+        auto heapBytes = [](u32 cap) { return sizeof(u64) * (cap + 2) + 3 * sizeof(u32) * size_t(cap); };
+        if (!solo && p.heapCap > kTinyLeaves) {
+            // by size: every table of up to kTinyLeaves leaves on a warp (5 KB
+            // of heap; the sequential merges of many small tables run 32 per
+            // SM); at the same time on the side stream, the tables whose leaf
+            // bound exceeds that (k_histPlan's lists): one CTA per SM with the
+            // full heap walks the big list, then 256-thread CTAs with a 41 KB
+            // heap walk the medium list.  Each builder takes the tables of its
+            // leaf range only, so every table is built once.
             CC_TRY_CUDA(cudaEventRecord(I->buildFork, st), "table build fork");
             CC_TRY_CUDA(cudaStreamWaitEvent(I->buildSide, I->buildFork, 0), "table build fork");
-            k_tableBuild<<<p.T, kBuildThreads, buildSmem, I->buildSide>>>(big);
+            if (p.heapCap > kBuildSplitLeaves) {
+                EncParams big = q;
+                big.buildList = kBuildBig;
+                big.buildLo = kBuildSplitLeaves + 1;
+                k_tableBuild<kBuildThreads, tb::kMaxSegs><<<std::min(p.T, sms), kBuildThreads, buildSmem, I->buildSide>>>(big);
+                countLaunch();
+            }
+            EncParams mid = q;
+            mid.buildList = kBuildMid;
+            mid.buildLo = kTinyLeaves + 1;
+            mid.buildHi = kBuildSplitLeaves;
+            mid.heapCap = std::min(p.heapCap, kBuildSplitLeaves);
+            k_tableBuild<kBuildThreads, tb::kMaxSegs><<<std::min(p.T, 5u * sms), kBuildThreads, heapBytes(mid.heapCap),
+                                                         I->buildSide>>>(mid);
             countLaunch();
             CC_TRY_CUDA(cudaEventRecord(I->buildJoin, I->buildSide), "table build join");
-            k_tableBuild<<<p.T, kBuildThreads, small, st>>>(q);
+            EncParams tiny = q;
+            tiny.buildHi = kTinyLeaves;
+            tiny.heapCap = kTinyLeaves;
+            k_tableBuild<32u, kTinySegs><<<p.T, 32, heapBytes(kTinyLeaves), st>>>(tiny);
             countLaunch();
             CC_TRY_CUDA(cudaStreamWaitEvent(st, I->buildJoin, 0), "table build join");
+        } else if (!solo) {
+            k_tableBuild<32u, kTinySegs><<<p.T, 32, heapBytes(p.heapCap), st>>>(q);
+            countLaunch();
         } else {
-            k_tableBuild<<<p.T, kBuildThreads, buildSmem, st>>>(q);
+            k_tableBuild<kBuildThreads, tb::kMaxSegs><<<p.T, kBuildThreads, buildSmem, st>>>(q);
             countLaunch();
         }
     }
@@ -1227,7 +1295,8 @@ int prepareKernelAttributes(cc_instance* I) {
     const u32 heapCap = std::min<u32>(I->leavesMax, kBuildSmemLeaves);
     size_t buildSmem = sizeof(u64) * (heapCap + 2) + 3 * sizeof(u32) * size_t(heapCap);
     if (I->tableBuildSoloSM) buildSmem = std::max(buildSmem, tableBuildSoloSmem(I->device));
-    CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild), kAttrTableBuild, I->device, buildSmem),
+    CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_tableBuild<kBuildThreads, tb::kMaxSegs>),
+                                    kAttrTableBuild, I->device, buildSmem),
                 "tableBuild smem");
     if (I->symBytes == 2)
         CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_write<u16>), kAttrWrite16, I->device,
@@ -1286,6 +1355,8 @@ int encodeLaunch(cc_instance* I, const EncPlan& hp, u32* out, u64 outCap) {
     p.parentWork = I->parentWork;
     p.orderWork = I->orderWork;
     p.leafSymWork = I->leafSymWork;
+    p.bigTables = I->bigTables;
+    p.midTables = I->midTables;
     p.heapCap = std::min<u32>(std::min<u32>(I->leavesMax, kBuildSmemLeaves), hp.maxCount + 1u);
     return I->symBytes == 2 ? launchEncode<u16>(I, p) : launchEncode<u32>(I, p);
 }

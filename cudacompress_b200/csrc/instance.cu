@@ -150,6 +150,8 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->hist = c.take<u32>(I->capHist);
     I->enc = c.take<uint2>(I->capHist);
     I->meta = c.take<TableMeta>(I->capTables);
+    I->bigTables = c.take<u32>(I->capTables);
+    I->midTables = c.take<u32>(I->capTables);
     I->headers = c.take<u32>(I->capHdr);
     I->blockBits = c.take<u32>(I->capBlocks + 1);
     I->blockOff = c.take<u32>(I->capBlocks + 1);
