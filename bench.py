@@ -910,13 +910,30 @@ def run_heightfield(args, wl):
 def run_profile(args):
     """A small self-contained case for profilers (ncu): one batch of
     `--comps` seeded n^3 float32 fields (the vector field's generator and
-    seeds), `--warmup` encode + decode passes, then `--steps` more; no timing,
-    no other legs.  Launch order per step: the forward transform (one fused
+    seeds), or with `--workload bricks-4096` the 4096 uneven bricks, `--warmup`
+    encode + decode passes, then `--steps` more; no timing, no other legs.  Launch order per step: the forward transform (one fused
     launch per level, the quantizer included), the encoders, then the
     decoder and the inverse transform (three passes per level)."""
     import torch
     import cudacompress_b200 as cc
     from cudacompress_b200 import fields
+    if args.workload == "bricks-4096":
+        # the batched-vs-per-brick leg's brick set in one batch, at the
+        # autotuner's usual choice (coding block 64, tile depth 64)
+        wl = WORKLOADS["bricks-4096"]
+        bricks, q = fields.brick_set(wl["count"], wl["seed"])
+        vols = [torch.from_numpy(b).cuda() for b in bricks]
+        outs = [torch.empty_like(v) for v in vols]
+        with cc.Instance(0, 7, 32 ** 3, 64, 14) as inst:
+            with cc.VolumeBatch(inst, [v.shape for v in vols], wl["levels"], [float(x) for x in q], graph=True,
+                                z_chunk=64) as batch:
+                for _ in range(args.warmup + args.steps):
+                    batch.compress(vols)
+                    batch.decompress(outs)
+                torch.cuda.synchronize()
+                batch.status()
+        print(json.dumps({"profile_case": {"workload": args.workload, "passes": args.warmup + args.steps}}))
+        return
     n, C = args.n, args.comps
     vols = [torch.from_numpy(fields.turbulence_field(n, 1024, min(64, n // 4), seed)).cuda()
             for seed in fields.SEED_C2[:C]]

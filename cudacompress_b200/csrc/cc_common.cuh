@@ -60,6 +60,30 @@ __device__ __forceinline__ u32 warpMax(u32 v) {
     return v;
 }
 
+// Exclusive scan of in[0, n) into out by one warp (in == out allowed), each
+// lane taking eight consecutive elements per step; returns carry + the total.
+__device__ __forceinline__ u32 warpExclusiveScan8(const u32* in, u32* out, u32 n, u32 carry) {
+    const u32 lane = threadIdx.x & 31u;
+    for (u32 base = 0; base < n; base += 256) {
+        const u32 i0 = base + 8u * lane;
+        u32 v[8], sum = 0;
+#pragma unroll
+        for (u32 k = 0; k < 8; ++k) {
+            v[k] = i0 + k < n ? in[i0 + k] : 0u;
+            sum += v[k];
+        }
+        const u32 incl = warpInclusiveSum(sum);
+        u32 run = carry + incl - sum;
+#pragma unroll
+        for (u32 k = 0; k < 8; ++k) {
+            if (i0 + k < n) out[i0 + k] = run;
+            run += v[k];
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    return carry;
+}
+
 // Block-wide exclusive scan of one u32 per thread; returns the exclusive
 // prefix and writes the block total to *total.  `scratch` holds >= 33 u32.
 template <int kThreads>
@@ -80,6 +104,39 @@ __device__ __forceinline__ u32 blockExclusiveSum(u32 v, u32* scratch, u32* total
     if (total) *total = scratch[32];
     __syncthreads();
     return r;
+}
+
+// Block-wide exclusive scans of N values per thread at once (two barriers
+// for all N): ex[k] = the exclusive prefix of v[k], tot[k] = its block
+// total.  `scratch` holds >= 33 * N u32.
+template <int kThreads, int N>
+__device__ __forceinline__ void blockExclusiveSumN(const u32 (&v)[N], u32 (&ex)[N], u32 (&tot)[N], u32* scratch) {
+    static_assert(kThreads % 32 == 0 && kThreads <= 1024, "block size");
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    u32 inc[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) inc[k] = warpInclusiveSum(v[k]);
+    if (lane == 31) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) scratch[33 * k + warp] = inc[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const u32 w = lane < kThreads / 32 ? scratch[33 * k + lane] : 0u;
+            const u32 wi = warpInclusiveSum(w);
+            scratch[33 * k + lane] = wi - w;
+            if (lane == 31) scratch[33 * k + 32] = wi;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        ex[k] = scratch[33 * k + warp] + inc[k] - v[k];
+        tot[k] = scratch[33 * k + 32];
+    }
+    __syncthreads();
 }
 
 // Quantize.cuh:26-35: symbol = 2|v| for v >= 0, 2|v| - 1 for v < 0, and back.

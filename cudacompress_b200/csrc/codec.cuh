@@ -190,8 +190,8 @@ struct cc_instance {
     cudaStream_t stream = nullptr;
     // the table build's large-table launch runs on this side stream beside
     // the small-table launch on `stream` (fork / join by the two events)
-    cudaStream_t buildSide = nullptr;
-    cudaEvent_t buildFork = nullptr, buildJoin = nullptr;
+    cudaStream_t buildSide = nullptr, buildSide2 = nullptr;   // the table builders' other streams
+    cudaEvent_t buildFork = nullptr, buildJoin = nullptr, buildJoin2 = nullptr;
 
     // derived sizes
     ccb::u32 bins = 0;          // 1 << log2Max
@@ -223,8 +223,7 @@ struct cc_instance {
     ccb::u32* hist = nullptr;          // [capHist]
     uint2* enc = nullptr;              // [capHist] (code, len) by symbol
     ccb::TableMeta* meta = nullptr;    // [capTables]
-    ccb::u32* bigTables = nullptr;     // [capTables]: tables the big-heap build walks (k_histPlan)
-    ccb::u32* midTables = nullptr;     // [capTables]: tables the medium-heap build walks
+    ccb::u32* tierTables = nullptr;    // [4 capTables]: the tables of each leaf-count tier of a call
     ccb::u32* headers = nullptr;       // [capHdr]
     ccb::u32* blockBits = nullptr;     // [capBlocks]
     ccb::u32* blockOff = nullptr;      // [capBlocks]

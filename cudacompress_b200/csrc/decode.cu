@@ -184,17 +184,26 @@ __global__ void __launch_bounds__(64) k_decWalk(DecParams p) {
 
 // Symbol array offsets of the tables (prefix of nSym) and capacity check.
 __global__ void __launch_bounds__(1024) k_decSymPlan(DecParams p) {
+    constexpr u32 kPer = 4;   // consecutive tables per thread
     __shared__ u32 scratch[40];
     __shared__ unsigned long long carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (u32 base = 0; base < p.T; base += 1024) {
-        const u32 t = base + threadIdx.x;
-        u32 v = 0;
-        if (t < p.T) v = min(p.tables[t].nSym, p.leavesMax);
+    for (u32 base = 0; base < p.T; base += 1024 * kPer) {
+        const u32 t0 = base + threadIdx.x * kPer;
+        u32 v[kPer], sum = 0;
+#pragma unroll
+        for (u32 j = 0; j < kPer; ++j) {
+            v[j] = t0 + j < p.T ? min(p.tables[t0 + j].nSym, p.leavesMax) : 0u;
+            sum += v[j];
+        }
         u32 tot;
-        const u32 ex = blockExclusiveSum<1024>(v, scratch, &tot);
-        if (t < p.T) p.tables[t].symOff = u32(carry + ex);
+        unsigned long long at = carry + blockExclusiveSum<1024>(sum, scratch, &tot);
+#pragma unroll
+        for (u32 j = 0; j < kPer; ++j) {
+            if (t0 + j < p.T) p.tables[t0 + j].symOff = u32(at);
+            at += v[j];
+        }
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
         __syncthreads();
@@ -205,11 +214,14 @@ __global__ void __launch_bounds__(1024) k_decSymPlan(DecParams p) {
 // ---------------------------------------------------------------------------
 // Table parse and decode structures (HuffmanTable.cu:117-151, :205-266).
 // ---------------------------------------------------------------------------
-constexpr u32 kDecThreads = 256;
+// One 64-thread CTA per table (up to 32 tables per SM: the work per table is
+// a short chain of dependent steps).
+constexpr u32 kDecThreads = 64;
 
 __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
     __shared__ u32 cpl[32];
     __shared__ int sFirst[32], sMin[32], sMax[32];
+    __shared__ u32 sLim[kLutBits + 1];
     __shared__ u32 sScan[40];
     __shared__ u32 sCarry, sFail;
     const u32 t = blockIdx.x;
@@ -248,6 +260,13 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
             }
         }
         sFirst[31] = sMin[31] = sMax[31] = -1;
+        // left-justified kLutBits-bit limits: a prefix e holds a code of
+        // length l <= kLutBits iff sLim[l-1] <= e < sLim[l] (the canonical
+        // codes of one length are consecutive, each length starting where
+        // the previous one ends)
+        sLim[0] = 0;
+        for (u32 l = 1; l <= kLutBits; ++l)
+            sLim[l] = sMax[l - 1] >= 0 ? u32(sMax[l - 1] + 1) << (kLutBits - l) : sLim[l - 1];
         if (d.nLen == 0) ok = ok && d.nSym <= 1;
         else ok = ok && total == d.nSym;
         if (!ok) atomicOr(p.errors, DEV_ERR_CORRUPT);
@@ -269,14 +288,14 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
     const bool valueLut = p.symBytes == 2;
     if (valueLut) __syncthreads();   // syms[] of this table written above
     for (u32 e = threadIdx.x; e < (1u << kLutBits); e += kDecThreads) {
+        u32 below = 0;   // lengths whose codes all lie below e
+#pragma unroll
+        for (u32 l = 1; l <= kLutBits; ++l) below += e >= sLim[l] ? 1u : 0u;
+        const u32 l = below + 1;
         u32 entry = 0;
-        for (u32 l = 1; l <= kLutBits; ++l) {
-            int pref = int(e >> (kLutBits - l));
-            if (sMax[l - 1] >= 0 && pref <= sMax[l - 1]) {
-                const u32 idx = u32(sFirst[l - 1] + pref - sMin[l - 1]);
-                entry = (l << 24) | (valueLut ? syms[idx] : idx);
-                break;
-            }
+        if (l <= kLutBits) {
+            const u32 idx = u32(sFirst[l - 1] + int(e >> (kLutBits - l)) - sMin[l - 1]);
+            entry = (l << 24) | (valueLut ? syms[idx] : idx);
         }
         lut[e] = entry;
     }
@@ -291,23 +310,31 @@ __global__ void __launch_bounds__(kDecThreads) k_decTables(DecParams p) {
         D->single = p.symBytes == 2 ? (v0 & 0xFFFFu) : v0;
         sCarry = 0;
     }
-    // absolute block offsets: inclusive prefix of the u16 increments (PackInc.cu:220-229)
+    // absolute block offsets: inclusive prefix of the u16 increments
+    // (PackInc.cu:220-229), eight blocks (four words) per thread per step
     const u32 blocks = u32(ceilDiv(d.count, p.cb));
     u32* bo = p.blockOff + d.blockOff;
     __syncthreads();
-    for (u32 base = 0; base < blocks; base += kDecThreads) {
-        const u32 k = base + threadIdx.x;
-        u32 inc = 0;
-        if (k < blocks) {
-            const u32 w = ws.at(d.offWord + k / 2);
-            inc = (k & 1) ? (w >> 16) : (w & 0xFFFFu);
+    for (u32 base = 0; base < blocks; base += 8 * kDecThreads) {
+        const u32 k0 = base + 8 * threadIdx.x;
+        u32 inc[8], sum = 0;
+#pragma unroll
+        for (u32 j = 0; j < 4; ++j) {
+            const u32 w = k0 + 2 * j < blocks ? ws.at(d.offWord + k0 / 2 + j) : 0u;
+            inc[2 * j] = k0 + 2 * j < blocks ? (w & 0xFFFFu) : 0u;
+            inc[2 * j + 1] = k0 + 2 * j + 1 < blocks ? (w >> 16) : 0u;
+            sum += inc[2 * j] + inc[2 * j + 1];
         }
         u32 tot;
-        u32 ex = blockExclusiveSum<kDecThreads>(inc, sScan, &tot);
-        const u32 off = sCarry + ex + inc;
-        if (k < blocks) {
-            bo[k] = off;
-            if (off > d.cwBits) atomicOr(p.errors, DEV_ERR_CORRUPT);
+        const u32 ex = blockExclusiveSum<kDecThreads>(sum, sScan, &tot);
+        u32 off = sCarry + ex;
+#pragma unroll
+        for (u32 j = 0; j < 8; ++j) {
+            off += inc[j];
+            if (k0 + j < blocks) {
+                bo[k0 + j] = off;
+                if (off > d.cwBits) atomicOr(p.errors, DEV_ERR_CORRUPT);
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) sCarry += tot;
@@ -421,21 +448,32 @@ __device__ __forceinline__ u32 rlBlocksOf(const DecParams& p, const DecStreamDes
 // RLHuff stream's coding blocks in groups of 32, so that a warp's blocks
 // belong to one stream and warps without blocks are not started.
 __global__ void __launch_bounds__(1024) k_decRlTasks(DecParams p) {
+    constexpr u32 kPer = 4;   // consecutive streams per thread
     __shared__ u32 scratch[40];
     __shared__ u32 carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (u32 base = 0; base < p.nRl; base += 1024) {
-        const u32 k = base + threadIdx.x;
-        u32 s = 0, warps = 0;
-        if (k < p.nRl) {
-            s = p.rlList[k];
-            warps = u32(ceilDiv(rlBlocksOf(p, p.streams[s]), 32));
+    for (u32 base = 0; base < p.nRl; base += 1024 * kPer) {
+        const u32 k0 = base + threadIdx.x * kPer;
+        u32 s[kPer], warps[kPer], sum = 0;
+#pragma unroll
+        for (u32 j = 0; j < kPer; ++j) {
+            s[j] = 0;
+            warps[j] = 0;
+            if (k0 + j < p.nRl) {
+                s[j] = p.rlList[k0 + j];
+                warps[j] = u32(ceilDiv(rlBlocksOf(p, p.streams[s[j]]), 32));
+            }
+            sum += warps[j];
         }
         u32 tot;
-        const u32 ex = blockExclusiveSum<1024>(warps, scratch, &tot);
-        for (u32 i = 0; i < warps; ++i)
-            if (carry + ex + i < p.rlTaskCap) p.rlTasks[carry + ex + i] = (u64(s) << 32) | (32u * i);
+        u32 at = carry + blockExclusiveSum<1024>(sum, scratch, &tot);
+#pragma unroll
+        for (u32 j = 0; j < kPer; ++j) {
+            for (u32 i = 0; i < warps[j]; ++i)
+                if (at + i < p.rlTaskCap) p.rlTasks[at + i] = (u64(s[j]) << 32) | (32u * i);
+            at += warps[j];
+        }
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
         __syncthreads();
@@ -641,28 +679,16 @@ __global__ void __launch_bounds__(128) k_decRl(DecParams p) {
     if (corrupt) atomicOr(p.errors, DEV_ERR_CORRUPT);
 }
 
-// Exclusive scan of the per-block output lengths (one block per RLHuff stream).
-__global__ void __launch_bounds__(1024) k_decScan(DecParams p) {
-    __shared__ u32 scratch[40];
-    __shared__ u32 carry;
-    const u32 s = p.rlList[blockIdx.x];
-    const DecStreamDesc sd = p.streams[s];
+// Exclusive scan of the per-block output lengths: a warp per RLHuff stream.
+__global__ void __launch_bounds__(256) k_decScan(DecParams p) {
+    const u32 k = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (k >= p.nRl) return;
+    const DecStreamDesc sd = p.streams[p.rlList[k]];
     const u32 blocks = u32(ceilDiv(sd.m, p.cb));
     u32* bs = p.blockSum + p.tables[sd.tableFirst + 1].blockOff;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (u32 base = 0; base < blocks; base += 1024) {
-        const u32 i = base + threadIdx.x;
-        const u32 v = i < blocks ? bs[i] : 0u;
-        u32 tot;
-        const u32 ex = blockExclusiveSum<1024>(v, scratch, &tot);
-        if (i < blocks) bs[i] = carry + ex;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
-    }
+    const u32 total = warpExclusiveScan8(bs, bs, blocks, 0u);
     // the last symbol's position must be < n: total length <= n
-    if (threadIdx.x == 0 && carry > sd.n) atomicOr(p.errors, DEV_ERR_CORRUPT);
+    if ((threadIdx.x & 31u) == 0 && total > sd.n) atomicOr(p.errors, DEV_ERR_CORRUPT);
 }
 
 // ---------------------------------------------------------------------------
@@ -824,7 +850,7 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
             countLaunch();
         }
         { SectionTimer t(I, "dec.zero_counts", st); k_decRl<Sym, false><<<g, 128, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<p.nRl, 1024, 0, st>>>(p); countLaunch(); }
+        { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<u32(ceilDiv(p.nRl, 8)), 256, 0, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.symbols_scatter", st); k_decRl<Sym, true><<<g, 128, 0, st>>>(p); countLaunch(); }
     }
     CC_TRY_CUDA(cudaGetLastError(), "decode launch");

@@ -51,11 +51,10 @@ struct EncParams {
     u32* parentWork;
     u32* orderWork;
     u32* leafSymWork;
-    u32* bigTables;   // tables whose leaf bound exceeds kBuildSplitLeaves (k_histPlan); count in totals[4]
-    u32* midTables;   // tables whose leaf bound exceeds kTinyLeaves; count in totals[5]
+    u32* tierTables;  // [4][T]: the tables of each leaf-count tier (k_leafTiers); counts in totals[4..7]
     u32 heapCap;      // leaves that fit the shared-memory builder of tableBuild
     u32 buildLo, buildHi;   // k_tableBuild builds the tables with buildLo <= leaves <= buildHi
-    u32 buildList;    // k_tableBuild: which tables its CTAs take (BuildList)
+    u32 buildTier;    // k_tableBuild: kBuildEach (table blockIdx.x) or the tier whose list its CTAs walk
 };
 
 
@@ -186,16 +185,17 @@ __global__ void __launch_bounds__(256) k_lookupMaps(EncParams p) {
 }
 
 // The coding blocks in use (those holding symbols after the run-length
-// step), listed table by table: CTA t writes t over its meta.blocks entries
+// step), listed table by table: warp t writes t over its meta.blocks entries
 // from meta.actOff (k_histPlan).  The block-level kernels walk this list
 // instead of every block a table could have.
 __global__ void __launch_bounds__(256) k_usedBlocks(EncParams p) {
-    if (blockFailed(p)) return;
-    const u32 t = blockIdx.x;
+    if (warpFailed(p)) return;
+    const u32 t = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;   // a warp per table
+    if (t >= p.T) return;
     const TableMeta& m = p.meta[t];
-    for (u32 k = threadIdx.x; k < m.blocks; k += 256) p.blockTable[m.actOff + k] = t;
+    for (u32 k = lane; k < m.blocks; k += 32) p.blockTable[m.actOff + k] = t;
     const u32 runs = u32(ceilDiv(m.blocks, kRunSymbols / p.cb));
-    for (u32 k = threadIdx.x; k < runs; k += 256) p.runTable[m.runOff + k] = t;
+    for (u32 k = lane; k < runs; k += 32) p.runTable[m.runOff + k] = t;
 }
 
 // ---------------------------------------------------------------------------
@@ -247,121 +247,133 @@ __global__ void __launch_bounds__(kRleThreads) k_summary(EncParams p) {
     if (threadIdx.x == 0 && sMaxSym) atomicMax(p.streamMax + s, sMaxSym);
 }
 
-// Pass 2: one block per stream scans its tile summaries.
-__global__ void __launch_bounds__(1024) k_scan(EncParams p) {
-    __shared__ RunSum warpTot[32];
-    __shared__ RunSum carry;
-    const u32 s = blockIdx.x;
+constexpr u32 kScanWarps = 8;   // warps (streams or tables) per CTA of the per-unit scans
+
+// Pass 2: the scan of each stream's tile summaries, a warp per stream.
+__global__ void __launch_bounds__(kScanWarps * 32) k_scan(EncParams p) {
+    const u32 s = blockIdx.x * kScanWarps + (threadIdx.x >> 5);
+    if (s >= p.S) return;
+    const u32 lane = threadIdx.x & 31u;
     const EncStreamDev sd = p.streams[s];
     if (sd.kind != KIND_RLHUFF) {
-        if (threadIdx.x == 0) p.counts[s] = sd.n;
+        if (lane == 0) p.counts[s] = sd.n;
         return;
     }
     const u32 tiles = u32(ceilDiv(sd.n, kRleTile));
     const RunSum* T = p.tiles + sd.tileOff;
     TileStart* TS = p.tileStart + sd.tileOff;
-    if (threadIdx.x == 0) carry = RunSum{0, 0, 0, 0};
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (u32 base = 0; base < tiles; base += 1024) {
-        const u32 i = base + threadIdx.x;
-        RunSum inc = warpInclusiveRun(i < tiles ? T[i] : RunSum{0, 0, 0, 0});
-        if (lane == 31) warpTot[warp] = inc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            RunSum acc = carry;
-            for (int w = 0; w < 32; ++w) {
-                RunSum x = warpTot[w];
-                warpTot[w] = acc;
-                acc = runCombine(acc, x);
-            }
-            carry = acc;
-        }
-        __syncthreads();
+    RunSum carry{0, 0, 0, 0};
+    for (u32 base = 0; base < tiles; base += 32) {
+        const u32 i = base + lane;
+        const RunSum inc = warpInclusiveRun(i < tiles ? T[i] : RunSum{0, 0, 0, 0});
         RunSum ex = shflUpRun(inc, 1);
         if (lane == 0) ex = RunSum{0, 0, 0, 0};
-        RunSum E = runCombine(warpTot[warp], ex);
+        const RunSum E = runCombine(carry, ex);
         if (i < tiles) {
             TileStart ts;
             ts.prevP1 = E.cnt ? E.lastP1 : 0u;
             ts.out = E.cnt ? E.cnt + E.ext + (E.firstP1 - 1u) / 256u : 0u;
             TS[i] = ts;
         }
-        __syncthreads();
+        RunSum last;
+        last.cnt = __shfl_sync(0xffffffffu, inc.cnt, 31);
+        last.ext = __shfl_sync(0xffffffffu, inc.ext, 31);
+        last.firstP1 = __shfl_sync(0xffffffffu, inc.firstP1, 31);
+        last.lastP1 = __shfl_sync(0xffffffffu, inc.lastP1, 31);
+        carry = runCombine(carry, last);
     }
-    if (threadIdx.x == 0) {
-        const RunSum E = carry;
-        p.counts[s] = E.cnt ? E.cnt + E.ext + (E.firstP1 - 1u) / 256u : 0u;
-    }
+    if (lane == 0) p.counts[s] = carry.cnt ? carry.cnt + carry.ext + (carry.firstP1 - 1u) / 256u : 0u;
 }
 
-// Table builders by size (k_tableBuild): a warp per table of up to
-// kTinyLeaves leaves (5 KB of heap, up to 32 tables per SM), 256 threads and
-// a 41 KB heap up to kBuildSplitLeaves, the full heap above.
+// Table builders by leaf count (k_leafTiers sorts the tables, k_tableBuild
+// builds them): the heap merge is a latency-bound chain on one thread, so a
+// smaller table gets a smaller CTA and heap and more of them share an SM.
+//   tier 0: up to 256 leaves, a warp, 5 KB of heap (32 per SM)
+//   tier 1: up to 1024 leaves, 64 threads, 20 KB (11 per SM)
+//   tier 2: up to 2048 leaves, 256 threads, 41 KB (5 per SM)
+//   tier 3: more, 256 threads, the full heap (one per SM)
 constexpr u32 kTinyLeaves = 256;
-constexpr int kTinySegs = int(kTinyLeaves / 17u) + 1;   // sort segments longer than 16 keys
+constexpr u32 kSmallLeaves = 1024;
 constexpr u32 kBuildSplitLeaves = 2048;
+constexpr int kTinySegs = int(kTinyLeaves / 17u) + 1;    // sort segments longer than 16 keys
+constexpr int kSmallSegs = int(kSmallLeaves / 17u) + 1;
+constexpr u32 kBuildEach = 0xFFFFFFFFu;                  // buildTier: one table per CTA
 
 // Pass 3 (one block): histogram / builder / header offsets of every table,
 // sized from the largest symbol of its stream.  A symbol outside the
 // instance's 2^log2Max range fails the call (HuffmanTable.cu:411-419).
 __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
-    __shared__ u32 scratch[40];
-    __shared__ unsigned long long cH, cL, cW, cA, cR, cB, cM;
-    if (threadIdx.x == 0) { cH = 0; cL = 0; cW = 0; cA = 0; cR = 0; cB = 0; cM = 0; }
+    constexpr u32 kPer = 4;   // consecutive tables per thread (their loads in flight together)
+    __shared__ u32 scratch[33 * 7];
+    // running offsets: (unused), (unused), bins, leaves, header words, blocks, runs
+    __shared__ unsigned long long carry[7];
+    if (threadIdx.x < 7) carry[threadIdx.x] = 0;
     __syncthreads();
-    for (u32 base = 0; base < p.T; base += 1024) {
-        const u32 t = base + threadIdx.x;
-        u32 hs = 0, ls = 0, ws = 0;
-        TableMeta m{};
-        if (t < p.T) {
-            const EncTableDev td = p.tables[t];
-            const u32 smax = p.streamMax[td.stream];
-            const u32 count = p.counts[td.stream];
-            if (td.which == 0 && smax >= p.bins) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
-            hs = td.which ? min(256u, p.bins) : min(smax, p.bins - 1u) + 1u;
-            ls = min(hs, count + 1u);
-            ws = headerWordsFor(ls, p.log2Max);
-            m.count = count;
-            m.histSize = hs;
-            m.blocks = u32(ceilDiv(count, p.cb));
+    for (u32 base = 0; base < p.T; base += 1024 * kPer) {
+        const u32 t0 = base + threadIdx.x * kPer;
+        u32 v[kPer][7];
+        TableMeta m[kPer];
+#pragma unroll
+        for (u32 j = 0; j < kPer; ++j) {
+            const u32 t = t0 + j;
+            m[j] = TableMeta{};
+            u32 hs = 0, ls = 0, ws = 0;
+            if (t < p.T) {
+                const EncTableDev td = p.tables[t];
+                const u32 smax = p.streamMax[td.stream];
+                const u32 count = p.counts[td.stream];
+                if (td.which == 0 && smax >= p.bins) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
+                hs = td.which ? min(256u, p.bins) : min(smax, p.bins - 1u) + 1u;
+                ls = min(hs, count + 1u);
+                ws = headerWordsFor(ls, p.log2Max);
+                m[j].count = count;
+                m[j].histSize = hs;
+                m[j].blocks = u32(ceilDiv(count, p.cb));
+            }
+            v[j][0] = 0;
+            v[j][1] = 0;
+            v[j][2] = hs;
+            v[j][3] = ls;
+            v[j][4] = ws;
+            v[j][5] = m[j].blocks;
+            v[j][6] = u32(ceilDiv(m[j].blocks, kRunSymbols / p.cb));
         }
-        // a table can have more leaves than a builder holds only if its bins
-        // and its symbols both exceed it: the lists of tables the medium and
-        // the big builders walk (a table on both is built by the one whose
-        // leaf range holds its exact leaf count)
-        const u32 bound = min(hs, m.count);
-        const u32 big = t < p.T && bound > kBuildSplitLeaves ? 1u : 0u;
-        const u32 mid = t < p.T && bound > kTinyLeaves ? 1u : 0u;
-        u32 tH, tL, tW, tA, tR, tB, tM;
-        const u32 eB = blockExclusiveSum<1024>(big, scratch, &tB);
-        const u32 eM = blockExclusiveSum<1024>(mid, scratch, &tM);
-        if (big) p.bigTables[cB + eB] = t;
-        if (mid) p.midTables[cM + eM] = t;
-        const u32 eH = blockExclusiveSum<1024>(hs, scratch, &tH);
-        const u32 eL = blockExclusiveSum<1024>(ls, scratch, &tL);
-        const u32 eW = blockExclusiveSum<1024>(ws, scratch, &tW);
-        const u32 eA = blockExclusiveSum<1024>(m.blocks, scratch, &tA);
-        const u32 eR = blockExclusiveSum<1024>(u32(ceilDiv(m.blocks, kRunSymbols / p.cb)), scratch, &tR);
-        if (t < p.T) {
-            m.histOff = cH + eH;
-            m.leafOff = cL + eL;
-            m.hdrOff = cW + eW;
-            m.actOff = u32(cA + eA);
-            m.runOff = u32(cR + eR);
-            p.meta[t] = m;
+        u32 sum[7], ex[7], tot[7];
+#pragma unroll
+        for (u32 k = 0; k < 7; ++k) {
+            sum[k] = 0;
+#pragma unroll
+            for (u32 j = 0; j < kPer; ++j) sum[k] += v[j][k];
+        }
+        blockExclusiveSumN<1024, 7>(sum, ex, tot, scratch);
+        unsigned long long at[7];
+#pragma unroll
+        for (u32 k = 0; k < 7; ++k) at[k] = carry[k] + ex[k];
+#pragma unroll
+        for (u32 j = 0; j < kPer; ++j) {
+            const u32 t = t0 + j;
+            if (t < p.T) {
+                m[j].histOff = at[2];
+                m[j].leafOff = at[3];
+                m[j].hdrOff = at[4];
+                m[j].actOff = u32(at[5]);
+                m[j].runOff = u32(at[6]);
+                p.meta[t] = m[j];
+            }
+#pragma unroll
+            for (u32 k = 0; k < 7; ++k) at[k] += v[j][k];
         }
         __syncthreads();
-        if (threadIdx.x == 0) { cH += tH; cL += tL; cW += tW; cA += tA; cR += tR; cB += tB; cM += tM; }
+        if (threadIdx.x < 7) carry[threadIdx.x] += tot[threadIdx.x];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        p.totals[2] = cA;
-        p.totals[3] = cR;
-        p.totals[4] = cB;
-        p.totals[5] = cM;
-        p.totals[1] = cH;
-        if (cH > p.capHist || cL > p.capLeaves || cW > p.capHdr) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+        p.totals[2] = carry[5];
+        p.totals[3] = carry[6];
+        for (u32 k = 4; k < 8; ++k) p.totals[k] = 0;   // the tier lists' counts (k_leafTiers)
+        p.totals[1] = carry[2];
+        if (carry[2] > p.capHist || carry[3] > p.capLeaves || carry[4] > p.capHdr)
+            atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
     }
 }
 
@@ -369,6 +381,26 @@ __global__ void __launch_bounds__(256) k_zeroHist(EncParams p) {
     if (*reinterpret_cast<volatile const u32*>(p.errors)) return;   // no barriers in this kernel
     const u64 total = p.totals[1];
     for (u64 i = u64(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += u64(gridDim.x) * blockDim.x) p.hist[i] = 0;
+}
+
+// The leaf count of every table (the nonzero bins of its histogram; a warp
+// per table) and the tier list it goes on (tierTables, counts totals[4..7]).
+// A table whose histogram is empty (its stream has no symbols) goes on tier
+// 0, the only builder that may then give it a leaf.
+__global__ void __launch_bounds__(256) k_leafTiers(EncParams p) {
+    if (warpFailed(p)) return;
+    const u32 t = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    if (t >= p.T) return;
+    const TableMeta m = p.meta[t];
+    const u32* h = p.hist + m.histOff;
+    u32 c = 0;
+    for (u32 b = lane; b < m.histSize; b += 32) c += h[b] ? 1u : 0u;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) {
+        const u32 tier = c <= kTinyLeaves ? 0u : c <= kSmallLeaves ? 1u : c <= kBuildSplitLeaves ? 2u : 3u;
+        const u32 pos = u32(atomicAdd(reinterpret_cast<unsigned long long*>(p.totals + 4 + tier), 1ull));
+        p.tierTables[u64(tier) * p.T + pos] = t;
+    }
 }
 
 // Pass 4: compact symbols + zero counts (RLHuff) and both histograms, or the
@@ -771,22 +803,15 @@ __device__ void buildTable(const EncParams& p, u32 t) {
     }
 }
 
-// Which tables a k_tableBuild launch builds (those of its leaf range among):
-enum BuildList : u32 {
-    kBuildEach = 0,   // table blockIdx.x
-    kBuildBig = 1,    // the big-bound list (bigTables, count totals[4]), grid-stride
-    kBuildMid = 2,    // the medium-bound list (midTables, count totals[5]), grid-stride
-};
-
+// One table per CTA (kBuildEach), or the CTAs walk the list of one tier.
 template <u32 kThreads, int kSegs>
 __global__ void __launch_bounds__(kThreads) k_tableBuild(EncParams p) {
-    if (p.buildList == kBuildEach) {
+    if (p.buildTier == kBuildEach) {
         buildTable<kThreads, kSegs>(p, blockIdx.x);
         return;
     }
-    const bool big = p.buildList == kBuildBig;
-    const u32 n = u32(p.totals[big ? 4 : 5]);
-    const u32* list = big ? p.bigTables : p.midTables;
+    const u32 n = u32(p.totals[4 + p.buildTier]);
+    const u32* list = p.tierTables + u64(p.buildTier) * p.T;
     for (u32 i = blockIdx.x; i < n; i += gridDim.x) {
         buildTable<kThreads, kSegs>(p, list[i]);
         __syncthreads();   // the next table reuses the shared memory
@@ -882,30 +907,53 @@ __global__ void __launch_bounds__(kPackWarps * 32) k_blockBits(EncParams p) {
     }
 }
 
-// Exclusive scan of one table's block bits (one block per table).
-__global__ void __launch_bounds__(1024) k_blockScan(EncParams p) {
-    __shared__ u32 scratch[40];
-    __shared__ u32 carry;
-    if (threadIdx.x == 0) carry = 0;
-    if (blockFailed(p)) return;
-    const u32 t = blockIdx.x;
+// Exclusive scan of each table's block bits: a warp per table, each lane
+// summing eight consecutive blocks per step (256 blocks per step).
+__global__ void __launch_bounds__(kScanWarps * 32) k_blockScan(EncParams p) {
+    if (warpFailed(p)) return;
+    const u32 t = blockIdx.x * kScanWarps + (threadIdx.x >> 5);
+    if (t >= p.T) return;
     const u32 blocks = p.meta[t].blocks;
-    const u32* bb = p.blockBits + p.tables[t].blockOff;
-    u32* bo = p.blockOff + p.tables[t].blockOff;
-    for (u32 base = 0; base < blocks; base += 1024) {
-        const u32 i = base + threadIdx.x;
-        const u32 v = i < blocks ? bb[i] : 0u;
-        u32 tot;
-        const u32 ex = blockExclusiveSum<1024>(v, scratch, &tot);
-        if (i < blocks) bo[i] = carry + ex;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) p.meta[t].codeBits = carry;
+    const u32 off = p.tables[t].blockOff;
+    const u32 total = warpExclusiveScan8(p.blockBits + off, p.blockOff + off, blocks, 0u);
+    if ((threadIdx.x & 31u) == 0) p.meta[t].codeBits = total;
 }
 
-// Segment layout per stream and exclusive scan over streams (one block).
+// Segment layout per stream (a thread per stream), then the exclusive scan
+// of the segments' words over the streams (one block).
+__global__ void __launch_bounds__(256) k_layoutSegments(EncParams p) {
+    if (*reinterpret_cast<volatile const u32*>(p.errors)) return;   // no barriers in this kernel
+    const u32 s = blockIdx.x * 256u + threadIdx.x;
+    if (s >= p.S) return;
+    SegmentLayout L{};
+    const EncStreamDev sd = p.streams[s];
+    const u32 offW = u32(ceilDiv(ceilDiv(p.counts[s], p.cb), 2));
+    const TableMeta ms = p.meta[sd.tableFirst];
+    u32 words;
+    if (sd.kind == KIND_RLHUFF) {
+        const TableMeta mz = p.meta[sd.tableFirst + 1];
+        L.countWord = 0;
+        L.hdrWord[0] = 1;
+        L.cwWord[0] = L.hdrWord[0] + u32(ceilDiv(ms.headerBits, 32)) + 1;
+        L.offWord[0] = L.cwWord[0] + u32(ceilDiv(ms.codeBits, 32));
+        L.hdrWord[1] = L.offWord[0] + offW;
+        L.cwWord[1] = L.hdrWord[1] + u32(ceilDiv(mz.headerBits, 32)) + 1;
+        L.offWord[1] = L.cwWord[1] + u32(ceilDiv(mz.codeBits, 32));
+        words = L.offWord[1] + offW;
+        L.startBit = 0;
+    } else {
+        const u32 r = sd.startBit;
+        L.hdrWord[0] = 0;
+        L.cwWord[0] = u32(ceilDiv(r + ms.headerBits, 32)) + 1;
+        L.offWord[0] = L.cwWord[0] + u32(ceilDiv(ms.codeBits, 32));
+        words = L.offWord[0] + offW;
+        L.startBit = r;
+    }
+    L.words = words;
+    L.bitLength = words * 32u;
+    p.layout[s] = L;
+}
+
 __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
     __shared__ u32 scratch[40];
     __shared__ unsigned long long carry;
@@ -913,41 +961,11 @@ __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
     if (blockFailed(p)) return;
     for (u32 base = 0; base < p.S; base += 1024) {
         const u32 s = base + threadIdx.x;
-        SegmentLayout L{};
-        u32 words = 0;
-        if (s < p.S) {
-            const EncStreamDev sd = p.streams[s];
-            const u32 offW = u32(ceilDiv(ceilDiv(p.counts[s], p.cb), 2));
-            const TableMeta ms = p.meta[sd.tableFirst];
-            if (sd.kind == KIND_RLHUFF) {
-                const TableMeta mz = p.meta[sd.tableFirst + 1];
-                L.countWord = 0;
-                L.hdrWord[0] = 1;
-                L.cwWord[0] = L.hdrWord[0] + u32(ceilDiv(ms.headerBits, 32)) + 1;
-                L.offWord[0] = L.cwWord[0] + u32(ceilDiv(ms.codeBits, 32));
-                L.hdrWord[1] = L.offWord[0] + offW;
-                L.cwWord[1] = L.hdrWord[1] + u32(ceilDiv(mz.headerBits, 32)) + 1;
-                L.offWord[1] = L.cwWord[1] + u32(ceilDiv(mz.codeBits, 32));
-                words = L.offWord[1] + offW;
-                L.startBit = 0;
-            } else {
-                const u32 r = sd.startBit;
-                L.hdrWord[0] = 0;
-                L.cwWord[0] = u32(ceilDiv(r + ms.headerBits, 32)) + 1;
-                L.offWord[0] = L.cwWord[0] + u32(ceilDiv(ms.codeBits, 32));
-                words = L.offWord[0] + offW;
-                L.startBit = r;
-            }
-            L.words = words;
-            L.bitLength = words * 32u;
-        }
+        const u32 words = s < p.S ? p.layout[s].words : 0u;
         // 64-bit carry across chunks; within a chunk a 32-bit scan suffices
         u32 tot;
         const u32 ex = blockExclusiveSum<1024>(words, scratch, &tot);
-        if (s < p.S) {
-            L.startWord = carry + ex;
-            p.layout[s] = L;
-        }
+        if (s < p.S) p.layout[s].startWord = carry + ex;
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
         __syncthreads();
@@ -1198,7 +1216,11 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     CC_TRY_CUDA(cudaMemsetAsync(I->streamMax, 0, sizeof(u32) * p.S, st), "memset stream max");
     if (p.S) { k_lookupMaps<<<p.S, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) { SectionTimer t(I, "enc.summary", st); k_summary<Sym><<<p.totalTiles, kRleThreads, 0, st>>>(p); countLaunch(); }
-    { SectionTimer t(I, "enc.rle_scan", st); k_scan<<<p.S, 1024, 0, st>>>(p); countLaunch(); }
+    {
+        SectionTimer t(I, "enc.rle_scan", st);
+        k_scan<<<u32(ceilDiv(p.S, kScanWarps)), kScanWarps * 32, 0, st>>>(p);
+        countLaunch();
+    }
     { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
     { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) {
@@ -1223,44 +1245,58 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         EncParams q = p;
         q.buildLo = 0;
         q.buildHi = ~0u;
+        q.buildTier = kBuildEach;
         const u32 sms = u32(std::max(1, I->smCount > 0 ? I->smCount : 148));
         const bool solo = I->tableBuildSoloSM && p.T <= sms;
         auto heapBytes = [](u32 cap) { return sizeof(u64) * (cap + 2) + 3 * sizeof(u32) * size_t(cap); };
-        if (!solo && p.heapCap > kTinyLeaves) {
-            // by size: every table of up to kTinyLeaves leaves on a warp (5 KB
-            // of heap; the sequential merges of many small tables run 32 per
-            // SM); at the same time on the side stream, the tables whose leaf
-            // bound exceeds that (k_histPlan's lists): one CTA per SM with the
-            // full heap walks the big list, then 256-thread CTAs with a 41 KB
-            // heap walk the medium list.  Each builder takes the tables of its
-            // leaf range only, so every table is built once.
-            CC_TRY_CUDA(cudaEventRecord(I->buildFork, st), "table build fork");
-            CC_TRY_CUDA(cudaStreamWaitEvent(I->buildSide, I->buildFork, 0), "table build fork");
-            if (p.heapCap > kBuildSplitLeaves) {
-                EncParams big = q;
-                big.buildList = kBuildBig;
-                big.buildLo = kBuildSplitLeaves + 1;
-                k_tableBuild<kBuildThreads, tb::kMaxSegs><<<std::min(p.T, sms), kBuildThreads, buildSmem, I->buildSide>>>(big);
+        if (!solo) {
+            // tables sorted by leaf count, each tier's list walked by its own
+            // builder, at the same time: tier 0 on the instance stream, tier 1
+            // on the second side stream, tiers 3 and 2 on the first
+            k_leafTiers<<<u32(ceilDiv(p.T, 8)), 256, 0, st>>>(q);
+            countLaunch();
+            const bool side = p.heapCap > kSmallLeaves, side2 = p.heapCap > kTinyLeaves;
+            if (side2) {
+                CC_TRY_CUDA(cudaEventRecord(I->buildFork, st), "table build fork");
+                CC_TRY_CUDA(cudaStreamWaitEvent(I->buildSide2, I->buildFork, 0), "table build fork");
+                EncParams small = q;
+                small.buildTier = 1;
+                small.buildLo = kTinyLeaves + 1;
+                small.buildHi = kSmallLeaves;
+                small.heapCap = std::min(p.heapCap, kSmallLeaves);
+                k_tableBuild<64u, kSmallSegs>
+                    <<<std::min(p.T, 10u * sms), 64, heapBytes(small.heapCap), I->buildSide2>>>(small);
                 countLaunch();
+                CC_TRY_CUDA(cudaEventRecord(I->buildJoin2, I->buildSide2), "table build join");
             }
-            EncParams mid = q;
-            mid.buildList = kBuildMid;
-            mid.buildLo = kTinyLeaves + 1;
-            mid.buildHi = kBuildSplitLeaves;
-            mid.heapCap = std::min(p.heapCap, kBuildSplitLeaves);
-            k_tableBuild<kBuildThreads, tb::kMaxSegs><<<std::min(p.T, 5u * sms), kBuildThreads, heapBytes(mid.heapCap),
-                                                         I->buildSide>>>(mid);
-            countLaunch();
-            CC_TRY_CUDA(cudaEventRecord(I->buildJoin, I->buildSide), "table build join");
+            if (side) {
+                CC_TRY_CUDA(cudaStreamWaitEvent(I->buildSide, I->buildFork, 0), "table build fork");
+                if (p.heapCap > kBuildSplitLeaves) {
+                    EncParams big = q;
+                    big.buildTier = 3;
+                    big.buildLo = kBuildSplitLeaves + 1;
+                    k_tableBuild<kBuildThreads, tb::kMaxSegs>
+                        <<<std::min(p.T, sms), kBuildThreads, buildSmem, I->buildSide>>>(big);
+                    countLaunch();
+                }
+                EncParams mid = q;
+                mid.buildTier = 2;
+                mid.buildLo = kSmallLeaves + 1;
+                mid.buildHi = kBuildSplitLeaves;
+                mid.heapCap = std::min(p.heapCap, kBuildSplitLeaves);
+                k_tableBuild<kBuildThreads, tb::kMaxSegs>
+                    <<<std::min(p.T, 5u * sms), kBuildThreads, heapBytes(mid.heapCap), I->buildSide>>>(mid);
+                countLaunch();
+                CC_TRY_CUDA(cudaEventRecord(I->buildJoin, I->buildSide), "table build join");
+            }
             EncParams tiny = q;
+            tiny.buildTier = 0;
             tiny.buildHi = kTinyLeaves;
-            tiny.heapCap = kTinyLeaves;
-            k_tableBuild<32u, kTinySegs><<<p.T, 32, heapBytes(kTinyLeaves), st>>>(tiny);
+            tiny.heapCap = std::min(p.heapCap, kTinyLeaves);
+            k_tableBuild<32u, kTinySegs><<<std::min(p.T, 32u * sms), 32, heapBytes(tiny.heapCap), st>>>(tiny);
             countLaunch();
-            CC_TRY_CUDA(cudaStreamWaitEvent(st, I->buildJoin, 0), "table build join");
-        } else if (!solo) {
-            k_tableBuild<32u, kTinySegs><<<p.T, 32, heapBytes(p.heapCap), st>>>(q);
-            countLaunch();
+            if (side2) CC_TRY_CUDA(cudaStreamWaitEvent(st, I->buildJoin2, 0), "table build join");
+            if (side) CC_TRY_CUDA(cudaStreamWaitEvent(st, I->buildJoin, 0), "table build join");
         } else {
             k_tableBuild<kBuildThreads, tb::kMaxSegs><<<p.T, kBuildThreads, buildSmem, st>>>(q);
             countLaunch();
@@ -1268,16 +1304,26 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
     }
     // used-block list (after the plan, k_histPlan); the block kernels walk it
     // with a grid of a few CTAs per SM
-    if (p.totalBlocks && p.T) { k_usedBlocks<<<p.T, 256, 0, st>>>(p); countLaunch(); }
+    if (p.totalBlocks && p.T) { k_usedBlocks<<<u32(ceilDiv(p.T, 8)), 256, 0, st>>>(p); countLaunch(); }
     const u32 blockGrid = u32(std::max(1, I->smCount > 0 ? I->smCount : 148)) * 8u;
     // runs of the call: at most the used blocks / blocks per run, plus one per table
     const u32 runBound = u32(ceilDiv(p.totalBlocks, kRunSymbols / p.cb)) + p.T;
     if (p.totalBlocks) {
         const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(runBound, kPackWarps)));
         { SectionTimer t(I, "enc.block_bits", st); k_blockBits<Sym><<<g, kPackWarps * 32, 0, st>>>(p); countLaunch(); }
-        { SectionTimer t(I, "enc.block_scan", st); k_blockScan<<<p.T, 1024, 0, st>>>(p); countLaunch(); }
+        {
+            SectionTimer t(I, "enc.block_scan", st);
+            k_blockScan<<<u32(ceilDiv(p.T, kScanWarps)), kScanWarps * 32, 0, st>>>(p);
+            countLaunch();
+        }
     }
-    { SectionTimer t(I, "enc.layout", st); k_layout<<<1, 1024, 0, st>>>(p); countLaunch(); }
+    {
+        SectionTimer t(I, "enc.layout", st);
+        k_layoutSegments<<<u32(ceilDiv(p.S, 256)), 256, 0, st>>>(p);
+        countLaunch();
+        k_layout<<<1, 1024, 0, st>>>(p);
+        countLaunch();
+    }
     if (p.totalBlocks) {
         const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(runBound, kPackWarps)));
         SectionTimer t(I, "enc.pack", st);
@@ -1355,8 +1401,7 @@ int encodeLaunch(cc_instance* I, const EncPlan& hp, u32* out, u64 outCap) {
     p.parentWork = I->parentWork;
     p.orderWork = I->orderWork;
     p.leafSymWork = I->leafSymWork;
-    p.bigTables = I->bigTables;
-    p.midTables = I->midTables;
+    p.tierTables = I->tierTables;
     p.heapCap = std::min<u32>(std::min<u32>(I->leavesMax, kBuildSmemLeaves), hp.maxCount + 1u);
     return I->symBytes == 2 ? launchEncode<u16>(I, p) : launchEncode<u32>(I, p);
 }

@@ -150,8 +150,7 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->hist = c.take<u32>(I->capHist);
     I->enc = c.take<uint2>(I->capHist);
     I->meta = c.take<TableMeta>(I->capTables);
-    I->bigTables = c.take<u32>(I->capTables);
-    I->midTables = c.take<u32>(I->capTables);
+    I->tierTables = c.take<u32>(4ull * I->capTables);
     I->headers = c.take<u32>(I->capHdr);
     I->blockBits = c.take<u32>(I->capBlocks + 1);
     I->blockOff = c.take<u32>(I->capBlocks + 1);
@@ -291,8 +290,10 @@ int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 el
         return cudaFail(e, "cudaHostAlloc(words)");
     }
     if ((e = cudaStreamCreateWithFlags(&I->buildSide, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&I->buildSide2, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&I->buildFork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&I->buildJoin, cudaEventDisableTiming)) != cudaSuccess) {
+        (e = cudaEventCreateWithFlags(&I->buildJoin, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&I->buildJoin2, cudaEventDisableTiming)) != cudaSuccess) {
         cc_destroy_instance(I);
         return cudaFail(e, "table build stream");
     }
@@ -326,7 +327,9 @@ void cc_destroy_instance(cc_instance* I) {
     if (I->hostWords) cudaFreeHost(I->hostWords);
     if (I->buildFork) cudaEventDestroy(I->buildFork);
     if (I->buildJoin) cudaEventDestroy(I->buildJoin);
+    if (I->buildJoin2) cudaEventDestroy(I->buildJoin2);
     if (I->buildSide) cudaStreamDestroy(I->buildSide);
+    if (I->buildSide2) cudaStreamDestroy(I->buildSide2);
     I->resolveTimings();
     for (cudaEvent_t e : I->freeEvents) cudaEventDestroy(e);
     if (I->arena) cudaFree(I->arena);
