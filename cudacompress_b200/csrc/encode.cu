@@ -298,6 +298,7 @@ constexpr u32 kBuildSplitLeaves = 2048;
 constexpr int kTinySegs = int(kTinyLeaves / 17u) + 1;    // sort segments longer than 16 keys
 constexpr int kSmallSegs = int(kSmallLeaves / 17u) + 1;
 constexpr u32 kBuildEach = 0xFFFFFFFFu;                  // buildTier: one table per CTA
+constexpr u32 kTierMinTables = 64;                       // calls of more tables use the tiers
 
 // Pass 3 (one block): histogram / builder / header offsets of every table,
 // sized from the largest symbol of its stream.  A symbol outside the
@@ -1098,7 +1099,7 @@ __global__ void __launch_bounds__(kPackWarps * 32, 3) k_pack(EncParams p) {
 }
 
 // Count words, table headers, codeword bit counts and offset increments.
-__global__ void __launch_bounds__(128) k_headers(EncParams p) {
+__global__ void __launch_bounds__(512) k_headers(EncParams p) {
     if (blockFailed(p)) return;
     const u32 s = blockIdx.x;
     const EncStreamDev sd = p.streams[s];
@@ -1249,7 +1250,10 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         const u32 sms = u32(std::max(1, I->smCount > 0 ? I->smCount : 148));
         const bool solo = I->tableBuildSoloSM && p.T <= sms;
         auto heapBytes = [](u32 cap) { return sizeof(u64) * (cap + 2) + 3 * sizeof(u32) * size_t(cap); };
-        if (!solo) {
+        // a call of few tables builds them in one launch, a CTA each (the
+        // tiers' pre-pass, launches and stream forks would cost it more than
+        // they save)
+        if (!solo && p.T > kTierMinTables) {
             // tables sorted by leaf count, each tier's list walked by its own
             // builder, at the same time: tier 0 on the instance stream, tier 1
             // on the second side stream, tiers 3 and 2 on the first
@@ -1330,7 +1334,7 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         k_pack<Sym><<<g, kPackWarps * 32, 0, st>>>(p);
         countLaunch();
     }
-    { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 128, 0, st>>>(p); countLaunch(); }
+    { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 512, 0, st>>>(p); countLaunch(); }
     CC_TRY_CUDA(cudaGetLastError(), "encode launch");
     return CC_OK;
 }
