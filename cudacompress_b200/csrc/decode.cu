@@ -390,11 +390,99 @@ __device__ __forceinline__ void decodeBlock(const Src& ws, const DecTable& D, co
     }
 }
 
+// One table's decode data in shared memory: the lookup table, and for codes
+// longer than it the left-justified limits - lim[l] = (maxCode[l] + 1) <<
+// (32 - l), carried over lengths without codes, so a 32-bit window v holds a
+// code longer than l iff v >= lim[l] (the canonical codes of one length are
+// consecutive and each length starts where the shorter ones end, so lim never
+// decreases) - and the first index / first code of each length.
+struct CanonSmem {
+    u32 lut[1u << kLutBits];
+    unsigned long long lim[36];   // lengths 1..31; 32..35 above every window
+    int first[32], minc[32];
+};
+
+// Stages table t into cs (all 32 lanes of the calling warp).
+__device__ __forceinline__ void stageCanon(CanonSmem& cs, const DecParams& p, u32 t) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32* g = p.lut + (u64(t) << kLutBits);
+    for (u32 e = lane; e < (1u << kLutBits); e += 32) cs.lut[e] = g[e];
+    const DecTable& D = p.dec[t];
+    const int mc = D.maxCode[lane];
+    const u32 l = lane + 1;
+    unsigned long long lim = l <= 31 && mc >= 0 ? (unsigned long long)(u32(mc) + 1u) << (32 - l) : 0ull;
+#pragma unroll
+    for (u32 d = 1; d < 32; d <<= 1) {
+        const unsigned long long o = __shfl_up_sync(0xffffffffu, lim, d);
+        if (lane >= d) lim = o > lim ? o : lim;   // running maximum
+    }
+    cs.lim[l] = l <= 31 ? lim : ~0ull;
+    if (lane < 4) cs.lim[32 + lane] = ~0ull;
+    if (lane == 0) cs.lim[0] = 0;
+    cs.first[lane] = D.firstIndex[lane];
+    cs.minc[lane] = D.minCode[lane];
+    __syncwarp();
+}
+
+// decodeBlock with the table in shared memory: the length of a code longer
+// than the lookup table is found four lengths per step.
+template <bool kValueLut, class Emit>
+__device__ __forceinline__ void decodeBlockStaged(const WordSrc& ws, const DecTable& D, const CanonSmem& cs,
+                                                  const u32* syms, u64 bit, u32 cnt, bool& corrupt, Emit emit) {
+    const u32 nSym = D.nSym;
+    if (nSym == 0xFFFFFFFFu) { corrupt = true; return; }
+    if (nSym <= 1) {
+        const u32 single = D.single;
+        for (u32 i = 0; i < cnt; ++i) emit(i, single);
+        return;
+    }
+    u64 w = bit >> 5;
+    u32 bpos = u32(bit & 31u);
+    u32 hi = ws.at(w), lo = ws.at(w + 1);
+    w += 2;
+    for (u32 i = 0; i < cnt; ++i) {
+        const u32 v = __funnelshift_l(lo, hi, bpos);
+        const u32 e = cs.lut[v >> (32 - kLutBits)];
+        u32 len, val;
+        if (e) {
+            len = e >> 24;
+            val = e & 0xFFFFFFu;
+            if (!kValueLut) {
+                if (val >= nSym) { corrupt = true; return; }
+                val = syms[val];
+            }
+        } else {
+            const unsigned long long vv = v;
+            len = kLutBits + 1;
+            for (;;) {
+                const u32 c = (vv >= cs.lim[len] ? 1u : 0u) + (vv >= cs.lim[len + 1] ? 1u : 0u) +
+                              (vv >= cs.lim[len + 2] ? 1u : 0u) + (vv >= cs.lim[len + 3] ? 1u : 0u);
+                len += c;
+                if (c < 4 || len > 31) break;
+            }
+            if (len > 31) { corrupt = true; return; }
+            const u32 idx = u32(cs.first[len - 1] + int(v >> (32 - len)) - cs.minc[len - 1]);
+            if (idx >= nSym) { corrupt = true; return; }
+            val = syms[idx];
+        }
+        emit(i, val);
+        bpos += len;
+        if (bpos >= 32) {
+            hi = lo;
+            lo = ws.at(w);
+            ++w;
+            bpos -= 32;
+        }
+    }
+}
+
 // decodeHuff: one thread per coding block; when a warp's 32 blocks belong to
-// one stream its output is staged through shared memory and written coalesced.
+// one stream its table is staged in shared memory and its output staged
+// there too and written coalesced.
 template <class Sym>
 __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
     extern __shared__ __align__(16) unsigned char stage[];
+    __shared__ CanonSmem cs;
     if (__any_sync(0xffffffffu, capacityFailed(p))) return;
     const u32 lane = threadIdx.x;
     const u32 b0 = blockIdx.x * 32;
@@ -412,6 +500,7 @@ __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
     bool corrupt = false;
     const bool mine = valid && b < blocks;
     const u32 i0 = b * p.cb;
+    if (uniform) stageCanon(cs, p, p.streams[s0].tableFirst);   // the warp's one table
     if (mine) {
         const u32 t = sd.tableFirst;
         const DecTableDesc& td = p.tables[t];
@@ -419,7 +508,7 @@ __global__ void __launch_bounds__(32) k_decHuff(DecParams p) {
         const u32 cnt = min(p.cb, sd.n - i0);
         const u64 bit = td.cwWord * 32ull + p.blockOff[td.blockOff + b];
         if (uniform)
-            decodeBlock<sizeof(Sym) == 2>(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,
+            decodeBlockStaged<sizeof(Sym) == 2>(ws, p.dec[t], cs, p.syms + td.symOff, bit, cnt, corrupt,
                         [&](u32 i, u32 v) { rows[lane * rowPitch + i] = Sym(v); });
         else
             decodeBlock<sizeof(Sym) == 2>(ws, p.dec[t], p.syms + td.symOff, p.lut + (u64(t) << kLutBits), bit, cnt, corrupt,

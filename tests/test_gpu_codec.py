@@ -286,6 +286,34 @@ def test_codes_longer_than_27_bits(oracle, kind):
             assert np.array_equal(host(outs[i]).view(np.uint16), streams[i])
 
 
+def test_tables_of_every_builder_tier(oracle):
+    """One call of 40 streams (80 tables, so the tables are built by the
+    leaf-count tiers) whose symbol tables have from a few to ~5800 leaves:
+    warp builders (<= 256 leaves), 64-thread builders (<= 1024), 256-thread
+    builders (<= 2048) and full-heap builders (more) in the same call.  Both
+    encoders' streams identical to the oracle's; the decode round trips."""
+    rng = np.random.default_rng(91)
+    n, S = 20000, 40
+    distinct = [8, 60, 200, 250, 400, 700, 1000, 1300, 1700, 2000, 3000, 6000]
+    streams = np.zeros((S, n), np.uint16)
+    for k in range(S):
+        d = distinct[k % len(distinct)]
+        v = rng.integers(1, d + 1, n)
+        streams[k] = np.where(rng.random(n) < 0.2, 0, v)   # zero runs for the run-length tables
+    with cc.Instance(0, S, n, 128, 14) as big:
+        for kind in (0, 1):
+            bs = encode_gpu(big, kind, streams)
+            ref_words, ref_bits, _ = oracle.encode(kind, streams)
+            assert bs.bit_size == ref_bits, kind
+            assert np.array_equal(bs.raw(), ref_words), kind
+            outs = [torch.full((n,), -1, dtype=torch.int16, device="cuda") for _ in range(S)]
+            dec = cc.decode_rlhuff if kind == 0 else cc.decode_huff
+            assert dec(big, cc.BitStream(ref_words, ref_bits), outs, n), cc.last_error()
+            assert cc.decode_status(big) == 0
+            for i in range(S):
+                assert np.array_equal(host(outs[i]).view(np.uint16), streams[i]), (kind, i)
+
+
 @pytest.mark.parametrize("cb", [32, 64, 256])
 def test_coding_block_sizes(oracle, cb):
     with cc.Instance(0, 4, 40000, cb, 14) as inst_cb:
