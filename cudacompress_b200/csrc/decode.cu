@@ -537,31 +537,36 @@ __device__ __forceinline__ u32 rlBlocksOf(const DecParams& p, const DecStreamDes
 // RLHuff stream's coding blocks in groups of 32, so that a warp's blocks
 // belong to one stream and warps without blocks are not started.
 __global__ void __launch_bounds__(1024) k_decRlTasks(DecParams p) {
-    constexpr u32 kPer = 4;   // consecutive streams per thread
     __shared__ u32 scratch[40];
+    __shared__ u32 sOff[1024], sStr[1024];   // a chunk's streams: first task, stream index
     __shared__ u32 carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (u32 base = 0; base < p.nRl; base += 1024 * kPer) {
-        const u32 k0 = base + threadIdx.x * kPer;
-        u32 s[kPer], warps[kPer], sum = 0;
-#pragma unroll
-        for (u32 j = 0; j < kPer; ++j) {
-            s[j] = 0;
-            warps[j] = 0;
-            if (k0 + j < p.nRl) {
-                s[j] = p.rlList[k0 + j];
-                warps[j] = u32(ceilDiv(rlBlocksOf(p, p.streams[s[j]]), 32));
-            }
-            sum += warps[j];
+    for (u32 base = 0; base < p.nRl; base += 1024) {
+        const u32 k = base + threadIdx.x;
+        u32 s = 0, warps = 0;
+        if (k < p.nRl) {
+            s = p.rlList[k];
+            warps = u32(ceilDiv(rlBlocksOf(p, p.streams[s]), 32));
         }
         u32 tot;
-        u32 at = carry + blockExclusiveSum<1024>(sum, scratch, &tot);
-#pragma unroll
-        for (u32 j = 0; j < kPer; ++j) {
-            for (u32 i = 0; i < warps[j]; ++i)
-                if (at + i < p.rlTaskCap) p.rlTasks[at + i] = (u64(s[j]) << 32) | (32u * i);
-            at += warps[j];
+        const u32 ex = blockExclusiveSum<1024>(warps, scratch, &tot);
+        sOff[threadIdx.x] = ex;
+        sStr[threadIdx.x] = s;
+        __syncthreads();
+        // the chunk's tasks over all threads: task i belongs to the last
+        // stream whose first task is <= i (streams without tasks share their
+        // offset with the next one, so that is never one of them)
+        const int n = int(min(1024u, p.nRl - base));
+        for (u32 i = threadIdx.x; i < tot; i += 1024) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sOff[mid] <= i) lo = mid;
+                else hi = mid - 1;
+            }
+            const u32 at = carry + i;
+            if (at < p.rlTaskCap) p.rlTasks[at] = (u64(sStr[lo]) << 32) | (32u * (i - sOff[lo]));
         }
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
