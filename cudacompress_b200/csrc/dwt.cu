@@ -1175,6 +1175,7 @@ __global__ void __launch_bounds__(256, 4) k_bLevelFwd(const BLevelDesc* __restri
 
     const int nSlices = ZCe + 8;
     int i0 = 0;
+    float2 hiE = make_float2(0.0f, 0.0f), hiO = hiE;   // highpass Z chains awaiting their last tap
     // slice i = i0 + k (kc: k as a constant; i0 is a multiple of 8)
     auto slice = [&](auto kc) {
         constexpr int k = decltype(kc)::value;
@@ -1221,20 +1222,40 @@ __global__ void __launch_bounds__(256, 4) k_bLevelFwd(const BLevelDesc* __restri
             no = fir9p<false, 1>(yw + 1);
         }
         // Z: output slice z = z0 + i - 8 once its nine input slices are in
-        // (z0 and i0 are even, so z has the parity of k): slices i-8 .. i-1
-        // from the ring (slot (k + q) & 7 holds slice i - 8 + q), slice i
-        // in registers
+        // (z0 and i0 are even, so z has the parity of k).  At an even k the
+        // ring (slot (k + q) & 7 holds slice i - 8 + q) and slice i, in
+        // registers, feed both chains in one read: the lowpass output z
+        // (slices i-8 .. i) and the highpass output z + 1 (slices i-7 .. i+1)
+        // up to its last tap, whose slice i + 1 arrives at the next (odd) k.
         if (i >= 8 && outOk) {
-            float2 ve = make_float2(0.0f, 0.0f), vo = make_float2(0.0f, 0.0f);
+            float2 ve, vo;
+            if constexpr ((k & 1) == 0) {
+                ve = make_float2(0.0f, 0.0f);
+                vo = make_float2(0.0f, 0.0f);
+                hiE = make_float2(0.0f, 0.0f);
+                hiO = make_float2(0.0f, 0.0f);
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const float c = kFwdTap[k & 1][q];
-                ve = __ffma2_rn(make_float2(c, c), sZ[(k + q) & 7][0][tid], ve);
-                vo = __ffma2_rn(make_float2(c, c), sZ[(k + q) & 7][1][tid], vo);
+                for (int q = 0; q < 8; ++q) {
+                    const float2 re = sZ[(k + q) & 7][0][tid], ro = sZ[(k + q) & 7][1][tid];
+                    const float c = kFwdTap[0][q];
+                    ve = __ffma2_rn(make_float2(c, c), re, ve);
+                    vo = __ffma2_rn(make_float2(c, c), ro, vo);
+                    if (q >= 1) {
+                        const float h = kFwdTap[1][q - 1];
+                        hiE = __ffma2_rn(make_float2(h, h), re, hiE);
+                        hiO = __ffma2_rn(make_float2(h, h), ro, hiO);
+                    }
+                }
+                constexpr float c8 = kFwdTap[0][8], h7 = kFwdTap[1][7];
+                ve = __ffma2_rn(make_float2(c8, c8), ne, ve);
+                vo = __ffma2_rn(make_float2(c8, c8), no, vo);
+                hiE = __ffma2_rn(make_float2(h7, h7), ne, hiE);
+                hiO = __ffma2_rn(make_float2(h7, h7), no, hiO);
+            } else {
+                constexpr float h8 = kFwdTap[1][8];
+                ve = __ffma2_rn(make_float2(h8, h8), ne, hiE);
+                vo = __ffma2_rn(make_float2(h8, h8), no, hiO);
             }
-            constexpr float c8 = kFwdTap[k & 1][8];
-            ve = __ffma2_rn(make_float2(c8, c8), ne, ve);
-            vo = __ffma2_rn(make_float2(c8, c8), no, vo);
             const u64 li = u64(u32((z0 + i - 8) >> 1)) * plane + inPlane;
             constexpr int bz = (k & 1) << 2;
             // octants (x even, y even), (x odd, y even), (x even, y odd), (x odd, y odd)
