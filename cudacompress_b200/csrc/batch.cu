@@ -33,6 +33,9 @@
 
 #include "batch.cuh"
 
+// Pinned pointer tables per batch (volume pointers of compress / decompress calls).
+constexpr unsigned kTabRing = 8;
+
 struct cc_volume_batch {
     cc_instance* I = nullptr;          // own instance, sized for the batch (highpass encode, decode)
     cc_instance* ILP = nullptr;        // own instance of the lowpass encode
@@ -46,10 +49,11 @@ struct cc_volume_batch {
     std::vector<float> q0;
     char* mem = nullptr;               // device
     size_t memBytes = 0;
-    char* hostPlan = nullptr;          // pinned: pointer tables
+    char* hostPlan = nullptr;          // pinned: a ring of kTabRing pointer tables
     ccb::u64* hostExt = nullptr;       // pinned: loaded streams' offsets and sizes
     cudaEvent_t extEvent = nullptr;
-    cudaEvent_t tabEvent = nullptr;
+    cudaEvent_t tabEvent[kTabRing] = {};   // per ring slot: its last upload has read it
+    unsigned tabNext = 0;
     // device pieces
     ccb::u16* syms = nullptr;
     size_t symBytes = 0;
@@ -318,7 +322,8 @@ static int batchEnqueueCompress(cc_volume_batch* b) {
         const u32 hpPer = 7 * b->levels;
         k_brickOffsets<<<1, 1024, 0, st>>>(ILP->layout, I->layout, hpPer, k, b->wordOff, b->bitSize, ILP->errors,
                                            I->errors);
-        const u32 parts = std::max<u32>(1, std::min<u32>(64, u32(ceilDiv(4 * 148, k))));
+        const u32 sms = u32(std::max(1, I->smCount > 0 ? I->smCount : 148));
+        const u32 parts = std::max<u32>(1, std::min<u32>(1024, u32(ceilDiv(16 * sms, k))));
         k_brickConcat<<<k * parts, 256, 0, st>>>(ILP->out, I->out, ILP->layout, I->layout, hpPer, parts, b->wordOff,
                                                  b->bitSize, b->words);
         countLaunch(2);
@@ -358,13 +363,18 @@ static int batchEnqueueDecompress(cc_volume_batch* b) {
     return CC_OK;
 }
 
-// Copies a volume pointer table to the device (outside any captured graph).
+// Copies a volume pointer table to the device (outside any captured graph)
+// through the next slot of a ring of pinned tables: the host waits only for
+// the upload kTabRing calls back, so it can enqueue several steps ahead of the
+// device instead of one call.
 static int uploadTable(cc_volume_batch* b, const void* const* ptrs, void* dTable) {
-    cudaEventSynchronize(b->tabEvent);   // the previous upload has read the pinned buffer
-    std::memcpy(b->hostPlan, ptrs, sizeof(void*) * b->active);
-    CC_TRY_CUDA(cudaMemcpyAsync(dTable, b->hostPlan, sizeof(void*) * b->active, cudaMemcpyHostToDevice, b->I->stream),
+    const unsigned r = b->tabNext++ % kTabRing;
+    cudaEventSynchronize(b->tabEvent[r]);   // the slot's last upload has read it
+    void** slot = reinterpret_cast<void**>(b->hostPlan) + size_t(r) * b->count;
+    std::memcpy(slot, ptrs, sizeof(void*) * b->active);
+    CC_TRY_CUDA(cudaMemcpyAsync(dTable, slot, sizeof(void*) * b->active, cudaMemcpyHostToDevice, b->I->stream),
                 "upload volume pointers");
-    cudaEventRecord(b->tabEvent, b->I->stream);
+    cudaEventRecord(b->tabEvent[r], b->I->stream);
     return CC_OK;
 }
 
@@ -794,8 +804,9 @@ int cc_volume_batch_create_ex(cc_instance* user, uint32_t count, const uint32_t*
     if (e == cudaSuccess) e = up(encAt, encHost.data(), b->enc.bytes);
     if (e == cudaSuccess) e = up(encLPAt, encLPHost.data(), b->encLP.bytes);
     if (e == cudaSuccess) e = up(decAt, decHost.data(), b->dec.bytes);
-    if (e == cudaSuccess) e = pinnedAlloc(reinterpret_cast<void**>(&b->hostPlan), sizeof(void*) * count);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->tabEvent, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = pinnedAlloc(reinterpret_cast<void**>(&b->hostPlan), sizeof(void*) * count * kTabRing);
+    for (unsigned r = 0; r < kTabRing && e == cudaSuccess; ++r)
+        e = cudaEventCreateWithFlags(&b->tabEvent[r], cudaEventDisableTiming);
     if (e == cudaSuccess) e = pinnedAlloc(reinterpret_cast<void**>(&b->hostExt), 2 * sizeof(u64) * count);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->extEvent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -883,7 +894,8 @@ void cc_volume_batch_destroy(cc_volume_batch* b) {
     if (b->sideStream) cudaStreamDestroy(b->sideStream);
     if (b->evFork) cudaEventDestroy(b->evFork);
     if (b->evJoin) cudaEventDestroy(b->evJoin);
-    if (b->tabEvent) cudaEventDestroy(b->tabEvent);
+    for (cudaEvent_t ev : b->tabEvent)
+        if (ev) cudaEventDestroy(ev);
     if (b->hostPlan) cudaFreeHost(b->hostPlan);
     if (b->hostExt) cudaFreeHost(b->hostExt);
     if (b->extEvent) cudaEventDestroy(b->extEvent);

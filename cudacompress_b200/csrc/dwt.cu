@@ -569,17 +569,31 @@ __device__ __forceinline__ int quotient(int k, float r) {
 
 template <bool kInverse>
 __device__ __forceinline__ void rowPairs4(const float* w, float4& a, float4& b) {
-    // four (even, odd) output pairs from the 16-sample window w[0..15]
-    const float e0 = fir9c<kInverse, 0>(w), o0 = fir9c<kInverse, 1>(w + 1);
-    const float e1 = fir9c<kInverse, 0>(w + 2), o1 = fir9c<kInverse, 1>(w + 3);
-    const float e2 = fir9c<kInverse, 0>(w + 4), o2 = fir9c<kInverse, 1>(w + 5);
-    const float e3 = fir9c<kInverse, 0>(w + 6), o3 = fir9c<kInverse, 1>(w + 7);
+    // four (even, odd) output pairs from the 16-sample window w[0..15]: pair
+    // p is one packed chain, lane x the even output over w[2p .. 2p+8], lane y
+    // the odd one over w[2p+1 .. 2p+9] (tap i: coefficients (even_i, odd_i),
+    // samples (w[2p+i], w[2p+i+1])), each lane rounded as fir9c's chain
+    constexpr float kF[2][9] = {
+        {0.0267488f, -0.0168641f, -0.0782233f, 0.2668641f, 0.6029490f, 0.2668641f, -0.0782233f, -0.0168641f, 0.0267488f},
+        {0.0f, 0.0456359f, -0.0287718f, -0.2956359f, 0.5575435f, -0.2956359f, -0.0287718f, 0.0456359f, 0.0f}};
+    constexpr float kI[2][9] = {
+        {0.0f, 0.0337282f, -0.0575435f, -0.5337281f, 1.1150871f, -0.5337281f, -0.0575435f, 0.0337282f, 0.0f},
+        {0.0534975f, -0.0912718f, -0.1564465f, 0.5912718f, 1.2058980f, 0.5912718f, -0.1564465f, -0.0912718f, 0.0534975f}};
+    float2 r[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) r[p] = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const float2 c = kInverse ? make_float2(kI[0][i], kI[1][i]) : make_float2(kF[0][i], kF[1][i]);
+#pragma unroll
+        for (int p = 0; p < 4; ++p) r[p] = __ffma2_rn(c, make_float2(w[2 * p + i], w[2 * p + i + 1]), r[p]);
+    }
     if (kInverse) {
-        a = make_float4(e0, o0, e1, o1);
-        b = make_float4(e2, o2, e3, o3);
+        a = make_float4(r[0].x, r[0].y, r[1].x, r[1].y);
+        b = make_float4(r[2].x, r[2].y, r[3].x, r[3].y);
     } else {
-        a = make_float4(e0, e1, e2, e3);
-        b = make_float4(o0, o1, o2, o3);
+        a = make_float4(r[0].x, r[1].x, r[2].x, r[3].x);
+        b = make_float4(r[0].y, r[1].y, r[2].y, r[3].y);
     }
 }
 
@@ -817,7 +831,7 @@ __device__ __forceinline__ void quantStorePair(const BColDesc& D, int x, int y, 
 // samples they use are read from shared memory once into registers (a
 // sliding window) instead of nine reads per output.  The tile's first row
 // is even, so output j has parity j & 1 and its taps are immediates.
-template <bool kInverse, bool kQuantize = false>
+template <bool kInverse, bool kQuantize = false, bool kPacked = false>
 __device__ __forceinline__ void colOutputs8(const BColDesc& D, const float2 (*s)[33], int tx, int ty, int x, int c,
                                             int a0) {
     static_assert(kBColTileA == 64, "eight outputs per thread row of an 8-row block");
@@ -830,14 +844,22 @@ __device__ __forceinline__ void colOutputs8(const BColDesc& D, const float2 (*s)
     for (int j = 0; j < 8; ++j) {
         const int a = a0 + k0 + j;
         if (a >= D.na) break;
-        float v0[9], v1[9];
+        float2 r;
+        if (kPacked) {
+            // both columns' chains in one packed fma.rn.f32x2 each tap
+            r = (j & 1) ? fir9p<kInverse, 1>(w + j) : fir9p<kInverse, 0>(w + j);
+        } else {
+            // two scalar chains: the passes held to 40 registers (six CTAs
+            // per SM) keep the window in registers this way without spills
+            float v0[9], v1[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            v0[i] = w[j + i].x;
-            v1[i] = w[j + i].y;
+            for (int i = 0; i < 9; ++i) {
+                v0[i] = w[j + i].x;
+                v1[i] = w[j + i].y;
+            }
+            r = (j & 1) ? make_float2(fir9c<kInverse, 1>(v0), fir9c<kInverse, 1>(v1))
+                        : make_float2(fir9c<kInverse, 0>(v0), fir9c<kInverse, 0>(v1));
         }
-        const float2 r = (j & 1) ? make_float2(fir9c<kInverse, 1>(v0), fir9c<kInverse, 1>(v1))
-                                 : make_float2(fir9c<kInverse, 0>(v0), fir9c<kInverse, 0>(v1));
         const int o = kInverse ? a : splitPos(a, D.na);
         if (kQuantize) quantStorePair(D, x, c, o, r);   // axis Z: a = z, c = y
         else *reinterpret_cast<float2*>(D.dst + size_t(x) + size_t(o) * D.da + size_t(c) * D.dc) = r;
@@ -869,14 +891,7 @@ __device__ __forceinline__ void colOutputs8Quantize(const BColDesc& D, const flo
     for (int j = 0; j < 8; ++j) {
         const int a = a0 + k0 + j;
         if (a >= D.na) break;
-        float v0[9], v1[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            v0[i] = w[j + i].x;
-            v1[i] = w[j + i].y;
-        }
-        const float2 r = (j & 1) ? make_float2(fir9c<false, 1>(v0), fir9c<false, 1>(v1))
-                                 : make_float2(fir9c<false, 0>(v0), fir9c<false, 0>(v1));
+        const float2 r = (j & 1) ? fir9p<false, 1>(w + j) : fir9p<false, 0>(w + j);
         const u64 lz = u64(a >> 1);
         if (j & 1) {
             const u32 s0 = symbolizeI(int(r.x * D.inv)) & 0xFFFFu, s1 = symbolizeI(int(r.y * D.inv)) & 0xFFFFu;
@@ -976,7 +991,7 @@ __global__ void __launch_bounds__(256, kSymbols ? 5 : (kQuantize ? 4 : 6)) k_bCo
     __syncthreads();
     if (x >= nx) return;
     if (kQuantize && !(D.hx & 1) && 2 * D.hz == na) colOutputs8Quantize(D, s, tx, ty, x, c, a0);
-    else colOutputs8<kInverse, kQuantize>(D, s, tx, ty, x, c, a0);
+    else colOutputs8<kInverse, kQuantize, kSymbols || kQuantize>(D, s, tx, ty, x, c, a0);
 }
 
 // Quantization of one band to u16 symbols (deadzone, Quantize.cuh:55-59), or
