@@ -603,9 +603,10 @@ __device__ __forceinline__ void rowPairs4(const float* w, float4& a, float4& b) 
 // path (descriptor flag `vec` and 16-byte aligned pointers): float4 loads of
 // the tile body - the inverse reads the low and high halves separately and
 // interleaves them on the way into shared memory - and float4 stores of four
-// pairs per thread.  Otherwise scalar loads and stores.
+// pairs per thread.  Otherwise scalar loads and stores.  The inverse, whose
+// packed chains fit 32 registers, runs eight CTAs per SM (the forward six).
 template <bool kInverse>
-__global__ void __launch_bounds__(256, 6) k_bRows(const BRowDesc* __restrict__ descs, const u32* __restrict__ map,
+__global__ void __launch_bounds__(256, kInverse ? 8 : 6) k_bRows(const BRowDesc* __restrict__ descs, const u32* __restrict__ map,
                                                const float* const* inTab, float* const* outTab) {
     __shared__ __align__(16) float s[kBRowSmem];
     const BRowDesc D = descs[map[blockIdx.x]];
@@ -911,13 +912,15 @@ __device__ __forceinline__ void colOutputs8Quantize(const BColDesc& D, const flo
 // shared memory (nine loads in flight per thread; tiles away from both ends
 // skip the mirroring), then every thread computes eight consecutive outputs
 // (colOutputs8).  The descriptor is a register copy; the register bounds
-// (six CTAs per SM for the plain passes, five with the dequantizer, four with
-// the quantizer) are the tightest that keep the 16-sample window in
-// registers without spills.
+// (six CTAs per SM for the plain passes and the one with the dequantizer -
+// whose packed chains fit 40 registers - four with the quantizer) are the
+// tightest that keep the 16-sample window in registers without spills.  The
+// symbol pass's loads are 4-byte pairs, so its bytes in flight per SM are
+// set by the CTAs resident.
 static_assert(kBColTileX == 64, "a column-pass CTA has 32 threads of column pairs per row");
 
 template <bool kInverse, bool kSymbols, bool kQuantize = false>
-__global__ void __launch_bounds__(256, kSymbols ? 5 : (kQuantize ? 4 : 6)) k_bCols(const BColDesc* __restrict__ descs, const u32* __restrict__ map) {
+__global__ void __launch_bounds__(256, kQuantize ? 4 : 6) k_bCols(const BColDesc* __restrict__ descs, const u32* __restrict__ map) {
     __shared__ float2 s[kBColTileA + 8][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const BColDesc D = descs[map[blockIdx.x]];   // a copy: the output stores cannot alias it
