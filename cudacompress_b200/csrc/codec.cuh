@@ -30,6 +30,12 @@ constexpr u32 kRleTile = kRleThreads * kRlePerThread;
 // of one table (32 per lane of a warp): 1024 / codingBlockSize blocks.
 constexpr u32 kRunSymbols = 1024;
 
+// Tables planned by one CTA of the encode's and decode's table plans (1024
+// threads, four tables each); a call of more tables runs one CTA per chunk
+// and a carry pass over the chunks' sums (planPart).
+constexpr u32 kPlanChunk = 4096;
+constexpr u64 planPartWords(u64 tables) { return 8 * ((tables + kPlanChunk - 1) / kPlanChunk + 1); }
+
 // Leaves of a table whose Huffman build runs in shared memory (20 bytes per
 // leaf: heap key, sort key, two parent links); larger tables use global memory.
 constexpr u32 kBuildSmemLeaves = 8192;
@@ -224,6 +230,7 @@ struct cc_instance {
     uint2* enc = nullptr;              // [capHist] (code, len) by symbol
     ccb::TableMeta* meta = nullptr;    // [capTables]
     ccb::u32* tierTables = nullptr;    // [4 capTables]: the tables of each leaf-count tier of a call
+    ccb::u64* planPart = nullptr;      // [2 planPartWords(capTables)]: sums of each chunk of a table plan
     ccb::u32* headers = nullptr;       // [capHdr]
     ccb::u32* blockBits = nullptr;     // [capBlocks]
     ccb::u32* blockOff = nullptr;      // [capBlocks]

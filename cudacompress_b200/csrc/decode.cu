@@ -46,6 +46,7 @@ struct DecParams {
     u64* rlTasks;              // RLHuff decode warp tasks (stream << 32 | first block); count at rlTasks[rlTaskCap]
     u32 rlTaskCap;
     char* zc;                  // decoded zero counts, by stream zcOff
+    u64* planPart;             // sums of each chunk of the symbol plan (k_decSymPlan)
     u32* errors;
 };
 
@@ -183,32 +184,57 @@ __global__ void __launch_bounds__(64) k_decWalk(DecParams p) {
 }
 
 // Symbol array offsets of the tables (prefix of nSym) and capacity check.
+// CTA b takes the kPlanChunk tables of chunk b (four consecutive per thread):
+// offsets within the chunk and the chunk's sum (planPart); with more than one
+// chunk, k_decSymPlanCarry adds the chunks before each one.
 __global__ void __launch_bounds__(1024) k_decSymPlan(DecParams p) {
-    constexpr u32 kPer = 4;   // consecutive tables per thread
+    constexpr u32 kPer = kPlanChunk / 1024;
     __shared__ u32 scratch[40];
-    __shared__ unsigned long long carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (u32 base = 0; base < p.T; base += 1024 * kPer) {
-        const u32 t0 = base + threadIdx.x * kPer;
-        u32 v[kPer], sum = 0;
+    const u32 t0 = blockIdx.x * kPlanChunk + threadIdx.x * kPer;
+    u32 v[kPer], sum = 0;
 #pragma unroll
-        for (u32 j = 0; j < kPer; ++j) {
-            v[j] = t0 + j < p.T ? min(p.tables[t0 + j].nSym, p.leavesMax) : 0u;
-            sum += v[j];
-        }
-        u32 tot;
-        unsigned long long at = carry + blockExclusiveSum<1024>(sum, scratch, &tot);
-#pragma unroll
-        for (u32 j = 0; j < kPer; ++j) {
-            if (t0 + j < p.T) p.tables[t0 + j].symOff = u32(at);
-            at += v[j];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
+    for (u32 j = 0; j < kPer; ++j) {
+        v[j] = t0 + j < p.T ? min(p.tables[t0 + j].nSym, p.leavesMax) : 0u;
+        sum += v[j];
     }
-    if (threadIdx.x == 0 && carry > p.capLeaves) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+    u32 tot;
+    u32 at = blockExclusiveSum<1024>(sum, scratch, &tot);
+#pragma unroll
+    for (u32 j = 0; j < kPer; ++j) {
+        if (t0 + j < p.T) p.tables[t0 + j].symOff = at;
+        at += v[j];
+    }
+    if (threadIdx.x == 0) {
+        if (gridDim.x == 1) {
+            if (tot > p.capLeaves) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+        } else {
+            p.planPart[blockIdx.x] = tot;
+        }
+    }
+}
+
+// Chunk b = blockIdx.x + 1 of a symbol plan of more than one chunk: the sum
+// of chunks 0 .. b-1 added to its tables' offsets; the last chunk's CTA
+// checks the capacity.
+__global__ void __launch_bounds__(1024) k_decSymPlanCarry(DecParams p) {
+    constexpr u32 kPer = kPlanChunk / 1024;
+    __shared__ unsigned long long sC;
+    const u32 b = blockIdx.x + 1;
+    if (threadIdx.x < 32) {
+        unsigned long long c = 0;
+        for (u32 i = threadIdx.x; i < b; i += 32) c += p.planPart[i];
+#pragma unroll
+        for (u32 o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (threadIdx.x == 0) sC = c;
+    }
+    __syncthreads();
+    const unsigned long long c = sC;
+    const u32 t0 = b * kPlanChunk + threadIdx.x * kPer;
+#pragma unroll
+    for (u32 j = 0; j < kPer; ++j)
+        if (t0 + j < p.T) p.tables[t0 + j].symOff += u32(c);
+    if (b == gridDim.x && threadIdx.x == 0 && c + p.planPart[b] > p.capLeaves)
+        atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
 }
 
 // ---------------------------------------------------------------------------
@@ -535,44 +561,61 @@ __device__ __forceinline__ u32 rlBlocksOf(const DecParams& p, const DecStreamDes
 
 // Warp tasks of the run-length decode, once the headers are walked: every
 // RLHuff stream's coding blocks in groups of 32, so that a warp's blocks
-// belong to one stream and warps without blocks are not started.
+// belong to one stream and warps without blocks are not started.  CTA b
+// takes the 1024 streams of chunk b; with more than one chunk,
+// k_decRlTaskCounts first writes each chunk's task count (planPart) and CTA b
+// starts its tasks after the counts of the chunks before it.
+__device__ __forceinline__ u32 rlTaskWarps(const DecParams& p, u32 k, u32& s) {
+    s = 0;
+    if (k >= p.nRl) return 0;
+    s = p.rlList[k];
+    return u32(ceilDiv(rlBlocksOf(p, p.streams[s]), 32));
+}
+
+__global__ void __launch_bounds__(1024) k_decRlTaskCounts(DecParams p) {
+    __shared__ u32 scratch[40];
+    u32 s, tot;
+    const u32 warps = rlTaskWarps(p, blockIdx.x * 1024 + threadIdx.x, s);
+    blockExclusiveSum<1024>(warps, scratch, &tot);
+    if (threadIdx.x == 0) p.planPart[blockIdx.x] = tot;
+}
+
 __global__ void __launch_bounds__(1024) k_decRlTasks(DecParams p) {
     __shared__ u32 scratch[40];
-    __shared__ u32 sOff[1024], sStr[1024];   // a chunk's streams: first task, stream index
-    __shared__ u32 carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (u32 base = 0; base < p.nRl; base += 1024) {
-        const u32 k = base + threadIdx.x;
-        u32 s = 0, warps = 0;
-        if (k < p.nRl) {
-            s = p.rlList[k];
-            warps = u32(ceilDiv(rlBlocksOf(p, p.streams[s]), 32));
-        }
-        u32 tot;
-        const u32 ex = blockExclusiveSum<1024>(warps, scratch, &tot);
-        sOff[threadIdx.x] = ex;
-        sStr[threadIdx.x] = s;
-        __syncthreads();
-        // the chunk's tasks over all threads: task i belongs to the last
-        // stream whose first task is <= i (streams without tasks share their
-        // offset with the next one, so that is never one of them)
-        const int n = int(min(1024u, p.nRl - base));
-        for (u32 i = threadIdx.x; i < tot; i += 1024) {
-            int lo = 0, hi = n - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sOff[mid] <= i) lo = mid;
-                else hi = mid - 1;
-            }
-            const u32 at = carry + i;
-            if (at < p.rlTaskCap) p.rlTasks[at] = (u64(sStr[lo]) << 32) | (32u * (i - sOff[lo]));
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
+    __shared__ u32 sOff[1024], sStr[1024];   // the chunk's streams: first task, stream index
+    __shared__ u32 sCarry;
+    const u32 b = blockIdx.x;
+    if (threadIdx.x < 32) {
+        // tasks of the chunks before this one
+        u32 c = 0;
+        for (u32 i = threadIdx.x; i < b; i += 32) c += u32(p.planPart[i]);
+        c = __reduce_add_sync(0xffffffffu, c);
+        if (threadIdx.x == 0) sCarry = c;
     }
-    if (threadIdx.x == 0) reinterpret_cast<u32*>(p.rlTasks + p.rlTaskCap)[0] = min(carry, p.rlTaskCap);
+    const u32 base = b * 1024;
+    u32 s, tot;
+    const u32 warps = rlTaskWarps(p, base + threadIdx.x, s);
+    const u32 ex = blockExclusiveSum<1024>(warps, scratch, &tot);   // synchronizes (sCarry visible)
+    sOff[threadIdx.x] = ex;
+    sStr[threadIdx.x] = s;
+    __syncthreads();
+    const u32 carry = sCarry;
+    // the chunk's tasks over all threads: task i belongs to the last stream
+    // whose first task is <= i (streams without tasks share their offset
+    // with the next one, so that is never one of them)
+    const int n = int(min(1024u, p.nRl - base));
+    for (u32 i = threadIdx.x; i < tot; i += 1024) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sOff[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const u32 at = carry + i;
+        if (at < p.rlTaskCap) p.rlTasks[at] = (u64(sStr[lo]) << 32) | (32u * (i - sOff[lo]));
+    }
+    if (b + 1 == gridDim.x && threadIdx.x == 0)
+        reinterpret_cast<u32*>(p.rlTasks + p.rlTaskCap)[0] = min(carry + tot, p.rlTaskCap);
 }
 
 // The RLHuff streams' outputs, zeroed before the symbol pass writes the
@@ -924,7 +967,13 @@ static int planDecode(cc_instance* I, const u32* kinds, const u32* ns, void* con
 template <class Sym>
 static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
     cudaStream_t st = I->stream;
-    { SectionTimer t(I, "dec.sym_plan", st); k_decSymPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
+    {
+        SectionTimer t(I, "dec.sym_plan", st);
+        const u32 chunks = std::max<u32>(1, u32(ceilDiv(p.T, kPlanChunk)));
+        k_decSymPlan<<<chunks, 1024, 0, st>>>(p);
+        countLaunch();
+        if (chunks > 1) { k_decSymPlanCarry<<<chunks - 1, 1024, 0, st>>>(p); countLaunch(); }
+    }
     { SectionTimer t(I, "dec.tables", st); k_decTables<<<p.T, kDecThreads, 0, st>>>(p); countLaunch(); }
     if (p.hBlocks) {
         const size_t smem = size_t(32) * (p.cb + 2) * sizeof(Sym);
@@ -937,7 +986,13 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
     }
     if (p.rlBlocks) {
         const u32 g = u32(ceilDiv(u64(p.rlBlocks) / 32 + p.nRl, 4));   // warp tasks <= rlBlocks / 32 + nRl
-        { SectionTimer t(I, "dec.rl_tasks", st); k_decRlTasks<<<1, 1024, 0, st>>>(p); countLaunch(); }
+        {
+            SectionTimer t(I, "dec.rl_tasks", st);
+            const u32 chunks = std::max<u32>(1, u32(ceilDiv(p.nRl, 1024)));
+            if (chunks > 1) { k_decRlTaskCounts<<<chunks, 1024, 0, st>>>(p); countLaunch(); }
+            k_decRlTasks<<<chunks, 1024, 0, st>>>(p);
+            countLaunch();
+        }
         {
             SectionTimer t(I, "dec.zero_fill", st);
             k_decZero<Sym><<<dim3(p.nRl, u32(ceilDiv(p.rlMaxN, kZeroChunk))), 256, 0, st>>>(p);
@@ -994,6 +1049,7 @@ static DecParams makeDecParams(cc_instance* I, const DecPlan& dc) {
     p.rlTasks = I->decRlTasks;
     p.rlTaskCap = u32(u64(I->capBlocks) / 32 + I->capStreams);
     p.zc = static_cast<char*>(I->zc);
+    p.planPart = I->planPart + planPartWords(I->capTables);
     p.errors = I->errors + 4;
     return p;
 }

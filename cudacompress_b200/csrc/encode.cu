@@ -52,6 +52,7 @@ struct EncParams {
     u32* orderWork;
     u32* leafSymWork;
     u32* tierTables;  // [4][T]: the tables of each leaf-count tier (k_leafTiers); counts in totals[4..7]
+    u64* planPart;    // [8 per chunk]: sums of each plan chunk (k_histPlan)
     u32 heapCap;      // leaves that fit the shared-memory builder of tableBuild
     u32 buildLo, buildHi;   // k_tableBuild builds the tables with buildLo <= leaves <= buildHi
     u32 buildTier;    // k_tableBuild: kBuildEach (table blockIdx.x) or the tier whose list its CTAs walk
@@ -300,81 +301,134 @@ constexpr int kSmallSegs = int(kSmallLeaves / 17u) + 1;
 constexpr u32 kBuildEach = 0xFFFFFFFFu;                  // buildTier: one table per CTA
 constexpr u32 kTierMinTables = 64;                       // calls of more tables use the tiers
 
-// Pass 3 (one block): histogram / builder / header offsets of every table,
-// sized from the largest symbol of its stream.  A symbol outside the
-// instance's 2^log2Max range fails the call (HuffmanTable.cu:411-419).
+// Pass 3: histogram / builder / header offsets of every table, sized from
+// the largest symbol of its stream.  A symbol outside the instance's
+// 2^log2Max range fails the call (HuffmanTable.cu:411-419).  CTA b plans the
+// kPlanChunk tables of chunk b, four consecutive per thread with their loads
+// in flight together: their offsets within the chunk, and the chunk's sums
+// (planPart); with more than one chunk, k_histPlanCarry adds the sums of the
+// chunks before each one - every CTA's work independent, so a call of 10^5
+// tables takes two short launches instead of a loop on one SM.
+constexpr u32 kPlanPer = 4;
+static_assert(kPlanChunk == 1024 * kPlanPer, "a plan chunk is one 1024-thread CTA's tables");
+
+// The call's totals from the offsets' grand sums c[2..6] (bins, leaves,
+// header words, coding blocks, runs), and the capacity check.
+__device__ __forceinline__ void planTotals(const EncParams& p, const unsigned long long (&c)[7]) {
+    p.totals[2] = c[5];
+    p.totals[3] = c[6];
+    for (u32 k = 4; k < 8; ++k) p.totals[k] = 0;   // the tier lists' counts (k_leafTiers)
+    p.totals[1] = c[2];
+    if (c[2] > p.capHist || c[3] > p.capLeaves || c[4] > p.capHdr) atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+}
+
 __global__ void __launch_bounds__(1024) k_histPlan(EncParams p) {
-    constexpr u32 kPer = 4;   // consecutive tables per thread (their loads in flight together)
     __shared__ u32 scratch[33 * 7];
-    // running offsets: (unused), (unused), bins, leaves, header words, blocks, runs
-    __shared__ unsigned long long carry[7];
-    if (threadIdx.x < 7) carry[threadIdx.x] = 0;
-    __syncthreads();
-    for (u32 base = 0; base < p.T; base += 1024 * kPer) {
-        const u32 t0 = base + threadIdx.x * kPer;
-        u32 v[kPer][7];
-        TableMeta m[kPer];
+    const u32 t0 = blockIdx.x * kPlanChunk + threadIdx.x * kPlanPer;
+    // per table: (unused), (unused), bins, leaves, header words, blocks, runs
+    u32 v[kPlanPer][7];
+    TableMeta m[kPlanPer];
 #pragma unroll
-        for (u32 j = 0; j < kPer; ++j) {
-            const u32 t = t0 + j;
-            m[j] = TableMeta{};
-            u32 hs = 0, ls = 0, ws = 0;
-            if (t < p.T) {
-                const EncTableDev td = p.tables[t];
-                const u32 smax = p.streamMax[td.stream];
-                const u32 count = p.counts[td.stream];
-                if (td.which == 0 && smax >= p.bins) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
-                hs = td.which ? min(256u, p.bins) : min(smax, p.bins - 1u) + 1u;
-                ls = min(hs, count + 1u);
-                ws = headerWordsFor(ls, p.log2Max);
-                m[j].count = count;
-                m[j].histSize = hs;
-                m[j].blocks = u32(ceilDiv(count, p.cb));
-            }
-            v[j][0] = 0;
-            v[j][1] = 0;
-            v[j][2] = hs;
-            v[j][3] = ls;
-            v[j][4] = ws;
-            v[j][5] = m[j].blocks;
-            v[j][6] = u32(ceilDiv(m[j].blocks, kRunSymbols / p.cb));
+    for (u32 j = 0; j < kPlanPer; ++j) {
+        const u32 t = t0 + j;
+        m[j] = TableMeta{};
+        u32 hs = 0, ls = 0, ws = 0;
+        if (t < p.T) {
+            const EncTableDev td = p.tables[t];
+            const u32 smax = p.streamMax[td.stream];
+            const u32 count = p.counts[td.stream];
+            if (td.which == 0 && smax >= p.bins) atomicOr(p.errors, DEV_ERR_SYMBOL_RANGE);
+            hs = td.which ? min(256u, p.bins) : min(smax, p.bins - 1u) + 1u;
+            ls = min(hs, count + 1u);
+            ws = headerWordsFor(ls, p.log2Max);
+            m[j].count = count;
+            m[j].histSize = hs;
+            m[j].blocks = u32(ceilDiv(count, p.cb));
         }
-        u32 sum[7], ex[7], tot[7];
+        v[j][0] = 0;
+        v[j][1] = 0;
+        v[j][2] = hs;
+        v[j][3] = ls;
+        v[j][4] = ws;
+        v[j][5] = m[j].blocks;
+        v[j][6] = u32(ceilDiv(m[j].blocks, kRunSymbols / p.cb));
+    }
+    u32 sum[7], ex[7], tot[7];
 #pragma unroll
-        for (u32 k = 0; k < 7; ++k) {
-            sum[k] = 0;
+    for (u32 k = 0; k < 7; ++k) {
+        sum[k] = 0;
 #pragma unroll
-            for (u32 j = 0; j < kPer; ++j) sum[k] += v[j][k];
+        for (u32 j = 0; j < kPlanPer; ++j) sum[k] += v[j][k];
+    }
+    blockExclusiveSumN<1024, 7>(sum, ex, tot, scratch);
+    unsigned long long at[7];
+#pragma unroll
+    for (u32 k = 0; k < 7; ++k) at[k] = ex[k];
+#pragma unroll
+    for (u32 j = 0; j < kPlanPer; ++j) {
+        const u32 t = t0 + j;
+        if (t < p.T) {
+            m[j].histOff = at[2];
+            m[j].leafOff = at[3];
+            m[j].hdrOff = at[4];
+            m[j].actOff = u32(at[5]);
+            m[j].runOff = u32(at[6]);
+            p.meta[t] = m[j];
         }
-        blockExclusiveSumN<1024, 7>(sum, ex, tot, scratch);
-        unsigned long long at[7];
 #pragma unroll
-        for (u32 k = 0; k < 7; ++k) at[k] = carry[k] + ex[k];
-#pragma unroll
-        for (u32 j = 0; j < kPer; ++j) {
-            const u32 t = t0 + j;
-            if (t < p.T) {
-                m[j].histOff = at[2];
-                m[j].leafOff = at[3];
-                m[j].hdrOff = at[4];
-                m[j].actOff = u32(at[5]);
-                m[j].runOff = u32(at[6]);
-                p.meta[t] = m[j];
-            }
-#pragma unroll
-            for (u32 k = 0; k < 7; ++k) at[k] += v[j][k];
-        }
-        __syncthreads();
-        if (threadIdx.x < 7) carry[threadIdx.x] += tot[threadIdx.x];
-        __syncthreads();
+        for (u32 k = 0; k < 7; ++k) at[k] += v[j][k];
     }
     if (threadIdx.x == 0) {
-        p.totals[2] = carry[5];
-        p.totals[3] = carry[6];
-        for (u32 k = 4; k < 8; ++k) p.totals[k] = 0;   // the tier lists' counts (k_leafTiers)
-        p.totals[1] = carry[2];
-        if (carry[2] > p.capHist || carry[3] > p.capLeaves || carry[4] > p.capHdr)
-            atomicOr(p.errors, DEV_ERR_TABLE_CAPACITY);
+        if (gridDim.x == 1) {
+            unsigned long long c[7];
+#pragma unroll
+            for (u32 k = 0; k < 7; ++k) c[k] = tot[k];
+            planTotals(p, c);
+        } else {
+#pragma unroll
+            for (u32 k = 0; k < 7; ++k) p.planPart[u64(blockIdx.x) * 8 + k] = tot[k];
+        }
+    }
+}
+
+// Chunk b = blockIdx.x + 1 of a plan of more than one chunk: the sums of
+// chunks 0 .. b-1 (a warp over planPart) added to its tables' offsets; the
+// last chunk's CTA forms the call's totals.
+__global__ void __launch_bounds__(1024) k_histPlanCarry(EncParams p) {
+    __shared__ unsigned long long sC[7];
+    const u32 b = blockIdx.x + 1;
+    if (threadIdx.x < 32) {
+        unsigned long long c[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (u32 i = threadIdx.x; i < b; i += 32)
+#pragma unroll
+            for (u32 k = 2; k < 7; ++k) c[k] += p.planPart[u64(i) * 8 + k];
+#pragma unroll
+        for (u32 k = 2; k < 7; ++k)
+#pragma unroll
+            for (u32 o = 16; o > 0; o >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], o);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (u32 k = 0; k < 7; ++k) sC[k] = c[k];
+    }
+    __syncthreads();
+    const u32 t0 = b * kPlanChunk + threadIdx.x * kPlanPer;
+#pragma unroll
+    for (u32 j = 0; j < kPlanPer; ++j) {
+        const u32 t = t0 + j;
+        if (t < p.T) {
+            TableMeta& m = p.meta[t];
+            m.histOff += sC[2];
+            m.leafOff += sC[3];
+            m.hdrOff += sC[4];
+            m.actOff += u32(sC[5]);
+            m.runOff += u32(sC[6]);
+        }
+    }
+    if (b == gridDim.x && threadIdx.x == 0) {
+        unsigned long long c[7];
+#pragma unroll
+        for (u32 k = 0; k < 7; ++k) c[k] = sC[k] + p.planPart[u64(b) * 8 + k];
+        planTotals(p, c);
     }
 }
 
@@ -1098,16 +1152,20 @@ __global__ void __launch_bounds__(kPackWarps * 32, 3) k_pack(EncParams p) {
     }
 }
 
-// Count words, table headers, codeword bit counts and offset increments.
-__global__ void __launch_bounds__(512) k_headers(EncParams p) {
+// Count words, table headers, codeword bit counts and offset increments.  A
+// group of g threads (a power of two, 32 .. 512) writes one stream: a call of
+// many streams packs 512 / g of them into a CTA instead of one (as many as
+// still leave four CTAs per SM).
+__global__ void __launch_bounds__(512) k_headers(EncParams p, u32 g) {
     if (blockFailed(p)) return;
-    const u32 s = blockIdx.x;
+    const u32 s = blockIdx.x * (blockDim.x / g) + threadIdx.x / g, gt = threadIdx.x & (g - 1u);
+    if (s >= p.S) return;   // no barriers below
     const EncStreamDev sd = p.streams[s];
     const SegmentLayout L = p.layout[s];
     u32* seg = p.out + L.startWord;
     const bool rl = sd.kind == KIND_RLHUFF;
     const u32 parts = rl ? 2u : 1u;
-    if (rl && threadIdx.x == 0) seg[L.countWord] = p.counts[s];
+    if (rl && gt == 0) seg[L.countWord] = p.counts[s];
     for (u32 part = 0; part < parts; ++part) {
         const u32 t = sd.tableFirst + part;
         const TableMeta m = p.meta[t];
@@ -1116,7 +1174,7 @@ __global__ void __launch_bounds__(512) k_headers(EncParams p) {
         const u32 hw = u32(ceilDiv(r + m.headerBits, 32));
         u32* dst = seg + L.hdrWord[part];
         const u32 srcWords = u32(ceilDiv(m.headerBits, 32));
-        for (u32 w = threadIdx.x; w < hw; w += blockDim.x) {
+        for (u32 w = gt; w < hw; w += g) {
             u32 v;
             if (r == 0) {
                 v = hdr[w];
@@ -1127,12 +1185,12 @@ __global__ void __launch_bounds__(512) k_headers(EncParams p) {
             }
             dst[w] = v;
         }
-        if (threadIdx.x == 0) seg[L.cwWord[part] - 1] = m.codeBits;
+        if (gt == 0) seg[L.cwWord[part] - 1] = m.codeBits;
         // offsets: u16 increments, two per word, first in the low half (LE memcpy)
         const u32 nOff = m.blocks;
         const u32* bo = p.blockOff + p.tables[t].blockOff;
         u32* od = seg + L.offWord[part];
-        for (u32 w = threadIdx.x; w < (nOff + 1) / 2; w += blockDim.x) {
+        for (u32 w = gt; w < (nOff + 1) / 2; w += g) {
             const u32 k0 = 2 * w, k1 = 2 * w + 1;
             const u32 a = k0 == 0 ? bo[0] : bo[k0] - bo[k0 - 1];
             const u32 b = k1 < nOff ? bo[k1] - bo[k1 - 1] : 0u;
@@ -1222,7 +1280,13 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         k_scan<<<u32(ceilDiv(p.S, kScanWarps)), kScanWarps * 32, 0, st>>>(p);
         countLaunch();
     }
-    { SectionTimer t(I, "enc.hist_plan", st); k_histPlan<<<1, 1024, 0, st>>>(p); countLaunch(); }
+    {
+        SectionTimer t(I, "enc.hist_plan", st);
+        const u32 chunks = std::max<u32>(1, u32(ceilDiv(p.T, kPlanChunk)));
+        k_histPlan<<<chunks, 1024, 0, st>>>(p);
+        countLaunch();
+        if (chunks > 1) { k_histPlanCarry<<<chunks - 1, 1024, 0, st>>>(p); countLaunch(); }
+    }
     { SectionTimer t(I, "enc.hist_zero", st); k_zeroHist<<<2 * 148, 256, 0, st>>>(p); countLaunch(); }
     if (p.totalTiles) {
         CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_write<Sym>),
@@ -1334,7 +1398,16 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         k_pack<Sym><<<g, kPackWarps * 32, 0, st>>>(p);
         countLaunch();
     }
-    { SectionTimer t(I, "enc.headers", st); k_headers<<<p.S, 512, 0, st>>>(p); countLaunch(); }
+    {
+        SectionTimer t(I, "enc.headers", st);
+        // streams per CTA: as few as keep four CTAs per SM busy
+        const u32 sms = u32(std::max(1, I->smCount > 0 ? I->smCount : 148));
+        u32 per = 1;
+        while (per < 16 && u64(2 * per) * 4 * sms <= p.S) per <<= 1;
+        const u32 g = 512 / per;
+        k_headers<<<u32(ceilDiv(p.S, per)), 512, 0, st>>>(p, g);
+        countLaunch();
+    }
     CC_TRY_CUDA(cudaGetLastError(), "encode launch");
     return CC_OK;
 }
@@ -1406,6 +1479,7 @@ int encodeLaunch(cc_instance* I, const EncPlan& hp, u32* out, u64 outCap) {
     p.orderWork = I->orderWork;
     p.leafSymWork = I->leafSymWork;
     p.tierTables = I->tierTables;
+    p.planPart = I->planPart;
     p.heapCap = std::min<u32>(std::min<u32>(I->leavesMax, kBuildSmemLeaves), hp.maxCount + 1u);
     return I->symBytes == 2 ? launchEncode<u16>(I, p) : launchEncode<u32>(I, p);
 }

@@ -151,6 +151,7 @@ void layoutArena(cc_instance* I, char* base, size_t* total) {
     I->enc = c.take<uint2>(I->capHist);
     I->meta = c.take<TableMeta>(I->capTables);
     I->tierTables = c.take<u32>(4ull * I->capTables);
+    I->planPart = c.take<u64>(2 * planPartWords(I->capTables));   // encode's, then decode's
     I->headers = c.take<u32>(I->capHdr);
     I->blockBits = c.take<u32>(I->capBlocks + 1);
     I->blockOff = c.take<u32>(I->capBlocks + 1);

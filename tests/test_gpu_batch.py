@@ -72,6 +72,14 @@ def test_batch_uneven_bricks_match_oracle(oracle):
     check_batch(oracle, vols, steps, 2, graph=False)
 
 
+def test_batch_of_many_tables_matches_oracle(oracle):
+    """600 bricks: 8400 highpass streams, 16800 encode tables and 17400
+    decode tables, so the encode's histogram plan and the decode's symbol
+    plan run as several chunk CTAs plus a carry pass over the chunks' sums."""
+    vols, steps = bricks(600, 2, seed=1007)
+    check_batch(oracle, vols, steps, 2, graph=True, rounds=1)
+
+
 def test_batch_graph_replay_matches_oracle(oracle):
     vols, steps = bricks(9, 2, seed=1006)
     check_batch(oracle, vols, steps, 2, graph=True, rounds=3)
