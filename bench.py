@@ -1159,9 +1159,14 @@ def run_ours(args, wl):
     # Every step moves its own fields in, its streams out and back in, and its
     # reconstruction out.  At least 40 steps are timed (about 0.2 s): the
     # pipeline's fill (the first step's copy in and codec) and drain (the
-    # last step's copy out) are a tenth of a 10-step region.
+    # last step's copy out) are a tenth of a 10-step region.  The PCIe link
+    # is shared with the host's other GPUs, so three such runs are timed and
+    # the median reported (all three are in the line).
     e2e_steps = max(args.steps, 40)
-    e2e = pipelined_e2e(torch, pool[:2], vols_h, vols, dev, C, cc, steps=e2e_steps)
+    e2e_runs = [pipelined_e2e(torch, pool[:2], vols_h, vols, dev, C, cc, steps=e2e_steps) for _ in range(3)]
+    e2e_runs_ms = [r["ms"] for r in e2e_runs]
+    e2e = sorted(e2e_runs, key=lambda r: r["ms"])[1]
+    e2e["identical"] = all(r["identical"] for r in e2e_runs)
     e2e_ms = replicas.max_over_ranks([e2e["ms"]], dist, dev)[0]
     e2e_value = replicas.job_gbs(world, raw_step, e2e_ms)
     h2d = raw_step + e2e["stream_bytes"]
@@ -1267,7 +1272,7 @@ def run_ours(args, wl):
             "q0_sweep": sweep, "compact_symbols_per_step": counts["compact"],
             "batched_vs_per_brick": bricks, "serving": serve,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": e2e_steps},
+                    "steps": e2e_steps, "runs_ms_per_step": [round(x, 4) for x in e2e_runs_ms], "reported": "median of 3"},
             "gpu_launches": launches,
             "roofline": roofline, "pipeline_roofline": pipeline,
             "sections_ms": {k: round(v[0], 4) for k, v in sorted(sections.items(), key=lambda kv: -kv[1][0])},
