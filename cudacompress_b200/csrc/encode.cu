@@ -975,7 +975,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_blockScan(EncParams p) {
 }
 
 // Segment layout per stream (a thread per stream), then the exclusive scan
-// of the segments' words over the streams (one block).
+// of the segments' words over the streams (k_layout, k_layoutCarry).
 __global__ void __launch_bounds__(256) k_layoutSegments(EncParams p) {
     if (*reinterpret_cast<volatile const u32*>(p.errors)) return;   // no barriers in this kernel
     const u32 s = blockIdx.x * 256u + threadIdx.x;
@@ -1009,25 +1009,49 @@ __global__ void __launch_bounds__(256) k_layoutSegments(EncParams p) {
     p.layout[s] = L;
 }
 
+// CTA b scans the segment words of streams 1024 b .. 1024 b + 1023; with more
+// than one chunk its sum goes to planPart and k_layoutCarry adds the chunks
+// before each one (the histogram plan's sums are consumed by then).
 __global__ void __launch_bounds__(1024) k_layout(EncParams p) {
     __shared__ u32 scratch[40];
-    __shared__ unsigned long long carry;
-    if (threadIdx.x == 0) carry = 0;
     if (blockFailed(p)) return;
-    for (u32 base = 0; base < p.S; base += 1024) {
-        const u32 s = base + threadIdx.x;
-        const u32 words = s < p.S ? p.layout[s].words : 0u;
-        // 64-bit carry across chunks; within a chunk a 32-bit scan suffices
-        u32 tot;
-        const u32 ex = blockExclusiveSum<1024>(words, scratch, &tot);
-        if (s < p.S) p.layout[s].startWord = carry + ex;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
-    }
+    const u32 s = blockIdx.x * 1024u + threadIdx.x;
+    const u32 words = s < p.S ? p.layout[s].words : 0u;
+    u32 tot;   // a chunk's words fit 32 bits; the offsets over chunks are 64-bit
+    const u32 ex = blockExclusiveSum<1024>(words, scratch, &tot);
+    if (s < p.S) p.layout[s].startWord = ex;
     if (threadIdx.x == 0) {
-        p.totals[0] = carry;
-        if (carry > p.outWordsMax) atomicOr(p.errors, DEV_ERR_OUTPUT_CAPACITY);
+        if (gridDim.x == 1) {
+            p.totals[0] = tot;
+            if (tot > p.outWordsMax) atomicOr(p.errors, DEV_ERR_OUTPUT_CAPACITY);
+        } else {
+            p.planPart[blockIdx.x] = tot;
+        }
+    }
+}
+
+// Chunk b = blockIdx.x + 1 of a layout of more than one chunk: the words of
+// chunks 0 .. b-1 added to its streams' start words; the last chunk's CTA
+// forms the call's total and checks the output capacity.
+__global__ void __launch_bounds__(1024) k_layoutCarry(EncParams p) {
+    __shared__ unsigned long long sC;
+    if (blockFailed(p)) return;
+    const u32 b = blockIdx.x + 1;
+    if (threadIdx.x < 32) {
+        unsigned long long c = 0;
+        for (u32 i = threadIdx.x; i < b; i += 32) c += p.planPart[i];
+#pragma unroll
+        for (u32 o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (threadIdx.x == 0) sC = c;
+    }
+    __syncthreads();
+    const unsigned long long c = sC;
+    const u32 s = b * 1024u + threadIdx.x;
+    if (s < p.S) p.layout[s].startWord += c;
+    if (b == gridDim.x && threadIdx.x == 0) {
+        const unsigned long long total = c + p.planPart[b];
+        p.totals[0] = total;
+        if (total > p.outWordsMax) atomicOr(p.errors, DEV_ERR_OUTPUT_CAPACITY);
     }
 }
 
@@ -1389,8 +1413,10 @@ static int launchEncode(cc_instance* I, const EncParams& p) {
         SectionTimer t(I, "enc.layout", st);
         k_layoutSegments<<<u32(ceilDiv(p.S, 256)), 256, 0, st>>>(p);
         countLaunch();
-        k_layout<<<1, 1024, 0, st>>>(p);
+        const u32 chunks = std::max<u32>(1, u32(ceilDiv(p.S, 1024)));
+        k_layout<<<chunks, 1024, 0, st>>>(p);
         countLaunch();
+        if (chunks > 1) { k_layoutCarry<<<chunks - 1, 1024, 0, st>>>(p); countLaunch(); }
     }
     if (p.totalBlocks) {
         const u32 g = std::min<u32>(blockGrid, u32(ceilDiv(runBound, kPackWarps)));
