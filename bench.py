@@ -19,7 +19,8 @@ to the plain single-volume codec's, replayed as CUDA graphs).
           fields, D2H of the streams (to page-locked host memory), H2D of the
           streams, D2H of the reconstructions, every step, inside the timed
           region; steps are software-pipelined (copy engines overlap the
-          codec; consecutive steps alternate between two batches)
+          codec; consecutive steps alternate between two batches); the
+          median of three runs of max(40, K) steps, all three in the line
   q0_sweep  the vector field at q0 in {0.002, 0.01, 0.05} std: per q0 the
           compression ratio, PSNR per component, encode / decode GB/s raw of
           one step at a time, and the FP32-vs-FP64 error of component 0
