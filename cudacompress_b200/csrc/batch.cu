@@ -54,6 +54,11 @@ struct cc_volume_batch {
     cudaEvent_t extEvent = nullptr;
     cudaEvent_t tabEvent[kTabRing] = {};   // per ring slot: its last upload has read it
     unsigned tabNext = 0;
+    // host copies of the descriptors that carry quantization steps (one per
+    // volume and level, as uploaded), patched by batchSetQuantSteps
+    std::vector<std::vector<ccb::BLevelDesc>> flHost;
+    std::vector<std::vector<ccb::BColDesc>> izHost;
+    std::vector<ccb::BQuantDesc> qdHost, dqHost;
     // device pieces
     ccb::u16* syms = nullptr;
     size_t symBytes = 0;
@@ -422,6 +427,52 @@ static int runMaybeGraph(cc_volume_batch* b, Enqueue fn, std::map<u32, cudaGraph
     }
     CC_TRY_CUDA(cudaGraphLaunch(exec, I->stream), "graph launch");
     countLaunch(launches);
+    return CC_OK;
+}
+
+// New quantization steps for the batch's volumes: the descriptors that carry
+// them (forward levels, LP quantizer, inverse Z passes, LP dequantizer) are
+// recomputed as at creation and re-uploaded, stream-ordered on the batch's
+// stream, so calls enqueued before keep their steps.
+int batchSetQuantSteps(cc_volume_batch* b, const float* q) {
+    if (!b || !q) { setError("volume batch quantization steps: null argument"); return CC_ERR_INVALID_ARGUMENT; }
+    bool same = true;
+    for (u32 v = 0; v < b->count; ++v) {
+        if (!(q[v] > 0.0f)) { setError("volume batch: volume %u: quantization step must be > 0", v); return CC_ERR_INVALID_ARGUMENT; }
+        same = same && q[v] == b->q0[v];
+    }
+    if (same) return CC_OK;
+    const u32 L = b->levels;
+    for (u32 v = 0; v < b->count; ++v) {
+        const float q0 = q[v];
+        b->q0[v] = q0;
+        for (u32 l = 0; l < L; ++l) {
+            b->flHost[l][v].inv = 1.0f / (q0 / float(1u << l));              // Quantize.cu:90: reciprocal on the host
+            b->flHost[l][v].invLP = 1.0f / (q0 / float(1u << (L - 1)));
+            b->izHost[l][v].step = q0 / float(1u << l);
+        }
+        BQuantDesc* qv = &b->qdHost[size_t(v) * (1 + 7 * L)];
+        qv[0].step = q0 / float(1u << (L - 1));
+        qv[0].inv = 1.0f / qv[0].step;
+        b->dqHost[v].step = qv[0].step;
+        b->dqHost[v].inv = qv[0].inv;
+        u32 k = 1;
+        for (int l = int(L) - 1; l >= 0; --l)
+            for (u32 bi = 1; bi < 8; ++bi, ++k) {
+                qv[k].step = q0 / float(1u << l);
+                qv[k].inv = 1.0f / qv[k].step;
+            }
+    }
+    cudaStream_t st = b->hasOwnStream ? b->ownStream : b->user->stream;
+    auto up = [&](const void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    for (u32 l = 0; l < L; ++l) {
+        CC_TRY_CUDA(up(b->fwdLevel[l].d, b->flHost[l].data(), b->flHost[l].size() * sizeof(BLevelDesc)), "patch steps");
+        CC_TRY_CUDA(up(b->invZ[l].d, b->izHost[l].data(), b->izHost[l].size() * sizeof(BColDesc)), "patch steps");
+    }
+    CC_TRY_CUDA(up(b->quant.d, b->qdHost.data(), b->qdHost.size() * sizeof(BQuantDesc)), "patch steps");
+    CC_TRY_CUDA(up(b->dequantLP.d, b->dqHost.data(), b->dqHost.size() * sizeof(BQuantDesc)), "patch steps");
     return CC_OK;
 }
 
@@ -811,6 +862,10 @@ int cc_volume_batch_create_ex(cc_instance* user, uint32_t count, const uint32_t*
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->extEvent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { cc_volume_batch_destroy(b); return cudaFail(e, "volume batch set-up"); }
+    b->flHost = fl;
+    b->izHost = iz;
+    b->qdHost = qd;
+    b->dqHost = dq;
     b->fwdLevel.resize(L);
     b->fwdRows.resize(L); b->invRows.resize(L); b->fwdY.resize(L); b->fwdZ.resize(L); b->invZ.resize(L); b->invY.resize(L);
     auto mapPtr = [&](size_t m) { return reinterpret_cast<const u32*>(base + mapAt[m]); };

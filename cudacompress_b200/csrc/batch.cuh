@@ -107,4 +107,7 @@ inline void batchRowTiling(int nx, int& W, int& R) {
     if (R > kBRowMaxRows) R = kBRowMaxRows;
 }
 
+// New quantization steps for a batch's volumes (batch.cu).
+int batchSetQuantSteps(cc_volume_batch* b, const float* q);
+
 }  // namespace ccb

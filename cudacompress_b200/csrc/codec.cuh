@@ -282,6 +282,10 @@ struct cc_instance {
     // whole-pipeline workspace (volume / heightfield codecs), grown on demand
     char* pipeWork = nullptr;
     size_t pipeWorkBytes = 0;
+    // decompressVolumeFloat's one-call volume batch, kept for the next call
+    // of the same channel count, sizes and levels (pipeline.cu)
+    cc_volume_batch* plainBatch = nullptr;
+    ccb::u32 plainBatchKey[5] = {};   // channels, nx, ny, nz, levels
 
     char* takeRingSlot();
 };

@@ -320,6 +320,7 @@ void cc_destroy_instance(cc_instance* I) {
     cudaGetDevice(&prev);
     if (I->device >= 0) cudaSetDevice(I->device);
     cudaDeviceSynchronize();
+    if (I->plainBatch) cc_volume_batch_destroy(I->plainBatch);   // it refers to this instance
     for (int i = 0; i < cc_instance::kRing; ++i) {
         if (I->ringEvent[i]) cudaEventDestroy(I->ringEvent[i]);
         if (I->hostRing[i]) cudaFreeHost(I->hostRing[i]);

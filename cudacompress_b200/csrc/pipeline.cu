@@ -12,7 +12,7 @@
 #include <cstring>
 #include <vector>
 
-#include "capi_internal.cuh"
+#include "batch.cuh"
 
 namespace ccb {
 
@@ -274,6 +274,57 @@ int compressVolumeFloat(cc_instance* I, const float* vol, u32 nx, u32 ny, u32 nz
     return encodeVolumeSymbols(I, syms, vs, L, rleOnly, dWords, cap, bitSize, what);
 }
 
+// decompressVolumeFloat(MultiChannel) through a volume batch of the call's
+// channels (csrc/batch.cu: one device-side walk of all streams, one decode of
+// all bands, the batched inverse passes, CUDA graphs), kept on the instance
+// for the next call of the same channel count, sizes and levels; a call with
+// other quantization steps patches the batch's steps.  The batch decodes the
+// same stream format bit-identically.  Returns kNoBatch, with nothing done,
+// when no batch can be made (sizes outside the batch's limits, or its
+// allocation failing): the caller then runs the level-by-level path.
+constexpr int kNoBatch = 1 << 20;
+
+int decompressVolumeFloatBatched(cc_instance* I, const cc_volume_channel* ch, u32 count, u32 nx, u32 ny, u32 nz,
+                                 u32 L, const char* what) {
+    // the instance's declared capacities bound the call, as on the level path
+    if (u64(count) * 7 > I->streamCountMax || cube(nx / 2, ny / 2, nz / 2) > I->elemCountPerStreamMax) {
+        setError("%s: instance needs >= %u streams of >= %llu symbols", what, count * 7,
+                 (unsigned long long)cube(nx / 2, ny / 2, nz / 2));
+        return CC_ERR_CAPACITY;
+    }
+    if (L > 8 || cube(nx, ny, nz) >= (u64(1) << 31)) return kNoBatch;
+    const u32 key[5] = {count, nx, ny, nz, L};
+    std::vector<float> q(count);
+    for (u32 c = 0; c < count; ++c) q[c] = ch[c].quant_step;
+    for (u32 c = 0; c < count; ++c)
+        if (!(q[c] > 0.0f)) { setError("%s: channel %u: quantization step must be > 0", what, c); return CC_ERR_INVALID_ARGUMENT; }
+    if (!I->plainBatch || std::memcmp(key, I->plainBatchKey, sizeof(key)) != 0) {
+        if (I->plainBatch) cc_volume_batch_destroy(I->plainBatch);
+        I->plainBatch = nullptr;
+        std::vector<u32> sizes(3 * size_t(count));
+        for (u32 c = 0; c < count; ++c) { sizes[3 * c] = nx; sizes[3 * c + 1] = ny; sizes[3 * c + 2] = nz; }
+        cc_volume_batch* b = nullptr;
+        if (cc_volume_batch_create(I, count, sizes.data(), L, q.data(), &b) != CC_OK || !b) {
+            cudaGetLastError();   // a failed allocation is not the caller's error
+            return kNoBatch;
+        }
+        cc_volume_batch_use_graph(b, 1);
+        I->plainBatch = b;
+        std::memcpy(I->plainBatchKey, key, sizeof(key));
+    }
+    cc_volume_batch* b = I->plainBatch;
+    int rc = cc_volume_batch_set_stream(b, I->stream);
+    if (!rc) rc = batchSetQuantSteps(b, q.data());
+    std::vector<const u32*> words(count);
+    std::vector<u64> bits(count);
+    std::vector<float*> outs(count);
+    for (u32 c = 0; c < count; ++c) { words[c] = ch[c].d_words; bits[c] = ch[c].bit_size; outs[c] = ch[c].d_volume; }
+    if (!rc) rc = cc_volume_batch_load_streams(b, words.data(), bits.data());
+    if (!rc) rc = cc_volume_batch_decompress(b, outs.data());
+    if (!rc) rc = cc_volume_batch_status(b);   // synchronizes the stream
+    return rc;
+}
+
 int decompressVolumeFloat(cc_instance* I, const cc_volume_channel* ch, u32 count, u32 nx, u32 ny, u32 nz, u32 L,
                           bool rleOnly, const char* what) {
     if (!I || !ch || count == 0) { setError("%s: bad argument", what); return CC_ERR_INVALID_ARGUMENT; }
@@ -282,6 +333,10 @@ int decompressVolumeFloat(cc_instance* I, const cc_volume_channel* ch, u32 count
     if (!volumeSizesOk(nx, ny, nz, L, what)) return CC_ERR_INVALID_ARGUMENT;
     if (I->symBytes != 2) { setError("%s: needs a 16-bit-symbol instance", what); return CC_ERR_INVALID_ARGUMENT; }
     DeviceGuard deviceGuard(I->device);
+    if (!rleOnly) {
+        const int rc = decompressVolumeFloatBatched(I, ch, count, nx, ny, nz, L, what);
+        if (rc != kNoBatch) return rc;
+    }
     cudaStream_t st = I->stream;
     const u64 N0 = cube(nx, ny, nz);
     const VolumeSymbols vs = volumeSymbols(nx, ny, nz, L);

@@ -2,6 +2,7 @@
 // (examples/CompressVolume.cpp, compiled unmodified from the reference tree
 // by oracle/ref/Makefile) behind a C ABI, so that tests/golden/make_golden.py
 // can record its bit streams and reconstructions as fixtures.  Never shipped.
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -90,6 +91,39 @@ int ref_volume_decompress_multichannel(float* const* dOuts, const uint32_t* cons
                                                     rleOnlyLevel0 != 0);
     cudaDeviceSynchronize();
     return 0;
+}
+
+// Timing of the reference's own codec on one device volume (baseline
+// infrastructure, oracle/ref/time_ref_gpu.py): one session, one untimed call
+// of each direction, then `reps` calls of compressVolumeFloat (device volume
+// -> host bit stream, its own API) and of decompressVolumeFloat (host bit
+// stream -> device volume), each followed by a device synchronize; msEnc /
+// msDec get the mean wall time of one call.
+int ref_volume_time(const float* dVol, float* dOut, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t levels, float q,
+                    uint32_t reps, double* msEnc, double* msDec, uint32_t* nWords) {
+    Session s(nx, ny, nz, 1);
+    if (!s.ok) return -1;
+    using clk = std::chrono::steady_clock;
+    std::vector<uint> bits;
+    double enc = 0.0, dec = 0.0;
+    for (uint32_t r = 0; r <= reps; ++r) {
+        bits.clear();
+        const auto t0 = clk::now();
+        if (!compressVolumeFloat(s.shared, s.res, dVol, nx, ny, nz, levels, bits, q, false)) return -2;
+        cudaDeviceSynchronize();
+        const auto t1 = clk::now();
+        decompressVolumeFloat(s.shared, s.res, dOut, nx, ny, nz, levels, bits, q, false);
+        cudaDeviceSynchronize();
+        const auto t2 = clk::now();
+        if (r > 0) {
+            enc += std::chrono::duration<double, std::milli>(t1 - t0).count();
+            dec += std::chrono::duration<double, std::milli>(t2 - t1).count();
+        }
+    }
+    *msEnc = reps ? enc / reps : 0.0;
+    *msDec = reps ? dec / reps : 0.0;
+    *nWords = uint32_t(bits.size());
+    return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 
 }  // extern "C"

@@ -42,6 +42,37 @@ def test_volume_codec_matches_oracle(oracle, n, levels, q0):
         assert fields.psnr(vol, rec) > 30
 
 
+def test_plain_decode_reuses_its_batch_across_steps_and_sizes(oracle):
+    """decompressVolumeFloat runs through a volume batch kept on the instance:
+    consecutive calls with other quantization steps (the batch's steps
+    patched), other sizes (the batch made again) and back, each bit-identical
+    to the oracle's reconstruction of the oracle's stream."""
+    cases = [((32, 32, 32), 2, 0.01), ((32, 32, 32), 2, 0.05), ((32, 32, 32), 2, 0.002),
+             ((32, 48, 64), 2, 0.01), ((32, 48, 64), 3, 0.01), ((32, 32, 32), 2, 0.05)]
+    with cc.Instance(0, 7, 32 ** 3, 128, 14) as inst:
+        for shape, levels, q0 in cases:
+            vol = np.ascontiguousarray(fields.turbulence_field(64, 256, 16, seed=2100)[: shape[0], : shape[1], : shape[2]])
+            ref_words, ref_bits = oracle.compress_volume(vol, levels, q0)
+            words = torch.from_numpy(ref_words.view(np.int32).copy()).cuda()
+            out = torch.full(shape, float("nan"), dtype=torch.float32, device="cuda")
+            cc.decompress_volume_float(inst, out, levels, q0, words, ref_bits)
+            ref_rec = oracle.decompress_volume(ref_words, ref_bits, vol.shape, levels, q0)
+            assert np.array_equal(out.cpu().numpy().view(np.uint32), ref_rec.view(np.uint32)), (shape, levels, q0)
+
+
+def test_plain_decode_beyond_instance_capacity_fails_cleanly(oracle):
+    """The instance's declared stream length bounds decompressVolumeFloat as
+    it bounds the encoder: a volume whose level-0 bands exceed it fails with
+    a capacity error and nothing is decoded."""
+    vol = fields.turbulence_field(32, 128, 8, seed=2101)
+    ref_words, ref_bits = oracle.compress_volume(vol, 2, 0.01)
+    words = torch.from_numpy(ref_words.view(np.int32).copy()).cuda()
+    with cc.Instance(0, 7, 15 ** 3, 128, 14) as inst:
+        out = torch.zeros((32, 32, 32), dtype=torch.float32, device="cuda")
+        with pytest.raises(cc.CudaCompressError):
+            cc.decompress_volume_float(inst, out, 2, 0.01, words, ref_bits)
+
+
 def test_volume_codec_c0_full_size(oracle):
     """128^3, 3 levels, q0 = 0.01 (the small lossy volume config)."""
     vol = fields.turbulence_field(128, 512, 32, fields.SEED_C0)
