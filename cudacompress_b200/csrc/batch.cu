@@ -476,6 +476,20 @@ int batchSetQuantSteps(cc_volume_batch* b, const float* q) {
     return CC_OK;
 }
 
+// Error flags of one direction only: the encoders' (highpass and lowpass
+// instances) or the decoder's, each reset by its own launches, so a failed
+// call of one direction does not surface on the next call of the other.
+int batchStatusOf(cc_volume_batch* b, bool decode) {
+    if (!b) return CC_ERR_INVALID_ARGUMENT;
+    u32 flags[8] = {}, lp = 0;
+    CC_TRY_CUDA(cudaMemcpyAsync(flags, b->I->errors, sizeof(flags), cudaMemcpyDeviceToHost, b->I->stream), "batch status");
+    CC_TRY_CUDA(cudaMemcpyAsync(&lp, b->ILP->errors, sizeof(lp), cudaMemcpyDeviceToHost, b->I->stream), "batch status");
+    CC_TRY_CUDA(cudaStreamSynchronize(b->I->stream), "batch status");
+    if (decode) return deviceErrorStatus(flags[4], "batch decompress");
+    if (lp) return deviceErrorStatus(lp, "batch compress (lowpass streams)");
+    return deviceErrorStatus(flags[0], "batch compress");
+}
+
 }  // namespace ccb
 
 using namespace ccb;

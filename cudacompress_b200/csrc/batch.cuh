@@ -109,5 +109,8 @@ inline void batchRowTiling(int nx, int& W, int& R) {
 
 // New quantization steps for a batch's volumes (batch.cu).
 int batchSetQuantSteps(cc_volume_batch* b, const float* q);
+// The error status of the batch's last compress (decode false) or decompress
+// (decode true), after synchronizing its stream (batch.cu).
+int batchStatusOf(cc_volume_batch* b, bool decode);
 
 }  // namespace ccb

@@ -216,6 +216,78 @@ int decodeVolumeSymbols(cc_instance* I, const u32* const* dWords, const u32* bit
     return CC_OK;
 }
 
+// compressVolumeFloat and decompressVolumeFloat(MultiChannel) run through a
+// volume batch of the call's volumes (csrc/batch.cu: the fused forward
+// levels, both encodes at once, one device-side walk and decode of all
+// streams, the batched inverse passes, CUDA graphs), kept on the instance
+// for the next call of the same volume count, sizes and levels; a call with
+// other quantization steps patches the batch's steps.  The batch writes and
+// reads the same stream format bit-identically.  kNoBatch: sizes outside the
+// batch's limits, nothing done - the caller runs the level-by-level path.
+constexpr int kNoBatch = 1 << 20;
+
+int plainBatchFor(cc_instance* I, u32 count, u32 nx, u32 ny, u32 nz, u32 L, const float* q, const char* what,
+                  cc_volume_batch** out) {
+    // the instance's declared capacities bound the call, as on the level path
+    if (u64(count) * 7 > I->streamCountMax || cube(nx / 2, ny / 2, nz / 2) > I->elemCountPerStreamMax) {
+        setError("%s: instance needs >= %u streams of >= %llu symbols", what, count * 7,
+                 (unsigned long long)cube(nx / 2, ny / 2, nz / 2));
+        return CC_ERR_CAPACITY;
+    }
+    if (L > 8 || cube(nx, ny, nz) >= (u64(1) << 31)) return kNoBatch;
+    for (u32 c = 0; c < count; ++c)
+        if (!(q[c] > 0.0f)) { setError("%s: volume %u: quantization step must be > 0", what, c); return CC_ERR_INVALID_ARGUMENT; }
+    const u32 key[5] = {count, nx, ny, nz, L};
+    if (!I->plainBatch || std::memcmp(key, I->plainBatchKey, sizeof(key)) != 0) {
+        if (I->plainBatch) cc_volume_batch_destroy(I->plainBatch);
+        I->plainBatch = nullptr;
+        std::vector<u32> sizes(3 * size_t(count));
+        for (u32 c = 0; c < count; ++c) { sizes[3 * c] = nx; sizes[3 * c + 1] = ny; sizes[3 * c + 2] = nz; }
+        cc_volume_batch* b = nullptr;
+        const int rc = cc_volume_batch_create(I, count, sizes.data(), L, q, &b);
+        if (rc) return rc;
+        cc_volume_batch_use_graph(b, 1);
+        I->plainBatch = b;
+        std::memcpy(I->plainBatchKey, key, sizeof(key));
+    }
+    int rc = cc_volume_batch_set_stream(I->plainBatch, I->stream);
+    if (!rc) rc = batchSetQuantSteps(I->plainBatch, q);
+    *out = I->plainBatch;
+    return rc;
+}
+
+int compressVolumeFloatBatched(cc_instance* I, const float* vol, u32 nx, u32 ny, u32 nz, u32 L, float q0,
+                               u32* dWords, u64 cap, u32* bitSize, const char* what) {
+    cc_volume_batch* b = nullptr;
+    int rc = plainBatchFor(I, 1, nx, ny, nz, L, &q0, what, &b);
+    if (rc) return rc;
+    const float* vols[1] = {vol};
+    rc = cc_volume_batch_compress(b, vols);
+    if (!rc) rc = batchStatusOf(b, false);   // synchronizes the stream
+    u64 bits = 0;
+    if (!rc) rc = cc_volume_batch_read_stream(b, 0, dWords, cap, &bits);
+    if (!rc && bits > 0xffffffffull) { setError("%s: stream exceeds 2^32 bits", what); rc = CC_ERR_CAPACITY; }
+    if (!rc) *bitSize = u32(bits);
+    return rc;
+}
+
+int decompressVolumeFloatBatched(cc_instance* I, const cc_volume_channel* ch, u32 count, u32 nx, u32 ny, u32 nz,
+                                 u32 L, const char* what) {
+    std::vector<float> q(count);
+    for (u32 c = 0; c < count; ++c) q[c] = ch[c].quant_step;
+    cc_volume_batch* b = nullptr;
+    int rc = plainBatchFor(I, count, nx, ny, nz, L, q.data(), what, &b);
+    if (rc) return rc;
+    std::vector<const u32*> words(count);
+    std::vector<u64> bits(count);
+    std::vector<float*> outs(count);
+    for (u32 c = 0; c < count; ++c) { words[c] = ch[c].d_words; bits[c] = ch[c].bit_size; outs[c] = ch[c].d_volume; }
+    rc = cc_volume_batch_load_streams(b, words.data(), bits.data());
+    if (!rc) rc = cc_volume_batch_decompress(b, outs.data());
+    if (!rc) rc = batchStatusOf(b, true);   // synchronizes the stream
+    return rc;
+}
+
 // ---- float codec ----
 int compressVolumeFloat(cc_instance* I, const float* vol, u32 nx, u32 ny, u32 nz, u32 L, float q0, bool rleOnly,
                         u32* dWords, u64 cap, u32* bitSize) {
@@ -229,6 +301,10 @@ int compressVolumeFloat(cc_instance* I, const float* vol, u32 nx, u32 ny, u32 nz
         return CC_ERR_CAPACITY;
     }
     DeviceGuard deviceGuard(I->device);
+    if (!rleOnly) {
+        const int rc = compressVolumeFloatBatched(I, vol, nx, ny, nz, L, q0, dWords, cap, bitSize, what);
+        if (rc != kNoBatch) return rc;
+    }
     cudaStream_t st = I->stream;
     const u64 N0 = cube(nx, ny, nz);
     const VolumeSymbols vs = volumeSymbols(nx, ny, nz, L);
@@ -272,57 +348,6 @@ int compressVolumeFloat(cc_instance* I, const float* vol, u32 nx, u32 ny, u32 nz
         }
     }
     return encodeVolumeSymbols(I, syms, vs, L, rleOnly, dWords, cap, bitSize, what);
-}
-
-// decompressVolumeFloat(MultiChannel) through a volume batch of the call's
-// channels (csrc/batch.cu: one device-side walk of all streams, one decode of
-// all bands, the batched inverse passes, CUDA graphs), kept on the instance
-// for the next call of the same channel count, sizes and levels; a call with
-// other quantization steps patches the batch's steps.  The batch decodes the
-// same stream format bit-identically.  Returns kNoBatch, with nothing done,
-// when no batch can be made (sizes outside the batch's limits, or its
-// allocation failing): the caller then runs the level-by-level path.
-constexpr int kNoBatch = 1 << 20;
-
-int decompressVolumeFloatBatched(cc_instance* I, const cc_volume_channel* ch, u32 count, u32 nx, u32 ny, u32 nz,
-                                 u32 L, const char* what) {
-    // the instance's declared capacities bound the call, as on the level path
-    if (u64(count) * 7 > I->streamCountMax || cube(nx / 2, ny / 2, nz / 2) > I->elemCountPerStreamMax) {
-        setError("%s: instance needs >= %u streams of >= %llu symbols", what, count * 7,
-                 (unsigned long long)cube(nx / 2, ny / 2, nz / 2));
-        return CC_ERR_CAPACITY;
-    }
-    if (L > 8 || cube(nx, ny, nz) >= (u64(1) << 31)) return kNoBatch;
-    const u32 key[5] = {count, nx, ny, nz, L};
-    std::vector<float> q(count);
-    for (u32 c = 0; c < count; ++c) q[c] = ch[c].quant_step;
-    for (u32 c = 0; c < count; ++c)
-        if (!(q[c] > 0.0f)) { setError("%s: channel %u: quantization step must be > 0", what, c); return CC_ERR_INVALID_ARGUMENT; }
-    if (!I->plainBatch || std::memcmp(key, I->plainBatchKey, sizeof(key)) != 0) {
-        if (I->plainBatch) cc_volume_batch_destroy(I->plainBatch);
-        I->plainBatch = nullptr;
-        std::vector<u32> sizes(3 * size_t(count));
-        for (u32 c = 0; c < count; ++c) { sizes[3 * c] = nx; sizes[3 * c + 1] = ny; sizes[3 * c + 2] = nz; }
-        cc_volume_batch* b = nullptr;
-        if (cc_volume_batch_create(I, count, sizes.data(), L, q.data(), &b) != CC_OK || !b) {
-            cudaGetLastError();   // a failed allocation is not the caller's error
-            return kNoBatch;
-        }
-        cc_volume_batch_use_graph(b, 1);
-        I->plainBatch = b;
-        std::memcpy(I->plainBatchKey, key, sizeof(key));
-    }
-    cc_volume_batch* b = I->plainBatch;
-    int rc = cc_volume_batch_set_stream(b, I->stream);
-    if (!rc) rc = batchSetQuantSteps(b, q.data());
-    std::vector<const u32*> words(count);
-    std::vector<u64> bits(count);
-    std::vector<float*> outs(count);
-    for (u32 c = 0; c < count; ++c) { words[c] = ch[c].d_words; bits[c] = ch[c].bit_size; outs[c] = ch[c].d_volume; }
-    if (!rc) rc = cc_volume_batch_load_streams(b, words.data(), bits.data());
-    if (!rc) rc = cc_volume_batch_decompress(b, outs.data());
-    if (!rc) rc = cc_volume_batch_status(b);   // synchronizes the stream
-    return rc;
 }
 
 int decompressVolumeFloat(cc_instance* I, const cc_volume_channel* ch, u32 count, u32 nx, u32 ny, u32 nz, u32 L,

@@ -94,8 +94,9 @@ def test_volume_batch_creation_survives_every_failed_allocation():
 
 
 def test_pipeline_workspace_failure_then_recovery():
-    """The plain volume codec grows its workspace on first use: a failure
-    there raises, and the next call allocates and codes correctly."""
+    """The plain volume codec makes its volume batch on first use: a failed
+    allocation there raises, and the next call allocates and codes
+    correctly."""
     lib = _ffi.lib()
     vol = fields.turbulence_field(32, 128, 8, seed=72)
     d = torch.from_numpy(vol).cuda()
