@@ -282,10 +282,18 @@ struct cc_instance {
     // whole-pipeline workspace (volume / heightfield codecs), grown on demand
     char* pipeWork = nullptr;
     size_t pipeWorkBytes = 0;
-    // decompressVolumeFloat's one-call volume batch, kept for the next call
-    // of the same channel count, sizes and levels (pipeline.cu)
-    cc_volume_batch* plainBatch = nullptr;
-    ccb::u32 plainBatchKey[5] = {};   // channels, nx, ny, nz, levels
+    // the plain volume calls' volume batches (pipeline.cu plainBatchFor):
+    // two kept, by (volume count, nx, ny, nz, levels), least recently used
+    // replaced; a shape gets one on its fifth consecutive call
+    struct PlainBatch {
+        cc_volume_batch* b = nullptr;
+        ccb::u32 key[5] = {};
+        ccb::u64 used = 0;
+    };
+    PlainBatch plainBatch[2];
+    ccb::u32 plainSeenKey[5] = {};
+    ccb::u32 plainSeenRun = 0;        // consecutive calls of plainSeenKey
+    ccb::u64 plainCalls = 0;
 
     char* takeRingSlot();
 };

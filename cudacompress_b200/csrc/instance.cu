@@ -320,7 +320,8 @@ void cc_destroy_instance(cc_instance* I) {
     cudaGetDevice(&prev);
     if (I->device >= 0) cudaSetDevice(I->device);
     cudaDeviceSynchronize();
-    if (I->plainBatch) cc_volume_batch_destroy(I->plainBatch);   // it refers to this instance
+    for (auto& pb : I->plainBatch)
+        if (pb.b) cc_volume_batch_destroy(pb.b);   // they refer to this instance
     for (int i = 0; i < cc_instance::kRing; ++i) {
         if (I->ringEvent[i]) cudaEventDestroy(I->ringEvent[i]);
         if (I->hostRing[i]) cudaFreeHost(I->hostRing[i]);

@@ -219,12 +219,18 @@ int decodeVolumeSymbols(cc_instance* I, const u32* const* dWords, const u32* bit
 // compressVolumeFloat and decompressVolumeFloat(MultiChannel) run through a
 // volume batch of the call's volumes (csrc/batch.cu: the fused forward
 // levels, both encodes at once, one device-side walk and decode of all
-// streams, the batched inverse passes, CUDA graphs), kept on the instance
-// for the next call of the same volume count, sizes and levels; a call with
-// other quantization steps patches the batch's steps.  The batch writes and
-// reads the same stream format bit-identically.  kNoBatch: sizes outside the
-// batch's limits, nothing done - the caller runs the level-by-level path.
+// streams, the batched inverse passes, CUDA graphs) that the instance keeps
+// for later calls of the same volume count, sizes and levels; a call with
+// other quantization steps patches the batch's steps.  Making a batch costs
+// 10-20 ms (allocations, plans, graph capture), so a shape gets one only on
+// its fifth consecutive call: calls that change shape every time, or every
+// compress / decompress pair (bricks of many sizes), stay on the
+// level-by-level path.  The batch
+// writes and reads the same stream format bit-identically.  kNoBatch: no
+// batch for this call (sizes outside the batch's limits, or a shape not yet
+// repeated), nothing done - the caller runs the level-by-level path.
 constexpr int kNoBatch = 1 << 20;
+constexpr u32 kPlainBatchRun = 5;   // consecutive calls of a shape before it gets a batch
 
 int plainBatchFor(cc_instance* I, u32 count, u32 nx, u32 ny, u32 nz, u32 L, const float* q, const char* what,
                   cc_volume_batch** out) {
@@ -238,21 +244,35 @@ int plainBatchFor(cc_instance* I, u32 count, u32 nx, u32 ny, u32 nz, u32 L, cons
     for (u32 c = 0; c < count; ++c)
         if (!(q[c] > 0.0f)) { setError("%s: volume %u: quantization step must be > 0", what, c); return CC_ERR_INVALID_ARGUMENT; }
     const u32 key[5] = {count, nx, ny, nz, L};
-    if (!I->plainBatch || std::memcmp(key, I->plainBatchKey, sizeof(key)) != 0) {
-        if (I->plainBatch) cc_volume_batch_destroy(I->plainBatch);
-        I->plainBatch = nullptr;
+    if (std::memcmp(key, I->plainSeenKey, sizeof(key)) == 0) {
+        ++I->plainSeenRun;
+    } else {
+        std::memcpy(I->plainSeenKey, key, sizeof(key));
+        I->plainSeenRun = 1;
+    }
+    cc_instance::PlainBatch* slot = nullptr;
+    for (auto& pb : I->plainBatch)
+        if (pb.b && std::memcmp(key, pb.key, sizeof(key)) == 0) slot = &pb;
+    if (!slot) {
+        if (I->plainSeenRun < kPlainBatchRun) return kNoBatch;
+        slot = &I->plainBatch[0];
+        for (auto& pb : I->plainBatch)
+            if (!pb.b || pb.used < slot->used) slot = &pb;   // an empty slot, else the least recently used
+        if (slot->b) cc_volume_batch_destroy(slot->b);
+        slot->b = nullptr;
         std::vector<u32> sizes(3 * size_t(count));
         for (u32 c = 0; c < count; ++c) { sizes[3 * c] = nx; sizes[3 * c + 1] = ny; sizes[3 * c + 2] = nz; }
         cc_volume_batch* b = nullptr;
         const int rc = cc_volume_batch_create(I, count, sizes.data(), L, q, &b);
         if (rc) return rc;
         cc_volume_batch_use_graph(b, 1);
-        I->plainBatch = b;
-        std::memcpy(I->plainBatchKey, key, sizeof(key));
+        slot->b = b;
+        std::memcpy(slot->key, key, sizeof(key));
     }
-    int rc = cc_volume_batch_set_stream(I->plainBatch, I->stream);
-    if (!rc) rc = batchSetQuantSteps(I->plainBatch, q);
-    *out = I->plainBatch;
+    slot->used = ++I->plainCalls;
+    int rc = cc_volume_batch_set_stream(slot->b, I->stream);
+    if (!rc) rc = batchSetQuantSteps(slot->b, q);
+    *out = slot->b;
     return rc;
 }
 

@@ -46,7 +46,8 @@ def time_ours(inst, d, out, reps):
     dw = torch.empty(cap, dtype=torch.int32, device="cuda")
     hw = torch.empty(cap, dtype=torch.int32).pin_memory()
     enc = dec = 0.0
-    for r in range(reps + 1):
+    warm = 3   # the instance makes its volume batch on the fifth consecutive call of a shape
+    for r in range(reps + warm):
         t0 = time.perf_counter()
         _, bits = cc.compress_volume_float(inst, d, LEVELS, Q0, dw)
         nw = (bits + 31) // 32
@@ -57,7 +58,7 @@ def time_ours(inst, d, out, reps):
         cc.decompress_volume_float(inst, out, LEVELS, Q0, dw, bits)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
-        if r:
+        if r >= warm:
             enc += (t1 - t0) * 1e3
             dec += (t2 - t1) * 1e3
     return enc / reps, dec / reps, nw

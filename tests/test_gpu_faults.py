@@ -94,8 +94,8 @@ def test_volume_batch_creation_survives_every_failed_allocation():
 
 
 def test_pipeline_workspace_failure_then_recovery():
-    """The plain volume codec makes its volume batch on first use: a failed
-    allocation there raises, and the next call allocates and codes
+    """The plain volume codec allocates its work memory on first use: a
+    failed allocation there raises, and the next call allocates and codes
     correctly."""
     lib = _ffi.lib()
     vol = fields.turbulence_field(32, 128, 8, seed=72)

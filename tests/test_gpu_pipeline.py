@@ -43,12 +43,15 @@ def test_volume_codec_matches_oracle(oracle, n, levels, q0):
 
 
 def test_plain_decode_reuses_its_batch_across_steps_and_sizes(oracle):
-    """decompressVolumeFloat runs through a volume batch kept on the instance:
-    consecutive calls with other quantization steps (the batch's steps
-    patched), other sizes (the batch made again) and back, each bit-identical
-    to the oracle's reconstruction of the oracle's stream."""
-    cases = [((32, 32, 32), 2, 0.01), ((32, 32, 32), 2, 0.05), ((32, 32, 32), 2, 0.002),
-             ((32, 48, 64), 2, 0.01), ((32, 48, 64), 3, 0.01), ((32, 32, 32), 2, 0.05)]
+    """decompressVolumeFloat takes the level-by-level path for a shape's
+    first four consecutive calls and a volume batch kept on the instance from
+    the fifth (two kept, least recently used replaced): calls with other
+    quantization steps (the batch's steps patched), a second shape, the first
+    again, a third shape (evicting one), each bit-identical to the oracle's
+    reconstruction of the oracle's stream."""
+    a, b, c = ((32, 32, 32), 2), ((32, 48, 64), 2), ((32, 48, 64), 3)
+    cases = ([a + (0.01,)] * 5 + [a + (0.05,), a + (0.002,)] + [b + (0.01,)] * 5 + [a + (0.01,)] +
+             [c + (0.01,)] * 5 + [b + (0.05,), a + (0.05,)])
     with cc.Instance(0, 7, 32 ** 3, 128, 14) as inst:
         for shape, levels, q0 in cases:
             vol = np.ascontiguousarray(fields.turbulence_field(64, 256, 16, seed=2100)[: shape[0], : shape[1], : shape[2]])
