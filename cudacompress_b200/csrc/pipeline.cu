@@ -265,11 +265,13 @@ int plainBatchFor(cc_instance* I, u32 count, u32 nx, u32 ny, u32 nz, u32 L, cons
         cc_volume_batch* b = nullptr;
         const int rc = cc_volume_batch_create(I, count, sizes.data(), L, q, &b);
         if (rc) return rc;
-        cc_volume_batch_use_graph(b, 1);
         slot->b = b;
         std::memcpy(slot->key, key, sizeof(key));
     }
     slot->used = ++I->plainCalls;
+    // with timing on, the calls run launch by launch so that every section is
+    // recorded (a graph replay records none)
+    cc_volume_batch_use_graph(slot->b, I->timing ? 0 : 1);
     int rc = cc_volume_batch_set_stream(slot->b, I->stream);
     if (!rc) rc = batchSetQuantSteps(slot->b, q);
     *out = slot->b;
@@ -284,6 +286,7 @@ int compressVolumeFloatBatched(cc_instance* I, const float* vol, u32 nx, u32 ny,
     const float* vols[1] = {vol};
     rc = cc_volume_batch_compress(b, vols);
     if (!rc) rc = batchStatusOf(b, false);   // synchronizes the stream
+    if (I->timing) cc_volume_batch_collect_timings(b);   // the batch's sections into the instance's
     u64 bits = 0;
     if (!rc) rc = cc_volume_batch_read_stream(b, 0, dWords, cap, &bits);
     if (!rc && bits > 0xffffffffull) { setError("%s: stream exceeds 2^32 bits", what); rc = CC_ERR_CAPACITY; }
@@ -305,6 +308,7 @@ int decompressVolumeFloatBatched(cc_instance* I, const cc_volume_channel* ch, u3
     rc = cc_volume_batch_load_streams(b, words.data(), bits.data());
     if (!rc) rc = cc_volume_batch_decompress(b, outs.data());
     if (!rc) rc = batchStatusOf(b, true);   // synchronizes the stream
+    if (I->timing) cc_volume_batch_collect_timings(b);   // the batch's sections into the instance's
     return rc;
 }
 

@@ -63,6 +63,38 @@ def test_plain_decode_reuses_its_batch_across_steps_and_sizes(oracle):
             assert np.array_equal(out.cpu().numpy().view(np.uint32), ref_rec.view(np.uint32)), (shape, levels, q0)
 
 
+def test_plain_calls_through_the_batch_report_their_sections(oracle):
+    """With timing on, compress / decompress calls that run through the
+    instance's volume batch fold the batch's sections into the instance's
+    (cc_timing_*), and still match the oracle."""
+    import ctypes
+    from cudacompress_b200 import _ffi
+    lib = _ffi.lib()
+    vol = fields.turbulence_field(32, 128, 8, seed=2102)
+    d = torch.from_numpy(vol).cuda()
+    ref_words, ref_bits = oracle.compress_volume(vol, 2, 0.01)
+    ref_rec = oracle.decompress_volume(ref_words, ref_bits, vol.shape, 2, 0.01)
+    with cc.Instance(0, 7, 16 ** 3, 128, 14) as inst:
+        for _ in range(3):   # the shape's batch comes on its fifth consecutive call
+            w, b = cc.compress_volume_float(inst, d, 2, 0.01)
+            out = torch.empty_like(d)
+            cc.decompress_volume_float(inst, out, 2, 0.01, w, b)
+        lib.cc_reset_timings(inst.handle)
+        lib.cc_set_timing(inst.handle, 1)
+        w, b = cc.compress_volume_float(inst, d, 2, 0.01)
+        out = torch.full_like(d, float("nan"))
+        cc.decompress_volume_float(inst, out, 2, 0.01, w, b)
+        lib.cc_set_timing(inst.handle, 0)
+        names = set()
+        for i in range(lib.cc_timing_count(inst.handle)):
+            name, ms, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_uint32()
+            lib.cc_timing_entry(inst.handle, i, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(cnt))
+            names.add(name.value.decode())
+        assert "batch.dwt_forward" in names and "batch.dwt_inverse" in names, sorted(names)
+        assert b == ref_bits and np.array_equal(stream_of(w, b), ref_words)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref_rec.view(np.uint32))
+
+
 def test_plain_decode_beyond_instance_capacity_fails_cleanly(oracle):
     """The instance's declared stream length bounds decompressVolumeFloat as
     it bounds the encoder: a volume whose level-0 bands exceed it fails with
