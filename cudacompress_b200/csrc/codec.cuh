@@ -198,6 +198,7 @@ struct cc_instance {
     // the small-table launch on `stream` (fork / join by the two events)
     cudaStream_t buildSide = nullptr, buildSide2 = nullptr;   // the table builders' other streams
     cudaEvent_t buildFork = nullptr, buildJoin = nullptr, buildJoin2 = nullptr;
+    cudaEvent_t decFork = nullptr, decJoin = nullptr;   // the decode's Huff branch on buildSide2
 
     // derived sizes
     ccb::u32 bins = 0;          // 1 << log2Max

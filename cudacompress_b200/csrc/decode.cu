@@ -975,15 +975,24 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
         if (chunks > 1) { k_decSymPlanCarry<<<chunks - 1, 1024, 0, st>>>(p); countLaunch(); }
     }
     { SectionTimer t(I, "dec.tables", st); k_decTables<<<p.T, kDecThreads, 0, st>>>(p); countLaunch(); }
+    // the Huff streams decode on a side stream beside the RLHuff chain (they
+    // share only the read-only tables and the error flags), joined below
+    const bool fork = p.hBlocks && p.rlBlocks;
+    cudaStream_t hs = fork ? I->buildSide2 : st;
+    if (fork) {
+        CC_TRY_CUDA(cudaEventRecord(I->decFork, st), "decode fork");
+        CC_TRY_CUDA(cudaStreamWaitEvent(hs, I->decFork, 0), "decode fork");
+    }
     if (p.hBlocks) {
         const size_t smem = size_t(32) * (p.cb + 2) * sizeof(Sym);
         CC_TRY_CUDA(ensureSmemAttribute(reinterpret_cast<const void*>(k_decHuff<Sym>),
                                         sizeof(Sym) == 2 ? kAttrDecHuff16 : kAttrDecHuff32, I->device, smem),
                     "decHuff smem");
-        SectionTimer t(I, "dec.huffman", st);
-        k_decHuff<Sym><<<u32(ceilDiv(p.hBlocks, 32)), 32, smem, st>>>(p);
+        SectionTimer t(I, "dec.huffman", hs);
+        k_decHuff<Sym><<<u32(ceilDiv(p.hBlocks, 32)), 32, smem, hs>>>(p);
         countLaunch();
     }
+    if (fork) CC_TRY_CUDA(cudaEventRecord(I->decJoin, hs), "decode join");
     if (p.rlBlocks) {
         const u32 g = u32(ceilDiv(u64(p.rlBlocks) / 32 + p.nRl, 4));   // warp tasks <= rlBlocks / 32 + nRl
         {
@@ -1002,6 +1011,7 @@ static int launchDecodeBackEnd(cc_instance* I, const DecParams& p) {
         { SectionTimer t(I, "dec.run_scan", st); k_decScan<<<u32(ceilDiv(p.nRl, 8)), 256, 0, st>>>(p); countLaunch(); }
         { SectionTimer t(I, "dec.symbols_scatter", st); k_decRl<Sym, true><<<g, 128, 0, st>>>(p); countLaunch(); }
     }
+    if (fork) CC_TRY_CUDA(cudaStreamWaitEvent(st, I->decJoin, 0), "decode join");
     CC_TRY_CUDA(cudaGetLastError(), "decode launch");
     return CC_OK;
 }

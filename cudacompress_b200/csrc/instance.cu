@@ -294,7 +294,9 @@ int createInstance(cc_instance** out, int cudaDevice, u32 streamCountMax, u32 el
         (e = cudaStreamCreateWithFlags(&I->buildSide2, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&I->buildFork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&I->buildJoin, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&I->buildJoin2, cudaEventDisableTiming)) != cudaSuccess) {
+        (e = cudaEventCreateWithFlags(&I->buildJoin2, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&I->decFork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&I->decJoin, cudaEventDisableTiming)) != cudaSuccess) {
         cc_destroy_instance(I);
         return cudaFail(e, "table build stream");
     }
@@ -331,6 +333,8 @@ void cc_destroy_instance(cc_instance* I) {
     if (I->buildFork) cudaEventDestroy(I->buildFork);
     if (I->buildJoin) cudaEventDestroy(I->buildJoin);
     if (I->buildJoin2) cudaEventDestroy(I->buildJoin2);
+    if (I->decFork) cudaEventDestroy(I->decFork);
+    if (I->decJoin) cudaEventDestroy(I->decJoin);
     if (I->buildSide) cudaStreamDestroy(I->buildSide);
     if (I->buildSide2) cudaStreamDestroy(I->buildSide2);
     I->resolveTimings();
